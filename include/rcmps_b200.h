@@ -1,0 +1,153 @@
+/* C ABI of the B200 fg_phi4 library (librcmps_b200.so).
+ *
+ * The phi^4 energy density of a relativistic continuous matrix product state and its
+ * Riemannian gradient, as the reference's GPU optimizer evaluates it (RcmpsCore.jl, package
+ * rcmps_gpu). Matrices are complex128, row-major (the memory of a C-ordered NumPy array),
+ * passed as `double*` pointing at interleaved (re, im) pairs. A batch packs its states one
+ * after the other: state i occupies dims[i]^2 complex values at offset sum_{j<i} dims[j]^2.
+ *
+ * Every entry returns an rcmps status (0 = success). A per-state status in the stats records
+ * which numerical requirement failed; rcmps_context_error() describes the last failure.
+ * No entry falls back to host arithmetic.
+ */
+#ifndef RCMPS_B200_H
+#define RCMPS_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes. 0-6 are the reference's device-controller codes
+ * (gpu/src/rcmps_gpu/optimizer/runtime/device_control_backend.py:23-27 and the timeout 6 of
+ * persistent_trajectory_backend.py:29). */
+#define RCMPS_OK 0
+#define RCMPS_MAX_STEPS 1
+#define RCMPS_STEP_UNDERFLOW 2
+#define RCMPS_NONFINITE_ERROR 3
+#define RCMPS_SOURCE_DOMAIN 4
+#define RCMPS_MISSING_SAMPLES 5
+#define RCMPS_DEVICE_TIMEOUT 6
+#define RCMPS_WAIT_LIMIT 7
+#define RCMPS_KRYLOV_FAILURE 8
+#define RCMPS_SOLVE_FAILURE 9
+#define RCMPS_NONFINITE_RESULT 10
+#define RCMPS_INVALID_ARGUMENT 20
+#define RCMPS_CUDA_ERROR 21
+#define RCMPS_OUT_OF_MEMORY 22
+
+typedef struct rcmps_context rcmps_context;
+
+/* Integration and solver controls. Defaults (rcmps_default_settings) are those of the
+ * reference's optimizer command line (gpu/src/rcmps_gpu/optimizer/cli.py:39-42 and
+ * runtime/sweep_driver.py:122-168). */
+typedef struct rcmps_settings {
+  double half_window;          /* W: the window is x in [-W, W], t in [-sqrt W, sqrt W]; 0 < W <= 40 */
+  int n_quad;                  /* Gauss-Legendre nodes per half window */
+  double atol, rtol;           /* DOP853 tolerances */
+  double initial_step;         /* first trial step in t */
+  long long max_steps;         /* attempted steps per trajectory */
+  double max_device_seconds;   /* device-clock watchdog per trajectory launch (0: none) */
+  int kinetic_nodes;           /* angular Gauss nodes of the kinetic resolvents */
+  double krylov_tolerance;     /* true relative residual of every shifted solve */
+  int krylov_initialdim;       /* first Arnoldi basis size (doubles until converged) */
+  int krylov_maxdim;           /* largest basis */
+  double metric_reg;           /* regulariser of the metric solve */
+  double boundary_tolerance;   /* GMRES tolerance of the boundary Poisson solve */
+} rcmps_settings;
+
+/* Per-state diagnostics. */
+typedef struct rcmps_state_stats {
+  int status;                  /* first failure of this state, RCMPS_OK if none */
+  int failed_component;        /* 0 none, 1 trajectory, 2 pullback, 3 kinetic, 4 boundary, 5 stationary */
+  long long attempts, accepted, rejected, dense_steps, rhs_calls;
+  double t_end, last_step, min_step, max_step;
+  double quartic_value;        /* g * <phi^4> */
+  double kinetic_value;        /* kinetic1 + kinetic2 */
+  int krylov_basis[4];         /* R forward, R adjoint, [Q,R] forward, [Q,R] adjoint */
+  double krylov_residual;      /* largest true relative residual of the shifted solves */
+  int gmres_iterations;        /* boundary Poisson solve */
+  double boundary_residual;
+} rcmps_state_stats;
+
+void rcmps_default_settings(rcmps_settings* settings);
+
+/* Context of one device: streams, events and a device workspace that grows on demand.
+ * Replaces the per-call solver objects of the reference (PersistentTrajectoryDOP853,
+ * persistent_trajectory_backend.py:339-403; KineticContext, kinetic_backend.py:236-275). */
+int rcmps_context_create(int device, rcmps_context** context);
+int rcmps_context_destroy(rcmps_context* context);
+const char* rcmps_context_error(const rcmps_context* context);
+const char* rcmps_status_name(int status);
+/* Device milliseconds of the phases of the last batched call: 0 trajectory, 1 pullback,
+ * 2 kinetic, 3 boundary/finish, 4 whole call. */
+int rcmps_last_timings(const rcmps_context* context, float* milliseconds, int n);
+/* Bytes of device workspace that rcmps_fg_phi4_batch needs for these dimensions. */
+long long rcmps_workspace_bytes(const rcmps_context* context, int n_states, const int* dims,
+                                const rcmps_settings* settings);
+
+/* phi^4 energy density and finished gradient of a batch of states, on device memory.
+ * Replaces the objective callable objective(r, k, rho, coupling, args, xp) ->
+ * (energy, gradient, stats) (runtime/sweep_driver.py:78-119; GPU form
+ * runtime/overlap_sweep_driver.py:132-212), for n_states states at once.
+ *   dims, couplings, stats: host arrays of n_states
+ *   R, K, rho: device, packed; K Hermitian, rho the stationary density of (Q, R)
+ *   energy: device [n_states]; gradient: device, packed
+ *   covector, environment: device, packed, or NULL (the raw summed components)
+ * `stream` is a cudaStream_t (NULL: the context's stream); the call returns after the
+ * results are complete. */
+int rcmps_fg_phi4_batch(rcmps_context* context, int n_states, const int* dims, const double* couplings,
+                        const double* R, const double* K, const double* rho, const rcmps_settings* settings,
+                        double* energy, double* gradient, double* covector, double* environment,
+                        rcmps_state_stats* stats, void* stream);
+
+/* Same with every array in host memory (copies in and out inside the call). */
+int rcmps_fg_phi4_batch_host(rcmps_context* context, int n_states, const int* dims, const double* couplings,
+                             const double* R, const double* K, const double* rho,
+                             const rcmps_settings* settings, double* energy, double* gradient,
+                             double* covector, double* environment, rcmps_state_stats* stats);
+
+/* The g*phi^4 term: value, raw covector and environment, scaled by the coupling, on device memory.
+ * Replaces evaluate_quartic_persistent_trajectory(R, Q, rho, g, ...) -> dict(value, covector,
+ * environment, stats) (runtime/persistent_trajectory_backend.py:439-461). */
+int rcmps_quartic_batch(rcmps_context* context, int n_states, const int* dims, const double* couplings,
+                        const double* R, const double* K, const double* rho, const rcmps_settings* settings,
+                        double* value, double* covector, double* environment, rcmps_state_stats* stats,
+                        void* stream);
+
+/* The trajectory alone, for one state: samples [2 n_quad + 1][7 d^2 + 1] complex (the seven
+ * channels at every Gauss node and the endpoint, and the scalar channel, only filled at the
+ * endpoint). Replaces PersistentTrajectoryDOP853.run() -> (samples, stats)
+ * (runtime/persistent_trajectory_backend.py:405-432). Device memory. */
+int rcmps_quartic_samples(rcmps_context* context, int d, const double* R, const double* K, const double* rho,
+                          const rcmps_settings* settings, double* samples, rcmps_state_stats* stats,
+                          void* stream);
+
+/* The two kinetic terms (unit coefficients), raw covector and environment, on device memory.
+ * Replaces kinetic_raw(q, r, rho, nodes, ...) -> dict(value, covector, environment, stats)
+ * (runtime/kinetic_backend.py:499-592; runtime/cooperative_arnoldi.py:293-316). */
+int rcmps_kinetic_batch(rcmps_context* context, int n_states, const int* dims, const double* R,
+                        const double* K, const double* rho, const rcmps_settings* settings, double* value,
+                        double* covector, double* environment, rcmps_state_stats* stats, void* stream);
+
+/* Boundary Poisson correction and metric solve, on device memory. Replaces
+ * finish_gradient(q, r, rho, covector, environment, metric_reg, tolerance) -> (gradient, stats)
+ * (runtime/numerics.py:120-126). */
+int rcmps_finish_gradient_batch(rcmps_context* context, int n_states, const int* dims, const double* R,
+                                const double* K, const double* rho, const double* covector,
+                                const double* environment, const rcmps_settings* settings, double* gradient,
+                                rcmps_state_stats* stats, void* stream);
+
+/* Stationary density rho of (Q, R) by GMRES on -L(X) + tr(X) I/D = I/D, on device memory.
+ * Replaces stationary_state(q, r, tolerance) -> (rho, stats) (runtime/numerics.py:74-100). */
+int rcmps_stationary_state_batch(rcmps_context* context, int n_states, const int* dims, const double* R,
+                                 const double* K, double tolerance, double* rho, rcmps_state_stats* stats,
+                                 void* stream);
+
+/* FP64 tensor-core throughput of this device (TFLOP/s), measured by a short in-register
+ * mma.sync loop: the denominator of the FP64 roofline. No counterpart in the reference. */
+double rcmps_fp64_peak_tflops(rcmps_context* context);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* RCMPS_B200_H */

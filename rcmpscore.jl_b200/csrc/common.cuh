@@ -1,0 +1,198 @@
+// Device primitives shared by the fg_phi4 kernels (sm_100a only).
+//
+// Complex matrices are row-major arrays of double2 (re, im), the layout of a C-ordered NumPy
+// complex128 array. Products run on the FP64 tensor-core instruction mma.sync m16n8k8 (A 16x8
+// row, B 8x8 col, C 16x8; fragment layout checked on B200 against a CPU product).
+// Every wait on an mbarrier is bounded: on timeout it raises the kernel's error flag and
+// returns, so control flow (and every cluster barrier) stays uniform.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+
+#ifndef RCMPS_DEVICE_INLINE
+#define RCMPS_DEVICE_INLINE __device__ __forceinline__
+#endif
+
+namespace rcmps {
+
+// ------------------------------------------------------------------ status codes
+// The numbers of the reference's device controller (device_control_backend.py:23-27 of
+// rcmps_gpu) plus the wait limit of this build.
+enum Status : int {
+  kOk = 0,
+  kMaxSteps = 1,
+  kStepUnderflow = 2,
+  kNonfiniteError = 3,
+  kSourceDomain = 4,
+  kMissingSamples = 5,
+  kDeviceTimeout = 6,       // device-clock watchdog (max_device_seconds)
+  kWaitLimit = 7,           // a bounded mbarrier wait gave up
+  kKrylovFailure = 8,       // shifted Arnoldi did not reach its true residual
+  kSolveFailure = 9,        // GMRES / dense solve did not reach its residual
+  kNonfiniteResult = 10,
+};
+
+// ------------------------------------------------------------------ complex helpers
+RCMPS_DEVICE_INLINE double2 zadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+RCMPS_DEVICE_INLINE double2 zsub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+RCMPS_DEVICE_INLINE double2 zscale(double s, double2 a) { return make_double2(s * a.x, s * a.y); }
+RCMPS_DEVICE_INLINE double2 zmul(double2 a, double2 b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+RCMPS_DEVICE_INLINE double2 zconj(double2 a) { return make_double2(a.x, -a.y); }
+RCMPS_DEVICE_INLINE double zabs2(double2 a) { return a.x * a.x + a.y * a.y; }
+RCMPS_DEVICE_INLINE double2 zaxpy(double s, double2 x, double2 y) {
+  return make_double2(fma(s, x.x, y.x), fma(s, x.y, y.y));
+}
+
+// ------------------------------------------------------------------ FP64 tensor-core tile
+// D(16x8) += A(16x8, row) * B(8x8, col); lane = 4 g + t:
+//   a = {A[g][t], A[g+8][t], A[g][t+4], A[g+8][t+4]}, b = {B[t][g], B[t+4][g]},
+//   c = {C[g][2t], C[g][2t+1], C[g+8][2t], C[g+8][2t+1]}.
+RCMPS_DEVICE_INLINE void dmma16x8x8(double* c, const double* a, const double* b) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 "
+      "{%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};"
+      : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
+      : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
+}
+
+// A complex 16x8 accumulator: re[4], im[4] in the C-fragment layout.
+struct ZFrag {
+  double re[4];
+  double im[4];
+  RCMPS_DEVICE_INLINE void zero() {
+#pragma unroll
+    for (int i = 0; i < 4; ++i) re[i] = im[i] = 0.0;
+  }
+};
+
+// acc += A(16x8 complex) * B(8x8 complex), the fragments already split into parts.
+// Four real products: re += Ar Br - Ai Bi, im += Ar Bi + Ai Br.
+RCMPS_DEVICE_INLINE void zmma(ZFrag& acc, const double* ar, const double* ai, const double* nai,
+                              const double* br, const double* bi) {
+  dmma16x8x8(acc.re, ar, br);
+  dmma16x8x8(acc.re, nai, bi);
+  dmma16x8x8(acc.im, ar, bi);
+  dmma16x8x8(acc.im, ai, br);
+}
+
+// Load the A fragment of rows [m0, m0+16) and columns [k0, k0+8) of a row-major complex
+// matrix with leading dimension lda (in complex elements) from shared memory.
+RCMPS_DEVICE_INLINE void load_a(const double2* A, int lda, int m0, int k0, int lane,
+                                double* ar, double* ai, double* nai) {
+  const int g = lane >> 2, t = lane & 3;
+  const double2* p = A + (m0 + g) * lda + k0 + t;
+  double2 v0 = p[0], v1 = p[8 * lda], v2 = p[4], v3 = p[8 * lda + 4];
+  ar[0] = v0.x; ar[1] = v1.x; ar[2] = v2.x; ar[3] = v3.x;
+  ai[0] = v0.y; ai[1] = v1.y; ai[2] = v2.y; ai[3] = v3.y;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) nai[i] = -ai[i];
+}
+
+// Load the B fragment of rows [k0, k0+8) and columns [n0, n0+8) of a row-major complex matrix.
+RCMPS_DEVICE_INLINE void load_b(const double2* B, int ldb, int k0, int n0, int lane,
+                                double* br, double* bi) {
+  const int g = lane >> 2, t = lane & 3;
+  double2 v0 = B[(k0 + t) * ldb + n0 + g], v1 = B[(k0 + t + 4) * ldb + n0 + g];
+  br[0] = v0.x; br[1] = v1.x;
+  bi[0] = v0.y; bi[1] = v1.y;
+}
+
+// Element coordinates (row, col) of C-fragment entry i for a lane.
+RCMPS_DEVICE_INLINE int frag_row(int lane, int i) { return (lane >> 2) + ((i & 2) ? 8 : 0); }
+RCMPS_DEVICE_INLINE int frag_col(int lane, int i) { return 2 * (lane & 3) + (i & 1); }
+
+// ------------------------------------------------------------------ shared-memory addresses
+RCMPS_DEVICE_INLINE uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// ------------------------------------------------------------------ mbarrier + bulk copy
+RCMPS_DEVICE_INLINE void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+RCMPS_DEVICE_INLINE void fence_mbar_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+RCMPS_DEVICE_INLINE void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+RCMPS_DEVICE_INLINE bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait for the phase of `parity` to complete. Returns false (and sets *flag) on timeout.
+constexpr long long kWaitIterations = 1ll << 24;
+RCMPS_DEVICE_INLINE bool mbar_wait(uint64_t* bar, uint32_t parity, int* flag) {
+  for (long long i = 0; i < kWaitIterations; ++i)
+    if (mbar_try_wait(bar, parity)) return true;
+  if (flag) atomicExch(flag, 1);
+  return false;
+}
+// 1-D bulk copy global -> shared of this CTA, completing on `bar`. 16-byte aligned, size % 16 == 0.
+RCMPS_DEVICE_INLINE void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+RCMPS_DEVICE_INLINE void fence_proxy_async_global() {
+  asm volatile("fence.proxy.async.global;" ::: "memory");
+}
+
+// ------------------------------------------------------------------ clusters
+RCMPS_DEVICE_INLINE uint32_t cluster_rank() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return r;
+}
+RCMPS_DEVICE_INLINE uint32_t cluster_id_x() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%clusterid.x;" : "=r"(r));
+  return r;
+}
+// Full cluster barrier with release/acquire semantics at cluster scope (orders global and
+// shared::cluster accesses of every thread of the cluster).
+RCMPS_DEVICE_INLINE void cluster_sync() {
+  asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+// Read a double from the shared memory of CTA `rank` of this cluster at the address that `p`
+// has in this CTA.
+RCMPS_DEVICE_INLINE double dsmem_load(const double* p, uint32_t rank) {
+  uint32_t local = smem_u32(p), remote;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(remote) : "r"(local), "r"(rank));
+  double v;
+  asm volatile("ld.shared::cluster.f64 %0, [%1];" : "=d"(v) : "r"(remote) : "memory");
+  return v;
+}
+RCMPS_DEVICE_INLINE int dsmem_load_int(const int* p, uint32_t rank) {
+  uint32_t local = smem_u32(p), remote;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(remote) : "r"(local), "r"(rank));
+  int v;
+  asm volatile("ld.shared::cluster.s32 %0, [%1];" : "=r"(v) : "r"(remote) : "memory");
+  return v;
+}
+
+// ------------------------------------------------------------------ timer
+RCMPS_DEVICE_INLINE unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// ------------------------------------------------------------------ reductions
+RCMPS_DEVICE_INLINE double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+}  // namespace rcmps

@@ -1,0 +1,107 @@
+// CTA-level complex FP64 GEMM on tensor cores: C(MB x DP) += A(MB x K) * B(K x DP).
+// A lives in shared memory (row-major, leading dimension lda, lda % 8 == 4 for conflict-free
+// fragment loads); B is a list of row-contiguous segments in global memory, streamed in
+// KC-row chunks by 1-D bulk copies into an NST-stage ring. C stays in registers: warp w owns
+// TPW consecutive 16x8 tiles of one 16-row band.
+#pragma once
+#include "common.cuh"
+
+namespace rcmps {
+
+template <int DP, int MB, int NW, int KC, int NST>
+struct RowGemm {
+  static constexpr int TN = DP / 8, TM = MB / 16, T = TM * TN, TPW = T / NW;
+  static_assert(T % NW == 0, "tiles per warp");
+  static_assert(TN % TPW == 0, "a warp's tiles share one band");
+  static constexpr int NT = 32 * NW;
+  static constexpr uint32_t CHUNK_BYTES = KC * DP * 16;
+
+  double2* ring;        // [NST][KC*DP]
+  uint64_t* full;       // [NST]
+  int* wait_flag;       // shared flag set when a bounded wait gives up
+  long long gq;         // running chunk counter (uniform across the CTA)
+
+  struct Segs {
+    const double2* ptr[6];
+    int rows[6];
+    int n;
+  };
+
+  __device__ static const double2* chunk_ptr(const Segs& s, int q) {
+    int r = q * KC;
+    for (int i = 0; i < s.n; ++i) {
+      if (r < s.rows[i]) return s.ptr[i] + (size_t)r * DP;
+      r -= s.rows[i];
+    }
+    return s.ptr[0];
+  }
+
+  __device__ void init() {
+    if (threadIdx.x == 0) {
+      for (int i = 0; i < NST; ++i) mbar_init(&full[i], 1);
+      fence_mbar_init();
+    }
+    gq = 0;
+  }
+
+  __device__ void issue(const Segs& s, int q) {
+    const long long g = gq + q;
+    const int slot = (int)(g % NST);
+    mbar_expect_tx(&full[slot], CHUNK_BYTES);
+    bulk_g2s(ring + slot * KC * DP, chunk_ptr(s, q), CHUNK_BYTES, &full[slot]);
+  }
+
+  // acc[TPW] += A * B. Call with all threads; ends with a __syncthreads.
+  __device__ void run(ZFrag* acc, const double2* A, int lda, const Segs& s) {
+    int krows = 0;
+    for (int i = 0; i < s.n; ++i) krows += s.rows[i];
+    const int nch = krows / KC;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int tile0 = warp * TPW;
+    const int mt = tile0 / TN;
+    if (threadIdx.x == 0) {
+      fence_proxy_async_global();
+      for (int q = 0; q < NST && q < nch; ++q) issue(s, q);
+    }
+    for (int q = 0; q < nch; ++q) {
+      const long long g = gq + q;
+      const int slot = (int)(g % NST);
+      mbar_wait(&full[slot], (uint32_t)((g / NST) & 1), wait_flag);
+      const double2* B = ring + slot * KC * DP;
+#pragma unroll
+      for (int ks = 0; ks < KC / 8; ++ks) {
+        double ar[4], ai[4], nai[4];
+        load_a(A, lda, mt * 16, q * KC + ks * 8, lane, ar, ai, nai);
+#pragma unroll
+        for (int j = 0; j < TPW; ++j) {
+          const int nt = (tile0 + j) % TN;
+          double br[2], bi[2];
+          load_b(B, DP, ks * 8, nt * 8, lane, br, bi);
+          zmma(acc[j], ar, ai, nai, br, bi);
+        }
+      }
+      __syncthreads();
+      if (threadIdx.x == 0 && q + NST < nch) issue(s, q + NST);
+    }
+    gq += nch;
+  }
+
+  // Coordinates of fragment entry i of tile j for this thread: row in [0, MB), col in [0, DP).
+  __device__ static void coord(int j, int i, int& row, int& col) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int tile = warp * TPW + j;
+    row = (tile / TN) * 16 + frag_row(lane, i);
+    col = (tile % TN) * 8 + frag_col(lane, i);
+  }
+
+  // After a wait gave up, wait (bounded) for the copies that may still be in flight.
+  __device__ void drain() {
+    if (threadIdx.x == 0 && *wait_flag) {
+      for (long long g = gq - 1; g >= 0 && g >= gq - NST; --g)
+        mbar_wait(&full[g % NST], (uint32_t)((g / NST) & 1), nullptr);
+    }
+    __syncthreads();
+  }
+};
+
+}  // namespace rcmps

@@ -1,0 +1,25 @@
+// Padding and per-state operator preparation (internal).
+#pragma once
+#include <cuda_runtime.h>
+
+namespace rcmps {
+// Number of dp x dp matrices in the operator block of one state (Q, Qh, R, Rh, fixed0, fixed6, S, rho).
+constexpr int kOps = 8;
+enum OpIndex { kQ = 0, kQh = 1, kR = 2, kRh = 3, kFixed0 = 4, kFixed6 = 5, kS = 6, kRho = 7 };
+
+cudaError_t launch_pad(const double* src, const long long* d_src_off, const int* d_dims, double* dst, int dp,
+                       long long stride, int nstates, cudaStream_t stream);
+cudaError_t launch_unpad(const double* src, long long stride, int dp, const long long* d_dst_off,
+                         const int* d_dims, double* dst, int nstates, cudaStream_t stream);
+// dst (packed d_i^2 per state) (+)= src (padded dp^2 per state)
+cudaError_t launch_unpad_acc(const double* src, long long stride, int dp, const long long* d_dst_off,
+                             const int* d_dims, double* dst, int nstates, bool accumulate, cudaStream_t stream);
+// dst[idx[i]] (+)= src[i]
+cudaError_t launch_scatter_values(const double* src, int n, const int* d_idx, double* dst, bool accumulate,
+                                  cudaStream_t stream);
+// samples (padded [npoints][7][dp][dp]) -> out [npoints][7 d^2 + 1]; the scalar is `value` at the endpoint
+cudaError_t launch_export_samples(const double2* samples, int dp, int d, int npoints, const double* value,
+                                  double* out, cudaStream_t stream);
+cudaError_t launch_prepare(const double* R, const double* K, const double* rho, double* ops, int dp,
+                           long long in_stride, long long ops_stride, int nstates, cudaStream_t stream);
+}  // namespace rcmps

@@ -1,0 +1,295 @@
+// Quadrature pullback of the quartic term: covector, environment and value from the samples.
+//
+// Reference: rcmps_gpu ode_backend.py:589-637 (_pullback with the reduced interfaces of
+// _reduced_quartic_pullback) and src/observables.jl:238-276. With forward samples
+// f_0 = rho, f_1..f_3 at node i, adjoint samples b_0..b_3 at node n-1-i, b_4 = I, and
+// w = weight 2|t|, j = weight source(t), c_k = (k+1) j:
+//   m  = sum_i sum_k f_k (w R^dag b_k + c_k b_{k+1}) - (sum_i sum_k w f_k b_k) R^dag
+//   nn = sum_i sum_k (w b_k R + c_k b_{k+1}) f_k - R (sum_i sum_k w b_k f_k)
+// The k = 0 terms are linear in the adjoint samples (f_0 = rho is constant) and are formed
+// once from B0 = sum w b_0 and B1 = sum j b_1 in the finalize kernel, as are the deferred
+// products with R^dag and R. Per node and k >= 1 this leaves six D^3 products, run as four
+// accumulation passes on FP64 tensor cores (RowGemm), each CTA owning one block of output rows
+// and a range of nodes; partial sums are reduced in a fixed order.
+#include <cuda_runtime.h>
+#include "common.cuh"
+#include "gemm.cuh"
+#include "pullback.h"
+
+namespace rcmps {
+
+template <int DP>
+struct PGeo {
+  static constexpr int MB = DP <= 64 ? DP : (DP == 96 ? 48 : 32);
+  static constexpr int NW = DP == 16 ? 2 : DP == 48 ? 6 : DP == 96 ? 12 : 8;
+  static constexpr int KC = DP <= 64 ? 16 : 8;
+  static constexpr int NST = 4;
+  static constexpr int LDA = DP + 4;
+  static constexpr int NRB = DP / MB;
+  using GM = RowGemm<DP, MB, NW, KC, NST>;
+  static constexpr int NT = 32 * NW;
+  static constexpr size_t BUF = (size_t)MB * LDA;      // double2 per A buffer
+  static constexpr size_t SMEM = (2 * BUF + (size_t)NST * KC * DP) * 16 + 128;
+};
+
+template <int DP>
+__global__ void __launch_bounds__(PGeo<DP>::NT, 1)
+pullback_kernel(PullbackArgs a) {
+  using PG = PGeo<DP>;
+  using GM = typename PG::GM;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  double2* bufX = reinterpret_cast<double2*>(smem_raw);
+  double2* bufY = bufX + PG::BUF;
+  double2* ring = bufY + PG::BUF;
+  uint64_t* full = reinterpret_cast<uint64_t*>(ring + (size_t)PG::NST * PG::KC * DP);
+  int* flag = reinterpret_cast<int*>(full + PG::NST);
+
+  constexpr int MAT = DP * DP, VEC = 7 * MAT;
+  const int blk = blockIdx.x;
+  const int state = blockIdx.y / PG::NRB, rb = blockIdx.y % PG::NRB;
+  const int n = a.nodes;
+  const int i0 = blk * a.nodes_per_block, i1 = min(n, i0 + a.nodes_per_block);
+  const double2* samples = a.samples + (size_t)state * a.samples_stride;
+  const double2* ops = a.ops + (size_t)state * a.ops_stride;
+  const double2* R = ops + 2 * MAT;
+  const double2* Rh = ops + 3 * MAT;
+  double2* wscr = a.scratch + ((size_t)blockIdx.y * gridDim.x + blk) * 3 * MAT;
+  const int tid = threadIdx.x;
+
+  GM gm{ring, full, flag, 0};
+  if (tid == 0) *flag = 0;
+  gm.init();
+  __syncthreads();
+
+  auto fwd = [&](int i, int k) { return samples + (size_t)i * VEC + (size_t)(k - 1) * MAT; };       // f_k, k=1..3
+  auto adj = [&](int i, int k) { return samples + (size_t)(n - 1 - i) * VEC + (size_t)(3 + k) * MAT; };  // b_k, k=0..3
+  auto load_rows = [&](double2* dst, const double2* src, int row0, double scale) {
+    for (int e = tid; e < PG::MB * DP; e += PG::NT) {
+      const int r = e / DP, c = e % DP;
+      dst[r * PG::LDA + c] = zscale(scale, src[(size_t)(row0 + r) * DP + c]);
+    }
+  };
+
+  ZFrag acc[GM::TPW], tmp[GM::TPW];
+  for (int pass = 0; pass < 4; ++pass) {
+#pragma unroll
+    for (int j = 0; j < GM::TPW; ++j) acc[j].zero();
+    if (pass == 0 && PG::NRB == 1) {
+      load_rows(bufX, Rh, 0, 1.0);
+      __syncthreads();
+    }
+    for (int i = i0; i < i1; ++i) {
+      const double w = a.wj[2 * i], jv = a.wj[2 * i + 1];
+      for (int k = 1; k <= 3; ++k) {
+        const double c = jv * (k + 1);
+        typename GM::Segs sb;
+        sb.n = 1;
+        sb.rows[0] = DP;
+        if (pass == 0) {
+          // W_k = w R^dag b_k + c b_{k+1} (all rows) -> scratch
+          for (int rbw = 0; rbw < PG::NRB; ++rbw) {
+            if (PG::NRB > 1) {
+              load_rows(bufX, Rh, rbw * PG::MB, 1.0);
+              __syncthreads();
+            }
+#pragma unroll
+            for (int j = 0; j < GM::TPW; ++j) tmp[j].zero();
+            sb.ptr[0] = adj(i, k);
+            gm.run(tmp, bufX, PG::LDA, sb);
+#pragma unroll
+            for (int j = 0; j < GM::TPW; ++j)
+#pragma unroll
+              for (int e = 0; e < 4; ++e) {
+                int row, col;
+                GM::coord(j, e, row, col);
+                row += rbw * PG::MB;
+                double2 v = make_double2(w * tmp[j].re[e], w * tmp[j].im[e]);
+                if (k < 3) v = zaxpy(c, adj(i, k + 1)[row * DP + col], v);
+                else if (row == col) v.x += c;
+                wscr[(k - 1) * MAT + row * DP + col] = v;
+              }
+          }
+          fence_proxy_async_global();   // W_k is read next by bulk copies
+          __syncthreads();
+          load_rows(bufY, fwd(i, k), rb * PG::MB, 1.0);
+          __syncthreads();
+          sb.ptr[0] = wscr + (k - 1) * MAT;
+          gm.run(acc, bufY, PG::LDA, sb);
+        } else if (pass == 1) {
+          load_rows(bufY, fwd(i, k), rb * PG::MB, w);   // P += w f_k b_k
+          __syncthreads();
+          sb.ptr[0] = adj(i, k);
+          gm.run(acc, bufY, PG::LDA, sb);
+        } else if (pass == 2) {
+          // W'_k rows = w b_k R + c b_{k+1} -> bufY; then nn += W'_k f_k
+          load_rows(bufX, adj(i, k), rb * PG::MB, 1.0);
+          __syncthreads();
+#pragma unroll
+          for (int j = 0; j < GM::TPW; ++j) tmp[j].zero();
+          sb.ptr[0] = R;
+          gm.run(tmp, bufX, PG::LDA, sb);
+#pragma unroll
+          for (int j = 0; j < GM::TPW; ++j)
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+              int row, col;
+              GM::coord(j, e, row, col);
+              const int grow = row + rb * PG::MB;
+              double2 v = make_double2(w * tmp[j].re[e], w * tmp[j].im[e]);
+              if (k < 3) v = zaxpy(c, adj(i, k + 1)[grow * DP + col], v);
+              else if (grow == col) v.x += c;
+              bufY[row * PG::LDA + col] = v;
+            }
+          __syncthreads();
+          sb.ptr[0] = fwd(i, k);
+          gm.run(acc, bufY, PG::LDA, sb);
+        } else {
+          load_rows(bufX, adj(i, k), rb * PG::MB, w);   // P' += w b_k f_k
+          __syncthreads();
+          sb.ptr[0] = fwd(i, k);
+          gm.run(acc, bufX, PG::LDA, sb);
+        }
+      }
+    }
+    // store this CTA's partial of matrix `pass` (m, P, nn, P') on its rows
+    double2* out = a.partial + (((size_t)state * gridDim.x + blk) * 4 + pass) * MAT;
+#pragma unroll
+    for (int j = 0; j < GM::TPW; ++j)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        int row, col;
+        GM::coord(j, e, row, col);
+        out[(row + rb * PG::MB) * DP + col] = make_double2(acc[j].re[e], acc[j].im[e]);
+      }
+    __syncthreads();
+  }
+  gm.drain();
+  if (tid == 0 && *flag) atomicExch(a.error_flag + state, 1);
+}
+
+// Naive dense helpers for the finalize step (a few D^3 products per state).
+__device__ void dmat_mul(double2* C, const double2* A, const double2* B, int dp, bool ah, bool bh, double alpha,
+                         bool add) {
+  for (int e = threadIdx.x; e < dp * dp; e += blockDim.x) {
+    const int i = e / dp, j = e % dp;
+    double2 s = make_double2(0.0, 0.0);
+    for (int l = 0; l < dp; ++l) {
+      const double2 x = ah ? zconj(A[l * dp + i]) : A[i * dp + l];
+      const double2 y = bh ? zconj(B[j * dp + l]) : B[l * dp + j];
+      s = zadd(s, zmul(x, y));
+    }
+    s = zscale(alpha, s);
+    C[e] = add ? zadd(C[e], s) : s;
+  }
+  __syncthreads();
+}
+
+// One CTA per state: reduce partials, add the k = 0 terms and the deferred products, and write
+// value, covector = g (m + nn^dag)/2 and environment = g Herm(b_0 at the endpoint).
+__global__ void pullback_finalize(PullbackArgs a, int nblk) {
+  const int state = blockIdx.x;
+  const int dp = a.dp, MAT = dp * dp, VEC = 7 * MAT, n = a.nodes;
+  const double2* samples = a.samples + (size_t)state * a.samples_stride;
+  const double2* ops = a.ops + (size_t)state * a.ops_stride;
+  const double2 *R = ops + 2 * MAT, *rho = ops + 7 * MAT;
+  double2* t = a.fin + (size_t)state * 8 * MAT;
+  double2 *m = t, *P = t + MAT, *nn = t + 2 * MAT, *Pp = t + 3 * MAT, *B0 = t + 4 * MAT, *B1 = t + 5 * MAT,
+          *T1 = t + 6 * MAT, *T2 = t + 7 * MAT;
+  for (int e = threadIdx.x; e < MAT; e += blockDim.x) {
+    double2 s[4] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}};
+    for (int b = 0; b < nblk; ++b) {
+      const double2* p = a.partial + (((size_t)state * nblk + b) * 4) * MAT;
+      for (int q = 0; q < 4; ++q) s[q] = zadd(s[q], p[q * MAT + e]);
+    }
+    m[e] = s[0];
+    P[e] = s[1];
+    nn[e] = s[2];
+    Pp[e] = s[3];
+    double2 b0 = make_double2(0, 0), b1 = make_double2(0, 0);
+    for (int i = 0; i < n; ++i) {
+      const double2* bs = samples + (size_t)(n - 1 - i) * VEC;
+      b0 = zaxpy(a.wj[2 * i], bs[3 * MAT + e], b0);
+      b1 = zaxpy(a.wj[2 * i + 1], bs[4 * MAT + e], b1);
+    }
+    B0[e] = b0;
+    B1[e] = b1;
+  }
+  __syncthreads();
+  // m += rho R^dag B0 + rho B1 - (P + rho B0) R^dag
+  dmat_mul(T1, R, B0, dp, true, false, 1.0, false);      // R^dag B0
+  dmat_mul(m, rho, T1, dp, false, false, 1.0, true);
+  dmat_mul(m, rho, B1, dp, false, false, 1.0, true);
+  dmat_mul(P, rho, B0, dp, false, false, 1.0, true);      // P + rho B0
+  dmat_mul(m, P, R, dp, false, true, -1.0, true);         // - (...) R^dag
+  // nn += B0 R rho + B1 rho - R (Pp + B0 rho)
+  dmat_mul(T2, B0, R, dp, false, false, 1.0, false);      // B0 R
+  dmat_mul(nn, T2, rho, dp, false, false, 1.0, true);
+  dmat_mul(nn, B1, rho, dp, false, false, 1.0, true);
+  dmat_mul(Pp, B0, rho, dp, false, false, 1.0, true);
+  dmat_mul(nn, R, Pp, dp, false, false, -1.0, true);
+  const double g = a.coupling[state];
+  const double2* env = samples + (size_t)(a.npoints - 1) * VEC + 3 * MAT;
+  double2* cov_out = a.cov_out + (size_t)state * MAT;
+  double2* env_out = a.env_out + (size_t)state * MAT;
+  for (int e = threadIdx.x; e < MAT; e += blockDim.x) {
+    const int i = e / dp, j = e % dp;
+    const double2 c = zadd(m[e], zconj(nn[j * dp + i]));
+    cov_out[e] = zscale(0.5 * g, c);
+    const double2 h = zadd(env[e], zconj(env[j * dp + i]));
+    env_out[e] = zscale(0.5 * g, h);
+  }
+  if (threadIdx.x == 0) a.value_out[state] = g * a.traj_value[state];
+}
+
+template <int DP>
+static cudaError_t launch_pb(const PullbackArgs& a, int nblk, cudaStream_t s) {
+  using PG = PGeo<DP>;
+  auto k = pullback_kernel<DP>;
+  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PG::SMEM);
+  if (e != cudaSuccess) return e;
+  dim3 grid(nblk, a.nstates * PG::NRB);
+  k<<<grid, PG::NT, PG::SMEM, s>>>(a);
+  return cudaGetLastError();
+}
+
+size_t pullback_smem_bytes(int dp) {
+  switch (dp) {
+    case 16: return PGeo<16>::SMEM;
+    case 32: return PGeo<32>::SMEM;
+    case 48: return PGeo<48>::SMEM;
+    case 64: return PGeo<64>::SMEM;
+    case 96: return PGeo<96>::SMEM;
+    case 128: return PGeo<128>::SMEM;
+  }
+  return 0;
+}
+
+int pullback_row_blocks(int dp) {
+  switch (dp) {
+    case 16: return PGeo<16>::NRB;
+    case 32: return PGeo<32>::NRB;
+    case 48: return PGeo<48>::NRB;
+    case 64: return PGeo<64>::NRB;
+    case 96: return PGeo<96>::NRB;
+    case 128: return PGeo<128>::NRB;
+  }
+  return 1;
+}
+
+cudaError_t pullback_launch(const PullbackArgs& a, int nblk, cudaStream_t s) {
+  cudaError_t e;
+  switch (a.dp) {
+    case 16: e = launch_pb<16>(a, nblk, s); break;
+    case 32: e = launch_pb<32>(a, nblk, s); break;
+    case 48: e = launch_pb<48>(a, nblk, s); break;
+    case 64: e = launch_pb<64>(a, nblk, s); break;
+    case 96: e = launch_pb<96>(a, nblk, s); break;
+    case 128: e = launch_pb<128>(a, nblk, s); break;
+    default: return cudaErrorInvalidValue;
+  }
+  if (e != cudaSuccess) return e;
+  pullback_finalize<<<a.nstates, 256, 0, s>>>(a, nblk);
+  return cudaGetLastError();
+}
+
+}  // namespace rcmps

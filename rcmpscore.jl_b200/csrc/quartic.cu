@@ -1,0 +1,285 @@
+// Host orchestration of the quartic term: states grouped by padded dimension, each group in
+// sub-batches that fit the device workspace; per sub-batch: pad, prepare, one trajectory launch
+// (all states co-scheduled), pullback, finalize, unpad.
+#include <cuda_runtime.h>
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+#include "../../include/rcmps_b200.h"
+#include "context.h"
+#include "prep.h"
+#include "pullback.h"
+#include "quartic.h"
+#include "trajectory.h"
+
+namespace rcmps {
+
+cudaError_t quartic_init() { return cudaSuccess; }
+
+namespace {
+
+struct Layout {
+  size_t total = 0;
+  size_t add(size_t bytes) {
+    const size_t off = total;
+    total += align256(bytes);
+    return off;
+  }
+};
+
+constexpr int kNodesPerBlock = 32;
+
+size_t state_bytes(int dp, int npoints, int nodes) {
+  const size_t mat = (size_t)dp * dp * 16;
+  const int nblk = (nodes + kNodesPerBlock - 1) / kNodesPerBlock;
+  const int nrb = pullback_row_blocks(dp);
+  size_t b = 0;
+  b += 3 * mat;                       // padded R, K, rho
+  b += kOps * mat;                    // operators
+  b += 21 * 7 * mat;                  // y, prop, k[16], z[2], P
+  b += (size_t)npoints * 7 * mat;     // samples
+  b += (size_t)nblk * nrb * 3 * mat;  // pullback W scratch
+  b += (size_t)nblk * 4 * mat;        // pullback partials
+  b += 8 * mat + 2 * mat;             // finalize temps, padded covector/environment
+  b += 1024;                          // small per-state records
+  return b;
+}
+
+}  // namespace
+
+int quartic_run(rcmps_context* ctx, QuarticJob& job, cudaStream_t stream) {
+  const rcmps_settings& S = job.settings;
+  std::vector<double> points, weights;
+  trajectory_points(S.half_window, S.n_quad, points, weights);
+  const int npoints = (int)points.size(), nodes = 2 * S.n_quad;
+  const int nblk = (nodes + kNodesPerBlock - 1) / kNodesPerBlock;
+
+  // offsets of the packed inputs/outputs
+  std::vector<long long> off(job.n + 1, 0);
+  for (int i = 0; i < job.n; ++i) off[i + 1] = off[i] + (long long)job.dims[i] * job.dims[i];
+
+  std::map<int, std::vector<int>> groups;
+  for (int i = 0; i < job.n; ++i) groups[padded_dim(job.dims[i])].push_back(i);
+
+  size_t free_b = 0, total_b = 0;
+  cudaMemGetInfo(&free_b, &total_b);
+  const size_t budget = std::max<size_t>((size_t)1 << 30, (free_b + ctx->arena_bytes) * 7 / 10);
+
+  cudaEvent_t e0 = ctx->ev_a, e1 = ctx->ev_b;
+  float traj_ms = 0.f, pull_ms = 0.f;
+
+  for (auto& kv : groups) {
+    const int dp = kv.first;
+    const std::vector<int>& all = kv.second;
+    const size_t per = state_bytes(dp, npoints, nodes);
+    const size_t fixed = (size_t)(npoints + 3 * nodes) * 8 + 4096;
+    int cap = (int)std::max<size_t>(1, (budget - std::min(budget, fixed)) / per);
+    for (size_t start = 0; start < all.size(); start += cap) {
+      const int n = (int)std::min<size_t>(cap, all.size() - start);
+      const std::vector<int> idx(all.begin() + start, all.begin() + start + n);
+      const size_t mat = (size_t)dp * dp;   // complex elements
+      Layout L;
+      const size_t o_dims = L.add(n * sizeof(int));
+      const size_t o_off = L.add(n * sizeof(long long));
+      const size_t o_idx = L.add(n * sizeof(int));
+      const size_t o_points = L.add(npoints * 8);
+      const size_t o_weights = L.add(nodes * 8);
+      const size_t o_wj = L.add(2 * nodes * 8);
+      const size_t o_coup = L.add(n * 8);
+      const size_t o_tval = L.add(n * 8);
+      const size_t o_vout = L.add(n * 8);
+      const size_t o_flag = L.add(n * sizeof(int));
+      const size_t o_states = L.add(n * sizeof(TrajState));
+      const size_t o_tstats = L.add(n * sizeof(TrajStats));
+      const size_t o_in = L.add(3 * n * mat * 16);
+      const size_t o_ops = L.add(n * kOps * mat * 16);
+      const size_t o_work = L.add(n * 21 * 7 * mat * 16);
+      const size_t o_samp = L.add((size_t)n * npoints * 7 * mat * 16);
+      const int nrb = pullback_row_blocks(dp);
+      const size_t o_wscr = L.add((size_t)n * nrb * nblk * 3 * mat * 16);
+      const size_t o_part = L.add((size_t)n * nblk * 4 * mat * 16);
+      const size_t o_fin = L.add((size_t)n * 8 * mat * 16);
+      const size_t o_cov = L.add((size_t)n * mat * 16);
+      const size_t o_env = L.add((size_t)n * mat * 16);
+      cudaError_t e = arena_reserve(ctx, L.total);
+      if (e != cudaSuccess)
+        return fail(ctx, RCMPS_OUT_OF_MEMORY, "quartic workspace: " + std::to_string(L.total) + " bytes");
+      char* base = static_cast<char*>(ctx->arena);
+      auto P = [&](size_t o) { return static_cast<void*>(base + o); };
+
+      // host-side tables through a pinned staging buffer
+      Layout H;
+      const size_t h_o_dims = H.add(n * sizeof(int));
+      const size_t h_o_off = H.add(n * 8);
+      const size_t h_o_idx = H.add(n * sizeof(int));
+      const size_t h_o_points = H.add(npoints * 8);
+      const size_t h_o_weights = H.add(nodes * 8);
+      const size_t h_o_coup = H.add(n * 8);
+      const size_t h_o_states = H.add(n * sizeof(TrajState));
+      const size_t h_o_tstats = H.add(n * sizeof(TrajStats));
+      const size_t h_o_flag = H.add(n * sizeof(int));
+      if (pinned_reserve(ctx, H.total) != cudaSuccess) return fail(ctx, RCMPS_CUDA_ERROR, "pinned host buffer");
+      char* h = static_cast<char*>(ctx->pinned);
+      int* h_dims = reinterpret_cast<int*>(h + h_o_dims);
+      long long* h_off = reinterpret_cast<long long*>(h + h_o_off);
+      int* h_idx = reinterpret_cast<int*>(h + h_o_idx);
+      double* h_points = reinterpret_cast<double*>(h + h_o_points);
+      double* h_weights = reinterpret_cast<double*>(h + h_o_weights);
+      double* h_coup = reinterpret_cast<double*>(h + h_o_coup);
+      TrajState* h_states = reinterpret_cast<TrajState*>(h + h_o_states);
+      TrajStats* h_tstats = reinterpret_cast<TrajStats*>(h + h_o_tstats);
+      int* h_flag = reinterpret_cast<int*>(h + h_o_flag);
+      for (int i = 0; i < n; ++i) {
+        h_dims[i] = job.dims[idx[i]];
+        h_off[i] = off[idx[i]];
+        h_idx[i] = idx[i];
+        h_coup[i] = job.couplings ? job.couplings[idx[i]] : 1.0;
+      }
+      std::memcpy(h_points, points.data(), npoints * 8);
+      std::memcpy(h_weights, weights.data(), nodes * 8);
+      double2* d_in = static_cast<double2*>(P(o_in));
+      double2* d_ops = static_cast<double2*>(P(o_ops));
+      double2* d_work = static_cast<double2*>(P(o_work));
+      double2* d_samp = static_cast<double2*>(P(o_samp));
+      for (int i = 0; i < n; ++i) {
+        TrajState& t = h_states[i];
+        const double2* ops = d_ops + (size_t)i * kOps * mat;
+        t.Q = ops + kQ * mat;
+        t.Qh = ops + kQh * mat;
+        t.R = ops + kR * mat;
+        t.Rh = ops + kRh * mat;
+        t.fixed0 = ops + kFixed0 * mat;
+        t.fixed6 = ops + kFixed6 * mat;
+        t.S = ops + kS * mat;
+        double2* w = d_work + (size_t)i * 21 * 7 * mat;
+        t.y = w;
+        t.prop = w + 7 * mat;
+        t.k = w + 14 * mat;
+        t.z = w + (14 + 16 * 7) * mat;
+        t.P = w + (14 + 18 * 7) * mat;
+        t.samples = d_samp + (size_t)i * npoints * 7 * mat;
+        t.stats = reinterpret_cast<TrajStats*>(base + o_tstats) + i;
+        t.atol = S.atol;
+        t.rtol = S.rtol;
+        t.max_steps = S.max_steps;
+        t.d = h_dims[i];
+      }
+      e = cudaMemcpyAsync(P(o_dims), h_dims, n * sizeof(int), cudaMemcpyHostToDevice, stream);
+      if (e == cudaSuccess) e = cudaMemcpyAsync(P(o_off), h_off, n * 8, cudaMemcpyHostToDevice, stream);
+      if (e == cudaSuccess) e = cudaMemcpyAsync(P(o_idx), h_idx, n * sizeof(int), cudaMemcpyHostToDevice, stream);
+      if (e == cudaSuccess) e = cudaMemcpyAsync(P(o_points), h_points, npoints * 8, cudaMemcpyHostToDevice, stream);
+      if (e == cudaSuccess) e = cudaMemcpyAsync(P(o_weights), h_weights, nodes * 8, cudaMemcpyHostToDevice, stream);
+      if (e == cudaSuccess) e = cudaMemcpyAsync(P(o_coup), h_coup, n * 8, cudaMemcpyHostToDevice, stream);
+      if (e == cudaSuccess)
+        e = cudaMemcpyAsync(P(o_states), h_states, n * sizeof(TrajState), cudaMemcpyHostToDevice, stream);
+      if (e == cudaSuccess) e = cudaMemsetAsync(P(o_flag), 0, n * sizeof(int), stream);
+      const long long in_stride = (long long)mat;
+      double* dR = reinterpret_cast<double*>(d_in);
+      double* dK = reinterpret_cast<double*>(d_in + n * mat);
+      double* dP = reinterpret_cast<double*>(d_in + 2 * n * mat);
+      if (e == cudaSuccess) e = launch_pad(job.R, (long long*)P(o_off), (int*)P(o_dims), dR, dp, in_stride, n, stream);
+      if (e == cudaSuccess) e = launch_pad(job.K, (long long*)P(o_off), (int*)P(o_dims), dK, dp, in_stride, n, stream);
+      if (e == cudaSuccess) e = launch_pad(job.rho, (long long*)P(o_off), (int*)P(o_dims), dP, dp, in_stride, n, stream);
+      if (e == cudaSuccess)
+        e = launch_prepare(dR, dK, dP, reinterpret_cast<double*>(d_ops), dp, in_stride, (long long)kOps * mat, n, stream);
+      if (e == cudaSuccess)
+        e = node_weights_launch((double*)P(o_points), (double*)P(o_weights), nodes, (double*)P(o_wj), stream);
+      TrajControls tc;
+      tc.endpoint = points.back();
+      tc.initial_h = S.initial_step;
+      tc.max_ns = (unsigned long long)(S.max_device_seconds * 1e9);
+      if (e == cudaSuccess) e = cudaEventRecord(e0, stream);
+      if (e == cudaSuccess)
+        e = trajectory_launch(dp, (TrajState*)P(o_states), n, (double*)P(o_points), npoints, tc, stream);
+      if (e == cudaSuccess) e = cudaEventRecord(e1, stream);
+      if (e != cudaSuccess) return fail(ctx, RCMPS_CUDA_ERROR, std::string("trajectory launch: ") + cudaGetErrorString(e));
+      // copy the trajectory values into a plain array for the finalize step
+      // (TrajStats::value of each state)
+      e = cudaMemcpy2DAsync(P(o_tval), 8, reinterpret_cast<char*>(P(o_tstats)) + offsetof(TrajStats, value),
+                            sizeof(TrajStats), 8, n, cudaMemcpyDeviceToDevice, stream);
+      PullbackArgs pa;
+      pa.dp = dp;
+      pa.nstates = n;
+      pa.nodes = nodes;
+      pa.npoints = npoints;
+      pa.nodes_per_block = kNodesPerBlock;
+      pa.samples = d_samp;
+      pa.samples_stride = (long long)npoints * 7 * mat;
+      pa.ops = d_ops;
+      pa.ops_stride = (long long)kOps * mat;
+      pa.wj = (double*)P(o_wj);
+      pa.coupling = (double*)P(o_coup);
+      pa.traj_value = (double*)P(o_tval);
+      pa.scratch = (double2*)P(o_wscr);
+      pa.partial = (double2*)P(o_part);
+      pa.fin = (double2*)P(o_fin);
+      pa.cov_out = (double2*)P(o_cov);
+      pa.env_out = (double2*)P(o_env);
+      pa.value_out = (double*)P(o_vout);
+      pa.error_flag = (int*)P(o_flag);
+      cudaEvent_t e2 = nullptr;
+      if (e == cudaSuccess) e = cudaEventCreate(&e2);
+      if (e == cudaSuccess) e = pullback_launch(pa, nblk, stream);
+      if (e == cudaSuccess) e = cudaEventRecord(e2, stream);
+      if (e != cudaSuccess) {
+        if (e2) cudaEventDestroy(e2);
+        return fail(ctx, RCMPS_CUDA_ERROR, std::string("pullback launch: ") + cudaGetErrorString(e));
+      }
+      // outputs
+      if (job.covector)
+        e = launch_unpad_acc(reinterpret_cast<double*>(P(o_cov)), (long long)mat, dp, (long long*)P(o_off),
+                             (int*)P(o_dims), job.covector, n, job.accumulate, stream);
+      if (e == cudaSuccess && job.environment)
+        e = launch_unpad_acc(reinterpret_cast<double*>(P(o_env)), (long long)mat, dp, (long long*)P(o_off),
+                             (int*)P(o_dims), job.environment, n, job.accumulate, stream);
+      if (e == cudaSuccess && job.value)
+        e = launch_scatter_values((double*)P(o_vout), n, (int*)P(o_idx), job.value, job.accumulate, stream);
+      if (e == cudaSuccess && job.samples_out)
+        e = launch_export_samples(d_samp, dp, h_dims[0], npoints, (double*)P(o_tval), job.samples_out, stream);
+      if (e == cudaSuccess) e = cudaMemcpyAsync(h_tstats, P(o_tstats), n * sizeof(TrajStats), cudaMemcpyDeviceToHost, stream);
+      if (e == cudaSuccess) e = cudaMemcpyAsync(h_flag, P(o_flag), n * sizeof(int), cudaMemcpyDeviceToHost, stream);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+      if (e != cudaSuccess) {
+        cudaEventDestroy(e2);
+        return fail(ctx, RCMPS_CUDA_ERROR, std::string("quartic: ") + cudaGetErrorString(e));
+      }
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      traj_ms += ms;
+      cudaEventElapsedTime(&ms, e1, e2);
+      pull_ms += ms;
+      cudaEventDestroy(e2);
+      for (int i = 0; i < n; ++i) {
+        const TrajStats& t = h_tstats[i];
+        rcmps_state_stats& o = job.stats[idx[i]];
+        o.attempts = t.attempts;
+        o.accepted = t.accepted;
+        o.rejected = t.rejected;
+        o.dense_steps = t.dense_steps;
+        o.rhs_calls = 1 + 12 * t.attempts + 3 * t.dense_steps;
+        o.t_end = t.t;
+        o.last_step = t.h;
+        o.min_step = t.min_h;
+        o.max_step = t.max_h;
+        o.quartic_value = (job.couplings ? job.couplings[idx[i]] : 1.0) * t.value;
+        if (t.status && !o.status) {
+          o.status = t.status;
+          o.failed_component = 1;
+        } else if (h_flag[i] && !o.status) {
+          o.status = RCMPS_WAIT_LIMIT;
+          o.failed_component = 2;
+        }
+      }
+    }
+  }
+  ctx->last_ms[0] = traj_ms;
+  ctx->last_ms[1] = pull_ms;
+  for (int i = 0; i < job.n; ++i)
+    if (job.stats[i].status) return job.stats[i].status;
+  return RCMPS_OK;
+}
+
+}  // namespace rcmps

@@ -1,0 +1,32 @@
+// Quartic term orchestration (internal).
+#pragma once
+#include <cuda_runtime.h>
+#include <vector>
+#include "../../include/rcmps_b200.h"
+#include "context.h"
+
+namespace rcmps {
+
+struct QuarticJob {
+  int n = 0;
+  const int* dims = nullptr;            // host
+  const double* couplings = nullptr;    // host, NULL: 1
+  const double *R = nullptr, *K = nullptr, *rho = nullptr;   // device, packed
+  rcmps_settings settings{};
+  double* value = nullptr;              // device [n] (g * quartic density), optional
+  double* covector = nullptr;           // device packed, optional
+  double* environment = nullptr;        // device packed, optional
+  double* samples_out = nullptr;        // device, single-state samples, optional
+  rcmps_state_stats* stats = nullptr;   // host [n]
+  bool accumulate = false;              // add into value/covector/environment instead of storing
+};
+
+cudaError_t quartic_init();
+int quartic_run(rcmps_context* ctx, QuarticJob& job, cudaStream_t stream);
+
+void gauss_legendre(int n, std::vector<double>& x, std::vector<double>& w);
+void trajectory_points(double half_window, int n_quad, std::vector<double>& points, std::vector<double>& weights);
+int check_settings(rcmps_context* ctx, const rcmps_settings* s);
+int check_dims(rcmps_context* ctx, int n, const int* dims);
+
+}  // namespace rcmps

@@ -1,0 +1,45 @@
+// Host/device interface of the DOP853 trajectory kernel (internal to the library).
+#pragma once
+#include <cuda_runtime.h>
+
+namespace rcmps {
+
+// Outcome of one trajectory (written by CTA 0 of the state's cluster). Names follow the
+// reference's diagnostics (device_control_backend.py:263-265 of rcmps_gpu).
+struct TrajStats {
+  int status;
+  int pad_;
+  long long attempts, accepted, rejected, dense_steps, next_point;
+  double t, h, min_h, max_h, last_error;
+  double value;   // the scalar channel at the endpoint: the quartic density before g
+};
+
+// One state of a batch: device pointers of dp x dp complex matrices (zero padded beyond d)
+// and its workspace. All matrices row-major double2.
+struct TrajState {
+  const double2 *Q, *Qh, *R, *Rh;     // Q, Q^dag, R, R^dag
+  const double2 *fixed0, *fixed6;     // R rho + rho R^dag, 4 (R + R^dag)
+  const double2* S;                   // conj(R) + R^T: weights of the scalar trace
+  double2 *y, *prop, *k, *z, *P;      // y, proposed [7 dp^2]; k [16][7 dp^2]; z [2][7 dp^2]; P [7 dp^2]
+  double2* samples;                   // [npoints][7 dp^2]
+  TrajStats* stats;
+  double atol, rtol;
+  long long max_steps;
+  int d;                              // physical bond dimension (d <= dp)
+  int pad_;
+};
+
+struct TrajControls {
+  double endpoint;          // sqrt(half_window)
+  double initial_h;
+  unsigned long long max_ns;  // device-clock watchdog in ns (0: none)
+};
+
+cudaError_t trajectory_set_tables();
+cudaError_t trajectory_launch(int dp, const TrajState* d_states, int nstates, const double* d_points,
+                              int npoints, const TrajControls& ctl, cudaStream_t stream);
+size_t trajectory_smem_bytes(int dp);
+cudaError_t node_weights_launch(const double* d_points, const double* d_weights, int n, double* d_wj,
+                                cudaStream_t stream);
+
+}  // namespace rcmps
