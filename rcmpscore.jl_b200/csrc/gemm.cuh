@@ -8,11 +8,16 @@
 
 namespace rcmps {
 
-template <int DP, int MB, int NW, int KC, int NST>
-struct RowGemm {
+template <int DP, int MB, int NW>
+struct Tiling {
   static constexpr int TN = DP / 8, TM = MB / 16, T = TM * TN, TPW = T / NW;
   static_assert(T % NW == 0, "tiles per warp");
   static_assert(TN % TPW == 0, "a warp's tiles share one band");
+};
+
+// The ring and its counter are shared by products of different row counts (run<MB>).
+template <int DP, int NW, int KC, int NST>
+struct RowGemmRing {
   static constexpr int NT = 32 * NW;
   static constexpr uint32_t CHUNK_BYTES = KC * DP * 16;
 
@@ -52,7 +57,9 @@ struct RowGemm {
   }
 
   // acc[TPW] += A * B. Call with all threads; ends with a __syncthreads.
+  template <int MB>
   __device__ void run(ZFrag* acc, const double2* A, int lda, const Segs& s) {
+    constexpr int TN = Tiling<DP, MB, NW>::TN, TPW = Tiling<DP, MB, NW>::TPW;
     int krows = 0;
     for (int i = 0; i < s.n; ++i) krows += s.rows[i];
     const int nch = krows / KC;
@@ -87,7 +94,9 @@ struct RowGemm {
   }
 
   // Coordinates of fragment entry i of tile j for this thread: row in [0, MB), col in [0, DP).
+  template <int MB>
   __device__ static void coord(int j, int i, int& row, int& col) {
+    constexpr int TN = Tiling<DP, MB, NW>::TN, TPW = Tiling<DP, MB, NW>::TPW;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int tile = warp * TPW + j;
     row = (tile / TN) * 16 + frag_row(lane, i);
@@ -102,6 +111,17 @@ struct RowGemm {
     }
     __syncthreads();
   }
+};
+
+// Single-row-count convenience form (the pullback's passes).
+template <int DP, int MB, int NW, int KC, int NST>
+struct RowGemm : RowGemmRing<DP, NW, KC, NST> {
+  using Base = RowGemmRing<DP, NW, KC, NST>;
+  static constexpr int TPW = Tiling<DP, MB, NW>::TPW;
+  __device__ void run(ZFrag* acc, const double2* A, int lda, const typename Base::Segs& s) {
+    Base::template run<MB>(acc, A, lda, s);
+  }
+  __device__ static void coord(int j, int i, int& row, int& col) { Base::template coord<MB>(j, i, row, col); }
 };
 
 }  // namespace rcmps

@@ -56,7 +56,11 @@ pullback_kernel(PullbackArgs a) {
   double2* wscr = a.scratch + ((size_t)blockIdx.y * gridDim.x + blk) * 3 * MAT;
   const int tid = threadIdx.x;
 
-  GM gm{ring, full, flag, 0};
+  GM gm;
+  gm.ring = ring;
+  gm.full = full;
+  gm.wait_flag = flag;
+  gm.gq = 0;
   if (tid == 0) *flag = 0;
   gm.init();
   __syncthreads();
