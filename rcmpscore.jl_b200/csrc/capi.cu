@@ -7,55 +7,75 @@
 #include <cstring>
 #include <map>
 #include <string>
+#include <thread>
 #include <vector>
 #include "../../include/rcmps_b200.h"
+#include "common.cuh"
 #include "context.h"
 #include "prep.h"
 #include "kinetic_host.h"
 #include "quartic.h"
+#include "solvers_host.h"
 #include "trajectory.h"
 
 namespace rcmps {
 
-cudaError_t arena_reserve(rcmps_context* ctx, size_t bytes) {
-  if (bytes <= ctx->arena_bytes) return cudaSuccess;
-  if (ctx->arena) {
-    cudaError_t e = cudaStreamSynchronize(ctx->stream);
+cudaError_t arena_reserve(rcmps_slot& sl, size_t bytes) {
+  if (bytes <= sl.arena_bytes) return cudaSuccess;
+  if (sl.arena) {
+    cudaError_t e = cudaStreamSynchronize(sl.stream);
     if (e != cudaSuccess) return e;
-    e = cudaStreamSynchronize(ctx->side);
-    if (e != cudaSuccess) return e;
-    cudaFree(ctx->arena);
-    ctx->arena = nullptr;
-    ctx->arena_bytes = 0;
+    cudaFree(sl.arena);
+    sl.arena = nullptr;
+    sl.arena_bytes = 0;
   }
   const size_t want = align256(bytes + bytes / 8);
-  cudaError_t e = cudaMalloc(&ctx->arena, want);
+  cudaError_t e = cudaMalloc(&sl.arena, want);
   if (e != cudaSuccess) {
     cudaGetLastError();
-    e = cudaMalloc(&ctx->arena, align256(bytes));
+    e = cudaMalloc(&sl.arena, align256(bytes));
     if (e != cudaSuccess) {
-      ctx->arena = nullptr;
+      cudaGetLastError();
+      sl.arena = nullptr;
       return e;
     }
-    ctx->arena_bytes = align256(bytes);
+    sl.arena_bytes = align256(bytes);
     return cudaSuccess;
   }
-  ctx->arena_bytes = want;
+  sl.arena_bytes = want;
   return cudaSuccess;
 }
 
-cudaError_t pinned_reserve(rcmps_context* ctx, size_t bytes) {
-  if (bytes <= ctx->pinned_bytes) return cudaSuccess;
-  if (ctx->pinned) cudaFreeHost(ctx->pinned);
-  ctx->pinned = nullptr;
-  ctx->pinned_bytes = 0;
-  cudaError_t e = cudaMallocHost(&ctx->pinned, bytes);
-  if (e == cudaSuccess) ctx->pinned_bytes = bytes;
+cudaError_t pinned_reserve(rcmps_slot& sl, size_t bytes) {
+  if (bytes <= sl.pinned_bytes) return cudaSuccess;
+  if (sl.pinned) {
+    cudaStreamSynchronize(sl.stream);
+    cudaFreeHost(sl.pinned);
+  }
+  sl.pinned = nullptr;
+  sl.pinned_bytes = 0;
+  cudaError_t e = cudaMallocHost(&sl.pinned, bytes);
+  if (e == cudaSuccess) sl.pinned_bytes = bytes;
+  return e;
+}
+
+cudaError_t aux_reserve(rcmps_context* ctx, size_t bytes) {
+  if (bytes <= ctx->aux_bytes) return cudaSuccess;
+  for (auto& sl : ctx->slot) cudaStreamSynchronize(sl.stream);
+  if (ctx->aux) cudaFree(ctx->aux);
+  ctx->aux = nullptr;
+  ctx->aux_bytes = 0;
+  cudaError_t e = cudaMalloc(&ctx->aux, align256(bytes));
+  if (e == cudaSuccess) ctx->aux_bytes = align256(bytes);
+  else cudaGetLastError();
   return e;
 }
 
 int fail(rcmps_context* ctx, int code, const std::string& message) {
-  if (ctx) ctx->error = message;
+  if (ctx) {
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    ctx->error = message;
+  }
   return code;
 }
 
@@ -149,6 +169,35 @@ int check_dims(rcmps_context* ctx, int n, const int* dims) {
   return RCMPS_OK;
 }
 
+// energy = vq + vk; covector = cq + ck; environment = eq + ek (packed arrays of `total` complex values)
+__global__ void sum_parts_kernel(int n, long long total, const double* vq, const double* vk, const double2* cq,
+                                 const double2* ck, const double2* eq, const double2* ek, double* energy,
+                                 double2* cov, double2* env) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i < n) energy[i] = vq[i] + vk[i];
+  for (long long e = i; e < total; e += (long long)gridDim.x * blockDim.x) {
+    cov[e] = zadd(cq[e], ck[e]);
+    env[e] = zadd(eq[e], ek[e]);
+  }
+}
+
+// FP64 tensor-core throughput: an in-register chain of independent mma.sync m16n8k8 per warp.
+__global__ void fp64_peak_kernel(double* out, int iters) {
+  double a[4], b[2], c[8][4];
+  for (int j = 0; j < 4; ++j) a[j] = 1e-3 * (threadIdx.x + j);
+  b[0] = 1.0;
+  b[1] = 0.5;
+  for (int t = 0; t < 8; ++t)
+    for (int j = 0; j < 4; ++j) c[t][j] = 0.0;
+  for (int i = 0; i < iters; ++i)
+#pragma unroll
+    for (int t = 0; t < 8; ++t) dmma16x8x8(c[t], a, b);
+  double s = 0.0;
+  for (int t = 0; t < 8; ++t)
+    for (int j = 0; j < 4; ++j) s += c[t][j];
+  out[blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+
 }  // namespace rcmps
 
 using namespace rcmps;
@@ -184,10 +233,12 @@ int rcmps_context_create(int device, rcmps_context** out) {
   ctx->device = device;
   cudaError_t e = cudaSetDevice(device);
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&ctx->sms, cudaDevAttrMultiProcessorCount, device);
-  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
-  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->side, cudaStreamNonBlocking);
-  if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev_a);
-  if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev_b);
+  for (auto& sl : ctx->slot) {
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking);
+    for (auto& ev : sl.ev)
+      if (e == cudaSuccess) e = cudaEventCreate(&ev);
+  }
+  ctx->stream = ctx->slot[0].stream;
   if (e == cudaSuccess) e = trajectory_set_tables();
   if (e == cudaSuccess) e = quartic_init();
   if (e != cudaSuccess) {
@@ -202,14 +253,15 @@ int rcmps_context_create(int device, rcmps_context** out) {
 int rcmps_context_destroy(rcmps_context* ctx) {
   if (!ctx) return RCMPS_OK;
   cudaSetDevice(ctx->device);
-  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
-  if (ctx->side) cudaStreamSynchronize(ctx->side);
-  if (ctx->arena) cudaFree(ctx->arena);
-  if (ctx->pinned) cudaFreeHost(ctx->pinned);
-  if (ctx->ev_a) cudaEventDestroy(ctx->ev_a);
-  if (ctx->ev_b) cudaEventDestroy(ctx->ev_b);
-  if (ctx->stream) cudaStreamDestroy(ctx->stream);
-  if (ctx->side) cudaStreamDestroy(ctx->side);
+  for (auto& sl : ctx->slot) {
+    if (sl.stream) cudaStreamSynchronize(sl.stream);
+    if (sl.arena) cudaFree(sl.arena);
+    if (sl.pinned) cudaFreeHost(sl.pinned);
+    for (auto& ev : sl.ev)
+      if (ev) cudaEventDestroy(ev);
+    if (sl.stream) cudaStreamDestroy(sl.stream);
+  }
+  if (ctx->aux) cudaFree(ctx->aux);
   delete ctx;
   return RCMPS_OK;
 }
@@ -252,7 +304,7 @@ int rcmps_quartic_samples(rcmps_context* ctx, int d, const double* R, const doub
   if (rc) return rc;
   if (!R || !K || !rho || !samples) return fail(ctx, RCMPS_INVALID_ARGUMENT, "NULL matrix pointer");
   cudaSetDevice(ctx->device);
-  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
+  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : ctx->slot[0].stream;
   QuarticJob job;
   job.n = 1;
   job.dims = &d;
@@ -320,12 +372,251 @@ int rcmps_kinetic_batch(rcmps_context* ctx, int n, const int* dims, const double
   job.covector = covector;
   job.environment = environment;
   job.stats = stats;
-  cudaEventRecord(ctx->ev_a, s);
   rc = kinetic_run(ctx, job, s);
-  cudaEventRecord(ctx->ev_b, s);
-  cudaEventSynchronize(ctx->ev_b);
-  cudaEventElapsedTime(&ctx->last_ms[2], ctx->ev_a, ctx->ev_b);
   return rc;
+}
+
+int rcmps_finish_gradient_batch(rcmps_context* ctx, int n, const int* dims, const double* R, const double* K,
+                                const double* rho, const double* covector, const double* environment,
+                                const rcmps_settings* settings, double* gradient, rcmps_state_stats* stats,
+                                void* stream) {
+  if (!ctx) return RCMPS_INVALID_ARGUMENT;
+  int rc = check_settings(ctx, settings);
+  if (rc) return rc;
+  rc = check_dims(ctx, n, dims);
+  if (rc) return rc;
+  if (n == 0) return RCMPS_OK;
+  if (!R || !K || !rho || !covector || !environment || !gradient || !stats)
+    return fail(ctx, RCMPS_INVALID_ARGUMENT, "NULL pointer");
+  cudaSetDevice(ctx->device);
+  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : ctx->slot[2].stream;
+  for (int i = 0; i < n; ++i) std::memset(&stats[i], 0, sizeof(rcmps_state_stats));
+  FinishJob job;
+  job.n = n;
+  job.dims = dims;
+  job.R = R;
+  job.K = K;
+  job.rho = rho;
+  job.covector = covector;
+  job.environment = environment;
+  job.settings = *settings;
+  job.gradient = gradient;
+  job.stats = stats;
+  return finish_run(ctx, job, s);
+}
+
+int rcmps_stationary_state_batch(rcmps_context* ctx, int n, const int* dims, const double* R, const double* K,
+                                 double tolerance, double* rho, rcmps_state_stats* stats, void* stream) {
+  if (!ctx) return RCMPS_INVALID_ARGUMENT;
+  int rc = check_dims(ctx, n, dims);
+  if (rc) return rc;
+  if (n == 0) return RCMPS_OK;
+  if (!R || !K || !rho || !stats) return fail(ctx, RCMPS_INVALID_ARGUMENT, "NULL pointer");
+  cudaSetDevice(ctx->device);
+  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : ctx->slot[2].stream;
+  for (int i = 0; i < n; ++i) std::memset(&stats[i], 0, sizeof(rcmps_state_stats));
+  StationaryJob job;
+  job.n = n;
+  job.dims = dims;
+  job.R = R;
+  job.K = K;
+  job.tolerance = tolerance;
+  job.rho = rho;
+  job.stats = stats;
+  return stationary_run(ctx, job, s);
+}
+
+int rcmps_fg_phi4_batch(rcmps_context* ctx, int n, const int* dims, const double* couplings, const double* R,
+                        const double* K, const double* rho, const rcmps_settings* settings, double* energy,
+                        double* gradient, double* covector, double* environment, rcmps_state_stats* stats,
+                        void* stream) {
+  if (!ctx) return RCMPS_INVALID_ARGUMENT;
+  int rc = check_settings(ctx, settings);
+  if (rc) return rc;
+  rc = check_dims(ctx, n, dims);
+  if (rc) return rc;
+  if (n == 0) return RCMPS_OK;
+  if (!R || !K || !rho || !energy || !gradient || !stats || !couplings)
+    return fail(ctx, RCMPS_INVALID_ARGUMENT, "NULL pointer");
+  cudaSetDevice(ctx->device);
+  long long total = 0;
+  for (int i = 0; i < n; ++i) total += (long long)dims[i] * dims[i];
+  // aux: vq, vk [n]; cq, ck, eq, ek, cov, env [total complex]
+  const size_t vbytes = align256((size_t)n * 8), cbytes = align256((size_t)total * 16);
+  if (aux_reserve(ctx, 2 * vbytes + 6 * cbytes) != cudaSuccess)
+    return fail(ctx, RCMPS_OUT_OF_MEMORY, "fg_phi4 intermediate buffers");
+  char* a = static_cast<char*>(ctx->aux);
+  double* vq = (double*)a;
+  double* vk = (double*)(a + vbytes);
+  double* cq = (double*)(a + 2 * vbytes);
+  double* ck = (double*)(a + 2 * vbytes + cbytes);
+  double* eq = (double*)(a + 2 * vbytes + 2 * cbytes);
+  double* ek = (double*)(a + 2 * vbytes + 3 * cbytes);
+  double* csum = covector ? covector : (double*)(a + 2 * vbytes + 4 * cbytes);
+  double* esum = environment ? environment : (double*)(a + 2 * vbytes + 5 * cbytes);
+  // the inputs are ordered on the caller's stream
+  cudaStream_t cs = stream ? static_cast<cudaStream_t>(stream) : nullptr;
+  cudaEvent_t ready = ctx->slot[2].ev[3];
+  cudaEventRecord(ready, cs);
+  for (auto& sl : ctx->slot) cudaStreamWaitEvent(sl.stream, ready, 0);
+  cudaEventRecord(ctx->slot[2].ev[0], ctx->slot[0].stream);
+  for (int i = 0; i < n; ++i) std::memset(&stats[i], 0, sizeof(rcmps_state_stats));
+  std::vector<rcmps_state_stats> kst(n);
+  std::memset(kst.data(), 0, n * sizeof(rcmps_state_stats));
+  QuarticJob qj;
+  qj.n = n;
+  qj.dims = dims;
+  qj.couplings = couplings;
+  qj.R = R;
+  qj.K = K;
+  qj.rho = rho;
+  qj.settings = *settings;
+  qj.value = vq;
+  qj.covector = cq;
+  qj.environment = eq;
+  qj.stats = stats;
+  qj.slot = 0;
+  qj.memory_share = 0.4;
+  KineticJob kj;
+  kj.n = n;
+  kj.dims = dims;
+  kj.R = R;
+  kj.K = K;
+  kj.rho = rho;
+  kj.settings = *settings;
+  kj.value = vk;
+  kj.covector = ck;
+  kj.environment = ek;
+  kj.stats = kst.data();
+  kj.slot = 1;
+  kj.memory_share = 0.3;
+  int krc = RCMPS_OK;
+  std::thread worker([&] {
+    cudaSetDevice(ctx->device);
+    krc = kinetic_run(ctx, kj, ctx->slot[1].stream);
+  });
+  const int qrc = quartic_run(ctx, qj, ctx->slot[0].stream);
+  worker.join();
+  for (int i = 0; i < n; ++i) {
+    stats[i].kinetic_value = kst[i].kinetic_value;
+    for (int q = 0; q < 4; ++q) stats[i].krylov_basis[q] = kst[i].krylov_basis[q];
+    stats[i].krylov_residual = kst[i].krylov_residual;
+    if (!stats[i].status && kst[i].status) {
+      stats[i].status = kst[i].status;
+      stats[i].failed_component = kst[i].failed_component;
+    }
+  }
+  if (qrc || krc) return qrc ? qrc : krc;
+  cudaStream_t s2 = ctx->slot[2].stream;
+  cudaEventRecord(ctx->slot[2].ev[1], s2);
+  sum_parts_kernel<<<(int)std::min<long long>(4096, (total + 255) / 256 + 1), 256, 0, s2>>>(
+      n, total, vq, vk, (double2*)cq, (double2*)ck, (double2*)eq, (double2*)ek, energy, (double2*)csum,
+      (double2*)esum);
+  std::vector<rcmps_state_stats> fst(n);
+  std::memset(fst.data(), 0, n * sizeof(rcmps_state_stats));
+  FinishJob fj;
+  fj.n = n;
+  fj.dims = dims;
+  fj.R = R;
+  fj.K = K;
+  fj.rho = rho;
+  fj.covector = csum;
+  fj.environment = esum;
+  fj.settings = *settings;
+  fj.gradient = gradient;
+  fj.stats = fst.data();
+  fj.slot = 2;
+  const int frc = finish_run(ctx, fj, s2);
+  cudaEventRecord(ctx->slot[2].ev[2], s2);
+  cudaEventSynchronize(ctx->slot[2].ev[2]);
+  cudaEventElapsedTime(&ctx->last_ms[3], ctx->slot[2].ev[1], ctx->slot[2].ev[2]);
+  cudaEventElapsedTime(&ctx->last_ms[4], ctx->slot[2].ev[0], ctx->slot[2].ev[2]);
+  for (int i = 0; i < n; ++i) {
+    stats[i].gmres_iterations = fst[i].gmres_iterations;
+    stats[i].boundary_residual = fst[i].boundary_residual;
+    if (!stats[i].status && fst[i].status) {
+      stats[i].status = fst[i].status;
+      stats[i].failed_component = fst[i].failed_component;
+    }
+  }
+  // the results are complete on the caller's stream too
+  cudaEventRecord(ready, s2);
+  cudaStreamWaitEvent(cs, ready, 0);
+  return frc;
+}
+
+int rcmps_fg_phi4_batch_host(rcmps_context* ctx, int n, const int* dims, const double* couplings, const double* R,
+                             const double* K, const double* rho, const rcmps_settings* settings, double* energy,
+                             double* gradient, double* covector, double* environment, rcmps_state_stats* stats) {
+  if (!ctx) return RCMPS_INVALID_ARGUMENT;
+  int rc = check_dims(ctx, n, dims);
+  if (rc) return rc;
+  if (n == 0) return RCMPS_OK;
+  if (!R || !K || !rho || !energy || !gradient) return fail(ctx, RCMPS_INVALID_ARGUMENT, "NULL pointer");
+  cudaSetDevice(ctx->device);
+  long long total = 0;
+  for (int i = 0; i < n; ++i) total += (long long)dims[i] * dims[i];
+  const size_t cb = (size_t)total * 16;
+  void* dev = nullptr;
+  // device copies of inputs and outputs (one allocation per call: the host entry is the
+  // convenience form; rcmps_fg_phi4_batch takes device buffers and allocates nothing per call)
+  cudaError_t e = cudaMalloc(&dev, 6 * cb + (size_t)n * 8 + 256);
+  if (e) return fail(ctx, RCMPS_OUT_OF_MEMORY, "host entry buffers");
+  char* d = static_cast<char*>(dev);
+  double *dR = (double*)d, *dK = (double*)(d + cb), *dP = (double*)(d + 2 * cb), *dG = (double*)(d + 3 * cb),
+         *dC = (double*)(d + 4 * cb), *dE = (double*)(d + 5 * cb), *dEn = (double*)(d + 6 * cb);
+  cudaStream_t s = ctx->slot[0].stream;
+  e = cudaMemcpyAsync(dR, R, cb, cudaMemcpyHostToDevice, s);
+  if (!e) e = cudaMemcpyAsync(dK, K, cb, cudaMemcpyHostToDevice, s);
+  if (!e) e = cudaMemcpyAsync(dP, rho, cb, cudaMemcpyHostToDevice, s);
+  if (!e) e = cudaStreamSynchronize(s);
+  if (e) {
+    cudaFree(dev);
+    return fail(ctx, RCMPS_CUDA_ERROR, std::string("host entry copies: ") + cudaGetErrorString(e));
+  }
+  rc = rcmps_fg_phi4_batch(ctx, n, dims, couplings, dR, dK, dP, settings, dEn, dG, dC, dE, stats, s);
+  if (!e) e = cudaMemcpyAsync(energy, dEn, (size_t)n * 8, cudaMemcpyDeviceToHost, s);
+  if (!e) e = cudaMemcpyAsync(gradient, dG, cb, cudaMemcpyDeviceToHost, s);
+  if (!e && covector) e = cudaMemcpyAsync(covector, dC, cb, cudaMemcpyDeviceToHost, s);
+  if (!e && environment) e = cudaMemcpyAsync(environment, dE, cb, cudaMemcpyDeviceToHost, s);
+  if (!e) e = cudaStreamSynchronize(s);
+  cudaFree(dev);
+  if (e) return fail(ctx, RCMPS_CUDA_ERROR, std::string("host entry copies: ") + cudaGetErrorString(e));
+  return rc;
+}
+
+long long rcmps_workspace_bytes(const rcmps_context* ctx, int n, const int* dims, const rcmps_settings* settings) {
+  if (!ctx || !dims || !settings || n < 0) return -1;
+  long long total = 0;
+  for (int i = 0; i < n; ++i) {
+    const int dp = padded_dim(dims[i]);
+    if (!dp) return -1;
+    const long long mat = (long long)dp * dp * 16;
+    const long long npoints = 2LL * settings->n_quad + 1;
+    const int kmax = std::min(settings->krylov_maxdim, dims[i] * dims[i]);
+    total += (npoints + 200) * 7 * mat;                                       // quartic
+    total += 4 * ((kmax + 1) * mat + (long long)settings->kinetic_nodes * mat) + 64 * mat;   // kinetic
+  }
+  return total;
+}
+
+double rcmps_fp64_peak_tflops(rcmps_context* ctx) {
+  if (!ctx) return 0.0;
+  cudaSetDevice(ctx->device);
+  const int blocks = 2 * ctx->sms, threads = 256, iters = 4096;
+  double* out = nullptr;
+  if (cudaMalloc(&out, (size_t)blocks * threads * 8)) return 0.0;
+  cudaStream_t s = ctx->slot[0].stream;
+  fp64_peak_kernel<<<blocks, threads, 0, s>>>(out, iters);   // warm-up
+  cudaEventRecord(ctx->slot[0].ev[0], s);
+  fp64_peak_kernel<<<blocks, threads, 0, s>>>(out, iters);
+  cudaEventRecord(ctx->slot[0].ev[1], s);
+  cudaEventSynchronize(ctx->slot[0].ev[1]);
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, ctx->slot[0].ev[0], ctx->slot[0].ev[1]);
+  cudaFree(out);
+  const double flops = 2.0 * 16 * 8 * 8 * 8.0 * iters * (double)blocks * (threads / 32);
+  return ms > 0.f ? flops / (ms * 1e-3) / 1e12 : 0.0;
 }
 
 }  // extern "C"

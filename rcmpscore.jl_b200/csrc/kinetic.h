@@ -38,8 +38,8 @@ struct ArnoldiProblem {
   double2* g;                // [kmax + 1] rotated residual vector
   double2* cs;               // [kmax] Givens cosines (real part used) and sines
   double2* sn;
-  double gtarget, gres, bnorm;
-  int converged, restarts, d;
+  double gtarget, gres, bnorm, gtol;
+  int converged, restarts, d, iters;
   double beta, estimate, residual;
   int n, n_phys, dp, kmax, kmax1, target;
   int k, exhausted, nonfinite, active, solve, reconstruct, adjoint;

@@ -67,9 +67,11 @@ int kinetic_run(rcmps_context* ctx, KineticJob& job, cudaStream_t stream) {
   for (int i = 0; i < job.n; ++i) off[i + 1] = off[i] + (long long)job.dims[i] * job.dims[i];
   std::map<int, std::vector<int>> groups;
   for (int i = 0; i < job.n; ++i) groups[padded_dim(job.dims[i])].push_back(i);
+  rcmps_slot& SL = ctx->slot[job.slot];
   size_t free_b = 0, total_b = 0;
   cudaMemGetInfo(&free_b, &total_b);
-  const size_t budget = std::max<size_t>((size_t)1 << 30, (free_b + ctx->arena_bytes) * 7 / 10);
+  const size_t budget = std::max<size_t>((size_t)1 << 30, (free_b + SL.arena_bytes) * job.memory_share);
+  cudaEventRecord(SL.ev[0], stream);
   const size_t scratch_budget = (size_t)1 << 30;
 
   for (auto& kv : groups) {
@@ -111,10 +113,10 @@ int kinetic_run(rcmps_context* ctx, KineticJob& job, cudaStream_t stream) {
       const size_t o_val = L.add(n * 8);
       const size_t o_ptrs = L.add((size_t)(4 * n + 5 * n) * sizeof(void*));
       const size_t o_scr = L.add(scratch_budget);
-      cudaError_t e = arena_reserve(ctx, L.total);
+      cudaError_t e = arena_reserve(SL, L.total);
       if (e != cudaSuccess)
         return fail(ctx, RCMPS_OUT_OF_MEMORY, "kinetic workspace: " + std::to_string(L.total) + " bytes");
-      char* base = static_cast<char*>(ctx->arena);
+      char* base = static_cast<char*>(SL.arena);
       auto P = [&](size_t o) { return static_cast<void*>(base + o); };
       double2* d_in = (double2*)P(o_in);
       double2* d_ops = (double2*)P(o_ops);
@@ -129,8 +131,8 @@ int kinetic_run(rcmps_context* ctx, KineticJob& job, cudaStream_t stream) {
                    h_weight = H.add(nshift * 8), h_probs = H.add(NP * sizeof(ArnoldiProblem)),
                    h_rt = H.add((size_t)NP * nshift * sizeof(LindbladTask)), h_ptrs = H.add((size_t)9 * n * sizeof(void*)),
                    h_flag = H.add(n * 4), h_idx = H.add(n * 4);
-      if (pinned_reserve(ctx, H.total) != cudaSuccess) return fail(ctx, RCMPS_CUDA_ERROR, "pinned host buffer");
-      char* h = static_cast<char*>(ctx->pinned);
+      if (pinned_reserve(SL, H.total) != cudaSuccess) return fail(ctx, RCMPS_CUDA_ERROR, "pinned host buffer");
+      char* h = static_cast<char*>(SL.pinned);
       int* hd = (int*)(h + h_dims);
       long long* ho = (long long*)(h + h_off);
       double* hs = (double*)(h + h_shift);
@@ -415,6 +417,9 @@ int kinetic_run(rcmps_context* ctx, KineticJob& job, cudaStream_t stream) {
       }
     }
   }
+  cudaEventRecord(SL.ev[1], stream);
+  cudaEventSynchronize(SL.ev[1]);
+  cudaEventElapsedTime(&ctx->last_ms[2], SL.ev[0], SL.ev[1]);
   for (int i = 0; i < job.n; ++i)
     if (job.stats[i].status) return job.stats[i].status;
   return RCMPS_OK;

@@ -17,6 +17,8 @@ struct KineticJob {
   double* environment = nullptr;        // device packed, optional
   rcmps_state_stats* stats = nullptr;   // host [n]
   bool accumulate = false;
+  int slot = 1;
+  double memory_share = 0.7;
 };
 
 void angular_grid(int nodes, std::vector<double>& shifts, std::vector<double>& weights);

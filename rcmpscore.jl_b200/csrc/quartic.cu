@@ -64,11 +64,12 @@ int quartic_run(rcmps_context* ctx, QuarticJob& job, cudaStream_t stream) {
   std::map<int, std::vector<int>> groups;
   for (int i = 0; i < job.n; ++i) groups[padded_dim(job.dims[i])].push_back(i);
 
+  rcmps_slot& SL = ctx->slot[job.slot];
   size_t free_b = 0, total_b = 0;
   cudaMemGetInfo(&free_b, &total_b);
-  const size_t budget = std::max<size_t>((size_t)1 << 30, (free_b + ctx->arena_bytes) * 7 / 10);
+  const size_t budget = std::max<size_t>((size_t)1 << 30, (free_b + SL.arena_bytes) * job.memory_share);
 
-  cudaEvent_t e0 = ctx->ev_a, e1 = ctx->ev_b;
+  cudaEvent_t e0 = SL.ev[0], e1 = SL.ev[1], e2 = SL.ev[2];
   float traj_ms = 0.f, pull_ms = 0.f;
 
   for (auto& kv : groups) {
@@ -104,10 +105,10 @@ int quartic_run(rcmps_context* ctx, QuarticJob& job, cudaStream_t stream) {
       const size_t o_fin = L.add((size_t)n * 8 * mat * 16);
       const size_t o_cov = L.add((size_t)n * mat * 16);
       const size_t o_env = L.add((size_t)n * mat * 16);
-      cudaError_t e = arena_reserve(ctx, L.total);
+      cudaError_t e = arena_reserve(SL, L.total);
       if (e != cudaSuccess)
         return fail(ctx, RCMPS_OUT_OF_MEMORY, "quartic workspace: " + std::to_string(L.total) + " bytes");
-      char* base = static_cast<char*>(ctx->arena);
+      char* base = static_cast<char*>(SL.arena);
       auto P = [&](size_t o) { return static_cast<void*>(base + o); };
 
       // host-side tables through a pinned staging buffer
@@ -121,8 +122,8 @@ int quartic_run(rcmps_context* ctx, QuarticJob& job, cudaStream_t stream) {
       const size_t h_o_states = H.add(n * sizeof(TrajState));
       const size_t h_o_tstats = H.add(n * sizeof(TrajStats));
       const size_t h_o_flag = H.add(n * sizeof(int));
-      if (pinned_reserve(ctx, H.total) != cudaSuccess) return fail(ctx, RCMPS_CUDA_ERROR, "pinned host buffer");
-      char* h = static_cast<char*>(ctx->pinned);
+      if (pinned_reserve(SL, H.total) != cudaSuccess) return fail(ctx, RCMPS_CUDA_ERROR, "pinned host buffer");
+      char* h = static_cast<char*>(SL.pinned);
       int* h_dims = reinterpret_cast<int*>(h + h_o_dims);
       long long* h_off = reinterpret_cast<long long*>(h + h_o_off);
       int* h_idx = reinterpret_cast<int*>(h + h_o_idx);
@@ -220,14 +221,9 @@ int quartic_run(rcmps_context* ctx, QuarticJob& job, cudaStream_t stream) {
       pa.env_out = (double2*)P(o_env);
       pa.value_out = (double*)P(o_vout);
       pa.error_flag = (int*)P(o_flag);
-      cudaEvent_t e2 = nullptr;
-      if (e == cudaSuccess) e = cudaEventCreate(&e2);
       if (e == cudaSuccess) e = pullback_launch(pa, nblk, stream);
       if (e == cudaSuccess) e = cudaEventRecord(e2, stream);
-      if (e != cudaSuccess) {
-        if (e2) cudaEventDestroy(e2);
-        return fail(ctx, RCMPS_CUDA_ERROR, std::string("pullback launch: ") + cudaGetErrorString(e));
-      }
+      if (e != cudaSuccess) return fail(ctx, RCMPS_CUDA_ERROR, std::string("pullback launch: ") + cudaGetErrorString(e));
       // outputs
       if (job.covector)
         e = launch_unpad_acc(reinterpret_cast<double*>(P(o_cov)), (long long)mat, dp, (long long*)P(o_off),
@@ -242,16 +238,12 @@ int quartic_run(rcmps_context* ctx, QuarticJob& job, cudaStream_t stream) {
       if (e == cudaSuccess) e = cudaMemcpyAsync(h_tstats, P(o_tstats), n * sizeof(TrajStats), cudaMemcpyDeviceToHost, stream);
       if (e == cudaSuccess) e = cudaMemcpyAsync(h_flag, P(o_flag), n * sizeof(int), cudaMemcpyDeviceToHost, stream);
       if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
-      if (e != cudaSuccess) {
-        cudaEventDestroy(e2);
-        return fail(ctx, RCMPS_CUDA_ERROR, std::string("quartic: ") + cudaGetErrorString(e));
-      }
+      if (e != cudaSuccess) return fail(ctx, RCMPS_CUDA_ERROR, std::string("quartic: ") + cudaGetErrorString(e));
       float ms = 0.f;
       cudaEventElapsedTime(&ms, e0, e1);
       traj_ms += ms;
       cudaEventElapsedTime(&ms, e1, e2);
       pull_ms += ms;
-      cudaEventDestroy(e2);
       for (int i = 0; i < n; ++i) {
         const TrajStats& t = h_tstats[i];
         rcmps_state_stats& o = job.stats[idx[i]];

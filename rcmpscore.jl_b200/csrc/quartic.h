@@ -19,6 +19,8 @@ struct QuarticJob {
   double* samples_out = nullptr;        // device, single-state samples, optional
   rcmps_state_stats* stats = nullptr;   // host [n]
   bool accumulate = false;              // add into value/covector/environment instead of storing
+  int slot = 0;                         // context slot (workspace, staging, events)
+  double memory_share = 0.7;            // fraction of free device memory this job may hold
 };
 
 cudaError_t quartic_init();

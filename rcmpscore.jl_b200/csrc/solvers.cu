@@ -48,7 +48,10 @@ __global__ void gmres_start(ArnoldiProblem* __restrict__ probs, int nprob, int n
   double t = 0.0;
   for (int c = 0; c < nchunk; ++c) t += P.norms[c];
   const double beta = sqrt(t);
-  const bool conv = beta <= P.gtarget || !isfinite(beta);
+  // first residual (x = 0) is |b|: the stopping target is tol max(1, |b|) (scipy gmres with rtol = atol)
+  const double bn = P.bnorm >= 0.0 ? P.bnorm : beta;
+  const double target = P.gtol * fmax(1.0, bn);
+  const bool conv = beta <= target || !isfinite(beta);
   const int r0 = ch * GCH, r1 = min(P.n, r0 + GCH);
   if (!conv) {
     const double inv = 1.0 / beta;
@@ -57,6 +60,8 @@ __global__ void gmres_start(ArnoldiProblem* __restrict__ probs, int nprob, int n
   const int hsz = (P.kmax + 1) * P.kmax;
   for (int i = ch * blockDim.x + threadIdx.x; i < hsz; i += nchunk * blockDim.x) P.H[i] = make_double2(0, 0);
   if (ch == 0 && threadIdx.x == 0) {
+    P.bnorm = bn;
+    P.gtarget = target;
     P.gres = beta;
     P.residual = beta;
     if (!isfinite(beta)) P.nonfinite = 1;
@@ -111,6 +116,7 @@ __global__ void gmres_givens(ArnoldiProblem* __restrict__ probs, int nprob, int 
   P.g[j] = zscale(c, gj);
   const double res = hypot(P.g[j + 1].x, P.g[j + 1].y);
   P.gres = res;
+  P.iters += 1;
   if (!isfinite(res)) {
     P.nonfinite = 1;
     P.active = 0;
@@ -276,7 +282,7 @@ __global__ void boundary_rhs_kernel(FinishArgs a) {
 __global__ void finish_kernel(FinishArgs a) {
   const int s = blockIdx.x, dp = a.dp, MAT = dp * dp;
   const double2* ops = a.ops + (size_t)s * a.ops_stride;
-  const double2 *R = ops + 2 * MAT, *Rh = ops + 3 * MAT, *rho = ops + 7 * MAT;
+  const double2 *Rh = ops + 3 * MAT, *rho = ops + 7 * MAT;
   const double2* Hm = a.x + (size_t)s * MAT;
   double2* t = a.tmp + (size_t)s * 4 * MAT;
   double2 *c = t, *T1 = t + MAT, *Lm = t + 2 * MAT, *g = t + 3 * MAT;
@@ -334,9 +340,28 @@ __global__ void stationary_finish_kernel(StationaryArgs a) {
   herm = warp_sum(herm);
   if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = herm;
   __syncthreads();
+  // scale = max(1, 2|Q| + |R|^2) with Frobenius norms (bounds of the spectral norms of the reference)
+  double qn = 0.0, rn = 0.0;
+  for (int e = threadIdx.x; e < MAT; e += blockDim.x) {
+    qn += zabs2(a.ops[(size_t)s * a.ops_stride + e]);
+    rn += zabs2(a.ops[(size_t)s * a.ops_stride + 2 * MAT + e]);
+  }
+  qn = warp_sum(qn);
+  rn = warp_sum(rn);
+  __shared__ double red2[2][32];
+  if ((threadIdx.x & 31) == 0) {
+    red2[0][threadIdx.x >> 5] = qn;
+    red2[1][threadIdx.x >> 5] = rn;
+  }
+  __syncthreads();
   if (threadIdx.x == 0) {
-    double h = 0.0;
-    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) h += red[w];
+    double h = 0.0, q = 0.0, r = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+      h += red[w];
+      q += red2[0][w];
+      r += red2[1][w];
+    }
+    a.scale[s] = fmax(1.0, 2.0 * sqrt(q) + r);
     a.herm[s] = sqrt(h);
     if (!(sqrt(h) <= 100.0 * a.tolerance)) atomicExch(a.status + s, (int)kSolveFailure);
     if (!(den > 0.0) || !isfinite(den)) atomicExch(a.status + s, (int)kNonfiniteResult);

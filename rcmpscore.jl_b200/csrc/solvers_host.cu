@@ -1,0 +1,354 @@
+// Host orchestration of the batched GMRES solves: the boundary Poisson correction with the
+// metric solve (finish_gradient, numerics.py:103-126) and the stationary density
+// (stationary_state, numerics.py:74-100).
+#include <cuda_runtime.h>
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+#include "../../include/rcmps_b200.h"
+#include "context.h"
+#include "kinetic.h"
+#include "prep.h"
+#include "quartic.h"
+#include "solvers.h"
+#include "solvers_host.h"
+
+namespace rcmps {
+
+namespace {
+struct Layout {
+  size_t total = 0;
+  size_t add(size_t bytes) {
+    const size_t off = total;
+    total += align256(bytes);
+    return off;
+  }
+};
+constexpr int GCHROWS = 512;
+}  // namespace
+
+// Restarted GMRES(m) over NP problems that share dp; hp/d_probs hold set-up problems with x = 0.
+// Returns 0, or a CUDA error code. Convergence per problem is in hp[p].converged / residual.
+static cudaError_t gmres_run(ArnoldiProblem* hp, ArnoldiProblem* d_probs, int NP, int dp, int m, int maxrestart,
+                             LindbladTask* d_tasks, cudaStream_t stream) {
+  const int nvec = dp * dp;
+  cudaError_t e = cudaMemcpyAsync(d_probs, hp, NP * sizeof(ArnoldiProblem), cudaMemcpyHostToDevice, stream);
+  for (int it = 0; it <= maxrestart && !e; ++it) {
+    e = gmres_x_tasks_launch(d_probs, NP, d_tasks, stream);
+    if (!e) e = lindblad_launch(dp, d_tasks, NP, 0, stream);
+    if (!e) e = gmres_residual_launch(d_probs, NP, nvec, stream);
+    if (!e) e = cudaMemcpyAsync(hp, d_probs, NP * sizeof(ArnoldiProblem), cudaMemcpyDeviceToHost, stream);
+    if (!e) e = cudaStreamSynchronize(stream);
+    if (e) break;
+    bool all = true;
+    for (int p = 0; p < NP; ++p) all &= hp[p].converged != 0;
+    if (all || it == maxrestart) break;
+    for (int j = 0; j < m && !e; ++j) {
+      e = arnoldi_tasks_launch(d_probs, NP, j, d_tasks, stream);
+      if (!e) e = lindblad_launch(dp, d_tasks, NP, 0, stream);
+      if (!e) e = cgs_step_launch(d_probs, NP, j, nvec, stream);
+      if (!e) e = gmres_givens_launch(d_probs, NP, j, stream);
+    }
+    if (!e) e = gmres_update_launch(d_probs, NP, nvec, m, stream);
+  }
+  return e;
+}
+
+// Fill the GMRES fields of NP problems (dp, m) in the layout of slot `base`.
+struct GmresBuffers {
+  size_t o_probs, o_V, o_H, o_W, o_part, o_norms, o_x, o_g, o_cs, o_sn, o_flags, o_tasks;
+};
+static GmresBuffers gmres_layout(Layout& L, int NP, int dp, int m) {
+  const size_t mat = (size_t)dp * dp;
+  const int nchunk = (dp * dp + GCHROWS - 1) / GCHROWS;
+  GmresBuffers b;
+  b.o_probs = L.add(NP * sizeof(ArnoldiProblem));
+  b.o_V = L.add((size_t)NP * (m + 1) * mat * 16);
+  b.o_H = L.add((size_t)NP * (m + 1) * m * 16);
+  b.o_W = L.add((size_t)NP * mat * 16);
+  b.o_part = L.add((size_t)NP * nchunk * (m + 1) * 16);
+  b.o_norms = L.add((size_t)NP * 2 * nchunk * 8);
+  b.o_x = L.add((size_t)NP * mat * 16);
+  b.o_g = L.add((size_t)NP * (m + 1) * 16);
+  b.o_cs = L.add((size_t)NP * m * 16);
+  b.o_sn = L.add((size_t)NP * m * 16);
+  b.o_flags = L.add(NP * 4);
+  b.o_tasks = L.add(NP * sizeof(LindbladTask));
+  return b;
+}
+static void gmres_problem(ArnoldiProblem& A, char* base, const GmresBuffers& b, int p, int dp, int d, int m,
+                          double tol) {
+  const size_t mat = (size_t)dp * dp;
+  const int nchunk = (dp * dp + GCHROWS - 1) / GCHROWS;
+  std::memset(&A, 0, sizeof(A));
+  A.V = (double2*)(base + b.o_V) + (size_t)p * (m + 1) * mat;
+  A.ldv = (long long)mat;
+  A.H = (double2*)(base + b.o_H) + (size_t)p * (m + 1) * m;
+  A.W = (double2*)(base + b.o_W) + (size_t)p * mat;
+  A.partial = (double2*)(base + b.o_part) + (size_t)p * nchunk * (m + 1);
+  A.norms = (double*)(base + b.o_norms) + (size_t)p * 2 * nchunk;
+  A.x = (double2*)(base + b.o_x) + (size_t)p * mat;
+  A.g = (double2*)(base + b.o_g) + (size_t)p * (m + 1);
+  A.cs = (double2*)(base + b.o_cs) + (size_t)p * m;
+  A.sn = (double2*)(base + b.o_sn) + (size_t)p * m;
+  A.flag = (int*)(base + b.o_flags) + p;
+  A.n = dp * dp;
+  A.n_phys = d * d;
+  A.d = d;
+  A.dp = dp;
+  A.kmax = m;
+  A.kmax1 = m + 1;
+  A.target = std::min(m, d * d);
+  A.gtol = tol;
+  A.bnorm = -1.0;
+}
+
+int finish_run(rcmps_context* ctx, FinishJob& job, cudaStream_t stream) {
+  const rcmps_settings& S = job.settings;
+  const int m = 64, maxrestart = 200;
+  const double tol = S.boundary_tolerance;
+  if (!(tol > 0.0) || !(S.metric_reg >= 0.0)) return fail(ctx, RCMPS_INVALID_ARGUMENT, "invalid boundary controls");
+  std::vector<long long> off(job.n + 1, 0);
+  for (int i = 0; i < job.n; ++i) off[i + 1] = off[i] + (long long)job.dims[i] * job.dims[i];
+  std::map<int, std::vector<int>> groups;
+  for (int i = 0; i < job.n; ++i) groups[padded_dim(job.dims[i])].push_back(i);
+  rcmps_slot& SL = ctx->slot[job.slot];
+  for (auto& kv : groups) {
+    const int dp = kv.first;
+    const std::vector<int>& idx = kv.second;
+    const int n = (int)idx.size();
+    const size_t mat = (size_t)dp * dp;
+    Layout L;
+    const size_t o_dims = L.add(n * 4), o_off = L.add(n * 8);
+    const size_t o_in = L.add(5 * n * mat * 16), o_ops = L.add(n * 8 * mat * 16);
+    const size_t o_b = L.add(n * mat * 16), o_tmp = L.add(n * 4 * mat * 16), o_status = L.add(n * 4);
+    GmresBuffers gb = gmres_layout(L, n, dp, m);
+    cudaError_t e = arena_reserve(SL, L.total);
+    if (e) return fail(ctx, RCMPS_OUT_OF_MEMORY, "boundary workspace");
+    char* base = static_cast<char*>(SL.arena);
+    auto P = [&](size_t o) { return static_cast<void*>(base + o); };
+    Layout H;
+    const size_t h_dims = H.add(n * 4), h_off = H.add(n * 8), h_probs = H.add(n * sizeof(ArnoldiProblem)),
+                 h_status = H.add(n * 4);
+    if (pinned_reserve(SL, H.total)) return fail(ctx, RCMPS_CUDA_ERROR, "pinned host buffer");
+    char* h = static_cast<char*>(SL.pinned);
+    int* hd = (int*)(h + h_dims);
+    long long* ho = (long long*)(h + h_off);
+    ArnoldiProblem* hp = (ArnoldiProblem*)(h + h_probs);
+    int* hs = (int*)(h + h_status);
+    for (int i = 0; i < n; ++i) {
+      hd[i] = job.dims[idx[i]];
+      ho[i] = off[idx[i]];
+    }
+    double2* d_in = (double2*)P(o_in);
+    double* dR = (double*)d_in;
+    double* dK = (double*)(d_in + n * mat);
+    double* dP = (double*)(d_in + 2 * n * mat);
+    double* dC = (double*)(d_in + 3 * n * mat);
+    double* dE = (double*)(d_in + 4 * n * mat);
+    e = cudaMemcpyAsync(P(o_dims), hd, n * 4, cudaMemcpyHostToDevice, stream);
+    if (!e) e = cudaMemcpyAsync(P(o_off), ho, n * 8, cudaMemcpyHostToDevice, stream);
+    if (!e) e = cudaMemsetAsync(P(o_status), 0, n * 4, stream);
+    if (!e) e = cudaMemsetAsync(P(gb.o_x), 0, (size_t)n * mat * 16, stream);
+    if (!e) e = launch_pad(job.R, (long long*)P(o_off), (int*)P(o_dims), dR, dp, mat, n, stream);
+    if (!e) e = launch_pad(job.K, (long long*)P(o_off), (int*)P(o_dims), dK, dp, mat, n, stream);
+    if (!e) e = launch_pad(job.rho, (long long*)P(o_off), (int*)P(o_dims), dP, dp, mat, n, stream);
+    if (!e) e = launch_pad(job.covector, (long long*)P(o_off), (int*)P(o_dims), dC, dp, mat, n, stream);
+    if (!e) e = launch_pad(job.environment, (long long*)P(o_off), (int*)P(o_dims), dE, dp, mat, n, stream);
+    if (!e) e = launch_prepare(dR, dK, dP, (double*)P(o_ops), dp, mat, 8 * mat, n, stream);
+    FinishArgs fa;
+    fa.dp = dp;
+    fa.dims = (int*)P(o_dims);
+    fa.ops = (double2*)P(o_ops);
+    fa.ops_stride = (long long)(8 * mat);
+    fa.env = (double2*)dE;
+    fa.cov = (double2*)dC;
+    fa.b = (double2*)P(o_b);
+    fa.x = (double2*)P(gb.o_x);
+    fa.tmp = (double2*)P(o_tmp);
+    fa.metric_reg = S.metric_reg;
+    fa.status = (int*)P(o_status);
+    if (!e) e = boundary_rhs_launch(fa, n, stream);
+    if (e) return fail(ctx, RCMPS_CUDA_ERROR, std::string("boundary set-up: ") + cudaGetErrorString(e));
+    for (int i = 0; i < n; ++i) {
+      ArnoldiProblem& A = hp[i];
+      gmres_problem(A, base, gb, i, dp, hd[i], m, tol);
+      const double2* ops = (double2*)P(o_ops) + (size_t)i * 8 * mat;
+      A.A1 = ops + 1 * mat;   // L*: Q^dag X + X Q + R^dag X R
+      A.A1h = ops;
+      A.A2 = ops + 3 * mat;
+      A.A2h = ops + 2 * mat;
+      A.trw = ops + 7 * mat;  // + tr(rho X) I
+      A.b = fa.b + (size_t)i * mat;
+    }
+    e = gmres_run(hp, (ArnoldiProblem*)P(gb.o_probs), n, dp, m, maxrestart, (LindbladTask*)P(gb.o_tasks), stream);
+    if (e) return fail(ctx, RCMPS_CUDA_ERROR, std::string("boundary GMRES: ") + cudaGetErrorString(e));
+    if (!e) e = finish_launch(fa, n, stream);
+    if (!e) e = launch_unpad_acc((double*)(fa.tmp + 3 * mat), (long long)(4 * mat), dp, (long long*)P(o_off),
+                                 (int*)P(o_dims), job.gradient, n, false, stream);
+    if (!e) e = cudaMemcpyAsync(hs, P(o_status), n * 4, cudaMemcpyDeviceToHost, stream);
+    if (!e) e = cudaStreamSynchronize(stream);
+    if (e) return fail(ctx, RCMPS_CUDA_ERROR, std::string("finish: ") + cudaGetErrorString(e));
+    for (int i = 0; i < n; ++i) {
+      rcmps_state_stats& st = job.stats[idx[i]];
+      const ArnoldiProblem& A = hp[i];
+      st.gmres_iterations = A.iters;
+      st.boundary_residual = A.residual;
+      const bool ok = A.converged || A.residual <= 20.0 * tol * std::max(1.0, A.bnorm);
+      if (st.status) continue;
+      if (A.nonfinite || !std::isfinite(A.residual) || !ok) {
+        st.status = RCMPS_SOLVE_FAILURE;
+        st.failed_component = 4;
+      } else if (hs[i]) {
+        st.status = hs[i];
+        st.failed_component = 4;
+      }
+    }
+  }
+  for (int i = 0; i < job.n; ++i)
+    if (job.stats[i].status) return job.stats[i].status;
+  return RCMPS_OK;
+}
+
+int stationary_run(rcmps_context* ctx, StationaryJob& job, cudaStream_t stream) {
+  const int m = 64, maxrestart = 200;
+  const double tol = job.tolerance;
+  if (!(tol > 0.0)) return fail(ctx, RCMPS_INVALID_ARGUMENT, "stationary tolerance must be positive");
+  std::vector<long long> off(job.n + 1, 0);
+  for (int i = 0; i < job.n; ++i) off[i + 1] = off[i] + (long long)job.dims[i] * job.dims[i];
+  std::map<int, std::vector<int>> groups;
+  for (int i = 0; i < job.n; ++i) groups[padded_dim(job.dims[i])].push_back(i);
+  rcmps_slot& SL = ctx->slot[job.slot];
+  for (auto& kv : groups) {
+    const int dp = kv.first;
+    const std::vector<int>& idx = kv.second;
+    const int n = (int)idx.size();
+    const size_t mat = (size_t)dp * dp;
+    Layout L;
+    const size_t o_dims = L.add(n * 4), o_off = L.add(n * 8);
+    const size_t o_in = L.add(3 * n * mat * 16), o_ops = L.add(n * 8 * mat * 16);
+    const size_t o_b = L.add(n * mat * 16), o_trw = L.add(n * mat * 16), o_rho = L.add(n * mat * 16),
+                 o_tmp = L.add(n * mat * 16), o_lres = L.add((size_t)n * (dp / 16) * 8), o_herm = L.add(n * 16),
+                 o_status = L.add(n * 4), o_rt = L.add(n * sizeof(LindbladTask));
+    GmresBuffers gb = gmres_layout(L, n, dp, m);
+    cudaError_t e = arena_reserve(SL, L.total);
+    if (e) return fail(ctx, RCMPS_OUT_OF_MEMORY, "stationary workspace");
+    char* base = static_cast<char*>(SL.arena);
+    auto P = [&](size_t o) { return static_cast<void*>(base + o); };
+    Layout H;
+    const size_t h_dims = H.add(n * 4), h_off = H.add(n * 8), h_probs = H.add(n * sizeof(ArnoldiProblem)),
+                 h_status = H.add(n * 4), h_lres = H.add((size_t)n * (dp / 16) * 8), h_herm = H.add(n * 16),
+                 h_rt = H.add(n * sizeof(LindbladTask)), h_b = H.add(n * mat * 16);
+    if (pinned_reserve(SL, H.total)) return fail(ctx, RCMPS_CUDA_ERROR, "pinned host buffer");
+    char* h = static_cast<char*>(SL.pinned);
+    int* hd = (int*)(h + h_dims);
+    long long* ho = (long long*)(h + h_off);
+    ArnoldiProblem* hp = (ArnoldiProblem*)(h + h_probs);
+    int* hs = (int*)(h + h_status);
+    double* hl = (double*)(h + h_lres);
+    double* hh = (double*)(h + h_herm);
+    LindbladTask* hrt = (LindbladTask*)(h + h_rt);
+    double2* hb = (double2*)(h + h_b);
+    // b = I_d / d and the trace weights trw = I_d / d
+    std::memset(hb, 0, n * mat * 16);
+    for (int i = 0; i < n; ++i) {
+      hd[i] = job.dims[idx[i]];
+      ho[i] = off[idx[i]];
+      for (int q = 0; q < hd[i]; ++q) hb[(size_t)i * mat + (size_t)q * dp + q] = make_double2(1.0 / hd[i], 0.0);
+    }
+    double2* d_in = (double2*)P(o_in);
+    double* dR = (double*)d_in;
+    double* dK = (double*)(d_in + n * mat);
+    e = cudaMemcpyAsync(P(o_dims), hd, n * 4, cudaMemcpyHostToDevice, stream);
+    if (!e) e = cudaMemcpyAsync(P(o_off), ho, n * 8, cudaMemcpyHostToDevice, stream);
+    if (!e) e = cudaMemcpyAsync(P(o_b), hb, n * mat * 16, cudaMemcpyHostToDevice, stream);
+    if (!e) e = cudaMemcpyAsync(P(o_trw), hb, n * mat * 16, cudaMemcpyHostToDevice, stream);
+    if (!e) e = cudaMemsetAsync(P(o_status), 0, n * 4, stream);
+    if (!e) e = cudaMemsetAsync(P(gb.o_x), 0, (size_t)n * mat * 16, stream);
+    if (!e) e = cudaMemsetAsync(d_in + 2 * n * mat, 0, n * mat * 16, stream);   // rho placeholder
+    if (!e) e = launch_pad(job.R, (long long*)P(o_off), (int*)P(o_dims), dR, dp, mat, n, stream);
+    if (!e) e = launch_pad(job.K, (long long*)P(o_off), (int*)P(o_dims), dK, dp, mat, n, stream);
+    if (!e) e = launch_prepare(dR, dK, (double*)(d_in + 2 * n * mat), (double*)P(o_ops), dp, mat, 8 * mat, n, stream);
+    if (e) return fail(ctx, RCMPS_CUDA_ERROR, std::string("stationary set-up: ") + cudaGetErrorString(e));
+    for (int i = 0; i < n; ++i) {
+      ArnoldiProblem& A = hp[i];
+      gmres_problem(A, base, gb, i, dp, hd[i], m, tol);
+      const double2* ops = (double2*)P(o_ops) + (size_t)i * 8 * mat;
+      A.A1 = ops;             // L: Q X + X Q^dag + R X R^dag
+      A.A1h = ops + 1 * mat;
+      A.A2 = ops + 2 * mat;
+      A.A2h = ops + 3 * mat;
+      A.trw = (double2*)P(o_trw) + (size_t)i * mat;   // + tr(X)/d I
+      A.b = (double2*)P(o_b) + (size_t)i * mat;
+    }
+    e = gmres_run(hp, (ArnoldiProblem*)P(gb.o_probs), n, dp, m, maxrestart, (LindbladTask*)P(gb.o_tasks), stream);
+    if (e) return fail(ctx, RCMPS_CUDA_ERROR, std::string("stationary GMRES: ") + cudaGetErrorString(e));
+    StationaryArgs sa;
+    sa.dp = dp;
+    sa.dims = (int*)P(o_dims);
+    sa.x = (double2*)P(gb.o_x);
+    sa.rho = (double2*)P(o_rho);
+    sa.tmp = (double2*)P(o_tmp);
+    sa.herm = (double*)P(o_herm);
+    sa.scale = (double*)P(o_herm) + n;
+    sa.ops = (double2*)P(o_ops);
+    sa.ops_stride = (long long)(8 * mat);
+    sa.tolerance = tol;
+    sa.status = (int*)P(o_status);
+    e = stationary_finish_launch(sa, n, stream);
+    // |L(rho)|: the residual mode computes |X - shift L(X) - rhs|^2; with rhs = X and shift = 1 it
+    // is |L(rho)|^2.
+    for (int i = 0; i < n; ++i) {
+      const double2* ops = (double2*)P(o_ops) + (size_t)i * 8 * mat;
+      LindbladTask& t = hrt[i];
+      std::memset(&t, 0, sizeof(t));
+      t.X = sa.rho + (size_t)i * mat;
+      t.A1 = ops;
+      t.A1h = ops + mat;
+      t.A2 = ops + 2 * mat;
+      t.A2h = ops + 3 * mat;
+      t.rhs = t.X;
+      t.res = (double*)P(o_lres) + (size_t)i * (dp / 16);
+      t.shift = 1.0;
+      t.flag = (int*)P(gb.o_flags) + i;
+    }
+    if (!e) e = cudaMemcpyAsync(P(o_rt), hrt, n * sizeof(LindbladTask), cudaMemcpyHostToDevice, stream);
+    if (!e) e = lindblad_launch(dp, (LindbladTask*)P(o_rt), n, 1, stream);
+    if (!e) e = launch_unpad_acc((double*)P(o_rho), (long long)mat, dp, (long long*)P(o_off), (int*)P(o_dims),
+                                 job.rho, n, false, stream);
+    if (!e) e = cudaMemcpyAsync(hs, P(o_status), n * 4, cudaMemcpyDeviceToHost, stream);
+    if (!e) e = cudaMemcpyAsync(hl, P(o_lres), (size_t)n * (dp / 16) * 8, cudaMemcpyDeviceToHost, stream);
+    if (!e) e = cudaMemcpyAsync(hh, P(o_herm), n * 16, cudaMemcpyDeviceToHost, stream);
+    if (!e) e = cudaStreamSynchronize(stream);
+    if (e) return fail(ctx, RCMPS_CUDA_ERROR, std::string("stationary finish: ") + cudaGetErrorString(e));
+    for (int i = 0; i < n; ++i) {
+      rcmps_state_stats& st = job.stats[idx[i]];
+      const ArnoldiProblem& A = hp[i];
+      double l2 = 0.0;
+      for (int r = 0; r < dp / 16; ++r) l2 += hl[(size_t)i * (dp / 16) + r];
+      st.gmres_iterations = A.iters;
+      st.boundary_residual = std::sqrt(l2);   // |L(rho)|
+      const double scale = hh[n + i];
+      if (st.status) continue;
+      const bool ok = A.converged || A.residual <= 20.0 * tol * std::max(1.0, A.bnorm);
+      if (!ok || A.nonfinite) {
+        st.status = RCMPS_SOLVE_FAILURE;
+        st.failed_component = 5;
+      } else if (hs[i]) {
+        st.status = hs[i];
+        st.failed_component = 5;
+      } else if (!(std::sqrt(l2) <= tol * scale)) {
+        st.status = RCMPS_SOLVE_FAILURE;
+        st.failed_component = 5;
+      }
+    }
+  }
+  for (int i = 0; i < job.n; ++i)
+    if (job.stats[i].status) return job.stats[i].status;
+  return RCMPS_OK;
+}
+
+}  // namespace rcmps

@@ -1,0 +1,33 @@
+// Boundary/finish and stationary orchestration (internal).
+#pragma once
+#include <cuda_runtime.h>
+#include "../../include/rcmps_b200.h"
+#include "context.h"
+
+namespace rcmps {
+
+struct FinishJob {
+  int n = 0;
+  const int* dims = nullptr;                  // host
+  const double *R = nullptr, *K = nullptr, *rho = nullptr;   // device, packed
+  const double *covector = nullptr, *environment = nullptr;  // device, packed
+  rcmps_settings settings{};
+  double* gradient = nullptr;                 // device, packed
+  rcmps_state_stats* stats = nullptr;         // host [n]
+  int slot = 2;
+};
+
+struct StationaryJob {
+  int n = 0;
+  const int* dims = nullptr;
+  const double *R = nullptr, *K = nullptr;    // device, packed
+  double tolerance = 1e-11;
+  double* rho = nullptr;                      // device, packed
+  rcmps_state_stats* stats = nullptr;
+  int slot = 2;
+};
+
+int finish_run(rcmps_context* ctx, FinishJob& job, cudaStream_t stream);
+int stationary_run(rcmps_context* ctx, StationaryJob& job, cudaStream_t stream);
+
+}  // namespace rcmps
