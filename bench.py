@@ -1,0 +1,343 @@
+"""Benchmark: fg_phi4 evaluations per second (energy + finished gradient) on B200.
+
+Workload (default): 32 states at D = 64 — 16 random + 16 Z2-symmetric (i.i.d. standard complex
+Gaussian entries times 0.2, NumPy PCG64 seeds), g = 2 — at the reference optimizer's settings
+(W = 30, n_quad = 512, atol/rtol 1e-13/1e-12, 512 kinetic nodes, Krylov 1e-12, metric_reg 1e-3).
+A step is one batched fg_phi4 call over all states; rho is computed once (untimed) by the
+library's stationary solve. Inputs and workspaces (about 30 GB) exceed the 126 MB L2.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+With N > 1 (torchrun, one rank per GPU) every rank evaluates its own shard of states: no data-path
+collective (weak scaling); the elapsed time is the maximum over ranks. --impl reference times the
+CPU oracle (the NumPy restatement of the reference's path) on all host cores, rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path[:0] = [str(ROOT), str(ROOT / "rcmpscore.jl_b200")]
+
+import numpy as np  # noqa: E402
+
+METRIC = "fg_phi4 evals/s at D=64 (energy + finished gradient), FP64"
+FLOPS_PER_RHS_D3 = 224      # 28 complex D^3 products (8 flops per complex multiply-add) per right-hand side
+
+
+# ----------------------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi samples (200 ms) of SM clock and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ----------------------------------------------------------------------------- CPU oracle sample
+def _cpu_sample(args):
+    """Bounded sample of one state's fg_phi4 on one core with the oracle: `n_rhs` right-hand sides of
+    the quartic system, `n_nodes` pullback nodes and the full kinetic term, scaled to one evaluation
+    by the step/node counts of the same state on the GPU (rhs_calls, 1024 nodes). The boundary and
+    metric solve (under 1% of the reference's CPU time at D = 64) is not sampled."""
+    d, seed, z2, g, rhs_calls, n_rhs, n_nodes = args
+    os.environ.setdefault("OPENBLAS_NUM_THREADS", "1")
+    sys.path[:0] = [str(ROOT), str(ROOT / "rcmpscore.jl_b200")]
+    from oracle import fg_phi4_oracle as O
+    from rcmps_b200.batch import random_state, z2_state
+    R, K = (z2_state if z2 else random_state)(d, seed)
+    Q = O.left_canonical_q(R, K)
+    rho = O.stationary_state(Q, R) if d <= 32 else np.eye(d, dtype=complex) / d
+    system = O.QuarticSystem(Q, R, rho)
+    rng = np.random.default_rng(1)
+    y = (rng.standard_normal(system.size) + 1j * rng.standard_normal(system.size)) * 1e-3
+    t0 = time.perf_counter()
+    for i in range(n_rhs):
+        system(-2.0 + 0.01 * i, y)
+    t_rhs = (time.perf_counter() - t0) / n_rhs
+    samples = np.tile(y, (2 * n_nodes + 1, 1))
+    pts, wts = O.quadrature(30.0, n_nodes)
+    t0 = time.perf_counter()
+    O.quartic_pullback(system, samples, pts, wts)
+    t_node = (time.perf_counter() - t0) / (2 * n_nodes)
+    t0 = time.perf_counter()
+    O.kinetic_raw(Q, R, rho, 512)
+    t_kin = time.perf_counter() - t0
+    return rhs_calls * t_rhs + 1024 * t_node + t_kin, dict(t_rhs=t_rhs, t_node=t_node, t_kinetic=t_kin)
+
+
+def cpu_sample_plan(dims, rhs_calls):
+    return [(dims[i], i if i < 16 else 100 + (i - 16), i >= 16, 2.0, int(rhs_calls[i]), 24, 8) for i in range(len(dims))]
+
+
+# ----------------------------------------------------------------------------- reference arm
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    import multiprocessing as mp
+    cores = os.cpu_count() or 1
+    from rcmps_b200.batch import config_states
+    R, K, g, desc = config_states("d64_mixed")
+    dims = [len(r) for r in R]
+    # step counts of these states (measured on B200 by the b200 arm; a typical count if absent)
+    rhs = [6800] * len(dims)
+    plan = cpu_sample_plan(dims, rhs)
+    workers = min(cores, len(plan))
+    ctx = mp.get_context("spawn")
+    times = []
+    with ctx.Pool(workers) as pool:
+        for step in range(args.warmup + args.steps):
+            t0 = time.perf_counter()
+            res = pool.map(_cpu_sample, plan[:workers])
+            wall = time.perf_counter() - t0
+            if step >= args.warmup:
+                times.append((wall, [r[0] for r in res]))
+    # evals/s on all cores: each worker produced one (scaled) evaluation per estimated eval time
+    per_eval = [statistics.mean(t for _, ts in times for t in ts)]
+    value = workers / per_eval[0]
+    sample = (f"per worker one D=64 state: 24 quartic right-hand sides, 16 pullback nodes and the full kinetic term "
+              f"timed with the oracle, scaled to one evaluation with 6800 right-hand sides and 1024 nodes; "
+              f"{workers} workers")
+    line = {"metric": METRIC, "value": value, "unit": "evals/s", "impl": "reference", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * statistics.mean(w for w, _ in times),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": desc, "half_window": 30.0, "n_quad": 512, "kinetic_nodes": 512},
+            "cpu_baseline": {"value": value, "unit": "evals/s", "cores": workers, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": "evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ----------------------------------------------------------------------------- B200 arm
+def run_b200(args, rank, world, local_rank):
+    import torch
+    from rcmps_b200 import _lib
+    from rcmps_b200.batch import config_states, shard
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+    ctx = _lib.Context(local_rank)
+    lib = ctx.lib
+    R, K, g, desc = config_states(args.workload)
+    dims_all = [len(r) for r in R]
+    mine = shard(dims_all, rank, world)
+    R = [R[i] for i in mine]
+    K = [K[i] for i in mine]
+    g = [g[i] for i in mine]
+    dims = [len(r) for r in R]
+    n = len(dims)
+    total = sum(d * d for d in dims)
+    s = _lib.default_settings()
+    cdims = (C.c_int * n)(*dims)
+    cg = (C.c_double * n)(*g)
+    pack = lambda L: torch.from_numpy(np.concatenate([np.ascontiguousarray(x).ravel() for x in L])).cuda()
+    dR, dK = pack(R), pack(K)
+    drho = torch.zeros_like(dR)
+    stats = (_lib.StateStats * n)()
+    torch.cuda.synchronize()
+    rc = lib.rcmps_stationary_state_batch(ctx.handle, n, cdims, dR.data_ptr(), dK.data_ptr(), C.c_double(1e-13),
+                                          drho.data_ptr(), stats, None)
+    if rc:
+        raise RuntimeError(f"stationary states failed: {ctx.error()}")
+    energy = torch.zeros(n, dtype=torch.float64, device="cuda")
+    grad = torch.zeros(total, dtype=torch.complex128, device="cuda")
+    stream = torch.cuda.current_stream()
+    sptr = C.c_void_p(stream.cuda_stream)
+
+    def step():
+        rc = lib.rcmps_fg_phi4_batch(ctx.handle, n, cdims, cg, dR.data_ptr(), dK.data_ptr(), drho.data_ptr(),
+                                     C.byref(s), energy.data_ptr(), grad.data_ptr(), None, None, stats, sptr)
+        if rc:
+            raise RuntimeError(f"fg_phi4 failed: {_lib.STATUS_NAMES.get(rc)} {ctx.error()}")
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(args.warmup):
+        step()
+    traj_ms, pull_ms, kin_ms, fin_ms = [], [], [], []
+    barrier()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches0 = lib.rcmps_launch_count()
+    with ClockSampler(local_rank) as clocks:
+        start.record(stream)
+        for _ in range(args.steps):
+            step()
+            t = ctx.timings()
+            traj_ms.append(t[0])
+            pull_ms.append(t[1])
+            kin_ms.append(t[2])
+            fin_ms.append(t[3])
+        end.record(stream)
+        barrier()
+    launches = (lib.rcmps_launch_count() - launches0) // args.steps
+    elapsed = start.elapsed_time(end)
+    if dist is not None:
+        t = torch.tensor([elapsed], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed = float(t.item())
+    total_states = len(dims_all)
+    value = total_states * args.steps / (elapsed / 1000.0)
+    rhs_calls = [stats[i].rhs_calls for i in range(n)]
+    # roofline of the dominant kernel: the trajectory (FP64 tensor cores, mma.sync m16n8k8)
+    flops = sum(FLOPS_PER_RHS_D3 * rhs_calls[i] * dims[i] ** 3 for i in range(n))
+    traj = statistics.mean(traj_ms)
+    achieved = flops / (traj / 1000.0) / 1e12
+    peak = lib.rcmps_fp64_peak_tflops(ctx.handle)
+    traffic = None
+    tf = ROOT / "profiles" / "trajectory_traffic.json"
+    if tf.exists():
+        try:
+            rec = json.loads(tf.read_text())
+            if rec.get("workload") == args.workload:
+                traffic = rec.get("dram_bytes_per_launch")
+        except (OSError, ValueError):
+            traffic = None
+
+    # end to end through the host-buffer C entry: copies of inputs and results inside the timed region
+    e2e = None
+    if True:
+        hR = torch.from_numpy(np.concatenate([x.ravel() for x in R])).pin_memory()
+        hK = torch.from_numpy(np.concatenate([x.ravel() for x in K])).pin_memory()
+        hP = drho.cpu().pin_memory()
+        hE = torch.zeros(n, dtype=torch.float64).pin_memory()
+        hG = torch.zeros(total, dtype=torch.complex128).pin_memory()
+        e2e_steps = max(1, min(args.steps, 2))
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(e2e_steps):
+            rc = lib.rcmps_fg_phi4_batch_host(ctx.handle, n, cdims, cg, hR.data_ptr(), hK.data_ptr(), hP.data_ptr(),
+                                              C.byref(s), hE.data_ptr(), hG.data_ptr(), None, None, stats)
+            if rc:
+                raise RuntimeError(f"fg_phi4 (host buffers) failed: {ctx.error()}")
+        barrier()
+        wall = time.perf_counter() - t0
+        if dist is not None:
+            t = torch.tensor([wall], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            wall = float(t.item())
+        e2e = {"value": total_states * e2e_steps / wall, "unit": "evals/s",
+               "h2d_bytes_per_step": 3 * total * 16 * world, "d2h_bytes_per_step": (n * 8 + total * 16) * world}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        t_eval, parts = _cpu_sample(cpu_sample_plan(dims, rhs_calls)[0])
+        cpu = {"value": 1.0 / t_eval, "unit": "evals/s", "cores": 1, "kind": "port",
+               "sample": (f"state 0 (D={dims[0]}): 24 quartic right-hand sides, 16 pullback nodes and the full kinetic "
+                          f"term timed with the oracle on one core, scaled to its {rhs_calls[0]} right-hand sides "
+                          f"and 1024 nodes (t_rhs {parts['t_rhs'] * 1e3:.2f} ms, t_node {parts['t_node'] * 1e3:.2f} ms, "
+                          f"t_kinetic {parts['t_kinetic']:.2f} s)")}
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "evals/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": elapsed / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": desc, "states_per_gpu": n, "half_window": 30.0, "n_quad": 512,
+                           "kinetic_nodes": 512, "atol": 1e-13, "rtol": 1e-12, "krylov_tolerance": 1e-12,
+                           "l2": "inputs and workspaces exceed L2 (126 MB); no flush needed", "parallelism":
+                           f"state shards over {world} GPU(s)"},
+                "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                             "frac": achieved / peak if peak else None, "traffic": traffic,
+                             "kernel": "trajectory_kernel<64> (FP64 mma.sync m16n8k8)",
+                             "peak_source": "FP64 mma.sync throughput measured in this run (rcmps_fp64_peak_tflops)",
+                             "flops_per_launch": flops, "launch_ms": traj},
+                "phases_ms": {"trajectory": traj, "pullback": statistics.mean(pull_ms),
+                              "kinetic": statistics.mean(kin_ms), "boundary_finish": statistics.mean(fin_ms)},
+                "steps_per_state": {"rhs_calls_mean": statistics.mean(rhs_calls), "accepted_mean":
+                                    statistics.mean(stats[i].accepted for i in range(n))},
+                "gpu_launches": None, "gpu_launches_note": "library kernel launches per step (rcmps_launch_count)", "clocks": clocks.summary(), "e2e": e2e, "cpu_baseline": cpu}
+        line["gpu_launches"] = launches
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    p = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=3)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=("b200", "reference"), default="b200")
+    p.add_argument("--workload", default="d64_mixed")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    args = p.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    try:
+        run_b200(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -143,6 +143,10 @@ int rcmps_stationary_state_batch(rcmps_context* context, int n_states, const int
                                  const double* K, double tolerance, double* rho, rcmps_state_stats* stats,
                                  void* stream);
 
+/* Number of kernel launches this library has issued in the process (all contexts). No
+ * counterpart in the reference. */
+long long rcmps_launch_count(void);
+
 /* FP64 tensor-core throughput of this device (TFLOP/s), measured by a short in-register
  * mma.sync loop: the denominator of the FP64 roofline. No counterpart in the reference. */
 double rcmps_fp64_peak_tflops(rcmps_context* context);

@@ -5,6 +5,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <atomic>
 #include <map>
 #include <string>
 #include <thread>
@@ -19,6 +20,9 @@
 #include "trajectory.h"
 
 namespace rcmps {
+
+static std::atomic<long long> g_launches{0};
+void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
 cudaError_t arena_reserve(rcmps_slot& sl, size_t bytes) {
   if (bytes <= sl.arena_bytes) return cudaSuccess;
@@ -509,6 +513,7 @@ int rcmps_fg_phi4_batch(rcmps_context* ctx, int n, const int* dims, const double
   if (qrc || krc) return qrc ? qrc : krc;
   cudaStream_t s2 = ctx->slot[2].stream;
   cudaEventRecord(ctx->slot[2].ev[1], s2);
+  note_launch();
   sum_parts_kernel<<<(int)std::min<long long>(4096, (total + 255) / 256 + 1), 256, 0, s2>>>(
       n, total, vq, vk, (double2*)cq, (double2*)ck, (double2*)eq, (double2*)ek, energy, (double2*)csum,
       (double2*)esum);
@@ -600,6 +605,8 @@ long long rcmps_workspace_bytes(const rcmps_context* ctx, int n, const int* dims
   return total;
 }
 
+long long rcmps_launch_count(void) { return g_launches.load(); }
+
 double rcmps_fp64_peak_tflops(rcmps_context* ctx) {
   if (!ctx) return 0.0;
   cudaSetDevice(ctx->device);
@@ -607,8 +614,10 @@ double rcmps_fp64_peak_tflops(rcmps_context* ctx) {
   double* out = nullptr;
   if (cudaMalloc(&out, (size_t)blocks * threads * 8)) return 0.0;
   cudaStream_t s = ctx->slot[0].stream;
+  note_launch();
   fp64_peak_kernel<<<blocks, threads, 0, s>>>(out, iters);   // warm-up
   cudaEventRecord(ctx->slot[0].ev[0], s);
+  note_launch();
   fp64_peak_kernel<<<blocks, threads, 0, s>>>(out, iters);
   cudaEventRecord(ctx->slot[0].ev[1], s);
   cudaEventSynchronize(ctx->slot[0].ev[1]);

@@ -15,6 +15,9 @@
 
 namespace rcmps {
 
+// Kernel launches issued by the library in this process (every launch site calls note_launch).
+void note_launch();
+
 // ------------------------------------------------------------------ status codes
 // The numbers of the reference's device controller (device_control_backend.py:23-27 of
 // rcmps_gpu) plus the wait limit of this build.

@@ -842,6 +842,7 @@ static cudaError_t launch_l(const LindbladTask* tasks, int ntasks, int mode, cud
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)LG::SMEM);
   if (e != cudaSuccess) return e;
   if (ntasks == 0) return cudaSuccess;
+  note_launch();
   k<<<ntasks * (DP / 16), LG::NT, LG::SMEM, s>>>(tasks, ntasks, mode);
   return cudaGetLastError();
 }
@@ -860,11 +861,13 @@ cudaError_t lindblad_launch(int dp, const LindbladTask* d_tasks, int ntasks, int
 
 cudaError_t arnoldi_tasks_launch(const ArnoldiProblem* d_probs, int nprob, int j, LindbladTask* d_tasks,
                                 cudaStream_t s) {
+  note_launch();
   arnoldi_tasks<<<(nprob + 127) / 128, 128, 0, s>>>(d_probs, nprob, j, d_tasks);
   return cudaGetLastError();
 }
 
 cudaError_t arnoldi_start_launch(ArnoldiProblem* d_probs, int nprob, cudaStream_t s) {
+  note_launch();
   arnoldi_start<<<nprob, 256, 0, s>>>(d_probs, nprob);
   return cudaGetLastError();
 }
@@ -874,9 +877,12 @@ cudaError_t cgs_step_launch(ArnoldiProblem* d_probs, int nprob, int j, int n, cu
   dim3 grid(nchunk, nprob);
   const size_t hbytes = (size_t)(j + 1) * sizeof(double2);
   for (int pass = 0; pass < 2; ++pass) {
+    note_launch();
     cgs_partial<<<grid, 256, 0, s>>>(d_probs, nprob, j, nchunk, pass);
+    note_launch();
     cgs_subtract<<<grid, 256, hbytes, s>>>(d_probs, nprob, j, nchunk, pass);
   }
+  note_launch();
   cgs_finish<<<grid, 256, 0, s>>>(d_probs, nprob, j, nchunk);
   return cudaGetLastError();
 }
@@ -884,9 +890,18 @@ cudaError_t cgs_step_launch(ArnoldiProblem* d_probs, int nprob, int j, int n, cu
 cudaError_t hessenberg_launch(ArnoldiProblem* d_probs, int nprob, const double* d_shifts, int nshift,
                               double2* scratch, long long slot_elems, int nslots, int kmax, cudaStream_t s) {
   const int blocks = (nslots * 32 + 255) / 256;
-  if (kmax <= 256) hessenberg_solve<8><<<blocks, 256, 0, s>>>(d_probs, nprob, d_shifts, nshift, scratch, slot_elems, nslots);
-  else if (kmax <= 512) hessenberg_solve<16><<<blocks, 256, 0, s>>>(d_probs, nprob, d_shifts, nshift, scratch, slot_elems, nslots);
-  else hessenberg_solve<32><<<blocks, 256, 0, s>>>(d_probs, nprob, d_shifts, nshift, scratch, slot_elems, nslots);
+  if (kmax <= 256) {
+    note_launch();
+    hessenberg_solve<8><<<blocks, 256, 0, s>>>(d_probs, nprob, d_shifts, nshift, scratch, slot_elems, nslots);
+  }
+  else if (kmax <= 512) {
+    note_launch();
+    hessenberg_solve<16><<<blocks, 256, 0, s>>>(d_probs, nprob, d_shifts, nshift, scratch, slot_elems, nslots);
+  }
+  else {
+    note_launch();
+    hessenberg_solve<32><<<blocks, 256, 0, s>>>(d_probs, nprob, d_shifts, nshift, scratch, slot_elems, nslots);
+  }
   return cudaGetLastError();
 }
 
@@ -895,17 +910,20 @@ cudaError_t reconstruct_launch(ArnoldiProblem* d_probs, int nprob, int nshift, i
   const int smem = (2 * 64 * 20 + 2 * 16 * 64) * 16;
   cudaError_t e = cudaFuncSetAttribute(reconstruct_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   if (e != cudaSuccess) return e;
+  note_launch();
   reconstruct_kernel<<<grid, 256, smem, s>>>(d_probs, nprob, nshift);
   return cudaGetLastError();
 }
 
 cudaError_t residual_reduce_launch(ArnoldiProblem* d_probs, int nprob, const double* d_res, int nshift, int rbs,
                                    cudaStream_t s) {
+  note_launch();
   residual_reduce<<<nprob, 256, 0, s>>>(d_probs, nprob, d_res, nshift, rbs);
   return cudaGetLastError();
 }
 
 cudaError_t kinetic_rhs_launch(const KineticSetup& a, int nstates, cudaStream_t s) {
+  note_launch();
   kinetic_rhs_kernel<<<nstates, 256, 0, s>>>(a);
   return cudaGetLastError();
 }
@@ -917,6 +935,7 @@ static cudaError_t launch_c(const ContractArgs& a, int nblk, cudaStream_t s) {
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CG::SMEM);
   if (e != cudaSuccess) return e;
   dim3 grid(nblk, 2 * a.nstates * CG::NRB);
+  note_launch();
   k<<<grid, CG::NT, CG::SMEM, s>>>(a);
   return cudaGetLastError();
 }
@@ -933,6 +952,7 @@ cudaError_t contract_launch(const ContractArgs& a, int nblk, cudaStream_t s) {
     default: return cudaErrorInvalidValue;
   }
   if (e != cudaSuccess) return e;
+  note_launch();
   contract_finalize<<<a.nstates, 256, 0, s>>>(a, nblk);
   return cudaGetLastError();
 }

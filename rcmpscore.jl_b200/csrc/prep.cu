@@ -75,6 +75,7 @@ cudaError_t launch_pad(const double* src, const long long* d_src_off, const int*
                        long long stride, int nstates, cudaStream_t stream) {
   if (nstates == 0) return cudaSuccess;
   dim3 grid((dp * dp + 255) / 256, nstates);
+  note_launch();
   pad_kernel<<<grid, 256, 0, stream>>>(reinterpret_cast<const double2*>(src), d_src_off, d_dims,
                                        reinterpret_cast<double2*>(dst), dp, stride);
   return cudaGetLastError();
@@ -84,6 +85,7 @@ cudaError_t launch_unpad(const double* src, long long stride, int dp, const long
                          const int* d_dims, double* dst, int nstates, cudaStream_t stream) {
   if (nstates == 0) return cudaSuccess;
   dim3 grid((dp * dp + 255) / 256, nstates);
+  note_launch();
   unpad_kernel<<<grid, 256, 0, stream>>>(reinterpret_cast<const double2*>(src), stride, dp, d_dst_off, d_dims,
                                          reinterpret_cast<double2*>(dst));
   return cudaGetLastError();
@@ -127,6 +129,7 @@ cudaError_t launch_unpad_acc(const double* src, long long stride, int dp, const 
                              const int* d_dims, double* dst, int nstates, bool accumulate, cudaStream_t stream) {
   if (nstates == 0) return cudaSuccess;
   dim3 grid((dp * dp + 255) / 256, nstates);
+  note_launch();
   unpad_acc_kernel<<<grid, 256, 0, stream>>>(reinterpret_cast<const double2*>(src), stride, dp, d_dst_off, d_dims,
                                              reinterpret_cast<double2*>(dst), accumulate ? 1 : 0);
   return cudaGetLastError();
@@ -135,12 +138,14 @@ cudaError_t launch_unpad_acc(const double* src, long long stride, int dp, const 
 cudaError_t launch_scatter_values(const double* src, int n, const int* d_idx, double* dst, bool accumulate,
                                   cudaStream_t stream) {
   if (n == 0) return cudaSuccess;
+  note_launch();
   scatter_values_kernel<<<(n + 255) / 256, 256, 0, stream>>>(src, n, d_idx, dst, accumulate ? 1 : 0);
   return cudaGetLastError();
 }
 
 cudaError_t launch_export_samples(const double2* samples, int dp, int d, int npoints, const double* value,
                                   double* out, cudaStream_t stream) {
+  note_launch();
   export_samples_kernel<<<1024, 256, 0, stream>>>(samples, dp, d, npoints, value, reinterpret_cast<double2*>(out));
   return cudaGetLastError();
 }
@@ -148,6 +153,7 @@ cudaError_t launch_export_samples(const double2* samples, int dp, int d, int npo
 cudaError_t launch_prepare(const double* R, const double* K, const double* rho, double* ops, int dp,
                            long long in_stride, long long ops_stride, int nstates, cudaStream_t stream) {
   if (nstates == 0) return cudaSuccess;
+  note_launch();
   prepare_kernel<<<nstates, 256, 0, stream>>>(reinterpret_cast<const double2*>(R),
                                               reinterpret_cast<const double2*>(K),
                                               reinterpret_cast<const double2*>(rho),

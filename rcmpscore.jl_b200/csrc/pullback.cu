@@ -252,6 +252,7 @@ static cudaError_t launch_pb(const PullbackArgs& a, int nblk, cudaStream_t s) {
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PG::SMEM);
   if (e != cudaSuccess) return e;
   dim3 grid(nblk, a.nstates * PG::NRB);
+  note_launch();
   k<<<grid, PG::NT, PG::SMEM, s>>>(a);
   return cudaGetLastError();
 }
@@ -292,6 +293,7 @@ cudaError_t pullback_launch(const PullbackArgs& a, int nblk, cudaStream_t s) {
     default: return cudaErrorInvalidValue;
   }
   if (e != cudaSuccess) return e;
+  note_launch();
   pullback_finalize<<<a.nstates, 256, 0, s>>>(a, nblk);
   return cudaGetLastError();
 }

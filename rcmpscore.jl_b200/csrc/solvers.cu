@@ -174,20 +174,25 @@ __global__ void gmres_x_tasks(const ArnoldiProblem* __restrict__ probs, int npro
 
 cudaError_t gmres_residual_launch(ArnoldiProblem* d, int nprob, int n, cudaStream_t s) {
   const int nchunk = (n + GCH - 1) / GCH;
+  note_launch();
   gmres_residual<<<dim3(nchunk, nprob), 256, 0, s>>>(d, nprob, nchunk);
+  note_launch();
   gmres_start<<<dim3(nchunk, nprob), 256, 0, s>>>(d, nprob, nchunk);
   return cudaGetLastError();
 }
 cudaError_t gmres_givens_launch(ArnoldiProblem* d, int nprob, int j, cudaStream_t s) {
+  note_launch();
   gmres_givens<<<(nprob + 127) / 128, 128, 0, s>>>(d, nprob, j);
   return cudaGetLastError();
 }
 cudaError_t gmres_update_launch(ArnoldiProblem* d, int nprob, int n, int kmax, cudaStream_t s) {
   const int nchunk = (n + GCH - 1) / GCH;
+  note_launch();
   gmres_update<<<dim3(nchunk, nprob), 256, (size_t)kmax * sizeof(double2), s>>>(d, nprob, nchunk);
   return cudaGetLastError();
 }
 cudaError_t gmres_x_tasks_launch(const ArnoldiProblem* d, int nprob, LindbladTask* tasks, cudaStream_t s) {
+  note_launch();
   gmres_x_tasks<<<(nprob + 127) / 128, 128, 0, s>>>(d, nprob, tasks);
   return cudaGetLastError();
 }
@@ -380,14 +385,17 @@ __global__ void stationary_finish_kernel(StationaryArgs a) {
 }
 
 cudaError_t boundary_rhs_launch(const FinishArgs& a, int n, cudaStream_t s) {
+  note_launch();
   boundary_rhs_kernel<<<n, 256, 0, s>>>(a);
   return cudaGetLastError();
 }
 cudaError_t finish_launch(const FinishArgs& a, int n, cudaStream_t s) {
+  note_launch();
   finish_kernel<<<n, 256, 0, s>>>(a);
   return cudaGetLastError();
 }
 cudaError_t stationary_finish_launch(const StationaryArgs& a, int n, cudaStream_t s) {
+  note_launch();
   stationary_finish_kernel<<<n, 256, 0, s>>>(a);
   return cudaGetLastError();
 }

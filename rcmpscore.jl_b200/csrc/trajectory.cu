@@ -721,6 +721,7 @@ static cudaError_t launch_dp(const TrajState* d_states, int nstates, const doubl
   attr[0].val.clusterDim.z = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
+  note_launch();
   return cudaLaunchKernelEx(&cfg, kern, d_states, d_points, npoints, ctl);
 }
 
@@ -735,6 +736,7 @@ __global__ void node_weights_kernel(const double* points, const double* weights,
 
 cudaError_t node_weights_launch(const double* d_points, const double* d_weights, int n, double* d_wj,
                                 cudaStream_t stream) {
+  note_launch();
   node_weights_kernel<<<(n + 255) / 256, 256, 0, stream>>>(d_points, d_weights, n, d_wj);
   return cudaGetLastError();
 }

@@ -74,6 +74,7 @@ SIGNATURES = {
                                          C.POINTER(StateStats), _P]),
     "rcmps_stationary_state_batch": (_I, [_P, _I, C.POINTER(_I), _P, _P, _D, _P, C.POINTER(StateStats), _P]),
     "rcmps_fp64_peak_tflops": (_D, [_P]),
+    "rcmps_launch_count": (C.c_longlong, []),
 }
 
 _lib = None

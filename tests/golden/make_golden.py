@@ -1,0 +1,105 @@
+"""Generate the golden vectors of tests/golden/ by running RcmpsCore.jl's own NumPy path.
+
+This script imports the reference package rcmps_gpu read-only from a local checkout
+(default /root/reference/gpu/src; override with RCMPS_REFERENCE_SRC) and writes .npz files:
+  small.npz     D = 4, 6, 8 random and D = 8 Z2 states at W = 30, n_quad = 64, 128 kinetic nodes
+  d16.npz       one D = 16 random state at the optimizer defaults (W = 30, n_quad = 512, 512 nodes)
+  d64.npz       the seed-42 D = 64 random state at the optimizer defaults
+  samples_d5.npz  trajectory samples of the reduced quartic system, D = 5, W = 2, n_quad = 16
+Each state record holds R, K, rho (the reference's stationary_state at tolerance 1e-13), the
+coupling, the settings, and the reference outputs: quartic value/covector/environment and its
+DOP853 step counts, kinetic value/covector/environment, the summed energy and the finished
+gradient (finish_gradient, metric_reg 1e-3). The copied Julia fixture phi4_g2_D16_z2_portable/
+is the reference's test/fixtures/phi4_g2_D16_z2_portable (exported by RcmpsCore 0.2.0).
+
+States: NumPy PCG64 default_rng(seed); R and A with i.i.d. standard complex Gaussian entries
+times 0.2 (R drawn first), K = (A + A^dag)/2; Z2 states draw blocks in the order k1, k2, R12, R21.
+Run: python tests/golden/make_golden.py  (about a minute; the D = 64 record dominates)
+"""
+from __future__ import annotations
+
+import math
+import os
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+sys.path.insert(0, os.environ.get("RCMPS_REFERENCE_SRC", "/root/reference/gpu/src"))
+from rcmps_gpu.optimizer.runtime import kinetic_backend as kb  # noqa: E402
+from rcmps_gpu.optimizer.runtime import numerics as nm  # noqa: E402
+from rcmps_gpu.optimizer.runtime import ode_backend as ob  # noqa: E402
+
+
+def draw(rng, n):
+    return (rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))) / math.sqrt(2.0)
+
+
+def random_state(d, seed, scale=0.2):
+    rng = np.random.default_rng(seed)
+    r = scale * draw(rng, d)
+    a = scale * draw(rng, d)
+    return r, (a + a.conj().T) / 2
+
+
+def z2_state(d, seed, scale=0.2):
+    n = d // 2
+    rng = np.random.default_rng(seed)
+    z = np.zeros((n, n), complex)
+    k1, k2 = draw(rng, n), draw(rng, n)
+    r = scale * np.block([[z, draw(rng, n)], [draw(rng, n), z]])
+    k = scale * np.block([[(k1 + k1.conj().T) / 2, z], [z, (k2 + k2.conj().T) / 2]])
+    return r, k
+
+
+def evaluate(r, k, g, window, nq, nodes):
+    q = -1j * k - r.conj().T @ r / 2
+    rho, _ = nm.stationary_state(q, r, tolerance=1e-13)
+    quartic = ob.evaluate_quartic(r, q, rho, g, xp=np, half_window=window, n_quad=nq, atol=1e-13, rtol=1e-12,
+                                  reduced=True)
+    kinetic = kb.kinetic_raw(q, r, rho, nodes, xp=np, tolerance=1e-12, maxdim=1024)
+    cov = quartic["covector"] + kinetic["covector"]
+    env = quartic["environment"] + kinetic["environment"]
+    grad, _ = nm.finish_gradient(q, r, rho, cov, env, metric_reg=1e-3)
+    return dict(R=r, K=k, rho=rho, g=g, window=window, n_quad=nq, nodes=nodes,
+                quartic_value=quartic["value"], quartic_covector=quartic["covector"],
+                quartic_environment=quartic["environment"],
+                accepted=quartic["stats"]["accepted_steps"], rejected=quartic["stats"]["rejected_steps"],
+                kinetic_value=kinetic["value"], kinetic_covector=kinetic["covector"],
+                kinetic_environment=kinetic["environment"],
+                energy=quartic["value"] + kinetic["value"], gradient=grad)
+
+
+def save(name, records):
+    flat = {}
+    for i, rec in enumerate(records):
+        for key, value in rec.items():
+            flat[f"s{i}_{key}"] = np.asarray(value)
+    flat["count"] = np.asarray(len(records))
+    np.savez_compressed(HERE / name, **flat)
+
+
+def main():
+    t0 = time.time()
+    small = [evaluate(*random_state(d, 500 + d), 0.5 + 0.5 * i, 30.0, 64, 128) for i, d in enumerate((4, 6, 8))]
+    small.append(evaluate(*z2_state(8, 508), 2.0, 30.0, 64, 128))
+    save("small.npz", small)
+    save("d16.npz", [evaluate(*random_state(16, 16), 2.0, 30.0, 512, 512)])
+    save("d64.npz", [evaluate(*random_state(64, 42), 2.0, 30.0, 512, 512)])
+    # trajectory samples of the reduced system (the persistent kernel's channels)
+    r, k = random_state(5, 5)
+    q = -1j * k - r.conj().T @ r / 2
+    rho, _ = nm.stationary_state(q, r, tolerance=1e-13)
+    rhs = ob._UnpackedQuarticRHS(q, r, rho, np)
+    points, _ = ob.quadrature(2.0, 16)
+    samples, stats = ob._integrate(rhs, np.r_[points, math.sqrt(2.0)], atol=1e-13, rtol=1e-12, initial_step=None,
+                                   max_steps=100000)
+    np.savez_compressed(HERE / "samples_d5.npz", R=r, K=k, rho=rho, window=2.0, n_quad=16, samples=samples,
+                        accepted=stats["accepted_steps"], rejected=stats["rejected_steps"])
+    print(f"golden vectors written in {time.time() - t0:.1f} s")
+
+
+if __name__ == "__main__":
+    main()

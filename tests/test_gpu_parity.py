@@ -1,0 +1,180 @@
+"""Parity of the CUDA path (through the C ABI) with the reference and the oracle.
+
+Tolerances (written per test): integer outputs (DOP853 step counts, Krylov basis sizes) exactly;
+floating point at the north-star bar or tighter: energy |dE/E| <= 1e-10 and gradient <= 1e-8
+relative in the metric norm, with max(|g|, 1) as the scale (near minima |g| itself is tiny).
+"""
+import ctypes as C
+import math
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, julia_fixture, load_records
+from oracle import fg_phi4_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+ENERGY_TOL = 1e-10
+GRAD_TOL = 1e-8
+
+
+def metric_norm(rho, x):
+    return math.sqrt(max(0.0, O.metric(rho, x, x)))
+
+
+def grad_close(rho, got, ref, tol=GRAD_TOL):
+    return metric_norm(rho, got - ref) <= tol * max(1.0, metric_norm(rho, ref))
+
+
+def test_trajectory_samples_match_reference_and_oracle(gpu_context):
+    from rcmps_b200 import objective
+    data = np.load(GOLDEN / "samples_d5.npz")
+    R, K, rho = data["R"], data["K"], data["rho"]
+    Q = O.left_canonical_q(R, K)
+    out = objective.evaluate_quartic_persistent_trajectory(R, Q, rho, 1.0, half_window=float(data["window"]),
+                                                           n_quad=int(data["n_quad"]), return_samples=True)
+    st = out["stats"]
+    assert (st["accepted"], st["rejected"]) == (int(data["accepted"]), int(data["rejected"]))
+    ref = data["samples"]
+    got = out["samples"]
+    assert np.abs(got[:, :-1] - ref[:, :-1]).max() <= 1e-12 * np.abs(ref).max()
+    assert abs(got[-1, -1].real - ref[-1, -1].real) <= 1e-14
+
+
+@pytest.mark.parametrize("index", range(4))
+def test_components_match_reference_small(gpu_context, index):
+    from rcmps_b200 import objective
+    rec = load_records("small.npz")[index]
+    R, K, rho, g = rec["R"], rec["K"], rec["rho"], rec["g"]
+    Q = O.left_canonical_q(R, K)
+    q = objective.evaluate_quartic_persistent_trajectory(R, Q, rho, g, half_window=rec["window"], n_quad=int(rec["n_quad"]))
+    assert (q["stats"]["accepted"], q["stats"]["rejected"]) == (rec["accepted"], rec["rejected"])
+    assert abs(q["value"] - rec["quartic_value"]) <= 1e-12 * max(1.0, abs(rec["quartic_value"]))
+    assert np.abs(q["covector"] - rec["quartic_covector"]).max() <= 1e-11 * max(1.0, np.abs(rec["quartic_covector"]).max())
+    assert np.abs(q["environment"] - rec["quartic_environment"]).max() <= 1e-11
+    k = objective.kinetic_raw(Q, R, rho, int(rec["nodes"]))
+    assert abs(k["value"] - rec["kinetic_value"]) <= 1e-12 * max(1.0, abs(rec["kinetic_value"]))
+    assert np.abs(k["covector"] - rec["kinetic_covector"]).max() <= 1e-11 * max(1.0, np.abs(rec["kinetic_covector"]).max())
+    assert k["stats"]["maximum_relative_residual"] <= 1e-12
+    grad, st = objective.finish_gradient(Q, R, rho, q["covector"] + k["covector"], q["environment"] + k["environment"])
+    assert grad_close(rho, grad, rec["gradient"], 1e-10)
+
+
+def test_batched_fg_matches_reference_mixed_dims(gpu_context):
+    from rcmps_b200 import objective
+    recs = load_records("small.npz")
+    s = objective.settings_from_args(None, half_window=30.0, n_quad=64, kinetic_nodes=128)
+    E, G, stats = objective.fg_phi4_batch([r["R"] for r in recs], [r["K"] for r in recs], [r["rho"] for r in recs],
+                                          [r["g"] for r in recs], s)
+    for i, rec in enumerate(recs):
+        assert stats[i]["status"] == 0
+        assert abs(E[i] - rec["energy"]) <= ENERGY_TOL * abs(rec["energy"])
+        assert grad_close(rec["rho"], G[i], rec["gradient"])
+
+
+@pytest.mark.parametrize("name", ["d16.npz", "d64.npz"])
+def test_fg_default_settings_matches_reference(gpu_context, name):
+    from rcmps_b200 import objective
+    rec = load_records(name)[0]
+    energy, gradient, stats = objective.objective(rec["R"], rec["K"], rec["rho"], rec["g"], objective.default_args())
+    assert abs(energy - rec["energy"]) <= ENERGY_TOL * abs(rec["energy"])
+    assert grad_close(rec["rho"], gradient, rec["gradient"])
+    assert (stats["accepted"], stats["rejected"]) == (rec["accepted"], rec["rejected"])
+
+
+def test_julia_fixture(gpu_context):
+    """RcmpsCore's fg_phi4 (Julia, Vern7, ODE kinetic) at the fixture's settings W = 20, n_quad = 192:
+    energy within 1e-12 absolute (1e-11 relative); the gradient of this near-minimal state
+    (|g| = 2.7e-6) within 5e-9 in the metric norm, as the reference's own NumPy route (1.7e-9)."""
+    from rcmps_b200 import objective
+    fx = julia_fixture()
+    args = objective.default_args(window=20.0, quadrature=192)
+    energy, gradient, _ = objective.objective(fx["R"], fx["K"], fx["rho"], fx["meta"]["coupling"], args)
+    assert abs(energy - fx["meta"]["energy"]) < 1e-12
+    assert metric_norm(fx["rho"], gradient - fx["gradient"]) < 5e-9
+
+
+def test_stationary_state_matches_oracle(gpu_context):
+    from rcmps_b200 import objective
+    for rec in load_records("small.npz"):
+        Q = O.left_canonical_q(rec["R"], rec["K"])
+        rho, st = objective.stationary_state(Q, rec["R"], tolerance=1e-13)
+        assert np.abs(rho - rec["rho"]).max() < 1e-12
+        assert st["stationary_residual"] < 1e-12
+
+
+def test_finite_difference_gradient(gpu_context):
+    """d E[W] = metric(gradient, W) along a horizontal tangent W with the retraction
+    R -> R + eps W, K -> K + i eps/2 (W^dag R - R^dag W) and rho recomputed on the GPU
+    (test/runtests.jl:106-149 checks fg_phi4 the same way)."""
+    from rcmps_b200 import objective
+    R, K = O.phi4_state(4, 77)
+    rng = np.random.default_rng(5)
+    W = (rng.standard_normal((4, 4)) + 1j * rng.standard_normal((4, 4))) * 0.1
+    args = objective.default_args(quadrature=128, nodes=256)
+
+    def energy(eps):
+        r = R + eps * W
+        k = K + 1j * eps / 2 * (W.conj().T @ R - R.conj().T @ W)
+        k = (k + k.conj().T) / 2
+        rho, _ = objective.stationary_state(O.left_canonical_q(r, k), r, tolerance=1e-14)
+        return objective.objective(r, k, rho, 2.0, args)[0]
+
+    rho0, _ = objective.stationary_state(O.left_canonical_q(R, K), R, tolerance=1e-14)
+    _, g, _ = objective.objective(R, K, rho0, 2.0, args)
+    eps = 1e-5
+    fd = (energy(eps) - energy(-eps)) / (2 * eps)
+    assert abs(fd - O.metric(rho0, g, W)) < 1e-7 * max(1.0, abs(fd))
+
+
+def test_batch_results_are_independent_of_composition_and_deterministic(gpu_context):
+    from rcmps_b200 import objective
+    recs = load_records("small.npz")
+    s = objective.settings_from_args(None, half_window=30.0, n_quad=64, kinetic_nodes=128)
+    full = objective.fg_phi4_batch([r["R"] for r in recs], [r["K"] for r in recs], [r["rho"] for r in recs],
+                                   [r["g"] for r in recs], s)
+    again = objective.fg_phi4_batch([r["R"] for r in recs], [r["K"] for r in recs], [r["rho"] for r in recs],
+                                    [r["g"] for r in recs], s)
+    single = objective.fg_phi4_batch([recs[2]["R"]], [recs[2]["K"]], [recs[2]["rho"]], [recs[2]["g"]], s)
+    assert np.array_equal(full[0], again[0]) and all(np.array_equal(a, b) for a, b in zip(full[1], again[1]))
+    assert full[0][2] == single[0][0] and np.array_equal(full[1][2], single[1][0])
+
+
+def test_z2_state_keeps_its_structure_at_d64(gpu_context):
+    """Size-independent property at the benchmark's D = 64: the gradient of a Z2 state is odd
+    under the parity split (its diagonal blocks vanish), like R."""
+    from rcmps_b200 import objective
+    from rcmps_b200.batch import z2_state
+    R, K = z2_state(64, 101)
+    rho, _ = objective.stationary_state(O.left_canonical_q(R, K), R, tolerance=1e-13)
+    _, g, st = objective.objective(R, K, rho, 2.0, objective.default_args())
+    n = 32
+    odd = np.abs(g[:n, n:]).max() + np.abs(g[n:, :n]).max()
+    even = np.abs(g[:n, :n]).max() + np.abs(g[n:, n:]).max()
+    assert st["status"] == 0 and even <= 1e-10 * odd
+
+
+def test_failure_statuses_are_reported(gpu_context):
+    """Host-injected failures, no GPU fault: a step budget too small (max_steps), a device-clock
+    watchdog of 1 ns (device_clock_timeout), a nonfinite input and an unsupported size."""
+    from rcmps_b200 import objective
+    R, K = O.phi4_state(8, 3)
+    Q = O.left_canonical_q(R, K)
+    rho = O.stationary_state(Q, R)
+    with pytest.raises(objective.DeviceControlFailure) as err:
+        objective.evaluate_quartic_persistent_trajectory(R, Q, rho, 1.0, max_steps=5)
+    assert err.value.diagnostics["status_name"] == "max_steps"
+    with pytest.raises(objective.DeviceControlFailure) as err:
+        objective.evaluate_quartic_persistent_trajectory(R, Q, rho, 1.0, max_device_seconds=1e-9)
+    assert err.value.diagnostics["status_name"] == "device_clock_timeout"
+    bad = R.copy()
+    bad[0, 0] = np.nan
+    with pytest.raises(ValueError):
+        objective.evaluate_quartic_persistent_trajectory(bad, Q, rho, 1.0)
+    big = np.eye(129, dtype=complex)
+    with pytest.raises(ValueError):
+        objective.fg_phi4_batch([big], [big], [big], [1.0])
+    # the context stays usable after the failures
+    out = objective.evaluate_quartic_persistent_trajectory(R, Q, rho, 1.0, n_quad=16)
+    assert out["stats"]["status"] == 0
