@@ -53,7 +53,7 @@ RCMPS_DEVICE_INLINE double2 zaxpy(double s, double2 x, double2 y) {
 //   a = {A[g][t], A[g+8][t], A[g][t+4], A[g+8][t+4]}, b = {B[t][g], B[t+4][g]},
 //   c = {C[g][2t], C[g][2t+1], C[g+8][2t], C[g+8][2t+1]}.
 RCMPS_DEVICE_INLINE void dmma16x8x8(double* c, const double* a, const double* b) {
-  asm volatile(
+  asm(
       "mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 "
       "{%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};"
       : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
@@ -78,6 +78,23 @@ RCMPS_DEVICE_INLINE void zmma(ZFrag& acc, const double* ar, const double* ai, co
   dmma16x8x8(acc.re, nai, bi);
   dmma16x8x8(acc.im, ar, bi);
   dmma16x8x8(acc.im, ai, br);
+}
+
+// acc[j] += A * B_j for TPW tiles sharing the A fragment; the MMAs are issued so that
+// consecutive ones update different accumulators.
+template <int TPW>
+RCMPS_DEVICE_INLINE void zmma_tiles(ZFrag* acc, const double* ar, const double* ai, const double* nai,
+                                    const double (*br)[2], const double (*bi)[2]) {
+#pragma unroll
+  for (int j = 0; j < TPW; ++j) {
+    dmma16x8x8(acc[j].re, ar, br[j]);
+    dmma16x8x8(acc[j].im, ar, bi[j]);
+  }
+#pragma unroll
+  for (int j = 0; j < TPW; ++j) {
+    dmma16x8x8(acc[j].re, nai, bi[j]);
+    dmma16x8x8(acc[j].im, ai, br[j]);
+  }
 }
 
 // Load the A fragment of rows [m0, m0+16) and columns [k0, k0+8) of a row-major complex
@@ -139,6 +156,10 @@ RCMPS_DEVICE_INLINE bool mbar_wait(uint64_t* bar, uint32_t parity, int* flag) {
   if (flag) atomicExch(flag, 1);
   return false;
 }
+// Row padding of streamed B chunks in shared memory: a row stride of (cols + 2) complex values
+// (= 32 mod 128 bytes) puts the four k-rows a B fragment reads in different banks.
+constexpr int kBPad = 2;
+
 // 1-D bulk copy global -> shared of this CTA, completing on `bar`. 16-byte aligned, size % 16 == 0.
 RCMPS_DEVICE_INLINE void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
   asm volatile(

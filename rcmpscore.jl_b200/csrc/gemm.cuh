@@ -19,9 +19,11 @@ struct Tiling {
 template <int DP, int NW, int KC, int NST>
 struct RowGemmRing {
   static constexpr int NT = 32 * NW;
+  static constexpr int LDB = DP + kBPad;            // padded row stride of a chunk in the ring
   static constexpr uint32_t CHUNK_BYTES = KC * DP * 16;
+  static constexpr int SLOT = KC * LDB;             // ring slot size (double2)
 
-  double2* ring;        // [NST][KC*DP]
+  double2* ring;        // [NST][KC*LDB]
   uint64_t* full;       // [NST]
   int* wait_flag;       // shared flag set when a bounded wait gives up
   long long gq;         // running chunk counter (uniform across the CTA)
@@ -53,7 +55,9 @@ struct RowGemmRing {
     const long long g = gq + q;
     const int slot = (int)(g % NST);
     mbar_expect_tx(&full[slot], CHUNK_BYTES);
-    bulk_g2s(ring + slot * KC * DP, chunk_ptr(s, q), CHUNK_BYTES, &full[slot]);
+    const double2* src = chunk_ptr(s, q);
+#pragma unroll
+    for (int r = 0; r < KC; ++r) bulk_g2s(ring + slot * SLOT + r * LDB, src + r * DP, DP * 16, &full[slot]);
   }
 
   // acc[TPW] += A * B. Call with all threads; ends with a __syncthreads.
@@ -74,18 +78,15 @@ struct RowGemmRing {
       const long long g = gq + q;
       const int slot = (int)(g % NST);
       mbar_wait(&full[slot], (uint32_t)((g / NST) & 1), wait_flag);
-      const double2* B = ring + slot * KC * DP;
+      const double2* B = ring + slot * SLOT;
 #pragma unroll
       for (int ks = 0; ks < KC / 8; ++ks) {
         double ar[4], ai[4], nai[4];
         load_a(A, lda, mt * 16, q * KC + ks * 8, lane, ar, ai, nai);
+        double br[TPW][2], bi[TPW][2];
 #pragma unroll
-        for (int j = 0; j < TPW; ++j) {
-          const int nt = (tile0 + j) % TN;
-          double br[2], bi[2];
-          load_b(B, DP, ks * 8, nt * 8, lane, br, bi);
-          zmma(acc[j], ar, ai, nai, br, bi);
-        }
+        for (int j = 0; j < TPW; ++j) load_b(B, LDB, ks * 8, ((tile0 + j) % TN) * 8, lane, br[j], bi[j]);
+        zmma_tiles<TPW>(acc, ar, ai, nai, br, bi);
       }
       __syncthreads();
       if (threadIdx.x == 0 && q + NST < nch) issue(s, q + NST);

@@ -32,12 +32,12 @@ struct LGeo {
   static constexpr int NST = 4;
   static constexpr int LDP = DP + 4, LDA2 = 2 * DP + 4;
   static constexpr int NT = 32 * NW;
-  static constexpr size_t SMEM = ((size_t)32 * LDP + 16 * LDA2 + (size_t)NST * KC * DP) * 16 + 128;
+  static constexpr size_t SMEM = ((size_t)32 * LDP + 16 * LDA2 + (size_t)NST * KC * (DP + kBPad)) * 16 + 128;
 };
 template <>
 struct LGeo<96> {
   static constexpr int NW = 12, KC = 8, NST = 4, LDP = 100, LDA2 = 196, NT = 384;
-  static constexpr size_t SMEM = ((size_t)32 * LDP + 16 * LDA2 + (size_t)NST * KC * 96) * 16 + 128;
+  static constexpr size_t SMEM = ((size_t)32 * LDP + 16 * LDA2 + (size_t)NST * KC * (96 + kBPad)) * 16 + 128;
 };
 
 template <int DP>
@@ -51,7 +51,7 @@ lindblad_kernel(const LindbladTask* __restrict__ tasks, int ntasks, int mode) {
   double2* panel = reinterpret_cast<double2*>(smem_raw);       // [32][LDP]: A1 rows; A2 rows
   double2* aprime = panel + 32 * LG::LDP;                        // [16][LDA2]: X rows | T rows
   double2* ring = aprime + 16 * LG::LDA2;
-  uint64_t* full = reinterpret_cast<uint64_t*>(ring + (size_t)LG::NST * LG::KC * DP);
+  uint64_t* full = reinterpret_cast<uint64_t*>(ring + (size_t)LG::NST * LG::KC * (DP + kBPad));
   int* flag = reinterpret_cast<int*>(full + LG::NST);
   const int tid = threadIdx.x;
   const int rb = blockIdx.x % (DP / 16);
@@ -571,7 +571,7 @@ struct CGeo {
   static constexpr int NRB = DP / MB;
   static constexpr int NT = 32 * NW;
   static constexpr size_t BUF = (size_t)MB * LDA;
-  static constexpr size_t SMEM = (2 * BUF + (size_t)NST * KC * DP) * 16 + 128;
+  static constexpr size_t SMEM = (2 * BUF + (size_t)NST * KC * (DP + kBPad)) * 16 + 128;
 };
 
 template <int DP>
@@ -583,7 +583,7 @@ contract_kernel(ContractArgs a) {
   double2* bufX = reinterpret_cast<double2*>(smem_raw);
   double2* bufY = bufX + CG::BUF;
   double2* ring = bufY + CG::BUF;
-  uint64_t* full = reinterpret_cast<uint64_t*>(ring + (size_t)CG::NST * CG::KC * DP);
+  uint64_t* full = reinterpret_cast<uint64_t*>(ring + (size_t)CG::NST * CG::KC * (DP + kBPad));
   int* flag = reinterpret_cast<int*>(full + CG::NST);
   constexpr int MAT = DP * DP;
   const int blk = blockIdx.x;

@@ -29,7 +29,7 @@ struct PGeo {
   using GM = RowGemm<DP, MB, NW, KC, NST>;
   static constexpr int NT = 32 * NW;
   static constexpr size_t BUF = (size_t)MB * LDA;      // double2 per A buffer
-  static constexpr size_t SMEM = (2 * BUF + (size_t)NST * KC * DP) * 16 + 128;
+  static constexpr size_t SMEM = (2 * BUF + (size_t)NST * KC * (DP + kBPad)) * 16 + 128;
 };
 
 template <int DP>
@@ -41,7 +41,7 @@ pullback_kernel(PullbackArgs a) {
   double2* bufX = reinterpret_cast<double2*>(smem_raw);
   double2* bufY = bufX + PG::BUF;
   double2* ring = bufY + PG::BUF;
-  uint64_t* full = reinterpret_cast<uint64_t*>(ring + (size_t)PG::NST * PG::KC * DP);
+  uint64_t* full = reinterpret_cast<uint64_t*>(ring + (size_t)PG::NST * PG::KC * (DP + kBPad));
   int* flag = reinterpret_cast<int*>(full + PG::NST);
 
   constexpr int MAT = DP * DP, VEC = 7 * MAT;

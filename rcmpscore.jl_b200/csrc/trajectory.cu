@@ -69,38 +69,51 @@ __device__ __forceinline__ double ins_coef(int c) {
   return c == 1 ? 2.0 : c == 2 ? 3.0 : c == 3 ? 1.0 : c == 4 ? 2.0 : c == 5 ? 3.0 : 0.0;
 }
 
+// Tiling of one product pass: M rows (a multiple of 16) by DP columns over NW warps; a warp owns
+// TPW consecutive 16x8 tiles of one band, or (when there are fewer tiles than warps) one tile and a
+// 1/SK slice of the k-steps.
+template <int DP, int M, int NW>
+struct PassTiling {
+  static constexpr int NTN = DP / 8;
+  static constexpr int T = (M / 16) * NTN;
+  static constexpr int SK = T >= NW ? 1 : NW / T;
+  static constexpr int TPW = T >= NW ? T / NW : 1;
+  static_assert(T % NW == 0 || NW % T == 0, "tiling");
+  static_assert(SK > 1 || NTN % TPW == 0, "a warp's tiles share one band");
+  static constexpr int SPLIT = SK > 1 ? T * (SK - 1) * 128 : 0;   // split-K scratch (double2)
+};
+
 template <int DP>
 struct Geo {
   static constexpr int G = DP / 16;
-  static constexpr int NW = (DP == 48 || DP == 96) ? 12 : 8;
+  static constexpr int NW = (DP == 48 || DP == 96) ? 12 : (DP == 64 || DP == 128) ? 16 : 8;
   static constexpr int NT = 32 * NW;
   static constexpr int KC = DP <= 64 ? 16 : 8;       // rows of a streamed B chunk
   static constexpr int NST = 4;                       // ring stages
+  static constexpr int LDB = DP + kBPad;              // padded row stride of a ring chunk
   static constexpr int LDP = DP + 4;                  // panel leading dimension (complex)
   static constexpr int LDA2 = 2 * DP + 4;             // A' leading dimension
-  static constexpr bool RESIDENT = DP <= 64;          // both direction panels stay resident
-  static constexpr int NPANEL = RESIDENT ? 2 : 1;
-  static constexpr int NTN = DP / 8;                  // 8-column tiles
-  static constexpr int T1 = 2 * NTN, T2 = NTN;        // tiles of G1 (32 rows) and G2 (16 rows)
-  static constexpr int SK1 = T1 >= NW ? 1 : NW / T1, TPW1 = T1 >= NW ? T1 / NW : 1;
-  static constexpr int SK2 = T2 >= NW ? 1 : NW / T2, TPW2 = T2 >= NW ? T2 / NW : 1;
-  static_assert(T1 % NW == 0 || NW % T1 == 0, "G1 tiling");
-  static_assert(T2 % NW == 0 || NW % T2 == 0, "G2 tiling");
-  static constexpr int CH1 = DP / KC, CH2 = 2 * DP / KC;   // chunks per channel
-  static constexpr int NCHUNK = 7 * (CH1 + CH2);
+  static constexpr int GS = DP <= 64 ? 2 : 1;         // channels per G2 pass
+  static constexpr int NPASS = GS == 2 ? 4 : 7;       // G2 passes: {0,1},{2},{3,4},{5,6} or one per channel
+  using T1 = PassTiling<DP, 32, NW>;
+  using T2a = PassTiling<DP, 16 * GS, NW>;
+  using T2b = PassTiling<DP, 16, NW>;
+  static constexpr int CH1 = DP / KC, CH2 = 2 * DP / KC;   // chunks per G1 channel / G2 pass
+  static constexpr int NCHUNK = 7 * CH1 + NPASS * CH2;
   static constexpr int MAT = DP * DP;                 // elements of one channel matrix
   static constexpr int VEC = 7 * MAT;                 // elements of one stage vector
   static constexpr int OWN = 7 * 16 * DP;             // elements owned by one CTA
-  // shared memory (double2 units)
+  static constexpr int cmax(int a, int b) { return a > b ? a : b; }
+  // shared memory (double2 units): one direction panel, the A' rows of a pass, the ring, split-K
   static constexpr int OFF_PANEL = 0;
-  static constexpr int OFF_APRIME = OFF_PANEL + NPANEL * 32 * LDP;
-  static constexpr int OFF_RING = OFF_APRIME + 16 * LDA2;
-  static constexpr int SPLITTILES = (SK1 > 1 ? T1 * (SK1 - 1) : 0) > (SK2 > 1 ? T2 * (SK2 - 1) : 0)
-                                        ? (SK1 > 1 ? T1 * (SK1 - 1) : 0)
-                                        : (SK2 > 1 ? T2 * (SK2 - 1) : 0);
-  static constexpr int OFF_SPLIT = OFF_RING + NST * KC * DP;
-  static constexpr int END2 = OFF_SPLIT + SPLITTILES * 128;
+  static constexpr int OFF_APRIME = OFF_PANEL + 32 * LDP;
+  static constexpr int OFF_RING = OFF_APRIME + 16 * GS * LDA2;
+  static constexpr int OFF_SPLIT = OFF_RING + NST * KC * LDB;
+  static constexpr int END2 = OFF_SPLIT + cmax(T1::SPLIT, cmax(T2a::SPLIT, T2b::SPLIT));
   static constexpr size_t SMEM = (size_t)END2 * 16 + 2048;   // + barriers and scalars (see carve)
+  // G2 pass p: first channel and channel count
+  __device__ static int pass_first(int p) { return GS == 2 ? (p == 0 ? 0 : p == 1 ? 2 : p == 2 ? 3 : 5) : p; }
+  __device__ static int pass_count(int p) { return GS == 2 ? (p == 1 ? 1 : 2) : 1; }
 };
 
 // Scalars of the controller, one copy per CTA (identical in all CTAs of a cluster).
@@ -111,6 +124,7 @@ struct Ctl {
   double jac[16], src[16];               // per stage of the attempt
   long long attempts, accepted, rejected, dense_steps, next_point, first, last;
   int status, after_reject, accept, dense, done, wait_flag;
+  int kslot[16];                         // k buffer of each stage (permuted on acceptance)
 };
 
 struct Xch {                             // exchanged through distributed shared memory
@@ -121,9 +135,9 @@ struct Xch {                             // exchanged through distributed shared
 
 template <int DP>
 struct Smem {
-  double2* panel;     // [NPANEL][32][LDP]
-  double2* aprime;    // [16][LDA2]
-  double2* ring;      // [NST][KC*DP]
+  double2* panel;     // [32][LDP]: the current direction's [Qc; Rc] rows
+  double2* aprime;    // [16 GS][LDA2]
+  double2* ring;      // [NST][KC*LDB]
   double2* split;     // split-K partial fragments
   uint64_t* full;     // [NST]
   Ctl* ctl;
@@ -144,7 +158,7 @@ __device__ __forceinline__ Smem<DP> carve(unsigned char* base) {
   constexpr size_t o_ctl = 64;
   constexpr size_t o_xch = o_ctl + ((sizeof(Ctl) + 15) / 16) * 16;
   constexpr size_t o_red = o_xch + ((sizeof(Xch) + 15) / 16) * 16;
-  constexpr size_t o_ksc = o_red + 16 * sizeof(double) * 2;
+  constexpr size_t o_ksc = o_red + 32 * sizeof(double) * 2;
   static_assert(o_ksc + 16 * sizeof(double) <= 2048, "shared tail");
   unsigned char* tail = base + (size_t)GE::END2 * 16;
   s.full = reinterpret_cast<uint64_t*>(tail);
@@ -186,8 +200,8 @@ struct Rhs {
       return zb + c * GE::MAT + k * GE::KC * DP;
     }
     q -= 7 * GE::CH1;
-    const int c = q / GE::CH2, k = q % GE::CH2;
-    const bool fwd = c < 3;
+    const int p = q / GE::CH2, k = q % GE::CH2;
+    const bool fwd = GE::pass_first(p) < 3;
     const double2* top = fwd ? st->Qh : st->Q;     // (Qc)^dag
     const double2* bot = fwd ? st->Rh : st->R;     // (Rc)^dag
     const int r = k * GE::KC;
@@ -196,9 +210,11 @@ struct Rhs {
 
   __device__ void issue(long long gidx, int q, const double2* zb) {
     const int slot = (int)(gidx % GE::NST);
-    const uint32_t bytes = GE::KC * DP * 16;
-    mbar_expect_tx(&sm.full[slot], bytes);
-    bulk_g2s(sm.ring + slot * GE::KC * DP, chunk_src(q, zb), bytes, &sm.full[slot]);
+    mbar_expect_tx(&sm.full[slot], GE::KC * DP * 16);
+    const double2* src = chunk_src(q, zb);
+    double2* dst = sm.ring + slot * GE::KC * GE::LDB;
+#pragma unroll
+    for (int r = 0; r < GE::KC; ++r) bulk_g2s(dst + r * GE::LDB, src + r * DP, DP * 16, &sm.full[slot]);
   }
 
   // Wait for chunk (global index gidx); bounded.
@@ -206,7 +222,7 @@ struct Rhs {
     const int slot = (int)(gidx % GE::NST);
     const uint32_t parity = (uint32_t)((gidx / GE::NST) & 1);
     if (!mbar_wait(&sm.full[slot], parity, &sm.ctl->wait_flag)) {}
-    return sm.ring + slot * GE::KC * DP;
+    return sm.ring + slot * GE::KC * GE::LDB;
   }
 
   __device__ void load_panel(int dir, double2* dst) const {
@@ -219,7 +235,7 @@ struct Rhs {
     }
   }
 
-  // Split-K reduction of `ntile` fragments; warps with slice > 0 deposit, slice 0 adds.
+  // Split-K reduction; warps with slice > 0 deposit, slice 0 adds.
   template <int TPW, int SK>
   __device__ void split_reduce(ZFrag* acc, int tile0, int slice) {
     if constexpr (SK > 1) {
@@ -249,6 +265,81 @@ struct Rhs {
     }
   }
 
+  // acc += A (M rows in shared memory, lda) * the next nch streamed chunks. Ends with the chunks'
+  // slots released and the next chunks issued.
+  template <class TL>
+  __device__ void stream_product(ZFrag* acc, const double2* A, int lda, int nch, int& q, long long g0,
+                                 const double2* zb) {
+    constexpr int TPW = TL::TPW, SK = TL::SK;
+    const int tile0 = SK > 1 ? warp / SK : warp * TPW;
+    const int slice = SK > 1 ? warp % SK : 0;
+    const int mt = tile0 / TL::NTN;
+    for (int ch = 0; ch < nch; ++ch, ++q) {
+      const double2* B = await(g0 + q);
+#pragma unroll
+      for (int ks = 0; ks < GE::KC / 8; ++ks) {
+        const int kstep = ch * (GE::KC / 8) + ks;
+        if (kstep % SK != slice) continue;
+        double ar[4], ai[4], nai[4];
+        load_a(A, lda, mt * 16, kstep * 8, lane, ar, ai, nai);
+        double br[TPW][2], bi[TPW][2];
+#pragma unroll
+        for (int j = 0; j < TPW; ++j) load_b(B, GE::LDB, ks * 8, ((tile0 + j) % TL::NTN) * 8, lane, br[j], bi[j]);
+        zmma_tiles<TPW>(acc, ar, ai, nai, br, bi);
+      }
+      __syncthreads();
+      if (tid == 0 && q + GE::NST < GE::NCHUNK) issue(g0 + q + GE::NST, q + GE::NST, zb);
+    }
+    split_reduce<TPW, SK>(acc, tile0, slice);
+  }
+
+  // G2 pass over the channels first..first+NC-1 (same direction).
+  template <int NC>
+  __device__ void g2_pass(int first, const double2* zb, double2* kout, double jac, double src, int& q,
+                          long long g0) {
+    using TL = PassTiling<DP, 16 * NC, GE::NW>;
+    constexpr int TPW = TL::TPW, SK = TL::SK;
+    // A' = [jac X_c | jac P_c + src coef_c X_s] on this CTA's rows, channel i of the pass in rows 16 i..
+    for (int e = tid; e < 16 * NC * DP; e += GE::NT) {
+      const int r = e / DP, col = e % DP;
+      const int c = first + r / 16;
+      const int s = ins_src(c);
+      const size_t off = (size_t)(row0 + (r & 15)) * DP + col;
+      const double2 x = __ldcg(zb + (size_t)c * GE::MAT + off);
+      double2 m = zscale(jac, __ldcg(st->P + (size_t)c * GE::MAT + off));
+      if (s >= 0) m = zaxpy(src * ins_coef(c), __ldcg(zb + (size_t)s * GE::MAT + off), m);
+      sm.aprime[r * GE::LDA2 + col] = zscale(jac, x);
+      sm.aprime[r * GE::LDA2 + DP + col] = m;
+    }
+    __syncthreads();
+    ZFrag acc[TPW];
+#pragma unroll
+    for (int j = 0; j < TPW; ++j) acc[j].zero();
+    stream_product<TL>(acc, sm.aprime, GE::LDA2, GE::CH2, q, g0, zb);
+    const int tile0 = SK > 1 ? warp / SK : warp * TPW;
+    const int slice = SK > 1 ? warp % SK : 0;
+    if (slice == 0) {
+#pragma unroll
+      for (int j = 0; j < TPW; ++j) {
+        const int tile = tile0 + j, mt = tile / TL::NTN, nt = tile % TL::NTN;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          const int r = mt * 16 + frag_row(lane, i), col = nt * 8 + frag_col(lane, i);
+          const int c = first + r / 16;
+          const int s = ins_src(c);
+          const size_t loc = (size_t)(row0 + (r & 15)) * DP + col;
+          const size_t off = (size_t)c * GE::MAT + loc;
+          double2 v = zadd(make_double2(acc[j].re[i], acc[j].im[i]), kout[off]);
+          if (s >= 0) v = zaxpy(src * ins_coef(c), __ldcg(st->P + (size_t)s * GE::MAT + loc), v);
+          if (c == 0) v = zaxpy(src, st->fixed0[loc], v);
+          if (c == 6) v = zaxpy(src, st->fixed6[loc], v);
+          kout[off] = v;
+        }
+      }
+    }
+    __syncthreads();
+  }
+
   // One right-hand side: k_out = f(t, z) on this CTA's rows. zb: the full stage vector
   // (written by every CTA of the cluster before the barrier that precedes this call).
   __device__ void operator()(const double2* zb, double2* kout, double jac, double src) {
@@ -258,51 +349,27 @@ struct Rhs {
       for (int q = 0; q < GE::NST && q < GE::NCHUNK; ++q) issue(g0 + q, q, zb);
     }
     int q = 0;
-    // ------------------------------------------------------------------ G1
+    // ------------------------------------------------------------------ G1: [Qc; Rc] rows * X_c
     {
-      constexpr int TPW = GE::TPW1, SK = GE::SK1;
+      using TL = typename GE::T1;
+      constexpr int TPW = TL::TPW, SK = TL::SK;
       const int tile0 = SK > 1 ? warp / SK : warp * TPW;
       const int slice = SK > 1 ? warp % SK : 0;
-      const int mt = tile0 / GE::NTN;                 // 0: Qc rows, 1: Rc rows
+      const int mt = tile0 / TL::NTN;     // 0: Qc rows, 1: Rc rows
       for (int c = 0; c < 7; ++c) {
-        const int dir = c < 3 ? 0 : 1;
-        double2* panel = sm.panel;
-        if constexpr (GE::RESIDENT) {
-          panel = sm.panel + dir * 32 * GE::LDP;
-        } else {
-          if (c == 0 || c == 3) {
-            __syncthreads();
-            load_panel(dir, sm.panel);
-            __syncthreads();
-          }
+        if (c == 0 || c == 3) {
+          __syncthreads();
+          load_panel(c == 0 ? 0 : 1, sm.panel);
+          __syncthreads();
         }
         ZFrag acc[TPW];
 #pragma unroll
         for (int j = 0; j < TPW; ++j) acc[j].zero();
-        for (int ch = 0; ch < GE::CH1; ++ch, ++q) {
-          const double2* B = await(g0 + q);
-#pragma unroll
-          for (int ks = 0; ks < GE::KC / 8; ++ks) {
-            const int kstep = ch * (GE::KC / 8) + ks;
-            if (kstep % SK != slice) continue;
-            double ar[4], ai[4], nai[4];
-            load_a(panel, GE::LDP, mt * 16, kstep * 8, lane, ar, ai, nai);
-#pragma unroll
-            for (int j = 0; j < TPW; ++j) {
-              const int nt = (tile0 + j) % GE::NTN;
-              double br[2], bi[2];
-              load_b(B, DP, ks * 8, nt * 8, lane, br, bi);
-              zmma(acc[j], ar, ai, nai, br, bi);
-            }
-          }
-          __syncthreads();
-          if (tid == 0 && q + GE::NST < GE::NCHUNK) issue(g0 + q + GE::NST, q + GE::NST, zb);
-        }
-        split_reduce<TPW, SK>(acc, tile0, slice);
+        stream_product<TL>(acc, sm.panel, GE::LDP, GE::CH1, q, g0, zb);
         if (slice == 0) {
 #pragma unroll
           for (int j = 0; j < TPW; ++j) {
-            const int nt = (tile0 + j) % GE::NTN;
+            const int nt = (tile0 + j) % TL::NTN;
 #pragma unroll
             for (int i = 0; i < 4; ++i) {
               const int r = frag_row(lane, i), col = nt * 8 + frag_col(lane, i);
@@ -316,65 +383,14 @@ struct Rhs {
       }
     }
     __syncthreads();
-    // ------------------------------------------------------------------ G2
-    {
-      constexpr int TPW = GE::TPW2, SK = GE::SK2;
-      const int tile0 = SK > 1 ? warp / SK : warp * TPW;
-      const int slice = SK > 1 ? warp % SK : 0;
-      for (int c = 0; c < 7; ++c) {
-        const int s = ins_src(c);
-        const double cs = src * ins_coef(c);
-        // A' = [jac X_c | jac P_c + src coef_c X_s] on this CTA's rows
-        for (int e = tid; e < 16 * DP; e += GE::NT) {
-          const int r = e / DP, col = e % DP;
-          const size_t off = (size_t)(row0 + r) * DP + col;
-          const double2 x = zb[(size_t)c * GE::MAT + off];
-          double2 m = zscale(jac, st->P[(size_t)c * GE::MAT + off]);
-          if (s >= 0) m = zaxpy(cs, zb[(size_t)s * GE::MAT + off], m);
-          sm.aprime[r * GE::LDA2 + col] = zscale(jac, x);
-          sm.aprime[r * GE::LDA2 + DP + col] = m;
-        }
-        __syncthreads();
-        ZFrag acc[TPW];
-#pragma unroll
-        for (int j = 0; j < TPW; ++j) acc[j].zero();
-        for (int ch = 0; ch < GE::CH2; ++ch, ++q) {
-          const double2* B = await(g0 + q);
-#pragma unroll
-          for (int ks = 0; ks < GE::KC / 8; ++ks) {
-            const int kstep = ch * (GE::KC / 8) + ks;
-            if (kstep % SK != slice) continue;
-            double ar[4], ai[4], nai[4];
-            load_a(sm.aprime, GE::LDA2, 0, kstep * 8, lane, ar, ai, nai);
-#pragma unroll
-            for (int j = 0; j < TPW; ++j) {
-              const int nt = tile0 + j;
-              double br[2], bi[2];
-              load_b(B, DP, ks * 8, nt * 8, lane, br, bi);
-              zmma(acc[j], ar, ai, nai, br, bi);
-            }
-          }
-          __syncthreads();
-          if (tid == 0 && q + GE::NST < GE::NCHUNK) issue(g0 + q + GE::NST, q + GE::NST, zb);
-        }
-        split_reduce<TPW, SK>(acc, tile0, slice);
-        if (slice == 0) {
-          const double2* fixed = c == 0 ? st->fixed0 : c == 6 ? st->fixed6 : nullptr;
-#pragma unroll
-          for (int j = 0; j < TPW; ++j) {
-            const int nt = tile0 + j;
-#pragma unroll
-            for (int i = 0; i < 4; ++i) {
-              const int r = frag_row(lane, i), col = nt * 8 + frag_col(lane, i);
-              const size_t loc = (size_t)(row0 + r) * DP + col;
-              const size_t off = (size_t)c * GE::MAT + loc;
-              double2 v = zadd(make_double2(acc[j].re[i], acc[j].im[i]), kout[off]);
-              if (s >= 0) v = zaxpy(cs, st->P[(size_t)s * GE::MAT + loc], v);
-              if (fixed) v = zaxpy(src, fixed[loc], v);
-              kout[off] = v;
-            }
-          }
-        }
+    // ------------------------------------------------------------------ G2 passes
+    for (int p = 0; p < GE::NPASS; ++p) {
+      const int first = GE::pass_first(p);
+      if constexpr (GE::GS == 2) {
+        if (GE::pass_count(p) == 2) g2_pass<2>(first, zb, kout, jac, src, q, g0);
+        else g2_pass<1>(first, zb, kout, jac, src, q, g0);
+      } else {
+        g2_pass<1>(first, zb, kout, jac, src, q, g0);
       }
     }
     *gq = g0 + GE::NCHUNK;
@@ -422,21 +438,15 @@ trajectory_kernel(const TrajState* __restrict__ states, const double* __restrict
     C.src[0] = source_value(-ctl_in.endpoint);
     for (int i = 0; i < 16; ++i) { C.ksc[i] = 0.0; sm.kscp[i] = 0.0; }
   }
-  if constexpr (GE::RESIDENT) {
-    Rhs<DP> tmp{st, sm, row0, tid, lane, warp, &gq};
-    tmp.load_panel(0, sm.panel);
-    tmp.load_panel(1, sm.panel + 32 * GE::LDP);
-  }
   __syncthreads();
   Rhs<DP> rhs{st, sm, row0, tid, lane, warp, &gq};
 
-  // slot permutation: kslot[s] is the k buffer of stage s; y and proposed swap on acceptance
-  int kslot[16];
-#pragma unroll
-  for (int i = 0; i < 16; ++i) kslot[i] = i;
+  // slot permutation: C.kslot[s] is the k buffer of stage s; y and proposed swap on acceptance
+  if (tid < 16) C.kslot[tid] = tid;
+  __syncthreads();
   double2* ybuf = st->y;
   double2* pbuf = st->prop;
-  auto kb = [&](int s) { return st->k + (size_t)kslot[s] * GE::VEC; };
+  auto kb = [&](int s) { return st->k + (size_t)C.kslot[s] * GE::VEC; };
   long long zcount = 0;
   auto zb = [&](long long n) { return st->z + (size_t)(n & 1) * GE::VEC; };
 
@@ -486,13 +496,21 @@ trajectory_kernel(const TrajState* __restrict__ states, const double* __restrict
       const int terms = s;   // a[s][0..s-1], b[0..11]
       double2* z = zb(zcount);
       double part = 0.0, dummy = 0.0;
+      const double2* kp[12];
+      double ha[12];
+#pragma unroll
+      for (int j = 0; j < 12; ++j) {
+        kp[j] = kb(j);
+        ha[j] = j < terms ? h * w[j] : 0.0;
+      }
       for (int e = tid; e < GE::OWN; e += GE::NT) {
         const size_t off = own_offset<DP>(e, row0);
+        double2 kv[12];
+#pragma unroll
+        for (int j = 0; j < 12; ++j) kv[j] = ha[j] != 0.0 ? __ldcg(kp[j] + off) : make_double2(0.0, 0.0);
         double2 v = ybuf[off];
-        for (int j = 0; j < terms; ++j) {
-          const double a = w[j];
-          if (a != 0.0) v = zaxpy(h * a, kb(j)[off], v);
-        }
+#pragma unroll
+        for (int j = 0; j < 12; ++j) v = zaxpy(ha[j], kv[j], v);
         z[off] = v;
         if (s == 12) pbuf[off] = v;
         if (e / (16 * DP) == 2) {
@@ -653,11 +671,11 @@ trajectory_kernel(const TrajState* __restrict__ states, const double* __restrict
       double2* tmp = ybuf;
       ybuf = pbuf;
       pbuf = tmp;
-      const int k0 = kslot[0];
-      kslot[0] = kslot[12];
-      kslot[12] = k0;
       __syncthreads();
       if (tid == 0) {
+        const int k0 = C.kslot[0];
+        C.kslot[0] = C.kslot[12];
+        C.kslot[12] = k0;
         C.y_sc = C.prop_sc;
         C.ksc[0] = C.ksc[12];
         C.t = C.t_new;
