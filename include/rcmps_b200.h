@@ -137,6 +137,25 @@ int rcmps_finish_gradient_batch(rcmps_context* context, int n_states, const int*
                                 const double* environment, const rcmps_settings* settings, double* gradient,
                                 rcmps_state_stats* stats, void* stream);
 
+/* rcmps_finish_gradient_batch for ONE state, without allocating anything: no cudaMalloc, no
+ * cudaFree, no pinned host buffer. No counterpart in the reference. It serves callers that may
+ * not allocate at the moment they need the finished gradient: a host whose memory planner
+ * reserves all device memory up front (a serving process, or a framework whose caching
+ * allocator owns the device), a plugin callback that must not allocate, or a process near its
+ * memory limit where an allocation in the middle of an optimizer step would fail or stall.
+ * Its workspace is one fixed 2 MiB array in the library's device image, so it supports
+ * 1 <= d <= 32 only; larger d returns RCMPS_INVALID_ARGUMENT with a message naming the limit.
+ * The first call on each device looks up that array's device address (cudaGetSymbolAddress),
+ * so make the first call before any stream capture begins. All calls share the one array:
+ * calls that overlap on the GPU (different streams or host threads) race on it, and the
+ * caller must order them. Each call clears what must start at zero (the Poisson solution and
+ * the status words). Arguments are those of rcmps_finish_gradient_batch with n_states = 1:
+ * R, K, rho, covector, environment and gradient are d x d device matrices. */
+int rcmps_finish_gradient_noalloc(rcmps_context* context, int d, const double* R, const double* K,
+                                  const double* rho, const double* covector, const double* environment,
+                                  const rcmps_settings* settings, double* gradient, rcmps_state_stats* stats,
+                                  void* stream);
+
 /* Stationary density rho of (Q, R) by GMRES on -L(X) + tr(X) I/D = I/D, on device memory.
  * Replaces stationary_state(q, r, tolerance) -> (rho, stats) (runtime/numerics.py:74-100). */
 int rcmps_stationary_state_batch(rcmps_context* context, int n_states, const int* dims, const double* R,
