@@ -217,7 +217,7 @@ def run_b200(args, rank, world, local_rank):
     traj_ms, pull_ms, kin_ms, fin_ms = [], [], [], []
     barrier()
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    launches0 = lib.rcmps_launch_count()
+    launches0 = lib.rcmps_launch_count()   # library launches before the timed region
     with ClockSampler(local_rank) as clocks:
         start.record(stream)
         for _ in range(args.steps):
@@ -243,13 +243,16 @@ def run_b200(args, rank, world, local_rank):
     traj = statistics.mean(traj_ms)
     achieved = flops / (traj / 1000.0) / 1e12
     peak = lib.rcmps_fp64_peak_tflops(ctx.handle)
+    # DRAM traffic of one launch: bytes per right-hand side of one state from an ncu capture of a
+    # smaller case at the same D, times this launch's right-hand sides (traffic grows with them)
     traffic = None
     tf = ROOT / "profiles" / "trajectory_traffic.json"
     if tf.exists():
         try:
             rec = json.loads(tf.read_text())
-            if rec.get("workload") == args.workload:
-                traffic = rec.get("dram_bytes_per_launch")
+            per = rec.get("dram_bytes_per_state_rhs", {})
+            if all(str(d) in per for d in dims):
+                traffic = sum(per[str(dims[i])] * rhs_calls[i] for i in range(n))
         except (OSError, ValueError):
             traffic = None
 
@@ -305,6 +308,7 @@ def run_b200(args, rank, world, local_rank):
                                     statistics.mean(stats[i].accepted for i in range(n))},
                 "gpu_launches": None, "gpu_launches_note": "library kernel launches per step (rcmps_launch_count)", "clocks": clocks.summary(), "e2e": e2e, "cpu_baseline": cpu}
         line["gpu_launches"] = launches
+        line["launches_before_timed"] = launches0
         print(json.dumps(line), flush=True)
 
 

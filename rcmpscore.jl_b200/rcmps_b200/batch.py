@@ -43,7 +43,8 @@ def z2_state(d, seed, scale=0.2):
 def config_states(name):
     """(R list, K list, couplings, description) of a named workload.
     d64_mixed: 16 random (seeds 0..15) + 16 Z2 (seeds 100..115) states at D = 64, g = 2;
-    d32_batch: 64 random D = 32 states (seeds 0..63), g ~ U[0.5, 3] (seed 12345)."""
+    d32_batch: 64 random D = 32 states (seeds 0..63), g ~ U[0.5, 3] (seed 12345);
+    d64_pair: the first random and the first Z2 state of d64_mixed (a small profiling case)."""
     if name == "d64_mixed":
         R, K = [], []
         for s in range(16):
@@ -55,6 +56,9 @@ def config_states(name):
             R.append(r)
             K.append(k)
         return R, K, [2.0] * 32, "32 states D=64: 16 random + 16 Z2 (scaling 0.2), g=2"
+    if name == "d64_pair":
+        (r0, k0), (r1, k1) = random_state(64, 0), z2_state(64, 100)
+        return [r0, r1], [k0, k1], [2.0, 2.0], "2 states D=64: 1 random + 1 Z2 (scaling 0.2), g=2"
     if name == "d32_batch":
         R, K = zip(*(random_state(32, s) for s in range(64)))
         g = np.random.default_rng(12345).uniform(0.5, 3.0, 64)
