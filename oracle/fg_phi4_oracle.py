@@ -308,6 +308,132 @@ def evaluate_quartic(r, q, rho, g=1.0, *, half_window=30.0, n_quad=512, atol=1e-
     return out
 
 
+# --------------------------------------------------------------------------- full ODE route
+
+# Channel specs of the all-ODE evaluation (ode_backend.py:60-73, 851-858; Julia's default
+# kinetic_backend=:ode, src/observables.jl:131-159): (channels, edges, commutator) with edges
+# (source, destination, side, coefficient), side "L" a left insertion O X, "R" a right one X O^dag.
+_SQRT2 = math.sqrt(2.0)
+KINETIC_EDGES = ((0, 1, "L", _SQRT2), (0, 2, "R", _SQRT2), (2, 3, "L", _SQRT2), (1, 3, "R", _SQRT2))
+QUARTIC_EDGES = tuple((k, k + 1, side, float(k + 1)) for k in range(4) for side in ("L", "R"))
+FULL_SPECS = ((4, KINETIC_EDGES, False), (4, KINETIC_EDGES, True), (5, QUARTIC_EDGES, False))
+
+
+class FullSystem:
+    """The 26 D x D channels of kinetic1 + kinetic2 + phi^4 as ODEs (ode_backend.py:76-167).
+
+    Forward channels 0..12 (specs at offsets 0, 4, 8), adjoint channels 13..25. Channel k has
+    (ql, rl, ol) = (Q, R, O) forward or (Q^dag, R^dag, O^dag) adjoint, O = R or the commutator
+    [Q, R] of its spec, and
+        dX_k/dt = jac (ql X_k + X_k ql^dag + rl X_k rl^dag)
+                  + src (sum_{left (a, c)} c ol_a X_a + sum_{right (b, c)} c X_b ol_b^dag).
+    A forward edge a -> b (side, c) inserts into forward b; its trace dual inserts adjoint b
+    into adjoint a on the other side (ode_backend.py:108-113). Initial values: rho in each
+    spec's first forward channel, I in its last adjoint channel, zero elsewhere."""
+
+    def __init__(self, q, r, rho, specs=FULL_SPECS):
+        self.q, self.r, self.rho = (np.asarray(x, dtype=np.complex128) for x in (q, r, rho))
+        self.d = d = len(self.q)
+        self.specs = specs
+        self.offsets = list(np.cumsum([0] + [sp[0] for sp in specs])[:-1])
+        self.half = half = sum(sp[0] for sp in specs)
+        self.channels = 2 * half
+        self.size = self.channels * d * d
+        comm = self.q @ self.r - self.r @ self.q
+        self.ops = [None] * self.channels
+        self.left = [[] for _ in range(self.channels)]
+        self.right = [[] for _ in range(self.channels)]
+        for off, (nch, edges, commutator) in zip(self.offsets, specs):
+            op = comm if commutator else self.r
+            for i in range(nch):
+                self.ops[off + i] = (self.q, self.r, op)
+                self.ops[half + off + i] = (adj(self.q), adj(self.r), adj(op))
+            for src, dst, side, coef in edges:
+                (self.left if side == "L" else self.right)[off + dst].append((off + src, coef))
+                (self.right if side == "L" else self.left)[half + off + src].append((half + off + dst, coef))
+        self.calls = 0
+
+    def initial(self):
+        d = self.d
+        y = np.zeros((self.channels, d, d), complex)
+        for off, (nch, _, _) in zip(self.offsets, self.specs):
+            y[off] = self.rho
+            y[self.half + off + nch - 1] = np.eye(d)
+        return y.reshape(-1)
+
+    def __call__(self, t, y, src=None):
+        self.calls += 1
+        d = self.d
+        jac = 2.0 * abs(t)
+        src = source(t) if src is None else src
+        x = y.reshape(self.channels, d, d)
+        out = np.empty_like(x)
+        for k in range(self.channels):
+            ql, rl, _ = self.ops[k]
+            value = jac * (ql @ x[k] + x[k] @ adj(ql) + rl @ x[k] @ adj(rl))
+            for a, coef in self.left[k]:
+                value = value + (src * coef) * (self.ops[a][2] @ x[a])
+            for b, coef in self.right[k]:
+                value = value + (src * coef) * (x[b] @ adj(self.ops[b][2]))
+            out[k] = value
+        return out.reshape(-1)
+
+
+def full_pullback(system, samples, points, weights, coefficients):
+    """Value, covector and environment of every spec, summed with `coefficients`
+    (ode_backend.py:589-619, 834-838; src/observables.jl:161-199). Per spec, with forward
+    samples f_k at node i, adjoint samples b_k at node n-1-i, w_i = weights_i 2|t_i| and
+    j_i = weights_i source(t_i):
+        m  = sum_i w_i sum_k f_k (R^dag b_k - b_k R^dag),  nn = sum_i w_i sum_k (b_k R - R b_k) f_k,
+        u  = sum_{left edges} c sum_i j_i f_src b_dst,     v  = sum_{right edges} c sum_i j_i b_dst f_src;
+    a commutator spec adds u Q - Q u - R u R^dag + u R R^dag to m and
+    Q^dag v - v Q^dag - R v R^dag + R R^dag v to nn, the others u and v;
+    covector = (m + nn^dag)/2, environment = Herm(first adjoint channel at the endpoint),
+    value = Re tr(last forward channel at the endpoint)."""
+    d, n = system.d, len(points)
+    q, r = system.q, system.r
+    rh = adj(r)
+    mats = samples.reshape(len(samples), system.channels, d, d)
+    wi = np.asarray(weights) * 2.0 * np.abs(points)
+    ji = np.asarray(weights) * np.array([source(t) for t in points])
+    total_value, total_cov, total_env = 0.0, np.zeros((d, d), complex), np.zeros((d, d), complex)
+    for coefficient, off, (nch, edges, commutator) in zip(coefficients, system.offsets, system.specs):
+        f = mats[:n, off:off + nch]
+        b = mats[n - 1::-1, system.half + off:system.half + off + nch]
+        m = np.einsum("i,ikab,ikbc->ac", wi, f, rh @ b - b @ rh)
+        nn = np.einsum("i,ikab,ikbc->ac", wi, b @ r - r @ b, f)
+        u = np.zeros((d, d), complex)
+        v = np.zeros((d, d), complex)
+        for src, dst, side, coef in edges:
+            if side == "L":
+                u += coef * np.einsum("i,iab,ibc->ac", ji, f[:, src], b[:, dst])
+            else:
+                v += coef * np.einsum("i,iab,ibc->ac", ji, b[:, dst], f[:, src])
+        if commutator:
+            m += u @ q - q @ u - r @ u @ rh + u @ r @ rh
+            nn += adj(q) @ v - v @ adj(q) - r @ v @ rh + r @ rh @ v
+        else:
+            m += u
+            nn += v
+        env = mats[-1, system.half + off]
+        total_value += coefficient * float(np.trace(mats[-1, off + nch - 1]).real)
+        total_cov += coefficient * (m + adj(nn)) / 2.0
+        total_env += coefficient * (env + adj(env)) / 2.0
+    return total_value, total_cov, total_env
+
+
+def evaluate_phi4(r, q, rho, g, *, half_window=20.0, n_quad=192, atol=1e-13, rtol=1e-12,
+                  max_steps=1_000_000):
+    """kinetic1 + kinetic2 + g phi^4 entirely by ODEs: value, raw covector, environment
+    (ode_backend.py:851-858, the objective's --mode ode, sweep_driver.py:90-92)."""
+    system = FullSystem(q, r, rho)
+    points, weights = quadrature(half_window, n_quad)
+    nodes = np.r_[points, math.sqrt(half_window)]
+    samples, stats = integrate(system, nodes, atol=atol, rtol=rtol, max_steps=max_steps)
+    value, cov, env = full_pullback(system, samples, points, weights, (1.0, 1.0, float(g)))
+    return dict(value=value, covector=cov, environment=env, stats=stats)
+
+
 # --------------------------------------------------------------------------- kinetic
 
 def _vec(x):

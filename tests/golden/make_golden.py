@@ -6,6 +6,9 @@ This script imports the reference package rcmps_gpu read-only from a local check
   d16.npz       one D = 16 random state at the optimizer defaults (W = 30, n_quad = 512, 512 nodes)
   d64.npz       the seed-42 D = 64 random state at the optimizer defaults
   samples_d5.npz  trajectory samples of the reduced quartic system, D = 5, W = 2, n_quad = 16
+  ode.npz       the all-ODE route (evaluate_phi4: kinetic1 + kinetic2 + g phi^4 as 26 channels):
+                D = 3 (W = 6, n_quad = 24), D = 8 random and Z2 (W = 20, n_quad = 64) and
+                D = 16 (W = 20, n_quad = 192, the Julia defaults of the fixture)
 Each state record holds R, K, rho (the reference's stationary_state at tolerance 1e-13), the
 coupling, the settings, and the reference outputs: quartic value/covector/environment and its
 DOP853 step counts, kinetic value/covector/environment, the summed energy and the finished
@@ -14,7 +17,8 @@ is the reference's test/fixtures/phi4_g2_D16_z2_portable (exported by RcmpsCore 
 
 States: NumPy PCG64 default_rng(seed); R and A with i.i.d. standard complex Gaussian entries
 times 0.2 (R drawn first), K = (A + A^dag)/2; Z2 states draw blocks in the order k1, k2, R12, R21.
-Run: python tests/golden/make_golden.py  (about a minute; the D = 64 record dominates)
+Run: python tests/golden/make_golden.py [name ...]  (all files by default, about a minute; the
+D = 64 record dominates; names: small d16 d64 samples ode)
 """
 from __future__ import annotations
 
@@ -72,6 +76,17 @@ def evaluate(r, k, g, window, nq, nodes):
                 energy=quartic["value"] + kinetic["value"], gradient=grad)
 
 
+def evaluate_ode(r, k, g, window, nq):
+    q = -1j * k - r.conj().T @ r / 2
+    rho, _ = nm.stationary_state(q, r, tolerance=1e-13)
+    out = ob.evaluate_phi4(r, q, rho, g, xp=np, half_window=window, n_quad=nq, atol=1e-13, rtol=1e-12)
+    grad, _ = nm.finish_gradient(q, r, rho, out["covector"], out["environment"], metric_reg=1e-3)
+    return dict(R=r, K=k, rho=rho, g=g, window=window, n_quad=nq, value=out["value"],
+                covector=out["covector"], environment=out["environment"],
+                accepted=out["stats"]["accepted_steps"], rejected=out["stats"]["rejected_steps"],
+                gradient=grad)
+
+
 def save(name, records):
     flat = {}
     for i, rec in enumerate(records):
@@ -81,13 +96,27 @@ def save(name, records):
     np.savez_compressed(HERE / name, **flat)
 
 
-def main():
+def main(names):
     t0 = time.time()
-    small = [evaluate(*random_state(d, 500 + d), 0.5 + 0.5 * i, 30.0, 64, 128) for i, d in enumerate((4, 6, 8))]
-    small.append(evaluate(*z2_state(8, 508), 2.0, 30.0, 64, 128))
-    save("small.npz", small)
-    save("d16.npz", [evaluate(*random_state(16, 16), 2.0, 30.0, 512, 512)])
-    save("d64.npz", [evaluate(*random_state(64, 42), 2.0, 30.0, 512, 512)])
+    if "small" in names:
+        small = [evaluate(*random_state(d, 500 + d), 0.5 + 0.5 * i, 30.0, 64, 128) for i, d in enumerate((4, 6, 8))]
+        small.append(evaluate(*z2_state(8, 508), 2.0, 30.0, 64, 128))
+        save("small.npz", small)
+    if "d16" in names:
+        save("d16.npz", [evaluate(*random_state(16, 16), 2.0, 30.0, 512, 512)])
+    if "d64" in names:
+        save("d64.npz", [evaluate(*random_state(64, 42), 2.0, 30.0, 512, 512)])
+    if "ode" in names:
+        save("ode.npz", [evaluate_ode(*random_state(3, 703), 1.5, 6.0, 24),
+                         evaluate_ode(*random_state(8, 708), 2.0, 20.0, 64),
+                         evaluate_ode(*z2_state(8, 718), 2.5, 20.0, 64),
+                         evaluate_ode(*random_state(16, 716), 2.0, 20.0, 192)])
+    if "samples" in names:
+        samples_d5()
+    print(f"golden vectors written in {time.time() - t0:.1f} s")
+
+
+def samples_d5():
     # trajectory samples of the reduced system (the persistent kernel's channels)
     r, k = random_state(5, 5)
     q = -1j * k - r.conj().T @ r / 2
@@ -98,8 +127,7 @@ def main():
                                    max_steps=100000)
     np.savez_compressed(HERE / "samples_d5.npz", R=r, K=k, rho=rho, window=2.0, n_quad=16, samples=samples,
                         accepted=stats["accepted_steps"], rejected=stats["rejected_steps"])
-    print(f"golden vectors written in {time.time() - t0:.1f} s")
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:] or ["small", "d16", "d64", "ode", "samples"])

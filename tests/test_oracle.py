@@ -75,6 +75,36 @@ def test_oracle_matches_julia_fixture():
     assert math.sqrt(max(0.0, O.metric(fx["rho"], diff, diff))) < 5e-9
 
 
+@pytest.mark.parametrize("index", range(4))
+def test_oracle_ode_route_matches_reference(index):
+    """The all-ODE route (26 channels: kinetic1, kinetic2 and g phi^4) against the reference's
+    evaluate_phi4 + finish_gradient (ode_backend.py:851-858)."""
+    rec = load_records("ode.npz")[index]
+    R, K, rho, g = rec["R"], rec["K"], rec["rho"], rec["g"]
+    Q = O.left_canonical_q(R, K)
+    out = O.evaluate_phi4(R, Q, rho, g, half_window=rec["window"], n_quad=int(rec["n_quad"]))
+    assert (out["stats"]["accepted"], out["stats"]["rejected"]) == (rec["accepted"], rec["rejected"])
+    assert abs(out["value"] - rec["value"]) <= 1e-12 * max(1.0, abs(rec["value"]))
+    assert rel(out["covector"], rec["covector"]) < 1e-11
+    assert rel(out["environment"], rec["environment"]) < 1e-11
+    grad = O.finish_gradient(Q, R, rho, out["covector"], out["environment"])
+    diff = grad - rec["gradient"]
+    assert math.sqrt(max(0.0, O.metric(rho, diff, diff))) < 1e-10 * max(1.0, math.sqrt(O.metric(rho, grad, grad)))
+
+
+def test_oracle_ode_route_matches_julia_fixture():
+    """Julia's default evaluation is this all-ODE route (Vern7 there, DOP853 here) at the
+    fixture's settings: energy -0.15648780475169466 to 1e-12, gradient to 5e-9 (metric norm)."""
+    fx = julia_fixture()
+    R, K, rho = fx["R"], fx["K"], fx["rho"]
+    Q = O.left_canonical_q(R, K)
+    out = O.evaluate_phi4(R, Q, rho, fx["meta"]["coupling"], half_window=20.0, n_quad=192)
+    assert abs(out["value"] - fx["meta"]["energy"]) < 1e-12
+    grad = O.finish_gradient(Q, R, rho, out["covector"], out["environment"])
+    diff = grad - fx["gradient"]
+    assert math.sqrt(max(0.0, O.metric(rho, diff, diff))) < 5e-9
+
+
 def test_source_and_quadrature():
     assert abs(O.source(0.0) - 1 / math.sqrt(math.pi)) < 1e-16
     assert abs(O.source(1e-9) - O.source(0.0)) < 1e-8
