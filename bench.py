@@ -91,71 +91,60 @@ class ClockSampler:
 
 
 # ----------------------------------------------------------------------------- CPU oracle sample
-def _cpu_sample(args):
-    """Bounded sample of one state's fg_phi4 on one core with the oracle: `n_rhs` right-hand sides of
-    the quartic system, `n_nodes` pullback nodes and the full kinetic term, scaled to one evaluation
-    by the step/node counts of the same state on the GPU (rhs_calls, 1024 nodes). The boundary and
-    metric solve (under 1% of the reference's CPU time at D = 64) is not sampled."""
-    d, seed, z2, g, rhs_calls, n_rhs, n_nodes = args
-    os.environ.setdefault("OPENBLAS_NUM_THREADS", "1")
+def _cpu_eval(args):
+    """One full fg_phi4 evaluation (quartic trajectory + pullback, kinetic, boundary/metric
+    solve) of one workload state with the oracle on one core; returns its seconds. rho is
+    computed first, untimed, as the B200 arm computes it before its timed region."""
+    d, seed, z2, g = args
     sys.path[:0] = [str(ROOT), str(ROOT / "rcmpscore.jl_b200")]
+    from threadpoolctl import threadpool_limits
     from oracle import fg_phi4_oracle as O
     from rcmps_b200.batch import random_state, z2_state
-    R, K = (z2_state if z2 else random_state)(d, seed)
-    Q = O.left_canonical_q(R, K)
-    rho = O.stationary_state(Q, R) if d <= 32 else np.eye(d, dtype=complex) / d
-    system = O.QuarticSystem(Q, R, rho)
-    rng = np.random.default_rng(1)
-    y = (rng.standard_normal(system.size) + 1j * rng.standard_normal(system.size)) * 1e-3
-    t0 = time.perf_counter()
-    for i in range(n_rhs):
-        system(-2.0 + 0.01 * i, y)
-    t_rhs = (time.perf_counter() - t0) / n_rhs
-    samples = np.tile(y, (2 * n_nodes + 1, 1))
-    pts, wts = O.quadrature(30.0, n_nodes)
-    t0 = time.perf_counter()
-    O.quartic_pullback(system, samples, pts, wts)
-    t_node = (time.perf_counter() - t0) / (2 * n_nodes)
-    t0 = time.perf_counter()
-    O.kinetic_raw(Q, R, rho, 512)
-    t_kin = time.perf_counter() - t0
-    return rhs_calls * t_rhs + 1024 * t_node + t_kin, dict(t_rhs=t_rhs, t_node=t_node, t_kinetic=t_kin)
+    with threadpool_limits(limits=1):   # one core per evaluation: BLAS single-threaded
+        R, K = (z2_state if z2 else random_state)(d, seed)
+        Q = O.left_canonical_q(R, K)
+        rho = O.stationary_state(Q, R, tolerance=1e-13, method="krylov")
+        t0 = time.perf_counter()
+        O.fg_phi4(R, K, rho, g, method="krylov")
+        return time.perf_counter() - t0
 
 
-def cpu_sample_plan(dims, rhs_calls):
-    return [(dims[i], i if i < 16 else 100 + (i - 16), i >= 16, 2.0, int(rhs_calls[i]), 24, 8) for i in range(len(dims))]
+def cpu_eval_plan(workload):
+    """(d, seed, z2, g) of every state of d64_mixed (the seeds of rcmps_b200.batch)."""
+    if workload != "d64_mixed":
+        return None
+    return [(64, i, False, 2.0) for i in range(16)] + [(64, 100 + i, True, 2.0) for i in range(16)]
 
 
 # ----------------------------------------------------------------------------- reference arm
 def run_reference(args, rank, world):
+    """The oracle (the NumPy restatement of the reference's path) on the host cores: one state per
+    worker process and step, every evaluation complete; rank 0 only."""
     if rank != 0:
         return
     import multiprocessing as mp
     cores = os.cpu_count() or 1
     from rcmps_b200.batch import config_states
-    R, K, g, desc = config_states("d64_mixed")
-    dims = [len(r) for r in R]
-    # step counts of these states (measured on B200 by the b200 arm; a typical count if absent)
-    rhs = [6800] * len(dims)
-    plan = cpu_sample_plan(dims, rhs)
+    desc = config_states(args.workload)[3]
+    plan = cpu_eval_plan(args.workload)
     workers = min(cores, len(plan))
+    for var in ("OPENBLAS_NUM_THREADS", "OMP_NUM_THREADS", "MKL_NUM_THREADS"):
+        os.environ[var] = "1"      # inherited by the spawned workers: one core each
     ctx = mp.get_context("spawn")
-    times = []
+    walls = []
     with ctx.Pool(workers) as pool:
         for step in range(args.warmup + args.steps):
+            chunk = [plan[(step * workers + i) % len(plan)] for i in range(workers)]
             t0 = time.perf_counter()
-            res = pool.map(_cpu_sample, plan[:workers])
+            pool.map(_cpu_eval, chunk)
             wall = time.perf_counter() - t0
             if step >= args.warmup:
-                times.append((wall, [r[0] for r in res]))
-    # evals/s on all cores: each worker produced one (scaled) evaluation per estimated eval time
-    per_eval = [statistics.mean(t for _, ts in times for t in ts)]
-    value = workers / per_eval[0]
-    sample = (f"per worker one D=64 state: 24 quartic right-hand sides, 16 pullback nodes and the full kinetic term "
-              f"timed with the oracle, scaled to one evaluation with 6800 right-hand sides and 1024 nodes; "
-              f"{workers} workers")
+                walls.append(wall)
+    value = workers * len(walls) / sum(walls)
+    sample = (f"each step: {workers} workload states, one complete fg_phi4 evaluation per worker process "
+              f"(oracle, single-threaded BLAS), states taken in turn from the {len(plan)}-state workload")
     line = {"metric": METRIC, "value": value, "unit": "evals/s", "impl": "reference", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * statistics.mean(w for w, _ in times),
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * statistics.mean(walls),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": desc, "half_window": 30.0, "n_quad": 512, "kinetic_nodes": 512},
             "cpu_baseline": {"value": value, "unit": "evals/s", "cores": workers, "kind": "port", "sample": sample},
@@ -200,11 +189,18 @@ def run_b200(args, rank, world, local_rank):
     stream = torch.cuda.current_stream()
     sptr = C.c_void_p(stream.cuda_stream)
 
+    quartic_only = args.component == "quartic"
+    cov = torch.zeros(total, dtype=torch.complex128, device="cuda") if quartic_only else None
+
     def step():
-        rc = lib.rcmps_fg_phi4_batch(ctx.handle, n, cdims, cg, dR.data_ptr(), dK.data_ptr(), drho.data_ptr(),
-                                     C.byref(s), energy.data_ptr(), grad.data_ptr(), None, None, stats, sptr)
+        if quartic_only:   # the quartic term alone (trajectory + pullback): the small profiling case
+            rc = lib.rcmps_quartic_batch(ctx.handle, n, cdims, cg, dR.data_ptr(), dK.data_ptr(), drho.data_ptr(),
+                                         C.byref(s), energy.data_ptr(), cov.data_ptr(), grad.data_ptr(), stats, sptr)
+        else:
+            rc = lib.rcmps_fg_phi4_batch(ctx.handle, n, cdims, cg, dR.data_ptr(), dK.data_ptr(), drho.data_ptr(),
+                                         C.byref(s), energy.data_ptr(), grad.data_ptr(), None, None, stats, sptr)
         if rc:
-            raise RuntimeError(f"fg_phi4 failed: {_lib.STATUS_NAMES.get(rc)} {ctx.error()}")
+            raise RuntimeError(f"{args.component} failed: {_lib.STATUS_NAMES.get(rc)} {ctx.error()}")
 
     def barrier():
         torch.cuda.synchronize()
@@ -258,7 +254,7 @@ def run_b200(args, rank, world, local_rank):
 
     # end to end through the host-buffer C entry: copies of inputs and results inside the timed region
     e2e = None
-    if True:
+    if not quartic_only:
         hR = torch.from_numpy(np.concatenate([x.ravel() for x in R])).pin_memory()
         hK = torch.from_numpy(np.concatenate([x.ravel() for x in K])).pin_memory()
         hP = drho.cpu().pin_memory()
@@ -282,15 +278,15 @@ def run_b200(args, rank, world, local_rank):
                "h2d_bytes_per_step": 3 * total * 16 * world, "d2h_bytes_per_step": (n * 8 + total * 16) * world}
 
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        t_eval, parts = _cpu_sample(cpu_sample_plan(dims, rhs_calls)[0])
+    plan = cpu_eval_plan(args.workload)
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and plan:
+        t_eval = _cpu_eval(plan[0])
         cpu = {"value": 1.0 / t_eval, "unit": "evals/s", "cores": 1, "kind": "port",
-               "sample": (f"state 0 (D={dims[0]}): 24 quartic right-hand sides, 16 pullback nodes and the full kinetic "
-                          f"term timed with the oracle on one core, scaled to its {rhs_calls[0]} right-hand sides "
-                          f"and 1024 nodes (t_rhs {parts['t_rhs'] * 1e3:.2f} ms, t_node {parts['t_node'] * 1e3:.2f} ms, "
-                          f"t_kinetic {parts['t_kinetic']:.2f} s)")}
+               "sample": (f"one complete fg_phi4 evaluation of workload state 0 (D={plan[0][0]}, random, seed "
+                          f"{plan[0][1]}) with the oracle on one core: {t_eval:.1f} s")}
     if rank == 0:
-        line = {"metric": METRIC, "value": value, "unit": "evals/s", "n_gpus": world, "steps": args.steps,
+        metric = METRIC if not quartic_only else "quartic term (trajectory + pullback) evals/s at D=64, FP64"
+        line = {"metric": metric, "value": value, "unit": "evals/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": elapsed / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
                 "config": {"workload": desc, "states_per_gpu": n, "half_window": 30.0, "n_quad": 512,
@@ -320,6 +316,8 @@ def main():
     p.add_argument("--impl", choices=("b200", "reference"), default="b200")
     p.add_argument("--workload", default="d64_mixed")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--component", choices=("fg", "quartic"), default="fg",
+                   help="time the whole evaluation (default) or the quartic term alone")
     args = p.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

@@ -114,6 +114,18 @@ int rcmps_quartic_batch(rcmps_context* context, int n_states, const int* dims, c
                         double* value, double* covector, double* environment, rcmps_state_stats* stats,
                         void* stream);
 
+/* All three terms (kinetic1 + kinetic2 + g phi^4) by ODEs: value, raw covector and environment,
+ * on device memory. The 26-channel system is integrated by the same DOP853 controller and
+ * pulled back per channel spec. Replaces evaluate_phi4(R, Q, rho, g, ...) -> dict(value,
+ * covector, environment, stats) (runtime/ode_backend.py:851-858), the objective's --mode ode
+ * (runtime/sweep_driver.py:90-92) and Julia's default kinetic_backend=:ode
+ * (src/observables.jl:131-159). stats[i].quartic_value holds the total value of state i and
+ * kinetic_value stays 0. Follow with rcmps_finish_gradient_batch for the finished gradient. */
+int rcmps_phi4_ode_batch(rcmps_context* context, int n_states, const int* dims, const double* couplings,
+                         const double* R, const double* K, const double* rho, const rcmps_settings* settings,
+                         double* value, double* covector, double* environment, rcmps_state_stats* stats,
+                         void* stream);
+
 /* The trajectory alone, for one state: samples [2 n_quad + 1][7 d^2 + 1] complex (the seven
  * channels at every Gauss node and the endpoint, and the scalar channel, only filled at the
  * endpoint). Replaces PersistentTrajectoryDOP853.run() -> (samples, stats)

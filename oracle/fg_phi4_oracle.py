@@ -564,15 +564,32 @@ def _superop(f, d):
     return out
 
 
-def stationary_state(q, r, *, tolerance=1e-11):
+def _solve(op, b, d, method, tolerance):
+    """x with op(x) = b for a linear map op on D x D matrices: a dense LU of the D^2 x D^2
+    matrix ("dense"), or restarted GMRES on its action ("krylov", as numerics.py:55-71 does,
+    unpreconditioned) for sizes where the dense matrix is too costly."""
+    if method == "dense":
+        return _mat(np.linalg.solve(_superop(op, d), _vec(b)), d)
+    if method != "krylov":
+        raise ValueError(f"unknown method {method!r}")
+    from scipy.sparse.linalg import LinearOperator, gmres
+    n = d * d
+    lin = LinearOperator((n, n), matvec=lambda v: _vec(op(_mat(np.asarray(v).ravel(), d))), dtype=np.complex128)
+    x, info = gmres(lin, _vec(b), rtol=tolerance, atol=0.0, restart=min(64, n), maxiter=400)
+    if info != 0:
+        raise OracleFailure(f"GMRES did not converge (info={info})")
+    return _mat(x, d)
+
+
+def stationary_state(q, r, *, tolerance=1e-11, method="dense"):
     """Stationary density: L(rho) = 0, tr rho = 1, Hermitian, positive (numerics.py:74-100,
     src/transfer.jl:33-115). The oracle solves the same bordered equation
-    -L(x) + tr(x) I / D = I / D directly; the checks of checked_density follow."""
+    -L(x) + tr(x) I / D = I / D (directly, or by GMRES with method="krylov"); the checks of
+    checked_density follow."""
     q, r = np.asarray(q, complex), np.asarray(r, complex)
     d = len(q)
     eye = np.eye(d, dtype=complex)
-    a = _superop(lambda x: -lindblad(q, r, x) + np.trace(x) / d * eye, d)
-    rho = _mat(np.linalg.solve(a, _vec(eye / d)), d)
+    rho = _solve(lambda x: -lindblad(q, r, x) + np.trace(x) / d * eye, eye / d, d, method, tolerance)
     rho = rho / np.trace(rho)
     if np.linalg.norm(rho - adj(rho)) > 100 * tolerance:
         raise OracleFailure("stationary state is not Hermitian")
@@ -584,20 +601,19 @@ def stationary_state(q, r, *, tolerance=1e-11):
     return rho
 
 
-def boundary_environment(q, r, rho, environment):
+def boundary_environment(q, r, rho, environment, *, method="dense"):
     """H with -L*(H) + tr(rho H) I = A - tr(rho A) I (numerics.py:103-117,
-    src/transfer.jl:119-153), solved directly."""
+    src/transfer.jl:119-153), solved directly (or by GMRES with method="krylov")."""
     d = len(q)
     eye = np.eye(d, dtype=complex)
     b = environment - np.trace(rho @ environment) * eye
-    a = _superop(lambda x: -lindblad_adjoint(q, r, x) + np.trace(rho @ x) * eye, d)
-    return _mat(np.linalg.solve(a, _vec(b)), d)
+    return _solve(lambda x: -lindblad_adjoint(q, r, x) + np.trace(rho @ x) * eye, b, d, method, 1e-13)
 
 
-def finish_gradient(q, r, rho, covector, environment, *, metric_reg=1e-3):
+def finish_gradient(q, r, rho, covector, environment, *, metric_reg=1e-3, method="dense"):
     """gradient = ((rho + reg I)^-1 (covector + rho R^dag H - rho H R^dag))^dag
     (numerics.py:120-126, src/observables.jl:278-289)."""
-    h = boundary_environment(q, r, rho, environment)
+    h = boundary_environment(q, r, rho, environment, method=method)
     c = covector + rho @ adj(r) @ h - rho @ h @ adj(r)
     return adj(np.linalg.solve(rho + metric_reg * np.eye(len(r)), c))
 
@@ -608,7 +624,7 @@ def metric(rho, x, y, metric_reg=1e-3):
 
 
 def fg_phi4(r, k, rho, g, *, half_window=30.0, n_quad=512, atol=1e-13, rtol=1e-12, nodes=512,
-            krylov_tolerance=1e-12, maxdim=1024, metric_reg=1e-3):
+            krylov_tolerance=1e-12, maxdim=1024, metric_reg=1e-3, method="dense"):
     """(energy, gradient, parts) of the phi^4 density: kinetic1 + kinetic2 + g phi^4, the
     sum computed by the reference's GPU objective (overlap_sweep_driver.py:132-212,
     sweep_driver.py:78-119; src/observables.jl:332-334)."""
@@ -619,6 +635,6 @@ def fg_phi4(r, k, rho, g, *, half_window=30.0, n_quad=512, atol=1e-13, rtol=1e-1
     covector = quartic["covector"] + kinetic["covector"]
     environment = quartic["environment"] + kinetic["environment"]
     energy = quartic["value"] + kinetic["value"]
-    gradient = finish_gradient(q, r, rho, covector, environment, metric_reg=metric_reg)
+    gradient = finish_gradient(q, r, rho, covector, environment, metric_reg=metric_reg, method=method)
     return energy, gradient, dict(quartic=quartic, kinetic=kinetic, covector=covector,
                                   environment=environment)

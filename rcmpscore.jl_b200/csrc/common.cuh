@@ -2,7 +2,8 @@
 //
 // Complex matrices are row-major arrays of double2 (re, im), the layout of a C-ordered NumPy
 // complex128 array. Products run on the FP64 tensor-core instruction mma.sync m16n8k8 (A 16x8
-// row, B 8x8 col, C 16x8; fragment layout checked on B200 against a CPU product).
+// row, B 8x8 col, C 16x8; fragment layout checked on B200 against a CPU product), three real
+// products per complex product (ZFrag).
 // Every wait on an mbarrier is bounded: on timeout it raises the kernel's error flag and
 // returns, so control flow (and every cluster barrier) stays uniform.
 #pragma once
@@ -60,63 +61,69 @@ RCMPS_DEVICE_INLINE void dmma16x8x8(double* c, const double* a, const double* b)
       : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
 }
 
-// A complex 16x8 accumulator: re[4], im[4] in the C-fragment layout.
+// A complex 16x8 accumulator in the C-fragment layout, kept as the three real sums of the
+// 3-multiplication complex product (Gauss): p = sum Ar Br, q = sum Ai Bi,
+// s = sum (Ar + Ai)(Br + Bi), so that re = p - q and im = s - p - q. Three real MMAs per complex
+// k-step instead of four, on three independent accumulators.
 struct ZFrag {
-  double re[4];
-  double im[4];
+  double p[4];
+  double q[4];
+  double s[4];
   RCMPS_DEVICE_INLINE void zero() {
 #pragma unroll
-    for (int i = 0; i < 4; ++i) re[i] = im[i] = 0.0;
+    for (int i = 0; i < 4; ++i) p[i] = q[i] = s[i] = 0.0;
+  }
+  RCMPS_DEVICE_INLINE double re(int i) const { return p[i] - q[i]; }
+  RCMPS_DEVICE_INLINE double im(int i) const { return s[i] - p[i] - q[i]; }
+  RCMPS_DEVICE_INLINE double2 value(int i) const { return make_double2(re(i), im(i)); }
+  // acc += v for entry i
+  RCMPS_DEVICE_INLINE void add(int i, double2 v) {
+    p[i] += v.x;
+    s[i] += v.x + v.y;
   }
 };
 
-// acc += A(16x8 complex) * B(8x8 complex), the fragments already split into parts.
-// Four real products: re += Ar Br - Ai Bi, im += Ar Bi + Ai Br.
-RCMPS_DEVICE_INLINE void zmma(ZFrag& acc, const double* ar, const double* ai, const double* nai,
-                              const double* br, const double* bi) {
-  dmma16x8x8(acc.re, ar, br);
-  dmma16x8x8(acc.re, nai, bi);
-  dmma16x8x8(acc.im, ar, bi);
-  dmma16x8x8(acc.im, ai, br);
-}
+// A fragments of a complex 16x8 A tile: real part, imaginary part and their sum.
+struct AFrag {
+  double r[4], i[4], s[4];
+};
+// B fragments of a complex 8x8 B tile: real part, imaginary part and their sum.
+struct BFrag {
+  double r[2], i[2], s[2];
+};
 
 // acc[j] += A * B_j for TPW tiles sharing the A fragment; the MMAs are issued so that
 // consecutive ones update different accumulators.
 template <int TPW>
-RCMPS_DEVICE_INLINE void zmma_tiles(ZFrag* acc, const double* ar, const double* ai, const double* nai,
-                                    const double (*br)[2], const double (*bi)[2]) {
+RCMPS_DEVICE_INLINE void zmma_tiles(ZFrag* acc, const AFrag& a, const BFrag* b) {
 #pragma unroll
   for (int j = 0; j < TPW; ++j) {
-    dmma16x8x8(acc[j].re, ar, br[j]);
-    dmma16x8x8(acc[j].im, ar, bi[j]);
-  }
-#pragma unroll
-  for (int j = 0; j < TPW; ++j) {
-    dmma16x8x8(acc[j].re, nai, bi[j]);
-    dmma16x8x8(acc[j].im, ai, br[j]);
+    dmma16x8x8(acc[j].p, a.r, b[j].r);
+    dmma16x8x8(acc[j].q, a.i, b[j].i);
+    dmma16x8x8(acc[j].s, a.s, b[j].s);
   }
 }
+RCMPS_DEVICE_INLINE void zmma(ZFrag& acc, const AFrag& a, const BFrag& b) { zmma_tiles<1>(&acc, a, &b); }
 
 // Load the A fragment of rows [m0, m0+16) and columns [k0, k0+8) of a row-major complex
 // matrix with leading dimension lda (in complex elements) from shared memory.
-RCMPS_DEVICE_INLINE void load_a(const double2* A, int lda, int m0, int k0, int lane,
-                                double* ar, double* ai, double* nai) {
+RCMPS_DEVICE_INLINE void load_a(const double2* A, int lda, int m0, int k0, int lane, AFrag& a) {
   const int g = lane >> 2, t = lane & 3;
   const double2* p = A + (m0 + g) * lda + k0 + t;
   double2 v0 = p[0], v1 = p[8 * lda], v2 = p[4], v3 = p[8 * lda + 4];
-  ar[0] = v0.x; ar[1] = v1.x; ar[2] = v2.x; ar[3] = v3.x;
-  ai[0] = v0.y; ai[1] = v1.y; ai[2] = v2.y; ai[3] = v3.y;
+  a.r[0] = v0.x; a.r[1] = v1.x; a.r[2] = v2.x; a.r[3] = v3.x;
+  a.i[0] = v0.y; a.i[1] = v1.y; a.i[2] = v2.y; a.i[3] = v3.y;
 #pragma unroll
-  for (int i = 0; i < 4; ++i) nai[i] = -ai[i];
+  for (int i = 0; i < 4; ++i) a.s[i] = a.r[i] + a.i[i];
 }
 
 // Load the B fragment of rows [k0, k0+8) and columns [n0, n0+8) of a row-major complex matrix.
-RCMPS_DEVICE_INLINE void load_b(const double2* B, int ldb, int k0, int n0, int lane,
-                                double* br, double* bi) {
+RCMPS_DEVICE_INLINE void load_b(const double2* B, int ldb, int k0, int n0, int lane, BFrag& b) {
   const int g = lane >> 2, t = lane & 3;
   double2 v0 = B[(k0 + t) * ldb + n0 + g], v1 = B[(k0 + t + 4) * ldb + n0 + g];
-  br[0] = v0.x; br[1] = v1.x;
-  bi[0] = v0.y; bi[1] = v1.y;
+  b.r[0] = v0.x; b.r[1] = v1.x;
+  b.i[0] = v0.y; b.i[1] = v1.y;
+  b.s[0] = v0.x + v0.y; b.s[1] = v1.x + v1.y;
 }
 
 // Element coordinates (row, col) of C-fragment entry i for a lane.

@@ -81,12 +81,12 @@ struct RowGemmRing {
       const double2* B = ring + slot * SLOT;
 #pragma unroll
       for (int ks = 0; ks < KC / 8; ++ks) {
-        double ar[4], ai[4], nai[4];
-        load_a(A, lda, mt * 16, q * KC + ks * 8, lane, ar, ai, nai);
-        double br[TPW][2], bi[TPW][2];
+        AFrag a;
+        load_a(A, lda, mt * 16, q * KC + ks * 8, lane, a);
+        BFrag b[TPW];
 #pragma unroll
-        for (int j = 0; j < TPW; ++j) load_b(B, LDB, ks * 8, ((tile0 + j) % TN) * 8, lane, br[j], bi[j]);
-        zmma_tiles<TPW>(acc, ar, ai, nai, br, bi);
+        for (int j = 0; j < TPW; ++j) load_b(B, LDB, ks * 8, ((tile0 + j) % TN) * 8, lane, b[j]);
+        zmma_tiles<TPW>(acc, a, b);
       }
       __syncthreads();
       if (threadIdx.x == 0 && q + NST < nch) issue(s, q + NST);

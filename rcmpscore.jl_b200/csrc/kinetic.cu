@@ -114,7 +114,7 @@ lindblad_kernel(const LindbladTask* __restrict__ tasks, int ntasks, int mode) {
     for (int i = 0; i < 4; ++i) {
       int row, col;
       GR::template coord<32>(j, i, row, col);
-      const double2 v = make_double2(acc1[j].re[i], acc1[j].im[i]);
+      const double2 v = acc1[j].value(i);
       keep[j][i] = v;
       if (row >= 16) aprime[(row - 16) * LG::LDA2 + DP + col] = v;
     }
@@ -147,7 +147,7 @@ lindblad_kernel(const LindbladTask* __restrict__ tasks, int ntasks, int mode) {
     for (int i = 0; i < 4; ++i) {
       int row, col;
       GR::template coord<16>(j, i, row, col);
-      double2 lx = zadd(make_double2(acc2[j].re[i], acc2[j].im[i]), stage[row * LG::LDP + col]);
+      double2 lx = zadd(acc2[j].value(i), stage[row * LG::LDP + col]);
       const size_t off = (size_t)(row0 + row) * DP + col;
       if (mode == 0) {
         if (T.trw) {
@@ -527,13 +527,13 @@ __global__ void __launch_bounds__(256, 1) reconstruct_kernel(ArnoldiProblem* __r
     if (kc + 1 < nk) load(kc + 1, buf ^ 1);
 #pragma unroll
     for (int ks = 0; ks < BK / 8; ++ks) {
-      double ar[4], ai[4], nai[4];
-      load_a(As[buf], LDA, mt * 16, ks * 8, lane, ar, ai, nai);
+      AFrag a;
+      load_a(As[buf], LDA, mt * 16, ks * 8, lane, a);
 #pragma unroll
       for (int j = 0; j < 4; ++j) {
-        double br[2], bi[2];
-        load_b(Bs[buf], LDB, ks * 8, (nt0 + j) * 8, lane, br, bi);
-        zmma(acc[j], ar, ai, nai, br, bi);
+        BFrag b;
+        load_b(Bs[buf], LDB, ks * 8, (nt0 + j) * 8, lane, b);
+        zmma(acc[j], a, b);
       }
     }
     __syncthreads();
@@ -545,7 +545,7 @@ __global__ void __launch_bounds__(256, 1) reconstruct_kernel(ArnoldiProblem* __r
     for (int i = 0; i < 4; ++i) {
       const int s = s0 + mt * 16 + frag_row(lane, i), col = c0 + (nt0 + j) * 8 + frag_col(lane, i);
       if (s < nshift && col < n) {
-        const double2 v = make_double2(acc[j].re[i], acc[j].im[i]);
+        const double2 v = acc[j].value(i);
         double2* X = P.X + (size_t)s * n;
         if (P.adjoint) {
           const int r = col / dp, cc = col % dp;
@@ -632,7 +632,7 @@ contract_kernel(ContractArgs a) {
           for (int e = 0; e < 4; ++e) {
             int row, col;
             GM::coord(j, e, row, col);
-            bufY[row * CG::LDA + col] = make_double2(wc * tmp[j].re[e], wc * tmp[j].im[e]);
+            bufY[row * CG::LDA + col] = zscale(wc, tmp[j].value(e));
           }
         __syncthreads();
         sb.ptr[0] = pass == 0 ? Ai : Xi;
@@ -651,7 +651,7 @@ contract_kernel(ContractArgs a) {
       for (int e = 0; e < 4; ++e) {
         int row, col;
         GM::coord(j, e, row, col);
-        out[(row + rb * CG::MB) * DP + col] = make_double2(acc[j].re[e], acc[j].im[e]);
+        out[(row + rb * CG::MB) * DP + col] = acc[j].value(e);
       }
     __syncthreads();
   }

@@ -71,6 +71,33 @@ __global__ void prepare_kernel(const double2* __restrict__ R, const double2* __r
   }
 }
 
+// Operators of the commutator channels of the all-ODE route: C = Q R - R Q at slot kC and
+// C^dag at slot kCh of each state's operator block (needs kOpsFull slots).
+__global__ void commutator_kernel(double2* __restrict__ ops, int dp, long long ops_stride) {
+  const int n = dp * dp;
+  double2* o = ops + blockIdx.x * ops_stride;
+  const double2 *Q = o + kQ * n, *R = o + kR * n;
+  double2 *Cm = o + kC * n, *Ch = o + kCh * n;
+  for (int e = threadIdx.x; e < n; e += blockDim.x) {
+    const int i = e / dp, j = e % dp;
+    double2 c = make_double2(0.0, 0.0);
+    for (int l = 0; l < dp; ++l) c = zadd(c, zsub(zmul(Q[i * dp + l], R[l * dp + j]), zmul(R[i * dp + l], Q[l * dp + j])));
+    Cm[e] = c;
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < n; e += blockDim.x) {
+    const int i = e / dp, j = e % dp;
+    Ch[e] = zconj(Cm[j * dp + i]);
+  }
+}
+
+cudaError_t launch_commutator(double* ops, int dp, long long ops_stride, int nstates, cudaStream_t stream) {
+  if (nstates == 0) return cudaSuccess;
+  note_launch();
+  commutator_kernel<<<nstates, 256, 0, stream>>>(reinterpret_cast<double2*>(ops), dp, ops_stride);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_pad(const double* src, const long long* d_src_off, const int* d_dims, double* dst, int dp,
                        long long stride, int nstates, cudaStream_t stream) {
   if (nstates == 0) return cudaSuccess;

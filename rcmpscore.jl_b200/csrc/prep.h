@@ -5,7 +5,9 @@
 namespace rcmps {
 // Number of dp x dp matrices in the operator block of one state (Q, Qh, R, Rh, fixed0, fixed6, S, rho).
 constexpr int kOps = 8;
-enum OpIndex { kQ = 0, kQh = 1, kR = 2, kRh = 3, kFixed0 = 4, kFixed6 = 5, kS = 6, kRho = 7 };
+enum OpIndex { kQ = 0, kQh = 1, kR = 2, kRh = 3, kFixed0 = 4, kFixed6 = 5, kS = 6, kRho = 7, kC = 8, kCh = 9 };
+// The all-ODE route adds the commutator C = QR - RQ and C^dag.
+constexpr int kOpsFull = 10;
 
 cudaError_t launch_pad(const double* src, const long long* d_src_off, const int* d_dims, double* dst, int dp,
                        long long stride, int nstates, cudaStream_t stream);
@@ -20,6 +22,7 @@ cudaError_t launch_scatter_values(const double* src, int n, const int* d_idx, do
 // samples (padded [npoints][7][dp][dp]) -> out [npoints][7 d^2 + 1]; the scalar is `value` at the endpoint
 cudaError_t launch_export_samples(const double2* samples, int dp, int d, int npoints, const double* value,
                                   double* out, cudaStream_t stream);
+cudaError_t launch_commutator(double* ops, int dp, long long ops_stride, int nstates, cudaStream_t stream);
 cudaError_t launch_prepare(const double* R, const double* K, const double* rho, double* ops, int dp,
                            long long in_stride, long long ops_stride, int nstates, cudaStream_t stream);
 }  // namespace rcmps

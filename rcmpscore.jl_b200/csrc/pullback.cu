@@ -107,7 +107,7 @@ pullback_kernel(PullbackArgs a) {
                 int row, col;
                 GM::coord(j, e, row, col);
                 row += rbw * PG::MB;
-                double2 v = make_double2(w * tmp[j].re[e], w * tmp[j].im[e]);
+                double2 v = zscale(w, tmp[j].value(e));
                 if (k < 3) v = zaxpy(c, adj(i, k + 1)[row * DP + col], v);
                 else if (row == col) v.x += c;
                 wscr[(k - 1) * MAT + row * DP + col] = v;
@@ -139,7 +139,7 @@ pullback_kernel(PullbackArgs a) {
               int row, col;
               GM::coord(j, e, row, col);
               const int grow = row + rb * PG::MB;
-              double2 v = make_double2(w * tmp[j].re[e], w * tmp[j].im[e]);
+              double2 v = zscale(w, tmp[j].value(e));
               if (k < 3) v = zaxpy(c, adj(i, k + 1)[grow * DP + col], v);
               else if (grow == col) v.x += c;
               bufY[row * PG::LDA + col] = v;
@@ -163,7 +163,7 @@ pullback_kernel(PullbackArgs a) {
       for (int e = 0; e < 4; ++e) {
         int row, col;
         GM::coord(j, e, row, col);
-        out[(row + rb * PG::MB) * DP + col] = make_double2(acc[j].re[e], acc[j].im[e]);
+        out[(row + rb * PG::MB) * DP + col] = acc[j].value(e);
       }
     __syncthreads();
   }

@@ -23,6 +23,40 @@ struct PullbackArgs {
 };
 
 cudaError_t pullback_launch(const PullbackArgs& a, int nblk, cudaStream_t s);
+
+// ---- the all-ODE route (pullback_full.cu)
+constexpr int kMaxPullSpecs = 3;
+constexpr int kMaxPullChannels = 5;
+constexpr int kMaxPullEdges = 8;
+
+// One channel spec of the all-ODE route: forward channels fwd0..fwd0+nch-1 and adjoint channels
+// adj0..adj0+nch-1 of a sample row; edges (src -> dst, left or right insertion, coefficient).
+struct FullPullSpec {
+  int nch, fwd0, adj0, comm, nedge, coupling_scaled;
+  int esrc[kMaxPullEdges], edst[kMaxPullEdges], eleft[kMaxPullEdges];
+  double ecoef[kMaxPullEdges];
+};
+
+struct FullPullbackArgs {
+  int dp, nstates, nodes, npoints, nodes_per_block, channels;
+  const double2* samples;      // [state][npoints][channels dp^2]
+  long long samples_stride;
+  const double2* ops;          // [state][...] (Q, Qh, R, Rh first)
+  long long ops_stride;
+  const double* wj;            // [nodes][2]
+  const double* coupling;      // [state]
+  double2* scratch;            // [CTAs][kMaxPullChannels dp^2]
+  double2* partial;            // [state][spec][nblk][6][dp^2]
+  double2* fin;                // [state][10 dp^2]
+  double2* cov_out;            // [state][dp^2] (padded)
+  double2* env_out;            // [state][dp^2] (padded)
+  double* value_out;           // [state]
+  int* error_flag;             // [state]
+};
+
+cudaError_t pullback_full_set_specs(const FullPullSpec* specs, int nspec);
+cudaError_t pullback_full_launch(const FullPullbackArgs& a, int nblk, int nspec, cudaStream_t s);
+int pullback_full_row_blocks(int dp);
 int pullback_row_blocks(int dp);
 size_t pullback_smem_bytes(int dp);
 

@@ -32,20 +32,78 @@ struct Layout {
 
 constexpr int kNodesPerBlock = 32;
 
-size_t state_bytes(int dp, int npoints, int nodes) {
+// Per-system sizes: channels of a stage vector, operator matrices, stage vectors of the
+// trajectory workspace (y, prop, k[16], z[2], P, and L for the all-ODE route), pullback
+// scratch, partial and finalize matrices per state.
+struct SysSizes {
+  int nch, nops, nwork;
+  size_t wscr, part, fin;   // in dp x dp matrices per state
+};
+SysSizes sys_sizes(int system, int dp, int nblk) {
+  SysSizes z;
+  z.nch = trajectory_channels(system);
+  if (system == 0) {
+    z.nops = kOps;
+    z.nwork = 21;
+    z.wscr = (size_t)nblk * pullback_row_blocks(dp) * 3;
+    z.part = (size_t)nblk * 4;
+    z.fin = 8;
+  } else {
+    z.nops = kOpsFull;
+    z.nwork = 22;
+    z.wscr = (size_t)nblk * pullback_full_row_blocks(dp) * kMaxPullSpecs * kMaxPullChannels;
+    z.part = (size_t)kMaxPullSpecs * nblk * 6;
+    z.fin = 10;
+  }
+  return z;
+}
+
+size_t state_bytes(int system, int dp, int npoints, int nodes) {
   const size_t mat = (size_t)dp * dp * 16;
   const int nblk = (nodes + kNodesPerBlock - 1) / kNodesPerBlock;
-  const int nrb = pullback_row_blocks(dp);
+  const SysSizes z = sys_sizes(system, dp, nblk);
   size_t b = 0;
-  b += 3 * mat;                       // padded R, K, rho
-  b += kOps * mat;                    // operators
-  b += 21 * 7 * mat;                  // y, prop, k[16], z[2], P
-  b += (size_t)npoints * 7 * mat;     // samples
-  b += (size_t)nblk * nrb * 3 * mat;  // pullback W scratch
-  b += (size_t)nblk * 4 * mat;        // pullback partials
-  b += 8 * mat + 2 * mat;             // finalize temps, padded covector/environment
-  b += 1024;                          // small per-state records
+  b += 3 * mat;                                 // padded R, K, rho
+  b += z.nops * mat;                            // operators
+  b += (size_t)z.nwork * z.nch * mat;           // trajectory workspace
+  b += (size_t)npoints * z.nch * mat;           // samples
+  b += (z.wscr + z.part + z.fin + 2) * mat;     // pullback scratch, partials, finalize, cov/env
+  b += 1024;                                    // small per-state records
   return b;
+}
+
+// Channel specs of the all-ODE route for the pullback (ode_backend.py:60-73): kinetic1 (R),
+// kinetic2 (commutator), g phi^4; forward channels from 0, adjoint from 13.
+void full_pull_specs(FullPullSpec* sp) {
+  std::memset(sp, 0, 3 * sizeof(FullPullSpec));
+  const double r2 = 1.4142135623730951;
+  const int kin_src[4] = {0, 0, 2, 1}, kin_dst[4] = {1, 2, 3, 3}, kin_left[4] = {1, 0, 1, 0};
+  for (int s = 0; s < 2; ++s) {
+    sp[s].nch = 4;
+    sp[s].fwd0 = 4 * s;
+    sp[s].adj0 = 13 + 4 * s;
+    sp[s].comm = s;
+    sp[s].nedge = 4;
+    for (int q = 0; q < 4; ++q) {
+      sp[s].esrc[q] = kin_src[q];
+      sp[s].edst[q] = kin_dst[q];
+      sp[s].eleft[q] = kin_left[q];
+      sp[s].ecoef[q] = r2;
+    }
+  }
+  sp[2].nch = 5;
+  sp[2].fwd0 = 8;
+  sp[2].adj0 = 21;
+  sp[2].nedge = 8;
+  sp[2].coupling_scaled = 1;
+  for (int k = 0; k < 4; ++k)
+    for (int side = 0; side < 2; ++side) {
+      const int q = 2 * k + side;
+      sp[2].esrc[q] = k;
+      sp[2].edst[q] = k + 1;
+      sp[2].eleft[q] = side == 0;
+      sp[2].ecoef[q] = k + 1;
+    }
 }
 
 }  // namespace
@@ -72,10 +130,18 @@ int quartic_run(rcmps_context* ctx, QuarticJob& job, cudaStream_t stream) {
   cudaEvent_t e0 = SL.ev[0], e1 = SL.ev[1], e2 = SL.ev[2];
   float traj_ms = 0.f, pull_ms = 0.f;
 
+  const int system = job.system;
+  if (system == 1) {
+    FullPullSpec specs[3];
+    full_pull_specs(specs);
+    if (pullback_full_set_specs(specs, 3) != cudaSuccess) return fail(ctx, RCMPS_CUDA_ERROR, "pullback specs");
+  }
   for (auto& kv : groups) {
     const int dp = kv.first;
     const std::vector<int>& all = kv.second;
-    const size_t per = state_bytes(dp, npoints, nodes);
+    const size_t per = state_bytes(system, dp, npoints, nodes);
+    const SysSizes zs = sys_sizes(system, dp, nblk);
+    const int NCH = zs.nch;
     const size_t fixed = (size_t)(npoints + 3 * nodes) * 8 + 4096;
     int cap = (int)std::max<size_t>(1, (budget - std::min(budget, fixed)) / per);
     for (size_t start = 0; start < all.size(); start += cap) {
@@ -96,13 +162,12 @@ int quartic_run(rcmps_context* ctx, QuarticJob& job, cudaStream_t stream) {
       const size_t o_states = L.add(n * sizeof(TrajState));
       const size_t o_tstats = L.add(n * sizeof(TrajStats));
       const size_t o_in = L.add(3 * n * mat * 16);
-      const size_t o_ops = L.add(n * kOps * mat * 16);
-      const size_t o_work = L.add(n * 21 * 7 * mat * 16);
-      const size_t o_samp = L.add((size_t)n * npoints * 7 * mat * 16);
-      const int nrb = pullback_row_blocks(dp);
-      const size_t o_wscr = L.add((size_t)n * nrb * nblk * 3 * mat * 16);
-      const size_t o_part = L.add((size_t)n * nblk * 4 * mat * 16);
-      const size_t o_fin = L.add((size_t)n * 8 * mat * 16);
+      const size_t o_ops = L.add((size_t)n * zs.nops * mat * 16);
+      const size_t o_work = L.add((size_t)n * zs.nwork * NCH * mat * 16);
+      const size_t o_samp = L.add((size_t)n * npoints * NCH * mat * 16);
+      const size_t o_wscr = L.add((size_t)n * zs.wscr * mat * 16);
+      const size_t o_part = L.add((size_t)n * zs.part * mat * 16);
+      const size_t o_fin = L.add((size_t)n * zs.fin * mat * 16);
       const size_t o_cov = L.add((size_t)n * mat * 16);
       const size_t o_env = L.add((size_t)n * mat * 16);
       cudaError_t e = arena_reserve(SL, L.total);
@@ -122,6 +187,7 @@ int quartic_run(rcmps_context* ctx, QuarticJob& job, cudaStream_t stream) {
       const size_t h_o_states = H.add(n * sizeof(TrajState));
       const size_t h_o_tstats = H.add(n * sizeof(TrajStats));
       const size_t h_o_flag = H.add(n * sizeof(int));
+      const size_t h_o_vals = H.add(n * 8);
       if (pinned_reserve(SL, H.total) != cudaSuccess) return fail(ctx, RCMPS_CUDA_ERROR, "pinned host buffer");
       char* h = static_cast<char*>(SL.pinned);
       int* h_dims = reinterpret_cast<int*>(h + h_o_dims);
@@ -133,6 +199,7 @@ int quartic_run(rcmps_context* ctx, QuarticJob& job, cudaStream_t stream) {
       TrajState* h_states = reinterpret_cast<TrajState*>(h + h_o_states);
       TrajStats* h_tstats = reinterpret_cast<TrajStats*>(h + h_o_tstats);
       int* h_flag = reinterpret_cast<int*>(h + h_o_flag);
+      double* h_vals = reinterpret_cast<double*>(h + h_o_vals);
       for (int i = 0; i < n; ++i) {
         h_dims[i] = job.dims[idx[i]];
         h_off[i] = off[idx[i]];
@@ -145,9 +212,11 @@ int quartic_run(rcmps_context* ctx, QuarticJob& job, cudaStream_t stream) {
       double2* d_ops = static_cast<double2*>(P(o_ops));
       double2* d_work = static_cast<double2*>(P(o_work));
       double2* d_samp = static_cast<double2*>(P(o_samp));
+      const size_t vec = (size_t)NCH * mat;   // one stage vector
       for (int i = 0; i < n; ++i) {
         TrajState& t = h_states[i];
-        const double2* ops = d_ops + (size_t)i * kOps * mat;
+        std::memset(&t, 0, sizeof(t));
+        const double2* ops = d_ops + (size_t)i * zs.nops * mat;
         t.Q = ops + kQ * mat;
         t.Qh = ops + kQh * mat;
         t.R = ops + kR * mat;
@@ -155,13 +224,19 @@ int quartic_run(rcmps_context* ctx, QuarticJob& job, cudaStream_t stream) {
         t.fixed0 = ops + kFixed0 * mat;
         t.fixed6 = ops + kFixed6 * mat;
         t.S = ops + kS * mat;
-        double2* w = d_work + (size_t)i * 21 * 7 * mat;
+        t.rho = ops + kRho * mat;
+        if (system == 1) {
+          t.C = ops + kC * mat;
+          t.Ch = ops + kCh * mat;
+        }
+        double2* w = d_work + (size_t)i * zs.nwork * vec;
         t.y = w;
-        t.prop = w + 7 * mat;
-        t.k = w + 14 * mat;
-        t.z = w + (14 + 16 * 7) * mat;
-        t.P = w + (14 + 18 * 7) * mat;
-        t.samples = d_samp + (size_t)i * npoints * 7 * mat;
+        t.prop = w + vec;
+        t.k = w + 2 * vec;
+        t.z = w + 18 * vec;
+        t.P = w + 20 * vec;
+        t.L = system == 1 ? w + 21 * vec : nullptr;
+        t.samples = d_samp + (size_t)i * npoints * vec;
         t.stats = reinterpret_cast<TrajStats*>(base + o_tstats) + i;
         t.atol = S.atol;
         t.rtol = S.rtol;
@@ -185,7 +260,10 @@ int quartic_run(rcmps_context* ctx, QuarticJob& job, cudaStream_t stream) {
       if (e == cudaSuccess) e = launch_pad(job.K, (long long*)P(o_off), (int*)P(o_dims), dK, dp, in_stride, n, stream);
       if (e == cudaSuccess) e = launch_pad(job.rho, (long long*)P(o_off), (int*)P(o_dims), dP, dp, in_stride, n, stream);
       if (e == cudaSuccess)
-        e = launch_prepare(dR, dK, dP, reinterpret_cast<double*>(d_ops), dp, in_stride, (long long)kOps * mat, n, stream);
+        e = launch_prepare(dR, dK, dP, reinterpret_cast<double*>(d_ops), dp, in_stride, (long long)zs.nops * mat, n,
+                           stream);
+      if (e == cudaSuccess && system == 1)
+        e = launch_commutator(reinterpret_cast<double*>(d_ops), dp, (long long)zs.nops * mat, n, stream);
       if (e == cudaSuccess)
         e = node_weights_launch((double*)P(o_points), (double*)P(o_weights), nodes, (double*)P(o_wj), stream);
       TrajControls tc;
@@ -194,34 +272,58 @@ int quartic_run(rcmps_context* ctx, QuarticJob& job, cudaStream_t stream) {
       tc.max_ns = (unsigned long long)(S.max_device_seconds * 1e9);
       if (e == cudaSuccess) e = cudaEventRecord(e0, stream);
       if (e == cudaSuccess)
-        e = trajectory_launch(dp, (TrajState*)P(o_states), n, (double*)P(o_points), npoints, tc, stream);
+        e = trajectory_launch(system, dp, (TrajState*)P(o_states), n, (double*)P(o_points), npoints, tc, stream);
       if (e == cudaSuccess) e = cudaEventRecord(e1, stream);
       if (e != cudaSuccess) return fail(ctx, RCMPS_CUDA_ERROR, std::string("trajectory launch: ") + cudaGetErrorString(e));
       // copy the trajectory values into a plain array for the finalize step
       // (TrajStats::value of each state)
       e = cudaMemcpy2DAsync(P(o_tval), 8, reinterpret_cast<char*>(P(o_tstats)) + offsetof(TrajStats, value),
                             sizeof(TrajStats), 8, n, cudaMemcpyDeviceToDevice, stream);
-      PullbackArgs pa;
-      pa.dp = dp;
-      pa.nstates = n;
-      pa.nodes = nodes;
-      pa.npoints = npoints;
-      pa.nodes_per_block = kNodesPerBlock;
-      pa.samples = d_samp;
-      pa.samples_stride = (long long)npoints * 7 * mat;
-      pa.ops = d_ops;
-      pa.ops_stride = (long long)kOps * mat;
-      pa.wj = (double*)P(o_wj);
-      pa.coupling = (double*)P(o_coup);
-      pa.traj_value = (double*)P(o_tval);
-      pa.scratch = (double2*)P(o_wscr);
-      pa.partial = (double2*)P(o_part);
-      pa.fin = (double2*)P(o_fin);
-      pa.cov_out = (double2*)P(o_cov);
-      pa.env_out = (double2*)P(o_env);
-      pa.value_out = (double*)P(o_vout);
-      pa.error_flag = (int*)P(o_flag);
-      if (e == cudaSuccess) e = pullback_launch(pa, nblk, stream);
+      if (system == 0) {
+        PullbackArgs pa;
+        pa.dp = dp;
+        pa.nstates = n;
+        pa.nodes = nodes;
+        pa.npoints = npoints;
+        pa.nodes_per_block = kNodesPerBlock;
+        pa.samples = d_samp;
+        pa.samples_stride = (long long)npoints * vec;
+        pa.ops = d_ops;
+        pa.ops_stride = (long long)zs.nops * mat;
+        pa.wj = (double*)P(o_wj);
+        pa.coupling = (double*)P(o_coup);
+        pa.traj_value = (double*)P(o_tval);
+        pa.scratch = (double2*)P(o_wscr);
+        pa.partial = (double2*)P(o_part);
+        pa.fin = (double2*)P(o_fin);
+        pa.cov_out = (double2*)P(o_cov);
+        pa.env_out = (double2*)P(o_env);
+        pa.value_out = (double*)P(o_vout);
+        pa.error_flag = (int*)P(o_flag);
+        if (e == cudaSuccess) e = pullback_launch(pa, nblk, stream);
+      } else {
+        FullPullbackArgs pa;
+        pa.dp = dp;
+        pa.nstates = n;
+        pa.nodes = nodes;
+        pa.npoints = npoints;
+        pa.nodes_per_block = kNodesPerBlock;
+        pa.channels = NCH;
+        pa.samples = d_samp;
+        pa.samples_stride = (long long)npoints * vec;
+        pa.ops = d_ops;
+        pa.ops_stride = (long long)zs.nops * mat;
+        pa.wj = (double*)P(o_wj);
+        pa.coupling = (double*)P(o_coup);
+        pa.scratch = (double2*)P(o_wscr);
+        pa.partial = (double2*)P(o_part);
+        pa.fin = (double2*)P(o_fin);
+        pa.cov_out = (double2*)P(o_cov);
+        pa.env_out = (double2*)P(o_env);
+        pa.value_out = (double*)P(o_vout);
+        pa.error_flag = (int*)P(o_flag);
+        if (e == cudaSuccess) e = pullback_full_launch(pa, nblk, kMaxPullSpecs, stream);
+      }
       if (e == cudaSuccess) e = cudaEventRecord(e2, stream);
       if (e != cudaSuccess) return fail(ctx, RCMPS_CUDA_ERROR, std::string("pullback launch: ") + cudaGetErrorString(e));
       // outputs
@@ -233,8 +335,10 @@ int quartic_run(rcmps_context* ctx, QuarticJob& job, cudaStream_t stream) {
                              (int*)P(o_dims), job.environment, n, job.accumulate, stream);
       if (e == cudaSuccess && job.value)
         e = launch_scatter_values((double*)P(o_vout), n, (int*)P(o_idx), job.value, job.accumulate, stream);
-      if (e == cudaSuccess && job.samples_out)
+      if (e == cudaSuccess && job.samples_out && system == 0)
         e = launch_export_samples(d_samp, dp, h_dims[0], npoints, (double*)P(o_tval), job.samples_out, stream);
+      if (e == cudaSuccess && system == 1)   // the route's value comes from the pullback
+        e = cudaMemcpyAsync(h_vals, P(o_vout), n * 8, cudaMemcpyDeviceToHost, stream);
       if (e == cudaSuccess) e = cudaMemcpyAsync(h_tstats, P(o_tstats), n * sizeof(TrajStats), cudaMemcpyDeviceToHost, stream);
       if (e == cudaSuccess) e = cudaMemcpyAsync(h_flag, P(o_flag), n * sizeof(int), cudaMemcpyDeviceToHost, stream);
       if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
@@ -256,7 +360,7 @@ int quartic_run(rcmps_context* ctx, QuarticJob& job, cudaStream_t stream) {
         o.last_step = t.h;
         o.min_step = t.min_h;
         o.max_step = t.max_h;
-        o.quartic_value = (job.couplings ? job.couplings[idx[i]] : 1.0) * t.value;
+        o.quartic_value = system == 0 ? (job.couplings ? job.couplings[idx[i]] : 1.0) * t.value : h_vals[i];
         if (t.status && !o.status) {
           o.status = t.status;
           o.failed_component = 1;

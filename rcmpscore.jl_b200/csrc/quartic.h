@@ -21,6 +21,7 @@ struct QuarticJob {
   bool accumulate = false;              // add into value/covector/environment instead of storing
   int slot = 0;                         // context slot (workspace, staging, events)
   double memory_share = 0.7;            // fraction of free device memory this job may hold
+  int system = 0;                       // 0: the quartic term (reduced system); 1: all terms by ODEs
 };
 
 cudaError_t quartic_init();

@@ -19,9 +19,16 @@
 //   * the scalar energy channel is integrated from per-CTA partial traces reduced once per
 //     attempt (its value never feeds back into the matrix channels);
 //   * the step controller runs identically in every CTA from the same reduced norms.
+// The channel structure comes from a table (SysTab) so that one kernel serves two systems:
+//   * the reduced quartic system above (7 channels + scalar; ode_backend.py:170-233);
+//   * the all-ODE route of kinetic1 + kinetic2 + g phi^4 (26 channels, ode_backend.py:76-167):
+//     per channel jac (ql X + X ql^dag + rl X rl^dag) + src (c_l ol_a X_a + c_r X_b ol_b^dag),
+//     where ol = R folds into the P products and ol = [Q, R] (the commutator spec) adds a
+//     G1 product C X and a third K block [.. | src c_r X_b] * C^dag to G2.
 #include <cuda_runtime.h>
 #include <cstdint>
 #include <cstdio>
+#include <cstring>
 #include "common.cuh"
 #include "dop853_tables.h"
 #include "source_table.h"
@@ -61,13 +68,26 @@ __device__ __forceinline__ double next_up(double t) {
   return __longlong_as_double(t > 0.0 ? b + 1 : b - 1);
 }
 
-// Insertion source channel and coefficient of each channel (ode_backend.py:193).
-__device__ __forceinline__ int ins_src(int c) {
-  return c == 1 ? 0 : c == 2 ? 1 : c == 3 ? 4 : c == 4 ? 5 : c == 5 ? 6 : -1;
-}
-__device__ __forceinline__ double ins_coef(int c) {
-  return c == 1 ? 2.0 : c == 2 ? 3.0 : c == 3 ? 1.0 : c == 4 ? 2.0 : c == 5 ? 3.0 : 0.0;
-}
+// Channel tables of the two systems (filled by trajectory_set_tables).
+//   g1: the G1 products in order: channel and panel kind (0 [Q;R] rows, 1 [Q^dag;R^dag] rows,
+//       2 C rows, 3 C^dag rows; kinds 2, 3 give L_c = ol X_c for the commutator spec);
+//   p_*[gs]: the G2 passes for the one-channel (gs 0) and two-channel (gs 1) tilings, k3 when
+//       the pass has the third K block (commutator spec);
+//   lsrc/lcoef/lkind: the left insertion c_l ol_a X_a (P_a for ol = R, L_a for the commutator);
+//   rsrc/rcoef: the right insertion c_r X_b ol_b^dag; fixed: 1 fixed0, 2 fixed6;
+//   init: initial value 0, rho (1) or the identity on the physical block (2).
+constexpr int kSysQuartic = 0, kSysFull = 1;
+constexpr int kMaxChannels = 26;
+struct SysTab {
+  int nch, ng1;
+  int g1_ch[32], g1_kind[32];
+  int np[2];
+  int p_first[2][32], p_count[2][32], p_k3[2][32];
+  int dir[kMaxChannels], lsrc[kMaxChannels], lkind[kMaxChannels], rsrc[kMaxChannels];
+  int fixed[kMaxChannels], init[kMaxChannels];
+  double lcoef[kMaxChannels], rcoef[kMaxChannels];
+};
+__constant__ SysTab c_sys[2];
 
 // Tiling of one product pass: M rows (a multiple of 16) by DP columns over NW warps; a warp owns
 // TPW consecutive 16x8 tiles of one band, or (when there are fewer tiles than warps) one tile and a
@@ -83,26 +103,27 @@ struct PassTiling {
   static constexpr int SPLIT = SK > 1 ? T * (SK - 1) * 128 : 0;   // split-K scratch (double2)
 };
 
-template <int DP>
+template <int DP, int SYS>
 struct Geo {
+  static constexpr int NCH = SYS == kSysQuartic ? 7 : 26;   // matrix channels
+  static constexpr bool SCALAR = SYS == kSysQuartic;       // the quartic system's scalar channel
+  static constexpr int KM = SYS == kSysQuartic ? 2 : 3;    // K blocks of the widest G2 pass
   static constexpr int G = DP / 16;
   static constexpr int NW = (DP == 48 || DP == 96) ? 12 : (DP == 64 || DP == 128) ? 16 : 8;
   static constexpr int NT = 32 * NW;
   static constexpr int KC = DP <= 64 ? 16 : 8;       // rows of a streamed B chunk
-  static constexpr int NST = 4;                       // ring stages
+  static constexpr int NST = (SYS == kSysFull && DP == 128) ? 3 : 4;   // ring stages
   static constexpr int LDB = DP + kBPad;              // padded row stride of a ring chunk
   static constexpr int LDP = DP + 4;                  // panel leading dimension (complex)
-  static constexpr int LDA2 = 2 * DP + 4;             // A' leading dimension
+  static constexpr int LDA2 = KM * DP + 4;            // A' leading dimension
   static constexpr int GS = DP <= 64 ? 2 : 1;         // channels per G2 pass
-  static constexpr int NPASS = GS == 2 ? 4 : 7;       // G2 passes: {0,1},{2},{3,4},{5,6} or one per channel
   using T1 = PassTiling<DP, 32, NW>;
   using T2a = PassTiling<DP, 16 * GS, NW>;
   using T2b = PassTiling<DP, 16, NW>;
-  static constexpr int CH1 = DP / KC, CH2 = 2 * DP / KC;   // chunks per G1 channel / G2 pass
-  static constexpr int NCHUNK = 7 * CH1 + NPASS * CH2;
+  static constexpr int CH1 = DP / KC;                 // chunks per G1 product; a G2 pass has 2 or 3 CH1
   static constexpr int MAT = DP * DP;                 // elements of one channel matrix
-  static constexpr int VEC = 7 * MAT;                 // elements of one stage vector
-  static constexpr int OWN = 7 * 16 * DP;             // elements owned by one CTA
+  static constexpr int VEC = NCH * MAT;               // elements of one stage vector
+  static constexpr int OWN = NCH * 16 * DP;           // elements owned by one CTA
   static constexpr int cmax(int a, int b) { return a > b ? a : b; }
   // shared memory (double2 units): one direction panel, the A' rows of a pass, the ring, split-K
   static constexpr int OFF_PANEL = 0;
@@ -111,9 +132,7 @@ struct Geo {
   static constexpr int OFF_SPLIT = OFF_RING + NST * KC * LDB;
   static constexpr int END2 = OFF_SPLIT + cmax(T1::SPLIT, cmax(T2a::SPLIT, T2b::SPLIT));
   static constexpr size_t SMEM = (size_t)END2 * 16 + 2048;   // + barriers and scalars (see carve)
-  // G2 pass p: first channel and channel count
-  __device__ static int pass_first(int p) { return GS == 2 ? (p == 0 ? 0 : p == 1 ? 2 : p == 2 ? 3 : 5) : p; }
-  __device__ static int pass_count(int p) { return GS == 2 ? (p == 1 ? 1 : 2) : 1; }
+  static_assert(SMEM <= 232448, "shared memory per CTA");
 };
 
 // Scalars of the controller, one copy per CTA (identical in all CTAs of a cluster).
@@ -133,7 +152,7 @@ struct Xch {                             // exchanged through distributed shared
   int flag;
 };
 
-template <int DP>
+template <int DP, int SYS>
 struct Smem {
   double2* panel;     // [32][LDP]: the current direction's [Qc; Rc] rows
   double2* aprime;    // [16 GS][LDA2]
@@ -146,10 +165,10 @@ struct Smem {
   double* kscp;       // [16] this CTA's partial scalar k by stage
 };
 
-template <int DP>
-__device__ __forceinline__ Smem<DP> carve(unsigned char* base) {
-  using GE = Geo<DP>;
-  Smem<DP> s;
+template <int DP, int SYS>
+__device__ __forceinline__ Smem<DP, SYS> carve(unsigned char* base) {
+  using GE = Geo<DP, SYS>;
+  Smem<DP, SYS> s;
   double2* z = reinterpret_cast<double2*>(base);
   s.panel = z + GE::OFF_PANEL;
   s.aprime = z + GE::OFF_APRIME;
@@ -170,9 +189,8 @@ __device__ __forceinline__ Smem<DP> carve(unsigned char* base) {
 }
 
 // Block-wide sum of two doubles; the result is returned to every thread.
-template <int DP>
+template <int NW>
 __device__ void block_sum2(double& a, double& b, double* red) {
-  using GE = Geo<DP>;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   a = warp_sum(a);
   b = warp_sum(b);
@@ -180,41 +198,61 @@ __device__ void block_sum2(double& a, double& b, double* red) {
   if (lane == 0) { red[2 * w] = a; red[2 * w + 1] = b; }
   __syncthreads();
   double x = 0.0, y = 0.0;
-  for (int i = 0; i < GE::NW; ++i) { x += red[2 * i]; y += red[2 * i + 1]; }
+  for (int i = 0; i < NW; ++i) { x += red[2 * i]; y += red[2 * i + 1]; }
   a = x;
   b = y;
 }
 
-template <int DP>
+template <int DP, int SYS>
 struct Rhs {
-  using GE = Geo<DP>;
+  using GE = Geo<DP, SYS>;
   const TrajState* st;
-  Smem<DP> sm;
+  Smem<DP, SYS> sm;
   int row0, tid, lane, warp;
   long long* gq;   // running chunk counter (uniform across the CTA)
+  int nchunk;      // chunks of one right-hand side (uniform)
+  int ce, cc;      // producer cursor (thread 0): entry (G1 products, then G2 passes), chunk in it
 
-  // Source pointer of chunk q (0 <= q < NCHUNK) of one right-hand side on stage vector zb.
-  __device__ const double2* chunk_src(int q, const double2* zb) const {
-    if (q < 7 * GE::CH1) {
-      const int c = q / GE::CH1, k = q % GE::CH1;
-      return zb + c * GE::MAT + k * GE::KC * DP;
-    }
-    q -= 7 * GE::CH1;
-    const int p = q / GE::CH2, k = q % GE::CH2;
-    const bool fwd = GE::pass_first(p) < 3;
-    const double2* top = fwd ? st->Qh : st->Q;     // (Qc)^dag
-    const double2* bot = fwd ? st->Rh : st->R;     // (Rc)^dag
-    const int r = k * GE::KC;
-    return r < DP ? top + r * DP : bot + (r - DP) * DP;
+  __device__ static const SysTab& T() { return c_sys[SYS]; }
+  __device__ static int gsi() { return GE::GS == 2 ? 1 : 0; }
+
+  // Chunks of entry e: a G1 product (CH1) or a G2 pass (2 or 3 CH1).
+  __device__ static int entry_chunks(int e) {
+    const SysTab& t = T();
+    if (e < t.ng1) return GE::CH1;
+    return (t.p_k3[gsi()][e - t.ng1] ? 3 : 2) * GE::CH1;
+  }
+  __device__ static int total_chunks() {
+    const SysTab& t = T();
+    int n = 0;
+    for (int e = 0; e < t.ng1 + t.np[gsi()]; ++e) n += entry_chunks(e);
+    return n;
   }
 
-  __device__ void issue(long long gidx, int q, const double2* zb) {
+  // Source of the cursor's chunk on stage vector zb.
+  __device__ const double2* cursor_src(const double2* zb) const {
+    const SysTab& t = T();
+    const int r = cc * GE::KC;
+    if (ce < t.ng1) return zb + (size_t)t.g1_ch[ce] * GE::MAT + (size_t)r * DP;
+    const int first = t.p_first[gsi()][ce - t.ng1];
+    const bool fwd = t.dir[first] == 0;
+    const int blk = r / DP, rr = r % DP;
+    // G2 B operand [Qc^dag; Rc^dag; Oc^dag]: forward (Q^dag, R^dag, C^dag), adjoint (Q, R, C)
+    const double2* m = blk == 0 ? (fwd ? st->Qh : st->Q) : blk == 1 ? (fwd ? st->Rh : st->R) : (fwd ? st->Ch : st->C);
+    return m + (size_t)rr * DP;
+  }
+
+  __device__ void issue(long long gidx, const double2* zb) {
     const int slot = (int)(gidx % GE::NST);
     mbar_expect_tx(&sm.full[slot], GE::KC * DP * 16);
-    const double2* src = chunk_src(q, zb);
+    const double2* src = cursor_src(zb);
     double2* dst = sm.ring + slot * GE::KC * GE::LDB;
 #pragma unroll
     for (int r = 0; r < GE::KC; ++r) bulk_g2s(dst + r * GE::LDB, src + r * DP, DP * 16, &sm.full[slot]);
+    if (++cc == entry_chunks(ce)) {
+      cc = 0;
+      ++ce;
+    }
   }
 
   // Wait for chunk (global index gidx); bounded.
@@ -225,12 +263,14 @@ struct Rhs {
     return sm.ring + slot * GE::KC * GE::LDB;
   }
 
-  __device__ void load_panel(int dir, double2* dst) const {
-    const double2* qs = dir == 0 ? st->Q : st->Qh;
-    const double2* rs = dir == 0 ? st->R : st->Rh;
-    for (int e = tid; e < 32 * DP; e += GE::NT) {
+  // The CTA's rows of the G1 A operand: kind 0 [Q; R], 1 [Q^dag; R^dag] (32 rows), 2 C, 3 C^dag (16).
+  __device__ void load_panel(int kind, double2* dst) const {
+    const int rows = kind < 2 ? 32 : 16;
+    for (int e = tid; e < rows * DP; e += GE::NT) {
       const int r = e / DP, col = e % DP;
-      const double2* srcm = r < 16 ? qs : rs;
+      const double2* srcm = kind == 0 ? (r < 16 ? st->Q : st->R)
+                            : kind == 1 ? (r < 16 ? st->Qh : st->Rh)
+                            : kind == 2 ? st->C : st->Ch;
       dst[r * GE::LDP + col] = srcm[(row0 + (r & 15)) * DP + col];
     }
   }
@@ -244,7 +284,7 @@ struct Rhs {
         for (int j = 0; j < TPW; ++j) {
           double2* p = sm.split + ((tile0 + j) * (SK - 1) + slice - 1) * 128;
 #pragma unroll
-          for (int i = 0; i < 4; ++i) p[i * 32 + lane] = make_double2(acc[j].re[i], acc[j].im[i]);
+          for (int i = 0; i < 4; ++i) p[i * 32 + lane] = acc[j].value(i);
         }
       }
       __syncthreads();
@@ -254,11 +294,7 @@ struct Rhs {
           for (int sl = 1; sl < SK; ++sl) {
             const double2* p = sm.split + ((tile0 + j) * (SK - 1) + sl - 1) * 128;
 #pragma unroll
-            for (int i = 0; i < 4; ++i) {
-              const double2 v = p[i * 32 + lane];
-              acc[j].re[i] += v.x;
-              acc[j].im[i] += v.y;
-            }
+            for (int i = 0; i < 4; ++i) acc[j].add(i, p[i * 32 + lane]);
           }
       }
       __syncthreads();
@@ -280,42 +316,80 @@ struct Rhs {
       for (int ks = 0; ks < GE::KC / 8; ++ks) {
         const int kstep = ch * (GE::KC / 8) + ks;
         if (kstep % SK != slice) continue;
-        double ar[4], ai[4], nai[4];
-        load_a(A, lda, mt * 16, kstep * 8, lane, ar, ai, nai);
-        double br[TPW][2], bi[TPW][2];
+        AFrag a;
+        load_a(A, lda, mt * 16, kstep * 8, lane, a);
+        BFrag b[TPW];
 #pragma unroll
-        for (int j = 0; j < TPW; ++j) load_b(B, GE::LDB, ks * 8, ((tile0 + j) % TL::NTN) * 8, lane, br[j], bi[j]);
-        zmma_tiles<TPW>(acc, ar, ai, nai, br, bi);
+        for (int j = 0; j < TPW; ++j) load_b(B, GE::LDB, ks * 8, ((tile0 + j) % TL::NTN) * 8, lane, b[j]);
+        zmma_tiles<TPW>(acc, a, b);
       }
       __syncthreads();
-      if (tid == 0 && q + GE::NST < GE::NCHUNK) issue(g0 + q + GE::NST, q + GE::NST, zb);
+      if (tid == 0 && q + GE::NST < nchunk) issue(g0 + q + GE::NST, zb);
     }
     split_reduce<TPW, SK>(acc, tile0, slice);
   }
 
-  // G2 pass over the channels first..first+NC-1 (same direction).
-  template <int NC>
+  // G1 product of channel c with a panel of 32 rows ([Qc; Rc]: Qc X_c -> kout scaled by jac,
+  // P_c = Rc X_c) or 16 rows (L_c = Oc X_c).
+  template <int M>
+  __device__ void g1_product(int c, const double2* zb, double2* kout, double jac, int& q, long long g0) {
+    using TL = PassTiling<DP, M, GE::NW>;
+    constexpr int TPW = TL::TPW, SK = TL::SK;
+    const int tile0 = SK > 1 ? warp / SK : warp * TPW;
+    const int slice = SK > 1 ? warp % SK : 0;
+    const int mt = tile0 / TL::NTN;     // M = 32: 0 Qc rows, 1 Rc rows
+    ZFrag acc[TPW];
+#pragma unroll
+    for (int j = 0; j < TPW; ++j) acc[j].zero();
+    stream_product<TL>(acc, sm.panel, GE::LDP, GE::CH1, q, g0, zb);
+    if (slice == 0) {
+#pragma unroll
+      for (int j = 0; j < TPW; ++j) {
+        const int nt = (tile0 + j) % TL::NTN;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          const int r = frag_row(lane, i), col = nt * 8 + frag_col(lane, i);
+          const size_t off = (size_t)c * GE::MAT + (size_t)(row0 + r) * DP + col;
+          const double2 v = acc[j].value(i);
+          if (M == 16) st->L[off] = v;
+          else if (mt == 0) kout[off] = zscale(jac, v);
+          else st->P[off] = v;
+        }
+      }
+    }
+  }
+
+  // G2 pass over the channels first..first+NC-1 (same direction and spec). K3: the pass has the
+  // third K block of the commutator spec.
+  template <int NC, bool K3>
   __device__ void g2_pass(int first, const double2* zb, double2* kout, double jac, double src, int& q,
                           long long g0) {
     using TL = PassTiling<DP, 16 * NC, GE::NW>;
     constexpr int TPW = TL::TPW, SK = TL::SK;
-    // A' = [jac X_c | jac P_c + src coef_c X_s] on this CTA's rows, channel i of the pass in rows 16 i..
+    const SysTab& t = T();
+    // A' = [jac X_c | jac P_c (+ src c_r X_b for ol = R) (| src c_r X_b for the commutator)]
     for (int e = tid; e < 16 * NC * DP; e += GE::NT) {
       const int r = e / DP, col = e % DP;
       const int c = first + r / 16;
-      const int s = ins_src(c);
+      const int b = t.rsrc[c];
       const size_t off = (size_t)(row0 + (r & 15)) * DP + col;
       const double2 x = __ldcg(zb + (size_t)c * GE::MAT + off);
       double2 m = zscale(jac, __ldcg(st->P + (size_t)c * GE::MAT + off));
-      if (s >= 0) m = zaxpy(src * ins_coef(c), __ldcg(zb + (size_t)s * GE::MAT + off), m);
+      double2 ins = make_double2(0.0, 0.0);
+      if (b >= 0) ins = zscale(src * t.rcoef[c], __ldcg(zb + (size_t)b * GE::MAT + off));
       sm.aprime[r * GE::LDA2 + col] = zscale(jac, x);
-      sm.aprime[r * GE::LDA2 + DP + col] = m;
+      if constexpr (K3) {
+        sm.aprime[r * GE::LDA2 + DP + col] = m;
+        sm.aprime[r * GE::LDA2 + 2 * DP + col] = ins;
+      } else {
+        sm.aprime[r * GE::LDA2 + DP + col] = zadd(m, ins);
+      }
     }
     __syncthreads();
     ZFrag acc[TPW];
 #pragma unroll
     for (int j = 0; j < TPW; ++j) acc[j].zero();
-    stream_product<TL>(acc, sm.aprime, GE::LDA2, GE::CH2, q, g0, zb);
+    stream_product<TL>(acc, sm.aprime, GE::LDA2, (K3 ? 3 : 2) * GE::CH1, q, g0, zb);
     const int tile0 = SK > 1 ? warp / SK : warp * TPW;
     const int slice = SK > 1 ? warp % SK : 0;
     if (slice == 0) {
@@ -326,13 +400,13 @@ struct Rhs {
         for (int i = 0; i < 4; ++i) {
           const int r = mt * 16 + frag_row(lane, i), col = nt * 8 + frag_col(lane, i);
           const int c = first + r / 16;
-          const int s = ins_src(c);
+          const int a = t.lsrc[c];
           const size_t loc = (size_t)(row0 + (r & 15)) * DP + col;
           const size_t off = (size_t)c * GE::MAT + loc;
-          double2 v = zadd(make_double2(acc[j].re[i], acc[j].im[i]), kout[off]);
-          if (s >= 0) v = zaxpy(src * ins_coef(c), __ldcg(st->P + (size_t)s * GE::MAT + loc), v);
-          if (c == 0) v = zaxpy(src, st->fixed0[loc], v);
-          if (c == 6) v = zaxpy(src, st->fixed6[loc], v);
+          double2 v = zadd(acc[j].value(i), kout[off]);
+          if (a >= 0) v = zaxpy(src * t.lcoef[c], __ldcg((t.lkind[c] ? st->L : st->P) + (size_t)a * GE::MAT + loc), v);
+          if (t.fixed[c] == 1) v = zaxpy(src, st->fixed0[loc], v);
+          if (t.fixed[c] == 2) v = zaxpy(src, st->fixed6[loc], v);
           kout[off] = v;
         }
       }
@@ -343,57 +417,53 @@ struct Rhs {
   // One right-hand side: k_out = f(t, z) on this CTA's rows. zb: the full stage vector
   // (written by every CTA of the cluster before the barrier that precedes this call).
   __device__ void operator()(const double2* zb, double2* kout, double jac, double src) {
+    const SysTab& t = T();
     const long long g0 = *gq;
     if (tid == 0) {
       fence_proxy_async_global();
-      for (int q = 0; q < GE::NST && q < GE::NCHUNK; ++q) issue(g0 + q, q, zb);
+      ce = 0;
+      cc = 0;
+      for (int q = 0; q < GE::NST && q < nchunk; ++q) issue(g0 + q, zb);
     }
     int q = 0;
-    // ------------------------------------------------------------------ G1: [Qc; Rc] rows * X_c
-    {
-      using TL = typename GE::T1;
-      constexpr int TPW = TL::TPW, SK = TL::SK;
-      const int tile0 = SK > 1 ? warp / SK : warp * TPW;
-      const int slice = SK > 1 ? warp % SK : 0;
-      const int mt = tile0 / TL::NTN;     // 0: Qc rows, 1: Rc rows
-      for (int c = 0; c < 7; ++c) {
-        if (c == 0 || c == 3) {
-          __syncthreads();
-          load_panel(c == 0 ? 0 : 1, sm.panel);
-          __syncthreads();
-        }
-        ZFrag acc[TPW];
-#pragma unroll
-        for (int j = 0; j < TPW; ++j) acc[j].zero();
-        stream_product<TL>(acc, sm.panel, GE::LDP, GE::CH1, q, g0, zb);
-        if (slice == 0) {
-#pragma unroll
-          for (int j = 0; j < TPW; ++j) {
-            const int nt = (tile0 + j) % TL::NTN;
-#pragma unroll
-            for (int i = 0; i < 4; ++i) {
-              const int r = frag_row(lane, i), col = nt * 8 + frag_col(lane, i);
-              const size_t off = (size_t)c * GE::MAT + (size_t)(row0 + r) * DP + col;
-              const double2 v = make_double2(acc[j].re[i], acc[j].im[i]);
-              if (mt == 0) kout[off] = zscale(jac, v);
-              else st->P[off] = v;
-            }
-          }
-        }
+    // ------------------------------------------------------------------ G1 products
+    int kind_prev = -1;
+    for (int e = 0; e < t.ng1; ++e) {
+      const int c = t.g1_ch[e], kind = t.g1_kind[e];
+      if (kind != kind_prev) {
+        __syncthreads();
+        load_panel(kind, sm.panel);
+        __syncthreads();
+        kind_prev = kind;
       }
+      if (kind < 2) g1_product<32>(c, zb, kout, jac, q, g0);
+      else if constexpr (GE::KM == 3) g1_product<16>(c, zb, kout, jac, q, g0);
     }
     __syncthreads();
     // ------------------------------------------------------------------ G2 passes
-    for (int p = 0; p < GE::NPASS; ++p) {
-      const int first = GE::pass_first(p);
+    const int gs = gsi();
+    for (int p = 0; p < t.np[gs]; ++p) {
+      const int first = t.p_first[gs][p];
+      const bool two = GE::GS == 2 && t.p_count[gs][p] == 2;
+      if constexpr (GE::KM == 3) {
+        if (t.p_k3[gs][p]) {
+          if constexpr (GE::GS == 2) {
+            if (two) g2_pass<2, true>(first, zb, kout, jac, src, q, g0);
+            else g2_pass<1, true>(first, zb, kout, jac, src, q, g0);
+          } else {
+            g2_pass<1, true>(first, zb, kout, jac, src, q, g0);
+          }
+          continue;
+        }
+      }
       if constexpr (GE::GS == 2) {
-        if (GE::pass_count(p) == 2) g2_pass<2>(first, zb, kout, jac, src, q, g0);
-        else g2_pass<1>(first, zb, kout, jac, src, q, g0);
+        if (two) g2_pass<2, false>(first, zb, kout, jac, src, q, g0);
+        else g2_pass<1, false>(first, zb, kout, jac, src, q, g0);
       } else {
-        g2_pass<1>(first, zb, kout, jac, src, q, g0);
+        g2_pass<1, false>(first, zb, kout, jac, src, q, g0);
       }
     }
-    *gq = g0 + GE::NCHUNK;
+    *gq = g0 + nchunk;
     __syncthreads();
   }
 };
@@ -405,13 +475,13 @@ __device__ __forceinline__ size_t own_offset(int e, int row0) {
   return (size_t)c * DP * DP + (size_t)(row0 + rem / DP) * DP + (rem % DP);
 }
 
-template <int DP>
-__global__ void __launch_bounds__(Geo<DP>::NT, 1)
+template <int DP, int SYS>
+__global__ void __launch_bounds__(Geo<DP, SYS>::NT, 1)
 trajectory_kernel(const TrajState* __restrict__ states, const double* __restrict__ points, int npoints,
                   TrajControls ctl_in) {
-  using GE = Geo<DP>;
+  using GE = Geo<DP, SYS>;
   extern __shared__ __align__(128) unsigned char smem_raw[];
-  Smem<DP> sm = carve<DP>(smem_raw);
+  Smem<DP, SYS> sm = carve<DP, SYS>(smem_raw);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const uint32_t rank = cluster_rank();
   const int sidx = (int)cluster_id_x();
@@ -439,7 +509,7 @@ trajectory_kernel(const TrajState* __restrict__ states, const double* __restrict
     for (int i = 0; i < 16; ++i) { C.ksc[i] = 0.0; sm.kscp[i] = 0.0; }
   }
   __syncthreads();
-  Rhs<DP> rhs{st, sm, row0, tid, lane, warp, &gq};
+  Rhs<DP, SYS> rhs{st, sm, row0, tid, lane, warp, &gq, Rhs<DP, SYS>::total_chunks(), 0, 0};
 
   // slot permutation: C.kslot[s] is the k buffer of stage s; y and proposed swap on acceptance
   if (tid < 16) C.kslot[tid] = tid;
@@ -450,18 +520,25 @@ trajectory_kernel(const TrajState* __restrict__ states, const double* __restrict
   long long zcount = 0;
   auto zb = [&](long long n) { return st->z + (size_t)(n & 1) * GE::VEC; };
 
-  // initial y = 0 on own rows, and f = RHS(-a, 0)
-  for (int e = tid; e < GE::OWN; e += GE::NT) {
-    const size_t off = own_offset<DP>(e, row0);
-    ybuf[off] = make_double2(0.0, 0.0);
-    zb(zcount)[off] = make_double2(0.0, 0.0);
+  // initial y on own rows (zero, rho or the identity of the physical block), and f = RHS(-a, y)
+  {
+    const SysTab& tab = c_sys[SYS];
+    for (int e = tid; e < GE::OWN; e += GE::NT) {
+      const size_t off = own_offset<DP>(e, row0);
+      const int c = e / (16 * DP), row = row0 + (e % (16 * DP)) / DP, col = e % DP;
+      double2 v = make_double2(0.0, 0.0);
+      if (tab.init[c] == 1) v = st->rho[row * DP + col];
+      else if (tab.init[c] == 2 && row == col && row < st->d) v.x = 1.0;
+      ybuf[off] = v;
+      zb(zcount)[off] = v;
+    }
   }
   fence_proxy_async_global();
   cluster_sync();
   rhs(zb(zcount), kb(0), C.jac[0], C.src[0]);
   ++zcount;
 
-  const double N = 7.0 * st->d * st->d + 1.0;
+  const double N = (double)GE::NCH * st->d * st->d + (GE::SCALAR ? 1.0 : 0.0);
   const double atol = st->atol, rtol = st->rtol;
   const long long max_steps = st->max_steps;
   const unsigned long long t_start = global_ns();
@@ -513,12 +590,14 @@ trajectory_kernel(const TrajState* __restrict__ states, const double* __restrict
         for (int j = 0; j < 12; ++j) v = zaxpy(ha[j], kv[j], v);
         z[off] = v;
         if (s == 12) pbuf[off] = v;
-        if (e / (16 * DP) == 2) {
-          const double2 sv = st->S[off - 2 * (size_t)GE::MAT];
-          part += v.x * sv.x - v.y * sv.y;
+        if constexpr (GE::SCALAR) {
+          if (e / (16 * DP) == 2) {
+            const double2 sv = st->S[off - 2 * (size_t)GE::MAT];
+            part += v.x * sv.x - v.y * sv.y;
+          }
         }
       }
-      block_sum2<DP>(part, dummy, sm.red);
+      block_sum2<GE::NW>(part, dummy, sm.red);
       if (tid == 0) sm.kscp[s] = 4.0 * C.src[s] * part;
       fence_proxy_async_global();
       cluster_sync();
@@ -543,7 +622,7 @@ trajectory_kernel(const TrajState* __restrict__ states, const double* __restrict
         s5 += zabs2(e5) / (scale * scale);
         s3 += zabs2(e3) / (scale * scale);
       }
-      block_sum2<DP>(s5, s3, sm.red);
+      block_sum2<GE::NW>(s5, s3, sm.red);
       if (tid == 0) {
         sm.xch->s5 = s5;
         sm.xch->s3 = s3;
@@ -720,11 +799,11 @@ trajectory_kernel(const TrajState* __restrict__ states, const double* __restrict
   cluster_sync();
 }
 
-template <int DP>
+template <int DP, int SYS>
 static cudaError_t launch_dp(const TrajState* d_states, int nstates, const double* d_points, int npoints,
                              const TrajControls& ctl, cudaStream_t stream) {
-  using GE = Geo<DP>;
-  auto kern = trajectory_kernel<DP>;
+  using GE = Geo<DP, SYS>;
+  auto kern = trajectory_kernel<DP, SYS>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GE::SMEM);
   if (e != cudaSuccess) return e;
   cudaLaunchConfig_t cfg = {};
@@ -759,6 +838,103 @@ cudaError_t node_weights_launch(const double* d_points, const double* d_weights,
   return cudaGetLastError();
 }
 
+// The channel tables of the two systems (host side, copied to c_sys).
+static void quartic_table(SysTab& t) {
+  std::memset(&t, 0, sizeof(t));
+  t.nch = 7;
+  for (int c = 0; c < 7; ++c) {
+    t.dir[c] = c < 3 ? 0 : 1;
+    t.lsrc[c] = t.rsrc[c] = -1;
+    t.g1_ch[c] = c;
+    t.g1_kind[c] = t.dir[c];
+  }
+  t.ng1 = 7;
+  // insertions c_s (R X_s + X_s R^dag) of ode_backend.py:193: 1<-0 (2), 2<-1 (3), 3<-4 (1), 4<-5 (2), 5<-6 (3)
+  const int src[7] = {-1, 0, 1, 4, 5, 6, -1};
+  const double coef[7] = {0, 2, 3, 1, 2, 3, 0};
+  for (int c = 0; c < 7; ++c) {
+    t.lsrc[c] = t.rsrc[c] = src[c];
+    t.lcoef[c] = t.rcoef[c] = coef[c];
+  }
+  t.fixed[0] = 1;
+  t.fixed[6] = 2;
+  // G2 passes: one per channel, or the same-direction pairs {0,1}, {2}, {3,4}, {5,6}
+  t.np[0] = 7;
+  for (int c = 0; c < 7; ++c) { t.p_first[0][c] = c; t.p_count[0][c] = 1; }
+  const int pf[4] = {0, 2, 3, 5}, pc[4] = {2, 1, 2, 2};
+  t.np[1] = 4;
+  for (int p = 0; p < 4; ++p) { t.p_first[1][p] = pf[p]; t.p_count[1][p] = pc[p]; }
+}
+
+// Specs of the all-ODE route (ode_backend.py:60-73, 851-858): kinetic1 (4 channels, O = R),
+// kinetic2 (4 channels, O = [Q, R]) and phi^4 (5 channels, O = R); forward channels 0..12,
+// adjoint 13..25. A forward edge a -> b inserts forward a into forward b on its side; its trace
+// dual inserts adjoint b into adjoint a on the other side (ode_backend.py:108-113).
+static void full_table(SysTab& t) {
+  std::memset(&t, 0, sizeof(t));
+  const int half = 13;
+  t.nch = 26;
+  struct Edge { int a, b; bool left; double c; };
+  const double r2 = 1.4142135623730951;
+  const Edge kin[4] = {{0, 1, true, r2}, {0, 2, false, r2}, {2, 3, true, r2}, {1, 3, false, r2}};
+  Edge quart[8];
+  for (int k = 0; k < 4; ++k) {
+    quart[2 * k] = {k, k + 1, true, (double)(k + 1)};
+    quart[2 * k + 1] = {k, k + 1, false, (double)(k + 1)};
+  }
+  const int off[3] = {0, 4, 8}, nch[3] = {4, 4, 5};
+  const bool comm[3] = {false, true, false};
+  for (int c = 0; c < 26; ++c) {
+    t.dir[c] = c < half ? 0 : 1;
+    t.lsrc[c] = t.rsrc[c] = -1;
+  }
+  bool is_comm[26] = {false}, lsource_comm[26] = {false};
+  for (int sp = 0; sp < 3; ++sp) {
+    const Edge* ed = sp == 2 ? quart : kin;
+    const int ne = sp == 2 ? 8 : 4;
+    for (int i = 0; i < nch[sp]; ++i) is_comm[off[sp] + i] = is_comm[half + off[sp] + i] = comm[sp];
+    t.init[off[sp]] = 1;                              // rho in the first forward channel
+    t.init[half + off[sp] + nch[sp] - 1] = 2;         // I in the last adjoint channel
+    for (int q = 0; q < ne; ++q) {
+      const int fa = off[sp] + ed[q].a, fb = off[sp] + ed[q].b;
+      const int aa = half + off[sp] + ed[q].a, ab = half + off[sp] + ed[q].b;
+      if (ed[q].left) {
+        t.lsrc[fb] = fa; t.lcoef[fb] = ed[q].c;       // forward b += c O X_a
+        t.rsrc[aa] = ab; t.rcoef[aa] = ed[q].c;       // adjoint a += c X_b O
+      } else {
+        t.rsrc[fb] = fa; t.rcoef[fb] = ed[q].c;       // forward b += c X_a O^dag
+        t.lsrc[aa] = ab; t.lcoef[aa] = ed[q].c;       // adjoint a += c O^dag X_b
+      }
+    }
+  }
+  for (int c = 0; c < 26; ++c)
+    if (t.lsrc[c] >= 0 && is_comm[c]) {
+      t.lkind[c] = 1;
+      lsource_comm[t.lsrc[c]] = true;
+    }
+  // G1: forward [Q;R] products, forward C products, adjoint [Q^dag;R^dag], adjoint C^dag products
+  int n = 0;
+  for (int c = 0; c < half; ++c) { t.g1_ch[n] = c; t.g1_kind[n++] = 0; }
+  for (int c = 0; c < half; ++c) if (lsource_comm[c]) { t.g1_ch[n] = c; t.g1_kind[n++] = 2; }
+  for (int c = half; c < 26; ++c) { t.g1_ch[n] = c; t.g1_kind[n++] = 1; }
+  for (int c = half; c < 26; ++c) if (lsource_comm[c]) { t.g1_ch[n] = c; t.g1_kind[n++] = 3; }
+  t.ng1 = n;
+  // G2 passes: one per channel, or pairs of consecutive channels of one spec
+  t.np[0] = 26;
+  for (int c = 0; c < 26; ++c) { t.p_first[0][c] = c; t.p_count[0][c] = 1; t.p_k3[0][c] = is_comm[c]; }
+  int p = 0;
+  for (int dir = 0; dir < 2; ++dir)
+    for (int sp = 0; sp < 3; ++sp)
+      for (int i = 0; i < nch[sp]; i += 2) {
+        const int c = dir * half + off[sp] + i;
+        t.p_first[1][p] = c;
+        t.p_count[1][p] = i + 1 < nch[sp] ? 2 : 1;
+        t.p_k3[1][p] = comm[sp];
+        ++p;
+      }
+  t.np[1] = p;
+}
+
 cudaError_t trajectory_set_tables() {
   cudaError_t e;
   if ((e = cudaMemcpyToSymbol(c_dop_a, rcmps_dop_a, sizeof(rcmps_dop_a))) != cudaSuccess) return e;
@@ -767,32 +943,34 @@ cudaError_t trajectory_set_tables() {
   if ((e = cudaMemcpyToSymbol(c_dop_e5, rcmps_dop_e5, sizeof(rcmps_dop_e5))) != cudaSuccess) return e;
   if ((e = cudaMemcpyToSymbol(c_dop_e3, rcmps_dop_e3, sizeof(rcmps_dop_e3))) != cudaSuccess) return e;
   if ((e = cudaMemcpyToSymbol(c_dop_d, rcmps_dop_d, sizeof(rcmps_dop_d))) != cudaSuccess) return e;
+  SysTab tabs[2];
+  quartic_table(tabs[0]);
+  full_table(tabs[1]);
+  if ((e = cudaMemcpyToSymbol(c_sys, tabs, sizeof(tabs))) != cudaSuccess) return e;
   return cudaMemcpyToSymbol(c_source, rcmps_source_table, sizeof(rcmps_source_table));
 }
 
-cudaError_t trajectory_launch(int dp, const TrajState* d_states, int nstates, const double* d_points,
+template <int SYS>
+static cudaError_t launch_sys(int dp, const TrajState* d_states, int nstates, const double* d_points,
                               int npoints, const TrajControls& ctl, cudaStream_t stream) {
   switch (dp) {
-    case 16: return launch_dp<16>(d_states, nstates, d_points, npoints, ctl, stream);
-    case 32: return launch_dp<32>(d_states, nstates, d_points, npoints, ctl, stream);
-    case 48: return launch_dp<48>(d_states, nstates, d_points, npoints, ctl, stream);
-    case 64: return launch_dp<64>(d_states, nstates, d_points, npoints, ctl, stream);
-    case 96: return launch_dp<96>(d_states, nstates, d_points, npoints, ctl, stream);
-    case 128: return launch_dp<128>(d_states, nstates, d_points, npoints, ctl, stream);
+    case 16: return launch_dp<16, SYS>(d_states, nstates, d_points, npoints, ctl, stream);
+    case 32: return launch_dp<32, SYS>(d_states, nstates, d_points, npoints, ctl, stream);
+    case 48: return launch_dp<48, SYS>(d_states, nstates, d_points, npoints, ctl, stream);
+    case 64: return launch_dp<64, SYS>(d_states, nstates, d_points, npoints, ctl, stream);
+    case 96: return launch_dp<96, SYS>(d_states, nstates, d_points, npoints, ctl, stream);
+    case 128: return launch_dp<128, SYS>(d_states, nstates, d_points, npoints, ctl, stream);
     default: return cudaErrorInvalidValue;
   }
 }
 
-size_t trajectory_smem_bytes(int dp) {
-  switch (dp) {
-    case 16: return Geo<16>::SMEM;
-    case 32: return Geo<32>::SMEM;
-    case 48: return Geo<48>::SMEM;
-    case 64: return Geo<64>::SMEM;
-    case 96: return Geo<96>::SMEM;
-    case 128: return Geo<128>::SMEM;
-    default: return 0;
-  }
+cudaError_t trajectory_launch(int system, int dp, const TrajState* d_states, int nstates, const double* d_points,
+                              int npoints, const TrajControls& ctl, cudaStream_t stream) {
+  if (system == kSysQuartic) return launch_sys<kSysQuartic>(dp, d_states, nstates, d_points, npoints, ctl, stream);
+  if (system == kSysFull) return launch_sys<kSysFull>(dp, d_states, nstates, d_points, npoints, ctl, stream);
+  return cudaErrorInvalidValue;
 }
+
+int trajectory_channels(int system) { return system == kSysFull ? 26 : 7; }
 
 }  // namespace rcmps

@@ -18,10 +18,13 @@ struct TrajStats {
 // and its workspace. All matrices row-major double2.
 struct TrajState {
   const double2 *Q, *Qh, *R, *Rh;     // Q, Q^dag, R, R^dag
-  const double2 *fixed0, *fixed6;     // R rho + rho R^dag, 4 (R + R^dag)
-  const double2* S;                   // conj(R) + R^T: weights of the scalar trace
-  double2 *y, *prop, *k, *z, *P;      // y, proposed [7 dp^2]; k [16][7 dp^2]; z [2][7 dp^2]; P [7 dp^2]
-  double2* samples;                   // [npoints][7 dp^2]
+  const double2 *fixed0, *fixed6;     // R rho + rho R^dag, 4 (R + R^dag) (quartic system)
+  const double2* S;                   // conj(R) + R^T: weights of the scalar trace (quartic system)
+  const double2 *C, *Ch;              // [Q, R] and its adjoint (all-ODE route)
+  const double2* rho;                 // initial value of the rho channels (all-ODE route)
+  double2 *y, *prop, *k, *z, *P;      // y, proposed [V]; k [16][V]; z [2][V]; P [V]; V = channels dp^2
+  double2* L;                         // [V] commutator products O X (all-ODE route)
+  double2* samples;                   // [npoints][V]
   TrajStats* stats;
   double atol, rtol;
   long long max_steps;
@@ -36,9 +39,10 @@ struct TrajControls {
 };
 
 cudaError_t trajectory_set_tables();
-cudaError_t trajectory_launch(int dp, const TrajState* d_states, int nstates, const double* d_points,
+// system: 0 the reduced quartic system (7 channels + scalar), 1 the all-ODE route (26 channels).
+cudaError_t trajectory_launch(int system, int dp, const TrajState* d_states, int nstates, const double* d_points,
                               int npoints, const TrajControls& ctl, cudaStream_t stream);
-size_t trajectory_smem_bytes(int dp);
+int trajectory_channels(int system);
 cudaError_t node_weights_launch(const double* d_points, const double* d_weights, int n, double* d_wj,
                                 cudaStream_t stream);
 

@@ -6,6 +6,7 @@ Mirrors (same names, argument meaning, return values and exceptions):
       OverlapObjective.__call__ (runtime/overlap_sweep_driver.py:132-212);
   * evaluate_quartic_persistent_trajectory(R, Q, rho, g, ...) -> dict
       (runtime/persistent_trajectory_backend.py:439-461);
+  * evaluate_phi4(R, Q, rho, g, ...) -> dict, every term by ODEs (runtime/ode_backend.py:851-858);
   * kinetic_raw(q, r, rho, nodes, ...) -> dict (runtime/kinetic_backend.py:499-592);
   * finish_gradient(q, r, rho, covector, environment, ...) -> (gradient, stats)
       (runtime/numerics.py:120-126);
@@ -30,7 +31,9 @@ from . import _lib
 
 __all__ = ["SolverFailure", "KineticFailure", "DeviceControlFailure", "OverlapFailure", "Settings",
            "settings_from_args", "fg_phi4_batch", "objective", "OverlapObjective",
-           "evaluate_quartic_persistent_trajectory", "kinetic_raw", "finish_gradient", "stationary_state",
+           "evaluate_quartic_persistent_trajectory", "evaluate_phi4", "evaluate_phi4_batch", "kinetic_raw",
+           "finish_gradient",
+           "stationary_state",
            "metric", "context"]
 
 
@@ -175,7 +178,9 @@ def fg_phi4_batch(R, K, rho, couplings, settings=None, *, device=None, return_pa
 
 def objective(r, k, rho, coupling, args=None, xp=None):
     """(energy, gradient, stats) of one state, the callable the reference's L-BFGS controllers
-    evaluate once per trial. r, k, rho: finite complex128 D x D; args: the optimizer's namespace."""
+    evaluate once per trial. r, k, rho: finite complex128 D x D; args: the optimizer's namespace.
+    args.mode == "ode" evaluates every term by ODEs (sweep_driver.py:90-92), otherwise the
+    kinetic resolvents plus the quartic trajectory."""
     mats = (r, k, rho)
     if any(np.asarray(x).dtype != np.complex128 for x in mats):
         raise SolverFailure("objective requires equally shaped finite complex128 matrices")
@@ -184,6 +189,15 @@ def objective(r, k, rho, coupling, args=None, xp=None):
     except ValueError as err:
         raise SolverFailure(f"objective requires equally shaped finite complex128 matrices: {err}") from None
     original = tuple(np.array(x, copy=True) for x in mats)
+    if getattr(args, "mode", None) == "ode":
+        s = settings_from_args(args)
+        q = -1j * np.asarray(k) - np.asarray(r).conj().T @ np.asarray(r) / 2
+        raw = evaluate_phi4(r, q, rho, coupling, half_window=s.half_window, n_quad=s.n_quad, atol=s.atol,
+                            rtol=s.rtol, max_steps=s.max_steps)
+        gradient, boundary = finish_gradient(q, r, rho, raw["covector"], raw["environment"], metric_reg=s.metric_reg)
+        if any(not np.array_equal(a, b) for a, b in zip(original, mats)):
+            raise OverlapFailure("a component mutated immutable R/K/rho inputs")
+        return float(raw["value"]), gradient, dict(ode=raw["stats"], boundary=boundary)
     energies, grads, stats = fg_phi4_batch([r], [k], [rho], [coupling], settings_from_args(args))
     if any(not np.array_equal(a, b) for a, b in zip(original, mats)):
         raise OverlapFailure("a component mutated immutable R/K/rho inputs")
@@ -265,6 +279,59 @@ def evaluate_quartic_persistent_trajectory(R, Q, rho, g=1.0, *, xp=None, half_wi
         _raise_for(rc, ctx, st2, "quartic samples")
         out["samples"] = samples.cpu().numpy()
     return out
+
+
+def evaluate_phi4(R, Q, rho, g, *, xp=None, half_window=20.0, n_quad=192, atol=1e-13, rtol=1e-12,
+                  initial_step=None, max_steps=1_000_000, max_device_seconds=60.0, **ignored):
+    """kinetic1 + kinetic2 + g phi^4, every term by ODEs (26 channels): dict(value, covector,
+    environment, stats), as ode_backend.evaluate_phi4 (ode_backend.py:851-858) returns them."""
+    import torch
+    d = _check_matrices(R, Q, rho)
+    ctx = context()
+    s = _lib.default_settings(half_window=float(half_window), n_quad=int(n_quad), atol=float(atol), rtol=float(rtol),
+                              max_steps=int(max_steps), max_device_seconds=float(max_device_seconds))
+    if initial_step is not None:
+        s.initial_step = float(initial_step)
+    K = _k_from_q(Q, R)
+    dR, dK, dP = _device([R]), _device([K]), _device([rho])
+    value = torch.zeros(1, dtype=torch.float64, device="cuda")
+    cov = torch.zeros(d * d, dtype=torch.complex128, device="cuda")
+    env = torch.zeros_like(cov)
+    stats = (_lib.StateStats * 1)()
+    rc = ctx.lib.rcmps_phi4_ode_batch(ctx.handle, 1, (C.c_int * 1)(d), (C.c_double * 1)(float(g)), dR.data_ptr(),
+                                      dK.data_ptr(), dP.data_ptr(), C.byref(s), value.data_ptr(), cov.data_ptr(),
+                                      env.data_ptr(), stats, _stream())
+    _raise_for(rc, ctx, stats[0], "ODE route")
+    st = stats[0].as_dict()
+    st.update(accepted_steps=st["accepted"], rejected_steps=st["rejected"], reduced_channels=False,
+              device_milliseconds=ctx.timings()[0])
+    return dict(value=float(value.cpu().item()), covector=_unpack(cov, [d])[0], environment=_unpack(env, [d])[0],
+                stats=st)
+
+
+def evaluate_phi4_batch(R, K, rho, couplings, settings=None, *, device=None):
+    """The all-ODE route for a batch of states (lists of D_i x D_i matrices, uneven D allowed):
+    (values [n], covectors, environments, stats) before the boundary/metric finish."""
+    import torch
+    n = len(R)
+    if not (len(K) == len(rho) == len(couplings) == n):
+        raise ValueError("R, K, rho and couplings must have the same length")
+    dims = [_check_matrices(R[i], K[i], rho[i]) for i in range(n)]
+    ctx = context(device)
+    s = settings if settings is not None else _lib.default_settings(half_window=20.0, n_quad=192)
+    dR, dK, dP = _device(R), _device(K), _device(rho)
+    total = sum(d * d for d in dims)
+    value = torch.zeros(n, dtype=torch.float64, device="cuda")
+    cov = torch.zeros(total, dtype=torch.complex128, device="cuda")
+    env = torch.zeros(total, dtype=torch.complex128, device="cuda")
+    stats = (_lib.StateStats * n)()
+    rc = ctx.lib.rcmps_phi4_ode_batch(ctx.handle, n, (C.c_int * n)(*dims), (C.c_double * n)(*map(float, couplings)),
+                                      dR.data_ptr(), dK.data_ptr(), dP.data_ptr(), C.byref(s), value.data_ptr(),
+                                      cov.data_ptr(), env.data_ptr(), stats, _stream())
+    if rc:
+        bad = next((i for i in range(n) if stats[i].status), 0)
+        _raise_for(rc, ctx, stats[bad], "ODE route")
+    return value.cpu().numpy(), _unpack(cov, dims), _unpack(env, dims), [stats[i].as_dict() for i in range(n)]
 
 
 def kinetic_raw(q, r, rho, nodes=128, *, xp=None, tolerance=1e-12, initialdim=16, maxdim=1024, gradient=True,

@@ -178,3 +178,52 @@ def test_failure_statuses_are_reported(gpu_context):
     # the context stays usable after the failures
     out = objective.evaluate_quartic_persistent_trajectory(R, Q, rho, 1.0, n_quad=16)
     assert out["stats"]["status"] == 0
+
+
+# ----------------------------------------------------------------------------- all-ODE route
+@pytest.mark.parametrize("index", range(4))
+def test_ode_route_matches_reference(gpu_context, index):
+    """Every term by ODEs (26 channels) against the reference's evaluate_phi4 + finish_gradient:
+    value/covector/environment and the finished gradient. On the long windows (W = 20) the step
+    sequence may differ from the reference's by a step or two (rounding of the 26-channel error
+    norm near the window edges, where the source is ~1e-10); the results agree to ~1e-14."""
+    from rcmps_b200 import objective
+    rec = load_records("ode.npz")[index]
+    R, K, rho, g = rec["R"], rec["K"], rec["rho"], rec["g"]
+    Q = O.left_canonical_q(R, K)
+    out = objective.evaluate_phi4(R, Q, rho, g, half_window=rec["window"], n_quad=int(rec["n_quad"]))
+    assert abs(out["stats"]["accepted"] - rec["accepted"]) <= 2 and abs(out["stats"]["rejected"] - rec["rejected"]) <= 2
+    assert abs(out["value"] - rec["value"]) <= ENERGY_TOL * abs(rec["value"])
+    assert np.abs(out["covector"] - rec["covector"]).max() <= 1e-10 * max(1.0, np.abs(rec["covector"]).max())
+    assert np.abs(out["environment"] - rec["environment"]).max() <= 1e-10 * max(1.0, np.abs(rec["environment"]).max())
+    grad, _ = objective.finish_gradient(Q, R, rho, out["covector"], out["environment"])
+    assert grad_close(rho, grad, rec["gradient"])
+
+
+def test_ode_route_batch_matches_single_states(gpu_context):
+    """One launch over the four states of ode.npz (D = 3, 8, 8, 16, one padded group) at common
+    settings against each state evaluated alone."""
+    from rcmps_b200 import _lib, objective
+    recs = load_records("ode.npz")
+    s = _lib.default_settings(half_window=8.0, n_quad=32)
+    vals, covs, envs, stats = objective.evaluate_phi4_batch([r["R"] for r in recs], [r["K"] for r in recs],
+                                                            [r["rho"] for r in recs], [r["g"] for r in recs], s)
+    for i, rec in enumerate(recs):
+        Q = O.left_canonical_q(rec["R"], rec["K"])
+        one = objective.evaluate_phi4(rec["R"], Q, rec["rho"], rec["g"], half_window=8.0, n_quad=32)
+        assert stats[i]["status"] == 0 and stats[i]["accepted"] == one["stats"]["accepted"]
+        assert abs(vals[i] - one["value"]) <= 1e-13 * max(1.0, abs(one["value"]))
+        assert np.abs(covs[i] - one["covector"]).max() <= 1e-12 * max(1.0, np.abs(one["covector"]).max())
+
+
+def test_ode_route_julia_fixture(gpu_context):
+    """Julia's default evaluation of the fixture state is this route (Vern7 there): energy
+    -0.15648780475169466 within 1e-12, gradient within 5e-9 in the metric norm."""
+    from rcmps_b200 import objective
+    fx = julia_fixture()
+    R, K, rho = fx["R"], fx["K"], fx["rho"]
+    Q = O.left_canonical_q(R, K)
+    out = objective.evaluate_phi4(R, Q, rho, fx["meta"]["coupling"], half_window=20.0, n_quad=192)
+    assert abs(out["value"] - fx["meta"]["energy"]) < 1e-12
+    grad, _ = objective.finish_gradient(Q, R, rho, out["covector"], out["environment"])
+    assert metric_norm(rho, grad - fx["gradient"]) < 5e-9
