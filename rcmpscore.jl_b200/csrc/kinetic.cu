@@ -191,17 +191,45 @@ __global__ void cgs_partial(ArnoldiProblem* __restrict__ probs, int nprob, int j
   for (int r = r0 + threadIdx.x; r < r0 + CH; r += blockDim.x) w[r - r0] = r < r1 ? P.W[r] : make_double2(0, 0);
   __syncthreads();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  for (int i = warp; i <= j; i += nw) {
-    const double2* v = P.V + (size_t)i * P.ldv;
-    double re = 0.0, im = 0.0;
-    for (int r = r0 + lane; r < r1; r += 32) {
-      const double2 a = v[r], b = w[r - r0];
-      re += a.x * b.x + a.y * b.y;
-      im += a.x * b.y - a.y * b.x;
+  // a warp takes two basis vectors at a time, four rows per lane per step: eight independent
+  // 16-byte loads in flight per lane (the pass streams the basis from HBM)
+  for (int i = warp; i <= j; i += 2 * nw) {
+    const bool two = i + nw <= j;
+    const double2* v0 = P.V + (size_t)i * P.ldv;
+    const double2* v1 = P.V + (size_t)(two ? i + nw : i) * P.ldv;
+    double re0 = 0.0, im0 = 0.0, re1 = 0.0, im1 = 0.0;
+    int r = r0 + lane;
+    for (; r + 96 < r1; r += 128) {
+      double2 a[4], c[4], b[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        a[u] = v0[r + 32 * u];
+        c[u] = v1[r + 32 * u];
+        b[u] = w[r - r0 + 32 * u];
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        re0 += a[u].x * b[u].x + a[u].y * b[u].y;
+        im0 += a[u].x * b[u].y - a[u].y * b[u].x;
+        re1 += c[u].x * b[u].x + c[u].y * b[u].y;
+        im1 += c[u].x * b[u].y - c[u].y * b[u].x;
+      }
     }
-    re = warp_sum(re);
-    im = warp_sum(im);
-    if (lane == 0) P.partial[(size_t)ch * P.kmax1 + i] = make_double2(re, im);
+    for (; r < r1; r += 32) {
+      const double2 a = v0[r], c = v1[r], b = w[r - r0];
+      re0 += a.x * b.x + a.y * b.y;
+      im0 += a.x * b.y - a.y * b.x;
+      re1 += c.x * b.x + c.y * b.y;
+      im1 += c.x * b.y - c.y * b.x;
+    }
+    re0 = warp_sum(re0);
+    im0 = warp_sum(im0);
+    re1 = warp_sum(re1);
+    im1 = warp_sum(im1);
+    if (lane == 0) {
+      P.partial[(size_t)ch * P.kmax1 + i] = make_double2(re0, im0);
+      if (two) P.partial[(size_t)ch * P.kmax1 + i + nw] = make_double2(re1, im1);
+    }
   }
   if (pass == 0 && warp == 0) {
     double s = 0.0;
@@ -229,10 +257,24 @@ __global__ void cgs_subtract(ArnoldiProblem* __restrict__ probs, int nprob, int 
   double nrm = 0.0;
   for (int r = r0 + threadIdx.x; r < r1; r += blockDim.x) {
     double2 acc = P.W[r];
-    for (int i = 0; i <= j; ++i) {
-      const double2 v = P.V[(size_t)i * P.ldv + r], c = h[i];
-      acc.x -= v.x * c.x - v.y * c.y;
-      acc.y -= v.x * c.y + v.y * c.x;
+    const double2* v = P.V + r;
+    int i = 0;
+    // four basis rows in flight per thread
+    for (; i + 3 <= j; i += 4) {
+      double2 x[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) x[u] = v[(size_t)(i + u) * P.ldv];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const double2 c = h[i + u];
+        acc.x -= x[u].x * c.x - x[u].y * c.y;
+        acc.y -= x[u].x * c.y + x[u].y * c.x;
+      }
+    }
+    for (; i <= j; ++i) {
+      const double2 x = v[(size_t)i * P.ldv], c = h[i];
+      acc.x -= x.x * c.x - x.y * c.y;
+      acc.y -= x.x * c.y + x.y * c.x;
     }
     P.W[r] = acc;
     nrm += zabs2(acc);
