@@ -932,7 +932,16 @@ cudaError_t cgs_step_launch(ArnoldiProblem* d_probs, int nprob, int j, int n, cu
 cudaError_t hessenberg_launch(ArnoldiProblem* d_probs, int nprob, const double* d_shifts, int nshift,
                               double2* scratch, long long slot_elems, int nslots, int kmax, cudaStream_t s) {
   const int blocks = (nslots * 32 + 255) / 256;
-  if (kmax <= 256) {
+  // MAXC = columns per lane: the smallest template that holds k columns (32 MAXC >= k)
+  if (kmax <= 64) {
+    note_launch();
+    hessenberg_solve<2><<<blocks, 256, 0, s>>>(d_probs, nprob, d_shifts, nshift, scratch, slot_elems, nslots);
+  }
+  else if (kmax <= 128) {
+    note_launch();
+    hessenberg_solve<4><<<blocks, 256, 0, s>>>(d_probs, nprob, d_shifts, nshift, scratch, slot_elems, nslots);
+  }
+  else if (kmax <= 256) {
     note_launch();
     hessenberg_solve<8><<<blocks, 256, 0, s>>>(d_probs, nprob, d_shifts, nshift, scratch, slot_elems, nslots);
   }

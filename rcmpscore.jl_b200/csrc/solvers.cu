@@ -87,14 +87,28 @@ __global__ void gmres_givens(ArnoldiProblem* __restrict__ probs, int nprob, int 
   if (!P.active || P.k != j + 1) return;
   double2* h = P.H;   // column j: h[i * kmax + j]
   const int ld = P.kmax;
-  for (int i = 0; i < j; ++i) {
-    const double2 a = h[i * ld + j], b = h[(i + 1) * ld + j];
-    const double c = P.cs[i].x;
-    const double2 s = P.sn[i];
-    h[i * ld + j] = zadd(zscale(c, a), zmul(s, b));
-    h[(i + 1) * ld + j] = zsub(zscale(c, b), zmul(zconj(s), a));
+  // apply the previous rotations to column j; the running entry stays in registers and the
+  // column, cosines and sines are read eight rows at a time (independent loads in flight)
+  double2 a = h[j];   // h[0][j]
+  for (int i0 = 0; i0 < j; i0 += 8) {
+    const int m = min(8, j - i0);
+    double2 b[8], sn[8];
+    double cs[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u)
+      if (u < m) {
+        b[u] = h[(i0 + u + 1) * ld + j];
+        cs[u] = P.cs[i0 + u].x;
+        sn[u] = P.sn[i0 + u];
+      }
+#pragma unroll
+    for (int u = 0; u < 8; ++u)
+      if (u < m) {
+        h[(i0 + u) * ld + j] = zadd(zscale(cs[u], a), zmul(sn[u], b[u]));
+        a = zsub(zscale(cs[u], b[u]), zmul(zconj(sn[u]), a));
+      }
   }
-  const double2 a = h[j * ld + j], b = h[(j + 1) * ld + j];
+  const double2 b = h[(j + 1) * ld + j];
   const double na = hypot(a.x, a.y), nb = hypot(b.x, b.y);
   double c;
   double2 s;
