@@ -189,6 +189,9 @@ __global__ void cgs_partial(ArnoldiProblem* __restrict__ probs, int nprob, int j
   const int r0 = ch * CH, r1 = min(n, r0 + CH);
   __shared__ double2 w[CH];
   for (int r = r0 + threadIdx.x; r < r0 + CH; r += blockDim.x) w[r - r0] = r < r1 ? P.W[r] : make_double2(0, 0);
+  // before the first projection w = L(V_j): keep it for the true residuals of the shifted solves
+  if (pass == 0 && P.LV)
+    for (int r = r0 + threadIdx.x; r < r1; r += blockDim.x) P.LV[(size_t)j * P.ldv + r] = w[r - r0];
   __syncthreads();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   // a warp takes two basis vectors at a time, four rows per lane per step: eight independent
@@ -532,14 +535,20 @@ __global__ void __launch_bounds__(256) hessenberg_solve(ArnoldiProblem* __restri
 }
 
 // ======================================================================= reconstruction
-// X[p][s][:] = sum_j Yt[p][s][j] V_p[j][:] on tensor cores: CTA tile 64 shifts x 64 columns.
-// Adjoint problems store the conjugate transpose of each solution matrix.
-__global__ void __launch_bounds__(256, 1) reconstruct_kernel(ArnoldiProblem* __restrict__ probs, int nprob,
-                                                             int nshift) {
+// X[p][s][:] = sum_j Yt[p][s][j] V_p[j][:] on tensor cores (CTA tile 64 shifts x 64 columns) and,
+// with the kept actions LV_j = L(V_j), the true residual r = X - c L(X) - rhs =
+// sum_j Yt[p][s][j] (V_j - c LV_j) - rhs (L is linear): its squared norm per 64-column tile into
+// res. Adjoint problems store the conjugate transpose of each solution matrix; their residual
+// norm is that of the untransposed equation (the norm is invariant under the conjugate transpose).
+__global__ void __launch_bounds__(256, 1) reconstruct_residual_kernel(ArnoldiProblem* __restrict__ probs, int nprob,
+                                                                      const double* __restrict__ shifts, int nshift,
+                                                                      double* __restrict__ res, int ntile) {
   constexpr int BM = 64, BN = 64, BK = 16, LDA = BK + 4, LDB = BN;
   extern __shared__ __align__(16) double2 rsm[];
   double2(*As)[BM * LDA] = reinterpret_cast<double2(*)[BM * LDA]>(rsm);
   double2(*Bs)[BK * LDB] = reinterpret_cast<double2(*)[BK * LDB]>(rsm + 2 * BM * LDA);
+  double2(*Cs)[BK * LDB] = reinterpret_cast<double2(*)[BK * LDB]>(rsm + 2 * BM * LDA + 2 * BK * LDB);
+  __shared__ double rowsum[8][16];
   const int p = blockIdx.z;
   ArnoldiProblem& P = probs[p];
   if (!P.reconstruct) return;
@@ -547,9 +556,12 @@ __global__ void __launch_bounds__(256, 1) reconstruct_kernel(ArnoldiProblem* __r
   const int s0 = blockIdx.y * BM, c0 = blockIdx.x * BN;
   if (s0 >= nshift || c0 >= n) return;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  ZFrag acc[4];
+  ZFrag ax[4], aw[4];
 #pragma unroll
-  for (int j = 0; j < 4; ++j) acc[j].zero();
+  for (int j = 0; j < 4; ++j) {
+    ax[j].zero();
+    aw[j].zero();
+  }
   const int mt = warp >> 1, nt0 = (warp & 1) * 4;   // warp: 16-row band mt, 4 tiles of 8 columns
   const int nk = (k + BK - 1) / BK;
   auto load = [&](int kc, int buf) {
@@ -559,7 +571,9 @@ __global__ void __launch_bounds__(256, 1) reconstruct_kernel(ArnoldiProblem* __r
     }
     for (int e = tid; e < BK * BN; e += 256) {
       const int q = e / BN, cc = e % BN, j = kc * BK + q, col = c0 + cc;
-      Bs[buf][q * LDB + cc] = (j < k && col < n) ? P.V[(size_t)j * P.ldv + col] : make_double2(0, 0);
+      const bool in = j < k && col < n;
+      Bs[buf][q * LDB + cc] = in ? P.V[(size_t)j * P.ldv + col] : make_double2(0, 0);
+      Cs[buf][q * LDB + cc] = in ? P.LV[(size_t)j * P.ldv + col] : make_double2(0, 0);
     }
   };
   load(0, 0);
@@ -573,30 +587,50 @@ __global__ void __launch_bounds__(256, 1) reconstruct_kernel(ArnoldiProblem* __r
       load_a(As[buf], LDA, mt * 16, ks * 8, lane, a);
 #pragma unroll
       for (int j = 0; j < 4; ++j) {
-        BFrag b;
+        BFrag b, c;
         load_b(Bs[buf], LDB, ks * 8, (nt0 + j) * 8, lane, b);
-        zmma(acc[j], a, b);
+        load_b(Cs[buf], LDB, ks * 8, (nt0 + j) * 8, lane, c);
+        zmma(ax[j], a, b);
+        zmma(aw[j], a, c);
       }
     }
     __syncthreads();
   }
   const int dp = P.dp;
+  double part[2] = {0.0, 0.0};   // rows g and g + 8 of the warp's band
 #pragma unroll
   for (int j = 0; j < 4; ++j)
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
       const int s = s0 + mt * 16 + frag_row(lane, i), col = c0 + (nt0 + j) * 8 + frag_col(lane, i);
       if (s < nshift && col < n) {
-        const double2 v = acc[j].value(i);
+        const double2 v = ax[j].value(i);
+        const double2 r = zsub(zsub(v, zscale(shifts[s], aw[j].value(i))), P.rhs[col]);
+        part[i >> 1] += zabs2(r);
         double2* X = P.X + (size_t)s * n;
         if (P.adjoint) {
-          const int r = col / dp, cc = col % dp;
-          X[(size_t)cc * dp + r] = zconj(v);
+          const int rr = col / dp, cc = col % dp;
+          X[(size_t)cc * dp + rr] = zconj(v);
         } else {
           X[col] = v;
         }
       }
     }
+  // sum over the four lanes of a row, then over the two warps of a band
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    part[h] += __shfl_xor_sync(0xffffffffu, part[h], 1);
+    part[h] += __shfl_xor_sync(0xffffffffu, part[h], 2);
+  }
+  if ((lane & 3) == 0) {
+    rowsum[warp][lane >> 2] = part[0];
+    rowsum[warp][8 + (lane >> 2)] = part[1];
+  }
+  __syncthreads();
+  if (tid < BM) {
+    const int band = tid >> 4, r = tid & 15, s = s0 + tid;
+    if (s < nshift) res[((size_t)p * nshift + s) * ntile + blockIdx.x] = rowsum[2 * band][r] + rowsum[2 * band + 1][r];
+  }
 }
 
 // ======================================================================= contraction
@@ -956,13 +990,14 @@ cudaError_t hessenberg_launch(ArnoldiProblem* d_probs, int nprob, const double* 
   return cudaGetLastError();
 }
 
-cudaError_t reconstruct_launch(ArnoldiProblem* d_probs, int nprob, int nshift, int n, cudaStream_t s) {
+cudaError_t reconstruct_residual_launch(ArnoldiProblem* d_probs, int nprob, const double* d_shifts, int nshift,
+                                        int n, double* d_res, cudaStream_t s) {
   dim3 grid((n + 63) / 64, (nshift + 63) / 64, nprob);
-  const int smem = (2 * 64 * 20 + 2 * 16 * 64) * 16;
-  cudaError_t e = cudaFuncSetAttribute(reconstruct_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  const int smem = (2 * 64 * 20 + 4 * 16 * 64) * 16;
+  cudaError_t e = cudaFuncSetAttribute(reconstruct_residual_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   if (e != cudaSuccess) return e;
   note_launch();
-  reconstruct_kernel<<<grid, 256, smem, s>>>(d_probs, nprob, nshift);
+  reconstruct_residual_kernel<<<grid, 256, smem, s>>>(d_probs, nprob, d_shifts, nshift, d_res, (n + 63) / 64);
   return cudaGetLastError();
 }
 

@@ -28,6 +28,7 @@ struct ArnoldiProblem {
   double2* partial;          // [nchunk][kmax1]
   double* norms;             // [2 nchunk]
   double2* Yt;               // [nshift][kmax] projected solutions
+  double2* LV;               // [kmax][ldv] L(V_j), kept for the true residuals (kinetic problems; else NULL)
   double2* X;                // [nshift][n] solutions (adjoint problems: conjugate transposed)
   const double2 *A1, *A1h, *A2, *A2h;   // L = A1 X + X A1h + A2 X A2h
   const double2* trw;        // GMRES operators: -L(X) + tr(trw X) I
@@ -77,7 +78,10 @@ cudaError_t arnoldi_start_launch(ArnoldiProblem* d_probs, int nprob, cudaStream_
 cudaError_t cgs_step_launch(ArnoldiProblem* d_probs, int nprob, int j, int n, cudaStream_t s);
 cudaError_t hessenberg_launch(ArnoldiProblem* d_probs, int nprob, const double* d_shifts, int nshift,
                               double2* scratch, long long slot_elems, int nslots, int kmax, cudaStream_t s);
-cudaError_t reconstruct_launch(ArnoldiProblem* d_probs, int nprob, int nshift, int n, cudaStream_t s);
+// X = V Y for every shift and the true residual |X - c L(X) - rhs|^2 = |(V - c LV) Y - rhs|^2 per
+// (problem, shift, 64-column tile) into res[p][s][n/64]
+cudaError_t reconstruct_residual_launch(ArnoldiProblem* d_probs, int nprob, const double* d_shifts, int nshift,
+                                        int n, double* d_res, cudaStream_t s);
 cudaError_t residual_reduce_launch(ArnoldiProblem* d_probs, int nprob, const double* d_res, int nshift, int rbs,
                                    cudaStream_t s);
 cudaError_t kinetic_rhs_launch(const KineticSetup& a, int nstates, cudaStream_t s);

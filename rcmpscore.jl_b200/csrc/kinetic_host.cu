@@ -35,9 +35,9 @@ size_t kinetic_state_bytes(int dp, int kmax, int nshift) {
   const int nchunk = (dp * dp + CHROWS - 1) / CHROWS;
   const int nblk = (nshift + kContractNodesPerBlock - 1) / kContractNodesPerBlock;
   size_t b = 3 * mat + 8 * mat + 2 * mat + 4 * mat;                 // inputs, ops, C, rhs
-  b += 4 * ((size_t)(kmax + 1) * mat + (size_t)(kmax + 1) * kmax * 16 + mat + (size_t)nchunk * (kmax + 1) * 16 +
-            (size_t)nshift * kmax * 16 + (size_t)nshift * mat);      // per problem
-  b += 4 * (size_t)nshift * (dp / 16) * 8 + 4 * (size_t)nshift * sizeof(LindbladTask);
+  b += 4 * ((size_t)(2 * kmax + 1) * mat + (size_t)(kmax + 1) * kmax * 16 + mat + (size_t)nchunk * (kmax + 1) * 16 +
+            (size_t)nshift * kmax * 16 + (size_t)nshift * mat);      // per problem (V, L(V), H, ...)
+  b += 4 * (size_t)nshift * ((dp * dp + 63) / 64) * 8;
   b += 2 * (size_t)nblk * 4 * mat + 12 * mat;                        // contraction
   return b + 4096;
 }
@@ -89,7 +89,7 @@ int kinetic_run(rcmps_context* ctx, KineticJob& job, cudaStream_t stream) {
       const size_t mat = (size_t)dp * dp;
       const int nvec = dp * dp;
       const int nchunk = (nvec + CHROWS - 1) / CHROWS;
-      const int rbs = dp / 16;
+      const int ntile = (nvec + 63) / 64;   // column tiles of the residual partial sums
       const int nblk = (nshift + kContractNodesPerBlock - 1) / kContractNodesPerBlock;
       Layout L;
       const size_t o_dims = L.add(n * 4), o_off = L.add(n * 8), o_idx = L.add(n * 4);
@@ -98,6 +98,7 @@ int kinetic_run(rcmps_context* ctx, KineticJob& job, cudaStream_t stream) {
       const size_t o_comm = L.add(n * 2 * mat * 16), o_rhs = L.add(n * 4 * mat * 16);
       const size_t o_probs = L.add(NP * sizeof(ArnoldiProblem));
       const size_t o_V = L.add((size_t)NP * (kmax + 1) * mat * 16);
+      const size_t o_LV = L.add((size_t)NP * kmax * mat * 16);
       const size_t o_H = L.add((size_t)NP * (kmax + 1) * kmax * 16);
       const size_t o_W = L.add((size_t)NP * mat * 16);
       const size_t o_part = L.add((size_t)NP * nchunk * (kmax + 1) * 16);
@@ -106,8 +107,7 @@ int kinetic_run(rcmps_context* ctx, KineticJob& job, cudaStream_t stream) {
       const size_t o_X = L.add((size_t)NP * nshift * mat * 16);
       const size_t o_flags = L.add(NP * 4 + n * 4);
       const size_t o_mtasks = L.add(NP * sizeof(LindbladTask));
-      const size_t o_rtasks = L.add((size_t)NP * nshift * sizeof(LindbladTask));
-      const size_t o_res = L.add((size_t)NP * nshift * rbs * 8);
+      const size_t o_res = L.add((size_t)NP * nshift * ntile * 8);
       const size_t o_cpart = L.add((size_t)2 * n * nblk * 4 * mat * 16);
       const size_t o_fin = L.add((size_t)n * 12 * mat * 16);
       const size_t o_val = L.add(n * 8);
@@ -129,7 +129,7 @@ int kinetic_run(rcmps_context* ctx, KineticJob& job, cudaStream_t stream) {
       Layout H;
       const size_t h_dims = H.add(n * 4), h_off = H.add(n * 8), h_shift = H.add(nshift * 8),
                    h_weight = H.add(nshift * 8), h_probs = H.add(NP * sizeof(ArnoldiProblem)),
-                   h_rt = H.add((size_t)NP * nshift * sizeof(LindbladTask)), h_ptrs = H.add((size_t)9 * n * sizeof(void*)),
+                   h_ptrs = H.add((size_t)9 * n * sizeof(void*)),
                    h_flag = H.add(n * 4), h_idx = H.add(n * 4);
       if (pinned_reserve(SL, H.total) != cudaSuccess) return fail(ctx, RCMPS_CUDA_ERROR, "pinned host buffer");
       char* h = static_cast<char*>(SL.pinned);
@@ -138,7 +138,6 @@ int kinetic_run(rcmps_context* ctx, KineticJob& job, cudaStream_t stream) {
       double* hs = (double*)(h + h_shift);
       double* hw = (double*)(h + h_weight);
       ArnoldiProblem* hp = (ArnoldiProblem*)(h + h_probs);
-      LindbladTask* hrt = (LindbladTask*)(h + h_rt);
       const void** hptr = (const void**)(h + h_ptrs);
       int* hflag = (int*)(h + h_flag);
       int* hidx = (int*)(h + h_idx);
@@ -175,6 +174,7 @@ int kinetic_run(rcmps_context* ctx, KineticJob& job, cudaStream_t stream) {
           ArnoldiProblem& A = hp[p];
           std::memset(&A, 0, sizeof(A));
           A.V = (double2*)P(o_V) + (size_t)p * (kmax + 1) * mat;
+          A.LV = (double2*)P(o_LV) + (size_t)p * kmax * mat;
           A.ldv = (long long)mat;
           A.H = (double2*)P(o_H) + (size_t)p * (kmax + 1) * kmax;
           A.W = (double2*)P(o_W) + (size_t)p * mat;
@@ -269,35 +269,10 @@ int kinetic_run(rcmps_context* ctx, KineticJob& job, cudaStream_t stream) {
           anyrec |= A.reconstruct;
         }
         if (anyrec) {
-          int nt = 0;
-          for (int p = 0; p < NP; ++p) {
-            const ArnoldiProblem& A = hp[p];
-            if (!A.reconstruct) continue;
-            const int i = p / 4, q = p % 4;
-            const double2* ops = d_ops + (size_t)i * 8 * mat;
-            // adjoint problems hold a = A^dag, whose residual uses rhs^dag = op (R or C)
-            const double2* rhs = (q & 1) ? (q == 1 ? ops + 2 * mat : d_comm + (size_t)i * 2 * mat) : A.rhs;
-            for (int s = 0; s < nshift; ++s) {
-              LindbladTask& t = hrt[nt++];
-              t.X = A.X + (size_t)s * mat;
-              t.out = nullptr;
-              t.A1 = A.A1;
-              t.A1h = A.A1h;
-              t.A2 = A.A2;
-              t.A2h = A.A2h;
-              t.rhs = rhs;
-              t.res = (double*)P(o_res) + ((size_t)p * nshift + s) * rbs;
-              t.shift = shifts[s];
-              t.flag = A.flag;
-              t.trw = nullptr;
-              t.d = 0;
-            }
-          }
+          // reconstruction and true residuals in one pass over the basis and its kept actions
           e = cudaMemcpyAsync(d_probs, hp, NP * sizeof(ArnoldiProblem), cudaMemcpyHostToDevice, stream);
-          if (!e) e = reconstruct_launch(d_probs, NP, nshift, nvec, stream);
-          if (!e) e = cudaMemcpyAsync(P(o_rtasks), hrt, (size_t)nt * sizeof(LindbladTask), cudaMemcpyHostToDevice, stream);
-          if (!e) e = lindblad_launch(dp, (LindbladTask*)P(o_rtasks), nt, 1, stream);
-          if (!e) e = residual_reduce_launch(d_probs, NP, (double*)P(o_res), nshift, rbs, stream);
+          if (!e) e = reconstruct_residual_launch(d_probs, NP, (double*)P(o_shift), nshift, nvec, (double*)P(o_res), stream);
+          if (!e) e = residual_reduce_launch(d_probs, NP, (double*)P(o_res), nshift, ntile, stream);
           if (!e) e = cudaMemcpyAsync(hp, d_probs, NP * sizeof(ArnoldiProblem), cudaMemcpyDeviceToHost, stream);
           if (!e) e = cudaStreamSynchronize(stream);
           if (e) return fail(ctx, RCMPS_CUDA_ERROR, std::string("kinetic residuals: ") + cudaGetErrorString(e));
