@@ -210,7 +210,7 @@ def run_b200(args, rank, world, local_rank):
 
     for _ in range(args.warmup):
         step()
-    traj_ms, pull_ms, kin_ms, fin_ms = [], [], [], []
+    traj_ms, pull_ms, kin_ms, fin_ms, call_ms = [], [], [], [], []
     barrier()
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     launches0 = lib.rcmps_launch_count()   # library launches before the timed region
@@ -223,6 +223,7 @@ def run_b200(args, rank, world, local_rank):
             pull_ms.append(t[1])
             kin_ms.append(t[2])
             fin_ms.append(t[3])
+            call_ms.append(t[4])
         end.record(stream)
         barrier()
     launches = (lib.rcmps_launch_count() - launches0) // args.steps
@@ -299,7 +300,8 @@ def run_b200(args, rank, world, local_rank):
                              "peak_source": "FP64 mma.sync throughput measured in this run (rcmps_fp64_peak_tflops)",
                              "flops_per_launch": flops, "launch_ms": traj},
                 "phases_ms": {"trajectory": traj, "pullback": statistics.mean(pull_ms),
-                              "kinetic": statistics.mean(kin_ms), "boundary_finish": statistics.mean(fin_ms)},
+                              "kinetic": statistics.mean(kin_ms), "boundary_finish": statistics.mean(fin_ms),
+                              "whole_call": statistics.mean(call_ms)},
                 "steps_per_state": {"rhs_calls_mean": statistics.mean(rhs_calls), "accepted_mean":
                                     statistics.mean(stats[i].accepted for i in range(n))},
                 "gpu_launches": None, "gpu_launches_note": "library kernel launches per step (rcmps_launch_count)", "clocks": clocks.summary(), "e2e": e2e, "cpu_baseline": cpu}
