@@ -303,7 +303,9 @@ def run_b200(args, rank, world, local_rank):
                               "kinetic": statistics.mean(kin_ms), "boundary_finish": statistics.mean(fin_ms),
                               "whole_call": statistics.mean(call_ms)},
                 "steps_per_state": {"rhs_calls_mean": statistics.mean(rhs_calls), "accepted_mean":
-                                    statistics.mean(stats[i].accepted for i in range(n))},
+                                    statistics.mean(stats[i].accepted for i in range(n)),
+                                    "gmres_iterations_mean": statistics.mean(stats[i].gmres_iterations for i in range(n)),
+                                    "krylov_basis_max": max(max(stats[i].krylov_basis) for i in range(n))},
                 "gpu_launches": None, "gpu_launches_note": "library kernel launches per step (rcmps_launch_count)", "clocks": clocks.summary(), "e2e": e2e, "cpu_baseline": cpu}
         line["gpu_launches"] = launches
         line["launches_before_timed"] = launches0

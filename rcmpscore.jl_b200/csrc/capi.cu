@@ -7,6 +7,7 @@
 #include <cstring>
 #include <atomic>
 #include <map>
+#include <mutex>
 #include <string>
 #include <thread>
 #include <vector>
@@ -95,7 +96,25 @@ int padded_dim(int d) {
 }
 
 // Gauss-Legendre nodes and weights on [-1, 1] by Newton's method on the Legendre recurrence.
+static void gauss_legendre_compute(int n, std::vector<double>& x, std::vector<double>& w);
+
+// Gauss-Legendre nodes and weights on [-1, 1], computed once per n and kept (the Newton iteration
+// costs tens of milliseconds at n = 512, and every call of the library needs the same rules).
 void gauss_legendre(int n, std::vector<double>& x, std::vector<double>& w) {
+  static std::mutex mu;
+  static std::map<int, std::pair<std::vector<double>, std::vector<double>>> cache;
+  std::lock_guard<std::mutex> lock(mu);
+  auto it = cache.find(n);
+  if (it == cache.end()) {
+    std::vector<double> cx, cw;
+    gauss_legendre_compute(n, cx, cw);
+    it = cache.emplace(n, std::make_pair(std::move(cx), std::move(cw))).first;
+  }
+  x = it->second.first;
+  w = it->second.second;
+}
+
+static void gauss_legendre_compute(int n, std::vector<double>& x, std::vector<double>& w) {
   x.assign(n, 0.0);
   w.assign(n, 0.0);
   const double pi = 3.14159265358979323846;
