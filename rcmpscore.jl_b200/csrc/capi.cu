@@ -6,6 +6,7 @@
 #include <cstdio>
 #include <cstring>
 #include <atomic>
+#include <future>
 #include <map>
 #include <mutex>
 #include <string>
@@ -192,15 +193,16 @@ int check_dims(rcmps_context* ctx, int n, const int* dims) {
   return RCMPS_OK;
 }
 
-// energy = vq + vk; covector = cq + ck; environment = eq + ek (packed arrays of `total` complex values)
+// energy = vq + vk; covector = cq + ck; environment = eq + ek (packed arrays of `total` complex values);
+// a NULL output is skipped
 __global__ void sum_parts_kernel(int n, long long total, const double* vq, const double* vk, const double2* cq,
                                  const double2* ck, const double2* eq, const double2* ek, double* energy,
                                  double2* cov, double2* env) {
   const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (i < n) energy[i] = vq[i] + vk[i];
+  if (i < n && energy) energy[i] = vq[i] + vk[i];
   for (long long e = i; e < total; e += (long long)gridDim.x * blockDim.x) {
-    cov[e] = zadd(cq[e], ck[e]);
-    env[e] = zadd(eq[e], ek[e]);
+    if (cov) cov[e] = zadd(cq[e], ck[e]);
+    if (env) env[e] = zadd(eq[e], ek[e]);
   }
 }
 
@@ -478,6 +480,9 @@ int rcmps_stationary_state_batch(rcmps_context* ctx, int n, const int* dims, con
   return stationary_run(ctx, job, s);
 }
 
+// SMs the quartic pullback leaves free for the boundary solve that overlaps it
+constexpr int kBoundarySMs = 32;
+
 int rcmps_fg_phi4_batch(rcmps_context* ctx, int n, const int* dims, const double* couplings, const double* R,
                         const double* K, const double* rho, const rcmps_settings* settings, double* energy,
                         double* gradient, double* covector, double* environment, rcmps_state_stats* stats,
@@ -542,29 +547,33 @@ int rcmps_fg_phi4_batch(rcmps_context* ctx, int n, const int* dims, const double
   kj.stats = kst.data();
   kj.slot = 1;
   kj.memory_share = 0.3;
-  int krc = RCMPS_OK;
-  std::thread worker([&] {
+  // The kinetic term runs on its own thread and stream, the quartic term on another. The boundary
+  // solve needs only the environment, which the quartic term writes right after its trajectory:
+  // the solve starts then and runs while the quartic pullback produces the covector.
+  int krc = RCMPS_OK, qrc = RCMPS_OK;
+  std::promise<bool> env_promise;
+  std::future<bool> env_future = env_promise.get_future();
+  bool env_signalled = false;
+  qj.env_ready = ctx->slot[0].ev[3];
+  // the pullback leaves SMs to the boundary solve that runs beside it
+  qj.pullback_ctas = std::max(1, ctx->sms - kBoundarySMs);
+  qj.on_env = [&] {
+    env_signalled = true;
+    env_promise.set_value(true);
+  };
+  std::thread kworker([&] {
     cudaSetDevice(ctx->device);
     krc = kinetic_run(ctx, kj, ctx->slot[1].stream);
   });
-  const int qrc = quartic_run(ctx, qj, ctx->slot[0].stream);
-  worker.join();
-  for (int i = 0; i < n; ++i) {
-    stats[i].kinetic_value = kst[i].kinetic_value;
-    for (int q = 0; q < 4; ++q) stats[i].krylov_basis[q] = kst[i].krylov_basis[q];
-    stats[i].krylov_residual = kst[i].krylov_residual;
-    if (!stats[i].status && kst[i].status) {
-      stats[i].status = kst[i].status;
-      stats[i].failed_component = kst[i].failed_component;
-    }
-  }
-  if (qrc || krc) return qrc ? qrc : krc;
+  std::thread qworker([&] {
+    cudaSetDevice(ctx->device);
+    qrc = quartic_run(ctx, qj, ctx->slot[0].stream);
+    if (!env_signalled) env_promise.set_value(false);
+  });
+  kworker.join();
+  const bool env_ok = env_future.get();
   cudaStream_t s2 = ctx->slot[2].stream;
-  cudaEventRecord(ctx->slot[2].ev[1], s2);
-  note_launch();
-  sum_parts_kernel<<<(int)std::min<long long>(4096, (total + 255) / 256 + 1), 256, 0, s2>>>(
-      n, total, vq, vk, (double2*)cq, (double2*)ck, (double2*)eq, (double2*)ek, energy, (double2*)csum,
-      (double2*)esum);
+  const int nsum = (int)std::min<long long>(4096, (total + 255) / 256 + 1);
   std::vector<rcmps_state_stats> fst(n);
   std::memset(fst.data(), 0, n * sizeof(rcmps_state_stats));
   FinishJob fj;
@@ -579,7 +588,36 @@ int rcmps_fg_phi4_batch(rcmps_context* ctx, int n, const int* dims, const double
   fj.gradient = gradient;
   fj.stats = fst.data();
   fj.slot = 2;
-  const int frc = finish_run(ctx, fj, s2);
+  FinishPlan plan;
+  int frc = RCMPS_OK;
+  const bool solve = env_ok && krc == RCMPS_OK;
+  if (solve) {
+    cudaStreamWaitEvent(s2, qj.env_ready, 0);
+    cudaEventRecord(ctx->slot[2].ev[1], s2);
+    note_launch();
+    sum_parts_kernel<<<nsum, 256, 0, s2>>>(n, total, vq, vk, (double2*)cq, (double2*)ck, (double2*)eq, (double2*)ek,
+                                           nullptr, nullptr, (double2*)esum);
+    frc = finish_solve(ctx, fj, s2, plan);
+  }
+  qworker.join();
+  for (int i = 0; i < n; ++i) {
+    stats[i].kinetic_value = kst[i].kinetic_value;
+    for (int q = 0; q < 4; ++q) stats[i].krylov_basis[q] = kst[i].krylov_basis[q];
+    stats[i].krylov_residual = kst[i].krylov_residual;
+    if (!stats[i].status && kst[i].status) {
+      stats[i].status = kst[i].status;
+      stats[i].failed_component = kst[i].failed_component;
+    }
+  }
+  if (qrc || krc) return qrc ? qrc : krc;
+  if (!solve) return fail(ctx, RCMPS_CUDA_ERROR, "fg_phi4: the quartic environment was not produced");
+  if (frc == RCMPS_OK) {
+    note_launch();
+    sum_parts_kernel<<<nsum, 256, 0, s2>>>(n, total, vq, vk, (double2*)cq, (double2*)ck, (double2*)eq,
+                                           (double2*)ek, energy, (double2*)csum, nullptr);
+    cudaStreamWaitEvent(s2, ctx->slot[0].ev[2], 0);   // the covector is complete with the pullback
+    frc = finish_complete(ctx, fj, s2, plan);
+  }
   cudaEventRecord(ctx->slot[2].ev[2], s2);
   cudaEventSynchronize(ctx->slot[2].ev[2]);
   cudaEventElapsedTime(&ctx->last_ms[3], ctx->slot[2].ev[1], ctx->slot[2].ev[2]);

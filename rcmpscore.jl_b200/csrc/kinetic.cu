@@ -29,19 +29,21 @@ struct LGeo {
   static constexpr int T2 = DP / 8;
   static constexpr int NW = T2 > 8 ? 8 : T2;           // 2, 4, 6, 8, 12->8? (96: 12 tiles)
   static constexpr int KC = DP <= 64 ? 16 : 8;
-  static constexpr int NST = 4;
+  static constexpr int NST = DP <= 64 ? 2 : 4;         // two ring stages keep two CTAs per SM at DP <= 64
   static constexpr int LDP = DP + 4, LDA2 = 2 * DP + 4;
   static constexpr int NT = 32 * NW;
   static constexpr size_t SMEM = ((size_t)32 * LDP + 16 * LDA2 + (size_t)NST * KC * (DP + kBPad)) * 16 + 128;
+  static constexpr int MINB = SMEM <= 110 * 1024 ? 2 : 1;   // resident CTAs per SM
 };
 template <>
 struct LGeo<96> {
   static constexpr int NW = 12, KC = 8, NST = 4, LDP = 100, LDA2 = 196, NT = 384;
   static constexpr size_t SMEM = ((size_t)32 * LDP + 16 * LDA2 + (size_t)NST * KC * (96 + kBPad)) * 16 + 128;
+  static constexpr int MINB = 1;
 };
 
 template <int DP>
-__global__ void __launch_bounds__(LGeo<DP>::NT, 1)
+__global__ void __launch_bounds__(LGeo<DP>::NT, LGeo<DP>::MINB)
 lindblad_kernel(const LindbladTask* __restrict__ tasks, int ntasks, int mode) {
   using LG = LGeo<DP>;
   using GR = RowGemmRing<DP, LG::NW, LG::KC, LG::NST>;

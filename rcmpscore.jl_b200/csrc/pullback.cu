@@ -12,6 +12,7 @@
 // accumulation passes on FP64 tensor cores (RowGemm), each CTA owning one block of output rows
 // and a range of nodes; partial sums are reduced in a fixed order.
 #include <cuda_runtime.h>
+#include <algorithm>
 #include "common.cuh"
 #include "gemm.cuh"
 #include "pullback.h"
@@ -45,15 +46,10 @@ pullback_kernel(PullbackArgs a) {
   int* flag = reinterpret_cast<int*>(full + PG::NST);
 
   constexpr int MAT = DP * DP, VEC = 7 * MAT;
-  const int blk = blockIdx.x;
-  const int state = blockIdx.y / PG::NRB, rb = blockIdx.y % PG::NRB;
   const int n = a.nodes;
-  const int i0 = blk * a.nodes_per_block, i1 = min(n, i0 + a.nodes_per_block);
-  const double2* samples = a.samples + (size_t)state * a.samples_stride;
-  const double2* ops = a.ops + (size_t)state * a.ops_stride;
-  const double2* R = ops + 2 * MAT;
-  const double2* Rh = ops + 3 * MAT;
-  double2* wscr = a.scratch + ((size_t)blockIdx.y * gridDim.x + blk) * 3 * MAT;
+  const int nblk = a.nblk;
+  const int items = nblk * a.nstates * PG::NRB;   // (node block, state, row block) work items
+  double2* wscr = a.scratch + (size_t)blockIdx.x * 3 * MAT;
   const int tid = threadIdx.x;
 
   GM gm;
@@ -65,110 +61,143 @@ pullback_kernel(PullbackArgs a) {
   gm.init();
   __syncthreads();
 
-  auto fwd = [&](int i, int k) { return samples + (size_t)i * VEC + (size_t)(k - 1) * MAT; };       // f_k, k=1..3
-  auto adj = [&](int i, int k) { return samples + (size_t)(n - 1 - i) * VEC + (size_t)(3 + k) * MAT; };  // b_k, k=0..3
-  auto load_rows = [&](double2* dst, const double2* src, int row0, double scale) {
-    for (int e = tid; e < PG::MB * DP; e += PG::NT) {
-      const int r = e / DP, c = e % DP;
-      dst[r * PG::LDA + c] = zscale(scale, src[(size_t)(row0 + r) * DP + c]);
-    }
-  };
+  // a CTA takes items in turn (the grid may be smaller than the item count, so that the pullback
+  // can leave SMs to concurrent work)
+  for (int item = blockIdx.x; item < items; item += gridDim.x) {
+    const int blk = item % nblk, ys = item / nblk;
+    const int state = ys / PG::NRB, rb = ys % PG::NRB;
+    const int i0 = blk * a.nodes_per_block, i1 = min(n, i0 + a.nodes_per_block);
+    const double2* samples = a.samples + (size_t)state * a.samples_stride;
+    const double2* ops = a.ops + (size_t)state * a.ops_stride;
+    const double2* R = ops + 2 * MAT;
+    const double2* Rh = ops + 3 * MAT;
 
-  ZFrag acc[GM::TPW], tmp[GM::TPW];
-  for (int pass = 0; pass < 4; ++pass) {
-#pragma unroll
-    for (int j = 0; j < GM::TPW; ++j) acc[j].zero();
-    if (pass == 0 && PG::NRB == 1) {
-      load_rows(bufX, Rh, 0, 1.0);
-      __syncthreads();
-    }
-    for (int i = i0; i < i1; ++i) {
-      const double w = a.wj[2 * i], jv = a.wj[2 * i + 1];
-      for (int k = 1; k <= 3; ++k) {
-        const double c = jv * (k + 1);
-        typename GM::Segs sb;
-        sb.n = 1;
-        sb.rows[0] = DP;
-        if (pass == 0) {
-          // W_k = w R^dag b_k + c b_{k+1} (all rows) -> scratch
-          for (int rbw = 0; rbw < PG::NRB; ++rbw) {
-            if (PG::NRB > 1) {
-              load_rows(bufX, Rh, rbw * PG::MB, 1.0);
-              __syncthreads();
+    auto fwd = [&](int i, int k) { return samples + (size_t)i * VEC + (size_t)(k - 1) * MAT; };       // f_k, k=1..3
+    auto adj = [&](int i, int k) { return samples + (size_t)(n - 1 - i) * VEC + (size_t)(3 + k) * MAT; };  // b_k, k=0..3
+    auto load_rows = [&](double2* dst, const double2* src, int row0, double scale) {
+      for (int e = tid; e < PG::MB * DP; e += PG::NT) {
+        const int r = e / DP, c = e % DP;
+        dst[r * PG::LDA + c] = zscale(scale, src[(size_t)(row0 + r) * DP + c]);
+      }
+    };
+
+    ZFrag acc[GM::TPW], tmp[GM::TPW];
+    for (int pass = 0; pass < 4; ++pass) {
+  #pragma unroll
+      for (int j = 0; j < GM::TPW; ++j) acc[j].zero();
+      if (pass == 0 && PG::NRB == 1) {
+        load_rows(bufX, Rh, 0, 1.0);
+        __syncthreads();
+      }
+      for (int i = i0; i < i1; ++i) {
+        const double w = a.wj[2 * i], jv = a.wj[2 * i + 1];
+        for (int k = 1; k <= 3; ++k) {
+          const double c = jv * (k + 1);
+          typename GM::Segs sb;
+          sb.n = 1;
+          sb.rows[0] = DP;
+          if (pass == 0) {
+            // W_k = w R^dag b_k + c b_{k+1} (all rows) -> scratch
+            for (int rbw = 0; rbw < PG::NRB; ++rbw) {
+              if (PG::NRB > 1) {
+                load_rows(bufX, Rh, rbw * PG::MB, 1.0);
+                __syncthreads();
+              }
+  #pragma unroll
+              for (int j = 0; j < GM::TPW; ++j) tmp[j].zero();
+              sb.ptr[0] = adj(i, k);
+              gm.run(tmp, bufX, PG::LDA, sb);
+  #pragma unroll
+              for (int j = 0; j < GM::TPW; ++j)
+  #pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                  int row, col;
+                  GM::coord(j, e, row, col);
+                  row += rbw * PG::MB;
+                  double2 v = zscale(w, tmp[j].value(e));
+                  if (k < 3) v = zaxpy(c, adj(i, k + 1)[row * DP + col], v);
+                  else if (row == col) v.x += c;
+                  wscr[(k - 1) * MAT + row * DP + col] = v;
+                }
             }
-#pragma unroll
-            for (int j = 0; j < GM::TPW; ++j) tmp[j].zero();
+            fence_proxy_async_global();   // W_k is read next by bulk copies
+            __syncthreads();
+            load_rows(bufY, fwd(i, k), rb * PG::MB, 1.0);
+            __syncthreads();
+            sb.ptr[0] = wscr + (k - 1) * MAT;
+            gm.run(acc, bufY, PG::LDA, sb);
+          } else if (pass == 1) {
+            load_rows(bufY, fwd(i, k), rb * PG::MB, w);   // P += w f_k b_k
+            __syncthreads();
             sb.ptr[0] = adj(i, k);
+            gm.run(acc, bufY, PG::LDA, sb);
+          } else if (pass == 2) {
+            // W'_k rows = w b_k R + c b_{k+1} -> bufY; then nn += W'_k f_k
+            load_rows(bufX, adj(i, k), rb * PG::MB, 1.0);
+            __syncthreads();
+  #pragma unroll
+            for (int j = 0; j < GM::TPW; ++j) tmp[j].zero();
+            sb.ptr[0] = R;
             gm.run(tmp, bufX, PG::LDA, sb);
-#pragma unroll
+  #pragma unroll
             for (int j = 0; j < GM::TPW; ++j)
-#pragma unroll
+  #pragma unroll
               for (int e = 0; e < 4; ++e) {
                 int row, col;
                 GM::coord(j, e, row, col);
-                row += rbw * PG::MB;
+                const int grow = row + rb * PG::MB;
                 double2 v = zscale(w, tmp[j].value(e));
-                if (k < 3) v = zaxpy(c, adj(i, k + 1)[row * DP + col], v);
-                else if (row == col) v.x += c;
-                wscr[(k - 1) * MAT + row * DP + col] = v;
+                if (k < 3) v = zaxpy(c, adj(i, k + 1)[grow * DP + col], v);
+                else if (grow == col) v.x += c;
+                bufY[row * PG::LDA + col] = v;
               }
+            __syncthreads();
+            sb.ptr[0] = fwd(i, k);
+            gm.run(acc, bufY, PG::LDA, sb);
+          } else {
+            load_rows(bufX, adj(i, k), rb * PG::MB, w);   // P' += w b_k f_k
+            __syncthreads();
+            sb.ptr[0] = fwd(i, k);
+            gm.run(acc, bufX, PG::LDA, sb);
           }
-          fence_proxy_async_global();   // W_k is read next by bulk copies
-          __syncthreads();
-          load_rows(bufY, fwd(i, k), rb * PG::MB, 1.0);
-          __syncthreads();
-          sb.ptr[0] = wscr + (k - 1) * MAT;
-          gm.run(acc, bufY, PG::LDA, sb);
-        } else if (pass == 1) {
-          load_rows(bufY, fwd(i, k), rb * PG::MB, w);   // P += w f_k b_k
-          __syncthreads();
-          sb.ptr[0] = adj(i, k);
-          gm.run(acc, bufY, PG::LDA, sb);
-        } else if (pass == 2) {
-          // W'_k rows = w b_k R + c b_{k+1} -> bufY; then nn += W'_k f_k
-          load_rows(bufX, adj(i, k), rb * PG::MB, 1.0);
-          __syncthreads();
-#pragma unroll
-          for (int j = 0; j < GM::TPW; ++j) tmp[j].zero();
-          sb.ptr[0] = R;
-          gm.run(tmp, bufX, PG::LDA, sb);
-#pragma unroll
-          for (int j = 0; j < GM::TPW; ++j)
-#pragma unroll
-            for (int e = 0; e < 4; ++e) {
-              int row, col;
-              GM::coord(j, e, row, col);
-              const int grow = row + rb * PG::MB;
-              double2 v = zscale(w, tmp[j].value(e));
-              if (k < 3) v = zaxpy(c, adj(i, k + 1)[grow * DP + col], v);
-              else if (grow == col) v.x += c;
-              bufY[row * PG::LDA + col] = v;
-            }
-          __syncthreads();
-          sb.ptr[0] = fwd(i, k);
-          gm.run(acc, bufY, PG::LDA, sb);
-        } else {
-          load_rows(bufX, adj(i, k), rb * PG::MB, w);   // P' += w b_k f_k
-          __syncthreads();
-          sb.ptr[0] = fwd(i, k);
-          gm.run(acc, bufX, PG::LDA, sb);
         }
       }
+      // store this CTA's partial of matrix `pass` (m, P, nn, P') on its rows
+      double2* out = a.partial + (((size_t)state * nblk + blk) * 4 + pass) * MAT;
+  #pragma unroll
+      for (int j = 0; j < GM::TPW; ++j)
+  #pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          int row, col;
+          GM::coord(j, e, row, col);
+          out[(row + rb * PG::MB) * DP + col] = acc[j].value(e);
+        }
+      __syncthreads();
     }
-    // store this CTA's partial of matrix `pass` (m, P, nn, P') on its rows
-    double2* out = a.partial + (((size_t)state * gridDim.x + blk) * 4 + pass) * MAT;
-#pragma unroll
-    for (int j = 0; j < GM::TPW; ++j)
-#pragma unroll
-      for (int e = 0; e < 4; ++e) {
-        int row, col;
-        GM::coord(j, e, row, col);
-        out[(row + rb * PG::MB) * DP + col] = acc[j].value(e);
-      }
-    __syncthreads();
+    if (tid == 0 && *flag) atomicExch(a.error_flag + state, 1);
   }
   gm.drain();
-  if (tid == 0 && *flag) atomicExch(a.error_flag + state, 1);
+}
+
+// The environment alone, g Herm(b_0 at the endpoint), which the finalize kernel also writes: a
+// caller that needs the environment before the pullback (the boundary solve) launches this right
+// after the trajectory.
+__global__ void quartic_env_kernel(PullbackArgs a) {
+  const int state = blockIdx.x;
+  const int dp = a.dp, MAT = dp * dp, VEC = 7 * MAT;
+  const double2* env = a.samples + (size_t)state * a.samples_stride + (size_t)(a.npoints - 1) * VEC + 3 * MAT;
+  double2* env_out = a.env_out + (size_t)state * MAT;
+  const double g = a.coupling[state];
+  for (int e = threadIdx.x; e < MAT; e += blockDim.x) {
+    const int i = e / dp, j = e % dp;
+    env_out[e] = zscale(0.5 * g, zadd(env[e], zconj(env[j * dp + i])));
+  }
+}
+
+cudaError_t quartic_env_launch(const PullbackArgs& a, cudaStream_t s) {
+  note_launch();
+  quartic_env_kernel<<<a.nstates, 256, 0, s>>>(a);
+  return cudaGetLastError();
 }
 
 // Naive dense helpers for the finalize step (a few D^3 products per state).
@@ -251,7 +280,8 @@ static cudaError_t launch_pb(const PullbackArgs& a, int nblk, cudaStream_t s) {
   auto k = pullback_kernel<DP>;
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PG::SMEM);
   if (e != cudaSuccess) return e;
-  dim3 grid(nblk, a.nstates * PG::NRB);
+  const int items = nblk * a.nstates * PG::NRB;
+  const int grid = a.ctas > 0 ? std::min(a.ctas, items) : items;
   note_launch();
   k<<<grid, PG::NT, PG::SMEM, s>>>(a);
   return cudaGetLastError();

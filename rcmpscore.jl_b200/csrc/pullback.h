@@ -6,6 +6,8 @@ namespace rcmps {
 
 struct PullbackArgs {
   int dp, nstates, nodes, npoints, nodes_per_block;
+  int nblk;                    // node blocks
+  int ctas;                    // CTAs of the pullback kernel (0: one per work item)
   const double2* samples;      // [state][npoints][7 dp^2]
   long long samples_stride;
   const double2* ops;          // [state][8 dp^2] (Q, Qh, R, Rh, fixed0, fixed6, S, rho)
@@ -23,6 +25,8 @@ struct PullbackArgs {
 };
 
 cudaError_t pullback_launch(const PullbackArgs& a, int nblk, cudaStream_t s);
+// env_out = g Herm(b_0 at the endpoint) only (the finalize kernel writes the same values later)
+cudaError_t quartic_env_launch(const PullbackArgs& a, cudaStream_t s);
 
 // ---- the all-ODE route (pullback_full.cu)
 constexpr int kMaxPullSpecs = 3;

@@ -146,6 +146,8 @@ int quartic_run(rcmps_context* ctx, QuarticJob& job, cudaStream_t stream) {
     int cap = (int)std::max<size_t>(1, (budget - std::min(budget, fixed)) / per);
     for (size_t start = 0; start < all.size(); start += cap) {
       const int n = (int)std::min<size_t>(cap, all.size() - start);
+      const bool early_env = system == 0 && job.on_env && job.environment && job.env_ready;
+      const bool last_batch = kv.first == groups.rbegin()->first && start + n >= all.size();
       const std::vector<int> idx(all.begin() + start, all.begin() + start + n);
       const size_t mat = (size_t)dp * dp;   // complex elements
       Layout L;
@@ -286,6 +288,8 @@ int quartic_run(rcmps_context* ctx, QuarticJob& job, cudaStream_t stream) {
         pa.nodes = nodes;
         pa.npoints = npoints;
         pa.nodes_per_block = kNodesPerBlock;
+        pa.nblk = nblk;
+        pa.ctas = job.pullback_ctas;
         pa.samples = d_samp;
         pa.samples_stride = (long long)npoints * vec;
         pa.ops = d_ops;
@@ -300,6 +304,16 @@ int quartic_run(rcmps_context* ctx, QuarticJob& job, cudaStream_t stream) {
         pa.env_out = (double2*)P(o_env);
         pa.value_out = (double*)P(o_vout);
         pa.error_flag = (int*)P(o_flag);
+        if (early_env) {
+          if (e == cudaSuccess) e = quartic_env_launch(pa, stream);
+          if (e == cudaSuccess)
+            e = launch_unpad_acc(reinterpret_cast<double*>(P(o_env)), (long long)mat, dp, (long long*)P(o_off),
+                                 (int*)P(o_dims), job.environment, n, job.accumulate, stream);
+          if (e == cudaSuccess && last_batch) {
+            e = cudaEventRecord(job.env_ready, stream);
+            if (e == cudaSuccess) job.on_env();
+          }
+        }
         if (e == cudaSuccess) e = pullback_launch(pa, nblk, stream);
       } else {
         FullPullbackArgs pa;
@@ -330,7 +344,7 @@ int quartic_run(rcmps_context* ctx, QuarticJob& job, cudaStream_t stream) {
       if (job.covector)
         e = launch_unpad_acc(reinterpret_cast<double*>(P(o_cov)), (long long)mat, dp, (long long*)P(o_off),
                              (int*)P(o_dims), job.covector, n, job.accumulate, stream);
-      if (e == cudaSuccess && job.environment)
+      if (e == cudaSuccess && job.environment && !early_env)
         e = launch_unpad_acc(reinterpret_cast<double*>(P(o_env)), (long long)mat, dp, (long long*)P(o_off),
                              (int*)P(o_dims), job.environment, n, job.accumulate, stream);
       if (e == cudaSuccess && job.value)

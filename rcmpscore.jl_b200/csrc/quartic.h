@@ -1,6 +1,7 @@
 // Quartic term orchestration (internal).
 #pragma once
 #include <cuda_runtime.h>
+#include <functional>
 #include <vector>
 #include "../../include/rcmps_b200.h"
 #include "context.h"
@@ -22,6 +23,13 @@ struct QuarticJob {
   int slot = 0;                         // context slot (workspace, staging, events)
   double memory_share = 0.7;            // fraction of free device memory this job may hold
   int system = 0;                       // 0: the quartic term (reduced system); 1: all terms by ODEs
+  // Early environment (system 0): when on_env is set, the environment is written to `environment`
+  // right after each trajectory, before the pullback; after the last one env_ready is recorded on
+  // the stream and on_env() is called (from the calling thread), so that a boundary solve can start
+  // while the pullback runs.
+  cudaEvent_t env_ready = nullptr;
+  int pullback_ctas = 0;                // CTAs of the quartic pullback (0: one per work item)
+  std::function<void()> on_env;
 };
 
 cudaError_t quartic_init();

@@ -106,77 +106,112 @@ static void gmres_problem(ArnoldiProblem& A, char* base, const GmresBuffers& b, 
   A.bnorm = -1.0;
 }
 
-int finish_run(rcmps_context* ctx, FinishJob& job, cudaStream_t stream) {
+static FinishArgs finish_args(const FinishPlan& plan, const FinishPlan::Group& g, char* base, double metric_reg);
+
+// The boundary solve needs only the environment; the covector enters after it. finish_solve runs
+// the Poisson GMRES of every state and finish_complete applies the covector and the metric solve,
+// so that a caller may produce the covector while the solve runs.
+struct FinishPlan::Group {
+  int dp = 0, n = 0;
+  std::vector<int> idx;
+  size_t o_dims = 0, o_off = 0, o_in = 0, o_ops = 0, o_b = 0, o_tmp = 0, o_status = 0;
+  GmresBuffers gb{};
+  size_t h_dims = 0, h_off = 0, h_probs = 0, h_status = 0;
+};
+
+static FinishArgs finish_args(const FinishPlan& plan, const FinishPlan::Group& g, char* base, double metric_reg) {
+  (void)plan;
+  const size_t mat = (size_t)g.dp * g.dp;
+  double2* d_in = (double2*)(base + g.o_in);
+  FinishArgs fa;
+  fa.dp = g.dp;
+  fa.dims = (int*)(base + g.o_dims);
+  fa.ops = (double2*)(base + g.o_ops);
+  fa.ops_stride = (long long)(8 * mat);
+  fa.env = d_in + 4 * g.n * mat;
+  fa.cov = d_in + 3 * g.n * mat;
+  fa.b = (double2*)(base + g.o_b);
+  fa.x = (double2*)(base + g.gb.o_x);
+  fa.tmp = (double2*)(base + g.o_tmp);
+  fa.metric_reg = metric_reg;
+  fa.status = (int*)(base + g.o_status);
+  return fa;
+}
+
+FinishPlan::FinishPlan() = default;
+FinishPlan::~FinishPlan() = default;
+
+int finish_solve(rcmps_context* ctx, FinishJob& job, cudaStream_t stream, FinishPlan& plan) {
   const rcmps_settings& S = job.settings;
   const int m = 64, maxrestart = 200;
   const double tol = S.boundary_tolerance;
   if (!(tol > 0.0) || !(S.metric_reg >= 0.0)) return fail(ctx, RCMPS_INVALID_ARGUMENT, "invalid boundary controls");
-  std::vector<long long> off(job.n + 1, 0);
-  for (int i = 0; i < job.n; ++i) off[i + 1] = off[i] + (long long)job.dims[i] * job.dims[i];
+  plan.off.assign(job.n + 1, 0);
+  for (int i = 0; i < job.n; ++i) plan.off[i + 1] = plan.off[i] + (long long)job.dims[i] * job.dims[i];
   std::map<int, std::vector<int>> groups;
   for (int i = 0; i < job.n; ++i) groups[padded_dim(job.dims[i])].push_back(i);
-  rcmps_slot& SL = ctx->slot[job.slot];
+  // one workspace region and one staging region per padded dimension, all held at once
+  plan.groups.clear();
+  Layout L, H;
   for (auto& kv : groups) {
-    const int dp = kv.first;
-    const std::vector<int>& idx = kv.second;
-    const int n = (int)idx.size();
+    FinishPlan::Group g;
+    g.dp = kv.first;
+    g.idx = kv.second;
+    g.n = (int)g.idx.size();
+    const size_t mat = (size_t)g.dp * g.dp;
+    const int n = g.n;
+    g.o_dims = L.add(n * 4);
+    g.o_off = L.add(n * 8);
+    g.o_in = L.add(5 * n * mat * 16);
+    g.o_ops = L.add(n * 8 * mat * 16);
+    g.o_b = L.add(n * mat * 16);
+    g.o_tmp = L.add(n * 4 * mat * 16);
+    g.o_status = L.add(n * 4);
+    g.gb = gmres_layout(L, n, g.dp, m);
+    g.h_dims = H.add(n * 4);
+    g.h_off = H.add(n * 8);
+    g.h_probs = H.add(n * sizeof(ArnoldiProblem));
+    g.h_status = H.add(n * 4);
+    plan.groups.push_back(std::move(g));
+  }
+  rcmps_slot& SL = ctx->slot[job.slot];
+  cudaError_t e = arena_reserve(SL, L.total);
+  if (e) return fail(ctx, RCMPS_OUT_OF_MEMORY, "boundary workspace");
+  if (pinned_reserve(SL, H.total)) return fail(ctx, RCMPS_CUDA_ERROR, "pinned host buffer");
+  char* base = static_cast<char*>(SL.arena);
+  char* h = static_cast<char*>(SL.pinned);
+  auto P = [&](size_t o) { return static_cast<void*>(base + o); };
+  for (auto& g : plan.groups) {
+    const int dp = g.dp, n = g.n;
     const size_t mat = (size_t)dp * dp;
-    Layout L;
-    const size_t o_dims = L.add(n * 4), o_off = L.add(n * 8);
-    const size_t o_in = L.add(5 * n * mat * 16), o_ops = L.add(n * 8 * mat * 16);
-    const size_t o_b = L.add(n * mat * 16), o_tmp = L.add(n * 4 * mat * 16), o_status = L.add(n * 4);
-    GmresBuffers gb = gmres_layout(L, n, dp, m);
-    cudaError_t e = arena_reserve(SL, L.total);
-    if (e) return fail(ctx, RCMPS_OUT_OF_MEMORY, "boundary workspace");
-    char* base = static_cast<char*>(SL.arena);
-    auto P = [&](size_t o) { return static_cast<void*>(base + o); };
-    Layout H;
-    const size_t h_dims = H.add(n * 4), h_off = H.add(n * 8), h_probs = H.add(n * sizeof(ArnoldiProblem)),
-                 h_status = H.add(n * 4);
-    if (pinned_reserve(SL, H.total)) return fail(ctx, RCMPS_CUDA_ERROR, "pinned host buffer");
-    char* h = static_cast<char*>(SL.pinned);
-    int* hd = (int*)(h + h_dims);
-    long long* ho = (long long*)(h + h_off);
-    ArnoldiProblem* hp = (ArnoldiProblem*)(h + h_probs);
-    int* hs = (int*)(h + h_status);
+    int* hd = (int*)(h + g.h_dims);
+    long long* ho = (long long*)(h + g.h_off);
+    ArnoldiProblem* hp = (ArnoldiProblem*)(h + g.h_probs);
     for (int i = 0; i < n; ++i) {
-      hd[i] = job.dims[idx[i]];
-      ho[i] = off[idx[i]];
+      hd[i] = job.dims[g.idx[i]];
+      ho[i] = plan.off[g.idx[i]];
     }
-    double2* d_in = (double2*)P(o_in);
+    double2* d_in = (double2*)P(g.o_in);
     double* dR = (double*)d_in;
     double* dK = (double*)(d_in + n * mat);
     double* dP = (double*)(d_in + 2 * n * mat);
-    double* dC = (double*)(d_in + 3 * n * mat);
     double* dE = (double*)(d_in + 4 * n * mat);
-    e = cudaMemcpyAsync(P(o_dims), hd, n * 4, cudaMemcpyHostToDevice, stream);
-    if (!e) e = cudaMemcpyAsync(P(o_off), ho, n * 8, cudaMemcpyHostToDevice, stream);
-    if (!e) e = cudaMemsetAsync(P(o_status), 0, n * 4, stream);
-    if (!e) e = cudaMemsetAsync(P(gb.o_x), 0, (size_t)n * mat * 16, stream);
-    if (!e) e = launch_pad(job.R, (long long*)P(o_off), (int*)P(o_dims), dR, dp, mat, n, stream);
-    if (!e) e = launch_pad(job.K, (long long*)P(o_off), (int*)P(o_dims), dK, dp, mat, n, stream);
-    if (!e) e = launch_pad(job.rho, (long long*)P(o_off), (int*)P(o_dims), dP, dp, mat, n, stream);
-    if (!e) e = launch_pad(job.covector, (long long*)P(o_off), (int*)P(o_dims), dC, dp, mat, n, stream);
-    if (!e) e = launch_pad(job.environment, (long long*)P(o_off), (int*)P(o_dims), dE, dp, mat, n, stream);
-    if (!e) e = launch_prepare(dR, dK, dP, (double*)P(o_ops), dp, mat, 8 * mat, n, stream);
-    FinishArgs fa;
-    fa.dp = dp;
-    fa.dims = (int*)P(o_dims);
-    fa.ops = (double2*)P(o_ops);
-    fa.ops_stride = (long long)(8 * mat);
-    fa.env = (double2*)dE;
-    fa.cov = (double2*)dC;
-    fa.b = (double2*)P(o_b);
-    fa.x = (double2*)P(gb.o_x);
-    fa.tmp = (double2*)P(o_tmp);
-    fa.metric_reg = S.metric_reg;
-    fa.status = (int*)P(o_status);
+    e = cudaMemcpyAsync(P(g.o_dims), hd, n * 4, cudaMemcpyHostToDevice, stream);
+    if (!e) e = cudaMemcpyAsync(P(g.o_off), ho, n * 8, cudaMemcpyHostToDevice, stream);
+    if (!e) e = cudaMemsetAsync(P(g.o_status), 0, n * 4, stream);
+    if (!e) e = cudaMemsetAsync(P(g.gb.o_x), 0, (size_t)n * mat * 16, stream);
+    if (!e) e = launch_pad(job.R, (long long*)P(g.o_off), (int*)P(g.o_dims), dR, dp, mat, n, stream);
+    if (!e) e = launch_pad(job.K, (long long*)P(g.o_off), (int*)P(g.o_dims), dK, dp, mat, n, stream);
+    if (!e) e = launch_pad(job.rho, (long long*)P(g.o_off), (int*)P(g.o_dims), dP, dp, mat, n, stream);
+    if (!e) e = launch_pad(job.environment, (long long*)P(g.o_off), (int*)P(g.o_dims), dE, dp, mat, n, stream);
+    if (!e) e = launch_prepare(dR, dK, dP, (double*)P(g.o_ops), dp, mat, 8 * mat, n, stream);
+    FinishArgs fa = finish_args(plan, g, base, S.metric_reg);
     if (!e) e = boundary_rhs_launch(fa, n, stream);
     if (e) return fail(ctx, RCMPS_CUDA_ERROR, std::string("boundary set-up: ") + cudaGetErrorString(e));
     for (int i = 0; i < n; ++i) {
       ArnoldiProblem& A = hp[i];
-      gmres_problem(A, base, gb, i, dp, hd[i], m, tol);
-      const double2* ops = (double2*)P(o_ops) + (size_t)i * 8 * mat;
+      gmres_problem(A, base, g.gb, i, dp, hd[i], m, tol);
+      const double2* ops = (double2*)P(g.o_ops) + (size_t)i * 8 * mat;
       A.A1 = ops + 1 * mat;   // L*: Q^dag X + X Q + R^dag X R
       A.A1h = ops;
       A.A2 = ops + 3 * mat;
@@ -184,16 +219,36 @@ int finish_run(rcmps_context* ctx, FinishJob& job, cudaStream_t stream) {
       A.trw = ops + 7 * mat;  // + tr(rho X) I
       A.b = fa.b + (size_t)i * mat;
     }
-    e = gmres_run(hp, (ArnoldiProblem*)P(gb.o_probs), n, dp, m, maxrestart, (LindbladTask*)P(gb.o_tasks), stream);
+    e = gmres_run(hp, (ArnoldiProblem*)P(g.gb.o_probs), n, dp, m, maxrestart, (LindbladTask*)P(g.gb.o_tasks), stream);
     if (e) return fail(ctx, RCMPS_CUDA_ERROR, std::string("boundary GMRES: ") + cudaGetErrorString(e));
+  }
+  return RCMPS_OK;
+}
+
+int finish_complete(rcmps_context* ctx, FinishJob& job, cudaStream_t stream, FinishPlan& plan) {
+  const rcmps_settings& S = job.settings;
+  const double tol = S.boundary_tolerance;
+  rcmps_slot& SL = ctx->slot[job.slot];
+  char* base = static_cast<char*>(SL.arena);
+  char* h = static_cast<char*>(SL.pinned);
+  auto P = [&](size_t o) { return static_cast<void*>(base + o); };
+  cudaError_t e = cudaSuccess;
+  for (auto& g : plan.groups) {
+    const int dp = g.dp, n = g.n;
+    const size_t mat = (size_t)dp * dp;
+    const ArnoldiProblem* hp = (const ArnoldiProblem*)(h + g.h_probs);
+    int* hs = (int*)(h + g.h_status);
+    double* dC = (double*)((double2*)P(g.o_in) + 3 * n * mat);
+    FinishArgs fa = finish_args(plan, g, base, S.metric_reg);
+    e = launch_pad(job.covector, (long long*)P(g.o_off), (int*)P(g.o_dims), dC, dp, mat, n, stream);
     if (!e) e = finish_launch(fa, n, stream);
-    if (!e) e = launch_unpad_acc((double*)(fa.tmp + 3 * mat), (long long)(4 * mat), dp, (long long*)P(o_off),
-                                 (int*)P(o_dims), job.gradient, n, false, stream);
-    if (!e) e = cudaMemcpyAsync(hs, P(o_status), n * 4, cudaMemcpyDeviceToHost, stream);
+    if (!e) e = launch_unpad_acc((double*)(fa.tmp + 3 * mat), (long long)(4 * mat), dp, (long long*)P(g.o_off),
+                                 (int*)P(g.o_dims), job.gradient, n, false, stream);
+    if (!e) e = cudaMemcpyAsync(hs, P(g.o_status), n * 4, cudaMemcpyDeviceToHost, stream);
     if (!e) e = cudaStreamSynchronize(stream);
     if (e) return fail(ctx, RCMPS_CUDA_ERROR, std::string("finish: ") + cudaGetErrorString(e));
     for (int i = 0; i < n; ++i) {
-      rcmps_state_stats& st = job.stats[idx[i]];
+      rcmps_state_stats& st = job.stats[g.idx[i]];
       const ArnoldiProblem& A = hp[i];
       st.gmres_iterations = A.iters;
       st.boundary_residual = A.residual;
@@ -211,6 +266,13 @@ int finish_run(rcmps_context* ctx, FinishJob& job, cudaStream_t stream) {
   for (int i = 0; i < job.n; ++i)
     if (job.stats[i].status) return job.stats[i].status;
   return RCMPS_OK;
+}
+
+int finish_run(rcmps_context* ctx, FinishJob& job, cudaStream_t stream) {
+  FinishPlan plan;
+  const int rc = finish_solve(ctx, job, stream, plan);
+  if (rc) return rc;
+  return finish_complete(ctx, job, stream, plan);
 }
 
 int stationary_run(rcmps_context* ctx, StationaryJob& job, cudaStream_t stream) {

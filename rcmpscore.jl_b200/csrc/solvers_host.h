@@ -1,6 +1,7 @@
 // Boundary/finish and stationary orchestration (internal).
 #pragma once
 #include <cuda_runtime.h>
+#include <vector>
 #include "../../include/rcmps_b200.h"
 #include "context.h"
 
@@ -28,6 +29,20 @@ struct StationaryJob {
 };
 
 int finish_run(rcmps_context* ctx, FinishJob& job, cudaStream_t stream);
+
+// finish_run in two halves: finish_solve needs R, K, rho and the environment (the boundary
+// Poisson GMRES); finish_complete then needs the covector (finish kernel, metric solve, gradient).
+// The plan keeps the workspace layout between the two; the slot's workspace must not be reused
+// in between.
+struct FinishPlan {
+  struct Group;
+  std::vector<Group> groups;
+  std::vector<long long> off;
+  FinishPlan();
+  ~FinishPlan();
+};
+int finish_solve(rcmps_context* ctx, FinishJob& job, cudaStream_t stream, FinishPlan& plan);
+int finish_complete(rcmps_context* ctx, FinishJob& job, cudaStream_t stream, FinishPlan& plan);
 int stationary_run(rcmps_context* ctx, StationaryJob& job, cudaStream_t stream);
 
 }  // namespace rcmps
