@@ -15,7 +15,9 @@
 //     jac L_c(X_c) + src (coef_c (Rc X_s + X_s Rc^dag) + fixed_c) with P_s = Rc X_s shared
 //     between the jump of channel s and the insertion into channel c;
 //   * products on FP64 tensor cores (mma.sync m16n8k8), B operands streamed by 1-D bulk copies
-//     into a 4-stage shared-memory ring, A operands resident in shared memory;
+//     into a 4-stage shared-memory ring, A operands resident in shared memory; one producer warp
+//     refills each ring slot once every MMA warp has released it (per-slot "full" and "empty"
+//     mbarriers), so the MMA warps never meet at a block barrier inside a product;
 //   * the scalar energy channel is integrated from per-CTA partial traces reduced once per
 //     attempt (its value never feeds back into the matrix channels);
 //   * the step controller runs identically in every CTA from the same reduced norms.
@@ -110,7 +112,8 @@ struct Geo {
   static constexpr int KM = SYS == kSysQuartic ? 2 : 3;    // K blocks of the widest G2 pass
   static constexpr int G = DP / 16;
   static constexpr int NW = (DP == 48 || DP == 96) ? 12 : (DP == 64 || DP == 128) ? 16 : 8;
-  static constexpr int NT = 32 * NW;
+  static constexpr int NWT = NW + 1;                  // + one producer warp that only streams B chunks
+  static constexpr int NT = 32 * NWT;
   static constexpr int KC = DP <= 64 ? 16 : 8;       // rows of a streamed B chunk
   static constexpr int NST = (SYS == kSysFull && DP == 128) ? 3 : 4;   // ring stages
   static constexpr int LDB = DP + kBPad;              // padded row stride of a ring chunk
@@ -158,7 +161,8 @@ struct Smem {
   double2* aprime;    // [16 GS][LDA2]
   double2* ring;      // [NST][KC*LDB]
   double2* split;     // split-K partial fragments
-  uint64_t* full;     // [NST]
+  uint64_t* full;     // [NST] chunk landed in the slot
+  uint64_t* empty;    // [NST] every MMA warp released the slot
   Ctl* ctl;
   Xch* xch;
   double* red;        // [NW * 2] block reduction scratch
@@ -174,13 +178,16 @@ __device__ __forceinline__ Smem<DP, SYS> carve(unsigned char* base) {
   s.aprime = z + GE::OFF_APRIME;
   s.ring = z + GE::OFF_RING;
   s.split = z + GE::OFF_SPLIT;
-  constexpr size_t o_ctl = 64;
+  // tail: full[NST] at 0, empty[NST] at 64, then the controller scalars
+  static_assert(GE::NST <= 8, "barrier slots");
+  constexpr size_t o_ctl = 128;
   constexpr size_t o_xch = o_ctl + ((sizeof(Ctl) + 15) / 16) * 16;
   constexpr size_t o_red = o_xch + ((sizeof(Xch) + 15) / 16) * 16;
   constexpr size_t o_ksc = o_red + 32 * sizeof(double) * 2;
   static_assert(o_ksc + 16 * sizeof(double) <= 2048, "shared tail");
   unsigned char* tail = base + (size_t)GE::END2 * 16;
   s.full = reinterpret_cast<uint64_t*>(tail);
+  s.empty = reinterpret_cast<uint64_t*>(tail + 64);
   s.ctl = reinterpret_cast<Ctl*>(tail + o_ctl);
   s.xch = reinterpret_cast<Xch*>(tail + o_xch);
   s.red = reinterpret_cast<double*>(tail + o_red);
@@ -279,7 +286,7 @@ struct Rhs {
   template <int TPW, int SK>
   __device__ void split_reduce(ZFrag* acc, int tile0, int slice) {
     if constexpr (SK > 1) {
-      if (slice > 0) {
+      if (slice > 0 && warp < GE::NW) {
 #pragma unroll
         for (int j = 0; j < TPW; ++j) {
           double2* p = sm.split + ((tile0 + j) * (SK - 1) + slice - 1) * 128;
@@ -288,7 +295,7 @@ struct Rhs {
         }
       }
       __syncthreads();
-      if (slice == 0) {
+      if (slice == 0 && warp < GE::NW) {
 #pragma unroll
         for (int j = 0; j < TPW; ++j)
           for (int sl = 1; sl < SK; ++sl) {
@@ -310,6 +317,21 @@ struct Rhs {
     const int tile0 = SK > 1 ? warp / SK : warp * TPW;
     const int slice = SK > 1 ? warp % SK : 0;
     const int mt = tile0 / TL::NTN;
+    if (warp == GE::NW) {
+      // producer warp: refill each slot once every MMA warp has released it
+      if (lane == 0)
+        for (int ch = 0; ch < nch; ++ch) {
+          const long long g = g0 + q + ch;
+          if (q + ch + GE::NST < nchunk) {
+            mbar_wait(&sm.empty[(int)(g % GE::NST)], (uint32_t)((g / GE::NST) & 1), &sm.ctl->wait_flag);
+            issue(g + GE::NST, zb);
+          }
+        }
+      __syncwarp();
+      q += nch;
+      split_reduce<TPW, SK>(acc, tile0, slice);
+      return;
+    }
     for (int ch = 0; ch < nch; ++ch, ++q) {
       const double2* B = await(g0 + q);
 #pragma unroll
@@ -323,8 +345,8 @@ struct Rhs {
         for (int j = 0; j < TPW; ++j) load_b(B, GE::LDB, ks * 8, ((tile0 + j) % TL::NTN) * 8, lane, b[j]);
         zmma_tiles<TPW>(acc, a, b);
       }
-      __syncthreads();
-      if (tid == 0 && q + GE::NST < nchunk) issue(g0 + q + GE::NST, zb);
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&sm.empty[(int)((g0 + q) % GE::NST)]);
     }
     split_reduce<TPW, SK>(acc, tile0, slice);
   }
@@ -342,7 +364,7 @@ struct Rhs {
 #pragma unroll
     for (int j = 0; j < TPW; ++j) acc[j].zero();
     stream_product<TL>(acc, sm.panel, GE::LDP, GE::CH1, q, g0, zb);
-    if (slice == 0) {
+    if (slice == 0 && warp < GE::NW) {
 #pragma unroll
       for (int j = 0; j < TPW; ++j) {
         const int nt = (tile0 + j) % TL::NTN;
@@ -392,7 +414,7 @@ struct Rhs {
     stream_product<TL>(acc, sm.aprime, GE::LDA2, (K3 ? 3 : 2) * GE::CH1, q, g0, zb);
     const int tile0 = SK > 1 ? warp / SK : warp * TPW;
     const int slice = SK > 1 ? warp % SK : 0;
-    if (slice == 0) {
+    if (slice == 0 && warp < GE::NW) {
 #pragma unroll
       for (int j = 0; j < TPW; ++j) {
         const int tile = tile0 + j, mt = tile / TL::NTN, nt = tile % TL::NTN;
@@ -419,7 +441,7 @@ struct Rhs {
   __device__ void operator()(const double2* zb, double2* kout, double jac, double src) {
     const SysTab& t = T();
     const long long g0 = *gq;
-    if (tid == 0) {
+    if (tid == GE::NW * 32) {
       fence_proxy_async_global();
       ce = 0;
       cc = 0;
@@ -491,7 +513,10 @@ trajectory_kernel(const TrajState* __restrict__ states, const double* __restrict
   long long gq = 0;
 
   if (tid == 0) {
-    for (int i = 0; i < GE::NST; ++i) mbar_init(&sm.full[i], 1);
+    for (int i = 0; i < GE::NST; ++i) {
+      mbar_init(&sm.full[i], 1);
+      mbar_init(&sm.empty[i], GE::NW);
+    }
     fence_mbar_init();
     C.t = -ctl_in.endpoint;
     C.h = fmin(ctl_in.initial_h, 2.0 * ctl_in.endpoint);
@@ -597,7 +622,7 @@ trajectory_kernel(const TrajState* __restrict__ states, const double* __restrict
           }
         }
       }
-      block_sum2<GE::NW>(part, dummy, sm.red);
+      block_sum2<GE::NWT>(part, dummy, sm.red);
       if (tid == 0) sm.kscp[s] = 4.0 * C.src[s] * part;
       fence_proxy_async_global();
       cluster_sync();
@@ -622,7 +647,7 @@ trajectory_kernel(const TrajState* __restrict__ states, const double* __restrict
         s5 += zabs2(e5) / (scale * scale);
         s3 += zabs2(e3) / (scale * scale);
       }
-      block_sum2<GE::NW>(s5, s3, sm.red);
+      block_sum2<GE::NWT>(s5, s3, sm.red);
       if (tid == 0) {
         sm.xch->s5 = s5;
         sm.xch->s3 = s3;
