@@ -100,7 +100,8 @@ int rcmps_fg_phi4_batch(rcmps_context* context, int n_states, const int* dims, c
                         double* energy, double* gradient, double* covector, double* environment,
                         rcmps_state_stats* stats, void* stream);
 
-/* Same with every array in host memory (copies in and out inside the call). */
+/* Same with every array in host memory (copies in and out inside the call, through a device
+ * buffer the context keeps and grows on demand). */
 int rcmps_fg_phi4_batch_host(rcmps_context* context, int n_states, const int* dims, const double* couplings,
                              const double* R, const double* K, const double* rho,
                              const rcmps_settings* settings, double* energy, double* gradient,

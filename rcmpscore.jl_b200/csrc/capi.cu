@@ -77,6 +77,18 @@ cudaError_t aux_reserve(rcmps_context* ctx, size_t bytes) {
   return e;
 }
 
+cudaError_t host_io_reserve(rcmps_context* ctx, size_t bytes) {
+  if (bytes <= ctx->host_io_bytes) return cudaSuccess;
+  for (auto& sl : ctx->slot) cudaStreamSynchronize(sl.stream);
+  if (ctx->host_io) cudaFree(ctx->host_io);
+  ctx->host_io = nullptr;
+  ctx->host_io_bytes = 0;
+  cudaError_t e = cudaMalloc(&ctx->host_io, align256(bytes));
+  if (e == cudaSuccess) ctx->host_io_bytes = align256(bytes);
+  else cudaGetLastError();
+  return e;
+}
+
 int fail(rcmps_context* ctx, int code, const std::string& message) {
   if (ctx) {
     std::lock_guard<std::mutex> lock(ctx->mu);
@@ -287,6 +299,7 @@ int rcmps_context_destroy(rcmps_context* ctx) {
     if (sl.stream) cudaStreamDestroy(sl.stream);
   }
   if (ctx->aux) cudaFree(ctx->aux);
+  if (ctx->host_io) cudaFree(ctx->host_io);
   delete ctx;
   return RCMPS_OK;
 }
@@ -648,12 +661,11 @@ int rcmps_fg_phi4_batch_host(rcmps_context* ctx, int n, const int* dims, const d
   long long total = 0;
   for (int i = 0; i < n; ++i) total += (long long)dims[i] * dims[i];
   const size_t cb = (size_t)total * 16;
-  void* dev = nullptr;
-  // device copies of inputs and outputs (one allocation per call: the host entry is the
-  // convenience form; rcmps_fg_phi4_batch takes device buffers and allocates nothing per call)
-  cudaError_t e = cudaMalloc(&dev, 6 * cb + (size_t)n * 8 + 256);
+  // device copies of inputs and outputs in a grow-only buffer of the context (reused by later
+  // calls of the same or smaller size)
+  cudaError_t e = host_io_reserve(ctx, 6 * cb + (size_t)n * 8 + 256);
   if (e) return fail(ctx, RCMPS_OUT_OF_MEMORY, "host entry buffers");
-  char* d = static_cast<char*>(dev);
+  char* d = static_cast<char*>(ctx->host_io);
   double *dR = (double*)d, *dK = (double*)(d + cb), *dP = (double*)(d + 2 * cb), *dG = (double*)(d + 3 * cb),
          *dC = (double*)(d + 4 * cb), *dE = (double*)(d + 5 * cb), *dEn = (double*)(d + 6 * cb);
   cudaStream_t s = ctx->slot[0].stream;
@@ -661,17 +673,13 @@ int rcmps_fg_phi4_batch_host(rcmps_context* ctx, int n, const int* dims, const d
   if (!e) e = cudaMemcpyAsync(dK, K, cb, cudaMemcpyHostToDevice, s);
   if (!e) e = cudaMemcpyAsync(dP, rho, cb, cudaMemcpyHostToDevice, s);
   if (!e) e = cudaStreamSynchronize(s);
-  if (e) {
-    cudaFree(dev);
-    return fail(ctx, RCMPS_CUDA_ERROR, std::string("host entry copies: ") + cudaGetErrorString(e));
-  }
+  if (e) return fail(ctx, RCMPS_CUDA_ERROR, std::string("host entry copies: ") + cudaGetErrorString(e));
   rc = rcmps_fg_phi4_batch(ctx, n, dims, couplings, dR, dK, dP, settings, dEn, dG, dC, dE, stats, s);
   if (!e) e = cudaMemcpyAsync(energy, dEn, (size_t)n * 8, cudaMemcpyDeviceToHost, s);
   if (!e) e = cudaMemcpyAsync(gradient, dG, cb, cudaMemcpyDeviceToHost, s);
   if (!e && covector) e = cudaMemcpyAsync(covector, dC, cb, cudaMemcpyDeviceToHost, s);
   if (!e && environment) e = cudaMemcpyAsync(environment, dE, cb, cudaMemcpyDeviceToHost, s);
   if (!e) e = cudaStreamSynchronize(s);
-  cudaFree(dev);
   if (e) return fail(ctx, RCMPS_CUDA_ERROR, std::string("host entry copies: ") + cudaGetErrorString(e));
   return rc;
 }

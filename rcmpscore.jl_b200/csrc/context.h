@@ -23,6 +23,8 @@ struct rcmps_context {
   rcmps_slot slot[3];
   void* aux = nullptr;                    // per-call intermediate results of the composite entry
   size_t aux_bytes = 0;
+  void* host_io = nullptr;                // device copies of the host-buffer entry's inputs and outputs
+  size_t host_io_bytes = 0;
   std::string error;
   std::mutex mu;                          // guards `error` (the composite entry runs two host threads)
   bool tables = false;
@@ -35,6 +37,7 @@ cudaError_t arena_reserve(rcmps_slot& slot, size_t bytes);
 // Ensure slot `k` has at least `bytes` of pinned host staging.
 cudaError_t pinned_reserve(rcmps_slot& slot, size_t bytes);
 cudaError_t aux_reserve(rcmps_context* ctx, size_t bytes);
+cudaError_t host_io_reserve(rcmps_context* ctx, size_t bytes);
 int fail(rcmps_context* ctx, int code, const std::string& message);
 inline size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 int padded_dim(int d);   // 16, 32, 48, 64, 96, 128, or 0 if d is unsupported
