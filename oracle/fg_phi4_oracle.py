@@ -33,7 +33,7 @@ __all__ = [
     "OracleFailure", "source", "quadrature", "angular_grid", "lindblad", "lindblad_adjoint",
     "QuarticSystem", "integrate", "quartic_pullback", "evaluate_quartic", "kinetic_raw",
     "stationary_state", "boundary_environment", "finish_gradient", "metric", "fg_phi4",
-    "phi4_state", "z2_state", "left_canonical_q",
+    "phi4_state", "z2_state", "left_canonical_q", "PackedZ2System", "z2_structure_ok",
 ]
 
 
@@ -174,6 +174,143 @@ class QuarticSystem:
         return out
 
 
+# --------------------------------------------------------------------------- packed Z2 route
+
+# Parity of the seven channels of a Z2-symmetric state (R odd, Q and rho even): odd channels
+# have only the off-diagonal blocks, even channels only the diagonal ones.
+PARITY = (1, 0, 1, 0, 1, 0, 1)
+# Packed vector: per channel its upper off-diagonal block (odd) or its two diagonal blocks
+# (even), in channel order, then the scalar; 10 (D/2)^2 + 1 entries (ode_backend.py:236-275).
+PACKED_BLOCKS = tuple((c, (0, 1)) if PARITY[c] else (c, blk) for c in range(7)
+                      for blk in (((0, 1),) if PARITY[c] else ((0, 0), (1, 1))))
+
+
+def z2_structure_ok(r, q, rho):
+    """The exact block structure the packed route requires (ode_backend.py:246-256): even D,
+    R's diagonal blocks and the off-diagonal blocks of Q and rho exactly zero, rho Hermitian to
+    1e-13 relative. Nothing is projected."""
+    d2 = len(q)
+    if d2 % 2 or d2 == 0:
+        return False
+    n = d2 // 2
+    zero = (r[:n, :n], r[n:, n:], q[:n, n:], q[n:, :n], rho[:n, n:], rho[n:, :n])
+    if any(np.any(b != 0) for b in zero):
+        return False
+    return np.linalg.norm(rho - adj(rho)) <= 1e-13 * max(1.0, np.linalg.norm(rho))
+
+
+def _bmul(a, b):
+    """Product of 2x2 block matrices whose blocks are arrays or None (structural zero)."""
+    out = [[None, None], [None, None]]
+    for i in range(2):
+        for j in range(2):
+            acc = None
+            for k in range(2):
+                if a[i][k] is not None and b[k][j] is not None:
+                    term = a[i][k] @ b[k][j]
+                    acc = term if acc is None else acc + term
+            out[i][j] = acc
+    return out
+
+
+def _badj(a):
+    return [[None if a[j][i] is None else adj(a[j][i]) for j in range(2)] for i in range(2)]
+
+
+def _blk(x, i, j):
+    return 0.0 if x[i][j] is None else x[i][j]
+
+
+class PackedZ2System:
+    """The quartic system of a Z2-symmetric state on its structurally nonzero blocks: the
+    seven-channel equations of QuarticSystem evaluated block by block (the reference writes the
+    same blocks as ten (D/2)^2 channels with gathered adjoints, ode_backend.py:236-473). An odd
+    channel [[0, U], [U^dag, 0]] is carried by U, an even one by its two diagonal blocks, so the
+    state vector and the DOP853 error norm have 10 (D/2)^2 + 1 entries. The scalar is
+    4 src Re tr(R F3 + F3 R^dag) = 8 src Re(tr(a U^dag) + tr(b U)) for F3 = [[0, U], [U^dag, 0]]
+    and R = [[0, a], [b, 0]]."""
+
+    def __init__(self, q, r, rho):
+        q, r, rho = (np.asarray(x, dtype=np.complex128) for x in (q, r, rho))
+        if not z2_structure_ok(r, q, rho):
+            raise ValueError("the packed Z2 route requires exact balanced block structure; nothing is projected")
+        self.q, self.r, self.rho = q, r, rho
+        self.full_d = len(q)
+        n = self.full_d // 2
+        self.n = n
+        self.d = self.full_d
+        self.size = 10 * n * n + 1
+        qb = [[q[:n, :n], None], [None, q[n:, n:]]]
+        rb = [[None, r[:n, n:]], [r[n:, :n], None]]
+        self.a, self.b = r[:n, n:], r[n:, :n]
+        self.ops = [(qb, rb) if c in FORWARD else (_badj(qb), _badj(rb)) for c in range(7)]
+        # fixed_0 = R rho + rho R^dag and fixed_6 = 4 (R + R^dag), both odd: their upper blocks
+        self.fixed = {0: [[None, self.a @ rho[n:, n:] + rho[:n, :n] @ adj(self.b)], [None, None]],
+                      6: [[None, 4.0 * (self.a + adj(self.b))], [None, None]]}
+        self.calls = 0
+
+    def initial(self):
+        return np.zeros(self.size, complex)
+
+    def unpack_channels(self, y):
+        """The seven channels as 2x2 block matrices (None = structural zero)."""
+        n = self.n
+        blocks = y[:-1].reshape(10, n, n)
+        chans = []
+        i = 0
+        for c in range(7):
+            if PARITY[c]:
+                u = blocks[i]
+                chans.append([[None, u], [adj(u), None]])
+                i += 1
+            else:
+                chans.append([[blocks[i], None], [None, blocks[i + 1]]])
+                i += 2
+        return chans
+
+    def unpack(self, y):
+        """Packed vector -> the dense seven-channel vector of QuarticSystem (7 D^2 + 1)."""
+        n, d = self.n, self.full_d
+        out = np.zeros(7 * d * d + 1, complex)
+        mats = out[:-1].reshape(7, d, d)
+        for c, x in enumerate(self.unpack_channels(y)):
+            for i in range(2):
+                for j in range(2):
+                    if x[i][j] is not None:
+                        mats[c, i * n:(i + 1) * n, j * n:(j + 1) * n] = x[i][j]
+        out[-1] = y[-1]
+        return out
+
+    def __call__(self, t, y, src=None):
+        self.calls += 1
+        n = self.n
+        jac = 2.0 * abs(t)
+        src = source(t) if src is None else src
+        x = self.unpack_channels(y)
+        out = np.empty_like(y)
+        blocks = out[:-1].reshape(10, n, n)
+        i = 0
+        for c in range(7):
+            qc, rc = self.ops[c]
+            qch, rch = _badj(qc), _badj(rc)
+            lin = [_bmul(qc, x[c]), _bmul(x[c], qch), _bmul(_bmul(rc, x[c]), rch)]
+            ins = None
+            if c in INSERTIONS:
+                s, coef = INSERTIONS[c]
+                ins = (coef, [_bmul(rc, x[s]), _bmul(x[s], rch)])
+            for (bi, bj) in (((0, 1),) if PARITY[c] else ((0, 0), (1, 1))):
+                v = jac * sum(_blk(m, bi, bj) for m in lin)
+                if ins is not None:
+                    v = v + (src * ins[0]) * sum(_blk(m, bi, bj) for m in ins[1])
+                if c in self.fixed:
+                    v = v + src * _blk(self.fixed[c], bi, bj)
+                blocks[i] = v
+                i += 1
+        u = x[2][0][1]
+        out[-1] = 8.0 * src * (np.trace(self.a @ adj(u)) + np.trace(self.b @ u)).real
+        return out
+
+
 # --------------------------------------------------------------------------- DOP853
 
 def integrate(system, points, *, atol=1e-13, rtol=1e-12, initial_step=None, max_steps=1_000_000,
@@ -294,14 +431,21 @@ def quartic_pullback(system, samples, points, weights):
 
 
 def evaluate_quartic(r, q, rho, g=1.0, *, half_window=30.0, n_quad=512, atol=1e-13, rtol=1e-12,
-                     max_steps=1_000_000, return_samples=False):
+                     max_steps=1_000_000, return_samples=False, packed_z2=False):
     """g times (value, covector, environment) of the quartic term
-    (persistent_trajectory_backend.py:439-461, ode_backend.py:861-870)."""
-    system = QuarticSystem(q, r, rho)
+    (persistent_trajectory_backend.py:439-461, ode_backend.py:861-870). packed_z2: integrate
+    the packed Z2 system (ValueError unless the state has the exact Z2 block structure) and
+    pull back from its unpacked samples (ode_backend.py:700-716); the samples returned are
+    then the packed ones."""
+    system = PackedZ2System(q, r, rho) if packed_z2 else QuarticSystem(q, r, rho)
     points, weights = quadrature(half_window, n_quad)
     nodes = np.r_[points, math.sqrt(half_window)]
     samples, stats = integrate(system, nodes, atol=atol, rtol=rtol, max_steps=max_steps)
-    value, cov, env = quartic_pullback(system, samples, points, weights)
+    if packed_z2:
+        dense = np.stack([system.unpack(x) for x in samples])
+        value, cov, env = quartic_pullback(system, dense, points, weights)
+    else:
+        value, cov, env = quartic_pullback(system, samples, points, weights)
     out = dict(value=g * value, covector=g * cov, environment=g * env, stats=stats)
     if return_samples:
         out["samples"] = samples
@@ -624,13 +768,15 @@ def metric(rho, x, y, metric_reg=1e-3):
 
 
 def fg_phi4(r, k, rho, g, *, half_window=30.0, n_quad=512, atol=1e-13, rtol=1e-12, nodes=512,
-            krylov_tolerance=1e-12, maxdim=1024, metric_reg=1e-3, method="dense"):
+            krylov_tolerance=1e-12, maxdim=1024, metric_reg=1e-3, method="dense", packed_z2=False):
     """(energy, gradient, parts) of the phi^4 density: kinetic1 + kinetic2 + g phi^4, the
     sum computed by the reference's GPU objective (overlap_sweep_driver.py:132-212,
-    sweep_driver.py:78-119; src/observables.jl:332-334)."""
+    sweep_driver.py:78-119; src/observables.jl:332-334). packed_z2 selects the packed Z2
+    quartic route (sweep_driver.py:48-50, 100-101)."""
     r, k, rho = (np.asarray(x, complex) for x in (r, k, rho))
     q = left_canonical_q(r, k)
-    quartic = evaluate_quartic(r, q, rho, g, half_window=half_window, n_quad=n_quad, atol=atol, rtol=rtol)
+    quartic = evaluate_quartic(r, q, rho, g, half_window=half_window, n_quad=n_quad, atol=atol, rtol=rtol,
+                               packed_z2=packed_z2)
     kinetic = kinetic_raw(q, r, rho, nodes, tolerance=krylov_tolerance, maxdim=maxdim)
     covector = quartic["covector"] + kinetic["covector"]
     environment = quartic["environment"] + kinetic["environment"]

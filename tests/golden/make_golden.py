@@ -6,6 +6,11 @@ This script imports the reference package rcmps_gpu read-only from a local check
   d16.npz       one D = 16 random state at the optimizer defaults (W = 30, n_quad = 512, 512 nodes)
   d64.npz       the seed-42 D = 64 random state at the optimizer defaults
   samples_d5.npz  trajectory samples of the reduced quartic system, D = 5, W = 2, n_quad = 16
+  packed.npz    the packed Z2 route (evaluate_quartic(..., packed_z2=True), the default of the
+                persistent trajectory) on Z2 states D = 4, 8 (W = 30, n_quad = 64), 16 and 32
+                (W = 30, n_quad = 512, 512 kinetic nodes: the optimizer defaults, with the
+                kinetic term and the finished gradient), and the packed trajectory samples of a
+                D = 4 Z2 state at W = 2, n_quad = 16
   ode.npz       the all-ODE route (evaluate_phi4: kinetic1 + kinetic2 + g phi^4 as 26 channels):
                 D = 3 (W = 6, n_quad = 24), D = 8 random and Z2 (W = 20, n_quad = 64) and
                 D = 16 (W = 20, n_quad = 192, the Julia defaults of the fixture)
@@ -18,7 +23,7 @@ is the reference's test/fixtures/phi4_g2_D16_z2_portable (exported by RcmpsCore 
 States: NumPy PCG64 default_rng(seed); R and A with i.i.d. standard complex Gaussian entries
 times 0.2 (R drawn first), K = (A + A^dag)/2; Z2 states draw blocks in the order k1, k2, R12, R21.
 Run: python tests/golden/make_golden.py [name ...]  (all files by default, about a minute; the
-D = 64 record dominates; names: small d16 d64 samples ode)
+D = 64 record dominates; names: small d16 d64 samples ode packed)
 """
 from __future__ import annotations
 
@@ -76,6 +81,35 @@ def evaluate(r, k, g, window, nq, nodes):
                 energy=quartic["value"] + kinetic["value"], gradient=grad)
 
 
+def evaluate_packed(r, k, g, window, nq, nodes=None):
+    q = -1j * k - r.conj().T @ r / 2
+    rho, _ = nm.stationary_state(q, r, tolerance=1e-13)
+    quartic = ob.evaluate_quartic(r, q, rho, g, xp=np, half_window=window, n_quad=nq, atol=1e-13, rtol=1e-12,
+                                  packed_z2=True)
+    rec = dict(R=r, K=k, rho=rho, g=g, window=window, n_quad=nq, quartic_value=quartic["value"],
+               quartic_covector=quartic["covector"], quartic_environment=quartic["environment"],
+               accepted=quartic["stats"]["accepted_steps"], rejected=quartic["stats"]["rejected_steps"])
+    if nodes:
+        kinetic = kb.kinetic_raw(q, r, rho, nodes, xp=np, tolerance=1e-12, maxdim=1024)
+        cov = quartic["covector"] + kinetic["covector"]
+        env = quartic["environment"] + kinetic["environment"]
+        grad, _ = nm.finish_gradient(q, r, rho, cov, env, metric_reg=1e-3)
+        rec.update(nodes=nodes, energy=quartic["value"] + kinetic["value"], gradient=grad)
+    return rec
+
+
+def packed_samples():
+    r, k = z2_state(4, 404)
+    q = -1j * k - r.conj().T @ r / 2
+    rho, _ = nm.stationary_state(q, r, tolerance=1e-13)
+    rhs = ob._PackedZ2QuarticRHS(q, r, rho, np)
+    points, _ = ob.quadrature(2.0, 16)
+    samples, stats = ob._integrate(rhs, np.r_[points, math.sqrt(2.0)], atol=1e-13, rtol=1e-12, initial_step=None,
+                                   max_steps=100000)
+    return dict(R=r, K=k, rho=rho, window=2.0, n_quad=16, samples=samples,
+                accepted=stats["accepted_steps"], rejected=stats["rejected_steps"])
+
+
 def evaluate_ode(r, k, g, window, nq):
     q = -1j * k - r.conj().T @ r / 2
     rho, _ = nm.stationary_state(q, r, tolerance=1e-13)
@@ -113,6 +147,12 @@ def main(names):
                          evaluate_ode(*random_state(16, 716), 2.0, 20.0, 192)])
     if "samples" in names:
         samples_d5()
+    if "packed" in names:
+        save("packed.npz", [evaluate_packed(*z2_state(4, 604), 1.5, 30.0, 64),
+                            evaluate_packed(*z2_state(8, 508), 2.0, 30.0, 64),
+                            evaluate_packed(*z2_state(16, 616), 2.0, 30.0, 512, 512),
+                            evaluate_packed(*z2_state(32, 632), 2.0, 30.0, 512, 512),
+                            packed_samples()])
     print(f"golden vectors written in {time.time() - t0:.1f} s")
 
 
@@ -130,4 +170,4 @@ def samples_d5():
 
 
 if __name__ == "__main__":
-    main(sys.argv[1:] or ["small", "d16", "d64", "ode", "samples"])
+    main(sys.argv[1:] or ["small", "d16", "d64", "ode", "samples", "packed"])
