@@ -53,6 +53,12 @@ typedef struct rcmps_settings {
   int krylov_maxdim;           /* largest basis */
   double metric_reg;           /* regulariser of the metric solve */
   double boundary_tolerance;   /* GMRES tolerance of the boundary Poisson solve */
+  int symmetry;                /* quartic route: 0 the unpacked channels for every state (the
+                                  reference's --reduced); 1 the packed Z2 route for every state,
+                                  a state without the exact Z2 block structure fails with
+                                  RCMPS_INVALID_ARGUMENT (--packed-z2, the default of
+                                  evaluate_quartic_persistent_trajectory); 2 packed for the states
+                                  with that structure, unpacked for the others */
 } rcmps_settings;
 
 /* Per-state diagnostics. */

@@ -21,7 +21,7 @@ void note_launch();
 
 // ------------------------------------------------------------------ status codes
 // The numbers of the reference's device controller (device_control_backend.py:23-27 of
-// rcmps_gpu) plus the wait limit of this build.
+// rcmps_gpu) plus the wait limit and the solver and input failures of this library.
 enum Status : int {
   kOk = 0,
   kMaxSteps = 1,
@@ -34,6 +34,7 @@ enum Status : int {
   kKrylovFailure = 8,       // shifted Arnoldi did not reach its true residual
   kSolveFailure = 9,        // GMRES / dense solve did not reach its residual
   kNonfiniteResult = 10,
+  kInvalidInput = 20,       // a state the requested route does not accept (RCMPS_INVALID_ARGUMENT)
 };
 
 // ------------------------------------------------------------------ complex helpers

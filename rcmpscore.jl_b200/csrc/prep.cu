@@ -98,6 +98,70 @@ cudaError_t launch_commutator(double* ops, int dp, long long ops_stride, int nst
   return cudaGetLastError();
 }
 
+// One CTA per state: the exact Z2 block structure test of the packed route
+// (ode_backend.py:246-256). K's off-diagonal blocks stand for Q's: with R's diagonal blocks zero,
+// R^dag R is block diagonal, so Q = -iK - R^dag R/2 has zero off-diagonal blocks iff K has.
+__global__ void z2_check_kernel(const double2* __restrict__ R, const double2* __restrict__ K,
+                                const double2* __restrict__ rho, const int* __restrict__ dims, int dp,
+                                long long stride, int mode, int* __restrict__ flags, long long flag_stride) {
+  const int s = blockIdx.x;
+  const int d = dims[s];
+  const int n = d / 2;
+  const double2* r = R + (long long)s * stride;
+  const double2* k = K + (long long)s * stride;
+  const double2* p = rho + (long long)s * stride;
+  __shared__ int bad;
+  __shared__ double red[2][32];
+  if (threadIdx.x == 0) bad = (d % 2) ? 1 : 0;
+  __syncthreads();
+  double herm = 0.0, nrm = 0.0;
+  int mine = 0;
+  for (int e = threadIdx.x; e < d * d; e += blockDim.x) {
+    const int i = e / d, j = e % d;
+    const double2 rv = r[i * dp + j], kv = k[i * dp + j], pv = p[i * dp + j], pt = p[j * dp + i];
+    if ((i < n) == (j < n)) {
+      if (rv.x != 0.0 || rv.y != 0.0) mine = 1;
+    } else if (kv.x != 0.0 || kv.y != 0.0 || pv.x != 0.0 || pv.y != 0.0) {
+      mine = 1;
+    }
+    const double dx = pv.x - pt.x, dy = pv.y + pt.y;   // (rho - rho^dag)_ij
+    herm += dx * dx + dy * dy;
+    nrm += pv.x * pv.x + pv.y * pv.y;
+  }
+  if (mine) atomicOr(&bad, 1);
+  for (int o = 16; o > 0; o >>= 1) {
+    herm += __shfl_xor_sync(0xffffffffu, herm, o);
+    nrm += __shfl_xor_sync(0xffffffffu, nrm, o);
+  }
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (lane == 0) {
+    red[0][warp] = herm;
+    red[1][warp] = nrm;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double h = 0.0, m = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+      h += red[0][w];
+      m += red[1][w];
+    }
+    const bool ok = !bad && sqrt(h) <= 1e-13 * fmax(1.0, sqrt(m));
+    flags[(long long)s * flag_stride] = ok ? 1 : (mode == 1 ? -1 : 0);
+  }
+}
+
+cudaError_t launch_z2_check(const double* R, const double* K, const double* rho, const int* d_dims, int dp,
+                            long long in_stride, int nstates, int mode, int* z2_flags, long long flag_stride,
+                            cudaStream_t stream) {
+  if (nstates == 0) return cudaSuccess;
+  note_launch();
+  z2_check_kernel<<<nstates, 256, 0, stream>>>(reinterpret_cast<const double2*>(R),
+                                                reinterpret_cast<const double2*>(K),
+                                                reinterpret_cast<const double2*>(rho), d_dims, dp, in_stride, mode,
+                                                z2_flags, flag_stride);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_pad(const double* src, const long long* d_src_off, const int* d_dims, double* dst, int dp,
                        long long stride, int nstates, cudaStream_t stream) {
   if (nstates == 0) return cudaSuccess;

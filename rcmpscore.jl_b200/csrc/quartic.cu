@@ -190,6 +190,7 @@ int quartic_run(rcmps_context* ctx, QuarticJob& job, cudaStream_t stream) {
       const size_t h_o_tstats = H.add(n * sizeof(TrajStats));
       const size_t h_o_flag = H.add(n * sizeof(int));
       const size_t h_o_vals = H.add(n * 8);
+      const size_t h_o_z2 = H.add(n * sizeof(int));
       if (pinned_reserve(SL, H.total) != cudaSuccess) return fail(ctx, RCMPS_CUDA_ERROR, "pinned host buffer");
       char* h = static_cast<char*>(SL.pinned);
       int* h_dims = reinterpret_cast<int*>(h + h_o_dims);
@@ -266,6 +267,29 @@ int quartic_run(rcmps_context* ctx, QuarticJob& job, cudaStream_t stream) {
                            stream);
       if (e == cudaSuccess && system == 1)
         e = launch_commutator(reinterpret_cast<double*>(d_ops), dp, (long long)zs.nops * mat, n, stream);
+      // the packed Z2 route: each state's flag in its TrajState (the dense route keeps 0)
+      if (e == cudaSuccess && system == 0 && S.symmetry != 0)
+        e = launch_z2_check(dR, dK, dP, (int*)P(o_dims), dp, in_stride, n, S.symmetry,
+                            reinterpret_cast<int*>(base + o_states + offsetof(TrajState, z2)),
+                            (long long)(sizeof(TrajState) / sizeof(int)), stream);
+      if (e == cudaSuccess && system == 0 && S.symmetry == 1) {
+        // the strict route fails before any integration, as the reference raises in the
+        // constructor of its packed system
+        int* h_z2 = reinterpret_cast<int*>(h + h_o_z2);
+        e = cudaMemcpy2DAsync(h_z2, sizeof(int), base + o_states + offsetof(TrajState, z2), sizeof(TrajState),
+                              sizeof(int), n, cudaMemcpyDeviceToHost, stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+        if (e == cudaSuccess)
+          for (int i = 0; i < n; ++i)
+            if (h_z2[i] < 0) {
+              job.stats[idx[i]].status = RCMPS_INVALID_ARGUMENT;
+              job.stats[idx[i]].failed_component = 1;
+              return fail(ctx, RCMPS_INVALID_ARGUMENT,
+                          "state " + std::to_string(idx[i]) +
+                              ": the packed Z2 route requires an even D and the exact block structure "
+                              "(R odd, K and rho even, rho Hermitian to 1e-13); no projection is performed");
+            }
+      }
       if (e == cudaSuccess)
         e = node_weights_launch((double*)P(o_points), (double*)P(o_weights), nodes, (double*)P(o_wj), stream);
       TrajControls tc;

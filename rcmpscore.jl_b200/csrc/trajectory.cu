@@ -511,6 +511,17 @@ trajectory_kernel(const TrajState* __restrict__ states, const double* __restrict
   const int row0 = (int)rank * 16;
   Ctl& C = *sm.ctl;
   long long gq = 0;
+  if (SYS == kSysQuartic && st->z2 < 0) {
+    // the packed Z2 route refused this state (no exact Z2 block structure): nothing is
+    // integrated; every CTA of the cluster leaves here, before any cluster barrier
+    if (rank == 0 && tid == 0) {
+      TrajStats* o = st->stats;
+      o->status = kInvalidInput;
+      o->attempts = o->accepted = o->rejected = o->dense_steps = o->next_point = 0;
+      o->t = o->h = o->min_h = o->max_h = o->last_error = o->value = 0.0;
+    }
+    return;
+  }
 
   if (tid == 0) {
     for (int i = 0; i < GE::NST; ++i) {
@@ -563,7 +574,14 @@ trajectory_kernel(const TrajState* __restrict__ states, const double* __restrict
   rhs(zb(zcount), kb(0), C.jac[0], C.src[0]);
   ++zcount;
 
-  const double N = (double)GE::NCH * st->d * st->d + (GE::SCALAR ? 1.0 : 0.0);
+  // The packed Z2 route counts, per channel, the upper off-diagonal block of an odd channel
+  // (F1, F3, A2, A4: c even) and the two diagonal blocks of an even one, 10 (d/2)^2 entries plus
+  // the scalar (persistent_trajectory_backend.py:68, 115); the structural zeros and the lower
+  // blocks, the adjoints of the upper ones, stay out of the norm.
+  const bool packed = SYS == kSysQuartic && st->z2 > 0;
+  const int half = st->d / 2;
+  const double N = packed ? 10.0 * half * half + 1.0
+                          : (double)GE::NCH * st->d * st->d + (GE::SCALAR ? 1.0 : 0.0);
   const double atol = st->atol, rtol = st->rtol;
   const long long max_steps = st->max_steps;
   const unsigned long long t_start = global_ns();
@@ -635,6 +653,11 @@ trajectory_kernel(const TrajState* __restrict__ states, const double* __restrict
       double s5 = 0.0, s3 = 0.0;
       for (int e = tid; e < GE::OWN; e += GE::NT) {
         const size_t off = own_offset<DP>(e, row0);
+        if (packed) {
+          const int c = e / (16 * DP), row = row0 + (e % (16 * DP)) / DP, col = e % DP;
+          const bool lo_r = row < half, lo_c = col < half;
+          if ((c % 2 == 0) ? !(lo_r && !lo_c) : (lo_r != lo_c)) continue;
+        }
         double2 e5 = make_double2(0.0, 0.0), e3 = make_double2(0.0, 0.0);
 #pragma unroll
         for (int s = 0; s <= 12; ++s) {

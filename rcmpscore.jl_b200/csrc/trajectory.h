@@ -29,7 +29,8 @@ struct TrajState {
   double atol, rtol;
   long long max_steps;
   int d;                              // physical bond dimension (d <= dp)
-  int pad_;
+  int z2;                             // quartic system: 1 the packed Z2 error norm (10 (d/2)^2 + 1
+                                      // entries), 0 the dense one, -1 refused (no exact Z2 structure)
 };
 
 struct TrajControls {

@@ -76,7 +76,8 @@ def context(device=None):
 
 def settings_from_args(args=None, **overrides):
     """Settings from an argparse namespace of the reference's optimizer (window, quadrature,
-    atol, rtol, max_steps, nodes, krylov_tolerance, maxdim, metric_reg)."""
+    atol, rtol, max_steps, nodes, krylov_tolerance, maxdim, metric_reg; packed_z2 or reduced
+    selects the quartic route, sweep_driver.py:48-50, 100-101)."""
     s = _lib.default_settings()
     if args is not None:
         mapping = dict(window="half_window", quadrature="n_quad", atol="atol", rtol="rtol",
@@ -85,11 +86,20 @@ def settings_from_args(args=None, **overrides):
         for src, dst in mapping.items():
             if getattr(args, src, None) is not None:
                 setattr(s, dst, type(getattr(s, dst))(getattr(args, src)))
+        packed, reduced = bool(getattr(args, "packed_z2", False)), bool(getattr(args, "reduced", False))
+        if packed and reduced:
+            raise ValueError("the quartic route takes one of --packed-z2, --reduced")
+        s.symmetry = SYMMETRY_Z2 if packed else SYMMETRY_NONE
     for key, value in overrides.items():
         if not hasattr(s, key):
             raise KeyError(f"unknown setting {key}")
         setattr(s, key, value)
     return s
+
+
+# Quartic routes of the library (rcmps_settings.symmetry): the unpacked channels, the packed Z2
+# route (states without the exact Z2 block structure raise ValueError), or packed where possible.
+SYMMETRY_NONE, SYMMETRY_Z2, SYMMETRY_AUTO = 0, 1, 2
 
 
 def _check_matrices(*mats):
@@ -135,13 +145,13 @@ def _raise_for(status, ctx, stats, what):
     detail = ctx.error()
     comp = stats.as_dict()["failed_component"] if stats is not None else None
     msg = f"{what}: {name} ({detail})" if detail else f"{what}: {name}"
+    if status == 20:
+        raise ValueError(msg)
     if comp == "trajectory" or (comp is None and status in range(1, 8)):
         raise DeviceControlFailure(dict(stats.as_dict() if stats is not None else {}, status_name=name,
                                         message=msg))
     if comp == "kinetic" or status == 8:
         raise KineticFailure(msg)
-    if status in (20,):
-        raise ValueError(msg)
     raise SolverFailure(msg)
 
 
@@ -245,14 +255,19 @@ def _k_from_q(q, r):
 
 def evaluate_quartic_persistent_trajectory(R, Q, rho, g=1.0, *, xp=None, half_window=30.0, n_quad=512,
                                            atol=1e-13, rtol=1e-12, initial_step=None, max_steps=1_000_000,
-                                           max_device_seconds=30.0, return_samples=False, **ignored):
+                                           max_device_seconds=30.0, return_samples=False, unpacked=False,
+                                           **ignored):
     """g times the quartic value, raw covector and environment:
-    dict(value, energy, covector, environment, stats[, samples])."""
+    dict(value, energy, covector, environment, stats[, samples]). As the reference
+    (persistent_trajectory_backend.py:439-461), the packed Z2 route is the default and a state
+    without the exact Z2 block structure raises ValueError; unpacked=True takes the seven
+    unpacked channels (any state). Packed samples have 10 (D/2)^2 + 1 entries per point."""
     import torch
     d = _check_matrices(R, Q, rho)
     ctx = context()
     s = _lib.default_settings(half_window=float(half_window), n_quad=int(n_quad), atol=float(atol), rtol=float(rtol),
-                              max_steps=int(max_steps), max_device_seconds=float(max_device_seconds))
+                              max_steps=int(max_steps), max_device_seconds=float(max_device_seconds),
+                              symmetry=SYMMETRY_NONE if unpacked else SYMMETRY_Z2)
     if initial_step is not None:
         s.initial_step = float(initial_step)
     K = _k_from_q(Q, R)
@@ -268,7 +283,8 @@ def evaluate_quartic_persistent_trajectory(R, Q, rho, g=1.0, *, xp=None, half_wi
     st = stats[0].as_dict()
     st.update(accepted_steps=st["accepted"], rejected_steps=st["rejected"], persistent_trajectory=True,
               trajectory_kernel_launches=1, host_step_synchronizations=0, implicit_fallbacks=0,
-              device_milliseconds=ctx.timings()[0])
+              device_milliseconds=ctx.timings()[0], packed_z2=not unpacked,
+              matrix_dimension=d if unpacked else d // 2)
     v = float(value.cpu().item())
     out = dict(value=v, energy=v, covector=_unpack(cov, [d])[0], environment=_unpack(env, [d])[0], stats=st)
     if return_samples:
@@ -277,7 +293,25 @@ def evaluate_quartic_persistent_trajectory(R, Q, rho, g=1.0, *, xp=None, half_wi
         rc = ctx.lib.rcmps_quartic_samples(ctx.handle, d, dR.data_ptr(), dK.data_ptr(), dP.data_ptr(), C.byref(s),
                                            samples.data_ptr(), C.byref(st2), _stream())
         _raise_for(rc, ctx, st2, "quartic samples")
-        out["samples"] = samples.cpu().numpy()
+        out["samples"] = samples.cpu().numpy() if unpacked else pack_z2_samples(samples.cpu().numpy(), d)
+    return out
+
+
+def pack_z2_samples(samples, d):
+    """Dense seven-channel samples [points][7 d^2 + 1] of a Z2 state -> the packed layout
+    [points][10 (d/2)^2 + 1] of the reference (ode_backend.py:262-275): per channel the upper
+    off-diagonal block (F1, F3, A2, A4) or the two diagonal blocks (F2, A1, A3), then the scalar."""
+    n = d // 2
+    mats = samples[:, :-1].reshape(len(samples), 7, d, d)
+    blocks = []
+    for c in range(7):
+        if c % 2 == 0:
+            blocks.append(mats[:, c, :n, n:])
+        else:
+            blocks += [mats[:, c, :n, :n], mats[:, c, n:, n:]]
+    out = np.empty((len(samples), 10 * n * n + 1), dtype=np.complex128)
+    out[:, :-1] = np.stack(blocks, axis=1).reshape(len(samples), -1)
+    out[:, -1] = samples[:, -1]
     return out
 
 

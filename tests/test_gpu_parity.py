@@ -33,7 +33,8 @@ def test_trajectory_samples_match_reference_and_oracle(gpu_context):
     R, K, rho = data["R"], data["K"], data["rho"]
     Q = O.left_canonical_q(R, K)
     out = objective.evaluate_quartic_persistent_trajectory(R, Q, rho, 1.0, half_window=float(data["window"]),
-                                                           n_quad=int(data["n_quad"]), return_samples=True)
+                                                           n_quad=int(data["n_quad"]), return_samples=True,
+                                                           unpacked=True)
     st = out["stats"]
     assert (st["accepted"], st["rejected"]) == (int(data["accepted"]), int(data["rejected"]))
     ref = data["samples"]
@@ -48,7 +49,8 @@ def test_components_match_reference_small(gpu_context, index):
     rec = load_records("small.npz")[index]
     R, K, rho, g = rec["R"], rec["K"], rec["rho"], rec["g"]
     Q = O.left_canonical_q(R, K)
-    q = objective.evaluate_quartic_persistent_trajectory(R, Q, rho, g, half_window=rec["window"], n_quad=int(rec["n_quad"]))
+    q = objective.evaluate_quartic_persistent_trajectory(R, Q, rho, g, half_window=rec["window"],
+                                                         n_quad=int(rec["n_quad"]), unpacked=True)
     assert (q["stats"]["accepted"], q["stats"]["rejected"]) == (rec["accepted"], rec["rejected"])
     assert abs(q["value"] - rec["quartic_value"]) <= 1e-12 * max(1.0, abs(rec["quartic_value"]))
     assert np.abs(q["covector"] - rec["quartic_covector"]).max() <= 1e-11 * max(1.0, np.abs(rec["quartic_covector"]).max())
@@ -163,20 +165,20 @@ def test_failure_statuses_are_reported(gpu_context):
     Q = O.left_canonical_q(R, K)
     rho = O.stationary_state(Q, R)
     with pytest.raises(objective.DeviceControlFailure) as err:
-        objective.evaluate_quartic_persistent_trajectory(R, Q, rho, 1.0, max_steps=5)
+        objective.evaluate_quartic_persistent_trajectory(R, Q, rho, 1.0, max_steps=5, unpacked=True)
     assert err.value.diagnostics["status_name"] == "max_steps"
     with pytest.raises(objective.DeviceControlFailure) as err:
-        objective.evaluate_quartic_persistent_trajectory(R, Q, rho, 1.0, max_device_seconds=1e-9)
+        objective.evaluate_quartic_persistent_trajectory(R, Q, rho, 1.0, max_device_seconds=1e-9, unpacked=True)
     assert err.value.diagnostics["status_name"] == "device_clock_timeout"
     bad = R.copy()
     bad[0, 0] = np.nan
     with pytest.raises(ValueError):
-        objective.evaluate_quartic_persistent_trajectory(bad, Q, rho, 1.0)
+        objective.evaluate_quartic_persistent_trajectory(bad, Q, rho, 1.0, unpacked=True)
     big = np.eye(129, dtype=complex)
     with pytest.raises(ValueError):
         objective.fg_phi4_batch([big], [big], [big], [1.0])
     # the context stays usable after the failures
-    out = objective.evaluate_quartic_persistent_trajectory(R, Q, rho, 1.0, n_quad=16)
+    out = objective.evaluate_quartic_persistent_trajectory(R, Q, rho, 1.0, n_quad=16, unpacked=True)
     assert out["stats"]["status"] == 0
 
 

@@ -55,7 +55,7 @@ def test_fg_batch_dp32_dp48(gpu_context):
 def test_quartic_and_kinetic_dp96_dp128(gpu_context, d):
     from rcmps_b200 import objective
     R, K, Q, rho = _state(d, 7000 + d)
-    q = objective.evaluate_quartic_persistent_trajectory(R, Q, rho, 2.0, half_window=1.0, n_quad=8)
+    q = objective.evaluate_quartic_persistent_trajectory(R, Q, rho, 2.0, half_window=1.0, n_quad=8, unpacked=True)
     ref = O.evaluate_quartic(R, Q, rho, 2.0, half_window=1.0, n_quad=8)
     assert (q["stats"]["accepted"], q["stats"]["rejected"]) == (ref["stats"]["accepted"], ref["stats"]["rejected"])
     assert abs(q["value"] - ref["value"]) <= ENERGY_TOL * max(1.0, abs(ref["value"]))
