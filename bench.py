@@ -105,7 +105,8 @@ def _cpu_eval(args):
         Q = O.left_canonical_q(R, K)
         rho = O.stationary_state(Q, R, tolerance=1e-13, method="krylov")
         t0 = time.perf_counter()
-        O.fg_phi4(R, K, rho, g, method="krylov")
+        # Z2 states on the packed route, as the reference's persistent trajectory takes them
+        O.fg_phi4(R, K, rho, g, method="krylov", packed_z2=z2)
         return time.perf_counter() - t0
 
 
@@ -172,7 +173,9 @@ def run_b200(args, rank, world, local_rank):
     dims = [len(r) for r in R]
     n = len(dims)
     total = sum(d * d for d in dims)
-    s = _lib.default_settings()
+    # the quartic route of each state as the reference takes it: packed Z2 for the Z2 states,
+    # the unpacked channels for the others
+    s = _lib.default_settings(symmetry=2 if args.quartic_route == "auto" else 0)
     cdims = (C.c_int * n)(*dims)
     cg = (C.c_double * n)(*g)
     pack = lambda L: torch.from_numpy(np.concatenate([np.ascontiguousarray(x).ravel() for x in L])).cuda()
@@ -236,7 +239,10 @@ def run_b200(args, rank, world, local_rank):
     value = total_states * args.steps / (elapsed / 1000.0)
     rhs_calls = [stats[i].rhs_calls for i in range(n)]
     # roofline of the dominant kernel: the trajectory (FP64 tensor cores, mma.sync m16n8k8)
-    flops = sum(FLOPS_PER_RHS_D3 * rhs_calls[i] * dims[i] ** 3 for i in range(n))
+    # a packed Z2 state needs a quarter of the products: each output block and each K half of a
+    # product is one of two parity blocks, the other is a structural zero
+    packed = [bool(stats[i].packed_z2) for i in range(n)]
+    flops = sum(FLOPS_PER_RHS_D3 * rhs_calls[i] * dims[i] ** 3 * (0.25 if packed[i] else 1.0) for i in range(n))
     traj = statistics.mean(traj_ms)
     achieved = flops / (traj / 1000.0) / 1e12
     peak = lib.rcmps_fp64_peak_tflops(ctx.handle)
@@ -298,7 +304,11 @@ def run_b200(args, rank, world, local_rank):
                 "config": {"workload": desc, "states_per_gpu": n, "half_window": 30.0, "n_quad": 512,
                            "kinetic_nodes": 512, "atol": 1e-13, "rtol": 1e-12, "krylov_tolerance": 1e-12,
                            "l2": "inputs and workspaces exceed L2 (126 MB); no flush needed", "parallelism":
-                           f"state shards over {world} GPU(s)"},
+                           f"state shards over {world} GPU(s)",
+                           "quartic_route": ("packed Z2 for the Z2 states (error norm over 10 (D/2)^2 + 1 entries, "
+                                             "structural zeros skipped), unpacked channels for the random states"
+                                             if args.quartic_route == "auto" else
+                                             "unpacked channels for every state")},
                 "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                              "frac": achieved / peak if peak else None, "traffic": traffic,
                              "kernel": "trajectory_kernel<64> (FP64 mma.sync m16n8k8)",
@@ -310,7 +320,12 @@ def run_b200(args, rank, world, local_rank):
                 "steps_per_state": {"rhs_calls_mean": statistics.mean(rhs_calls), "accepted_mean":
                                     statistics.mean(stats[i].accepted for i in range(n)),
                                     "gmres_iterations_mean": statistics.mean(stats[i].gmres_iterations for i in range(n)),
-                                    "krylov_basis_max": max(max(stats[i].krylov_basis) for i in range(n))},
+                                    "krylov_basis_max": max(max(stats[i].krylov_basis) for i in range(n)),
+                                    "packed_z2_states": sum(packed),
+                                    "rhs_calls_max_unpacked": max([rhs_calls[i] for i in range(n) if not packed[i]],
+                                                                  default=0),
+                                    "rhs_calls_max_packed": max([rhs_calls[i] for i in range(n) if packed[i]],
+                                                                default=0)},
                 "gpu_launches": None, "gpu_launches_note": "library kernel launches per step (rcmps_launch_count)", "clocks": clocks.summary(), "e2e": e2e, "cpu_baseline": cpu}
         line["gpu_launches"] = launches
         line["launches_before_timed"] = launches0
@@ -325,6 +340,9 @@ def main():
     p.add_argument("--impl", choices=("b200", "reference"), default="b200")
     p.add_argument("--workload", default="d64_mixed")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--quartic-route", choices=("auto", "unpacked"), default="auto",
+                   help="auto: the packed Z2 route for the Z2 states (the reference's default for them); "
+                        "unpacked: the seven unpacked channels for every state")
     p.add_argument("--component", choices=("fg", "quartic"), default="fg",
                    help="time the whole evaluation (default) or the quartic term alone")
     args = p.parse_args()

@@ -73,6 +73,7 @@ typedef struct rcmps_state_stats {
   double krylov_residual;      /* largest true relative residual of the shifted solves */
   int gmres_iterations;        /* boundary Poisson solve */
   double boundary_residual;
+  int packed_z2;               /* 1: the quartic term took the packed Z2 route */
 } rcmps_state_stats;
 
 void rcmps_default_settings(rcmps_settings* settings);

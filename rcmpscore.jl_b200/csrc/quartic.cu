@@ -398,6 +398,7 @@ int quartic_run(rcmps_context* ctx, QuarticJob& job, cudaStream_t stream) {
         o.last_step = t.h;
         o.min_step = t.min_h;
         o.max_step = t.max_h;
+        o.packed_z2 = t.packed;
         o.quartic_value = system == 0 ? (job.couplings ? job.couplings[idx[i]] : 1.0) * t.value : h_vals[i];
         if (t.status && !o.status) {
           o.status = t.status;

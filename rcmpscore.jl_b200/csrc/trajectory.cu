@@ -219,6 +219,10 @@ struct Rhs {
   long long* gq;   // running chunk counter (uniform across the CTA)
   int nchunk;      // chunks of one right-hand side (uniform)
   int ce, cc;      // producer cursor (thread 0): entry (G1 products, then G2 passes), chunk in it
+  // Packed Z2 state with d = DP and d/2 a multiple of 16 (zs): each CTA's 16 rows lie in one
+  // parity half hh of the two halves of hz rows; the structurally zero output tiles and K
+  // halves of every product are skipped.
+  int zs, hz, hh;
 
   __device__ static const SysTab& T() { return c_sys[SYS]; }
   __device__ static int gsi() { return GE::GS == 2 ? 1 : 0; }
@@ -310,9 +314,11 @@ struct Rhs {
 
   // acc += A (M rows in shared memory, lda) * the next nch streamed chunks. Ends with the chunks'
   // slots released and the next chunks issued.
+  // ztile: the warp's tiles are structurally zero (no math); kn0/kn1 >= 0: only K rows of that
+  // half of the first / second K block contribute (packed Z2 states), -1: all.
   template <class TL>
   __device__ void stream_product(ZFrag* acc, const double2* A, int lda, int nch, int& q, long long g0,
-                                 const double2* zb) {
+                                 const double2* zb, bool ztile, int kn0, int kn1) {
     constexpr int TPW = TL::TPW, SK = TL::SK;
     const int tile0 = SK > 1 ? warp / SK : warp * TPW;
     const int slice = SK > 1 ? warp % SK : 0;
@@ -333,17 +339,24 @@ struct Rhs {
       return;
     }
     for (int ch = 0; ch < nch; ++ch, ++q) {
-      const double2* B = await(g0 + q);
+      const double2* B = await(g0 + q);   // every warp waits, so a slot is refilled only once it landed
+      bool live = !ztile;
+      if (live && kn0 >= 0) {
+        const int kr = ch * GE::KC;        // a chunk lies in one half: hz is a multiple of KC
+        live = ((kr % DP) >= hz ? 1 : 0) == (kr < DP ? kn0 : kn1);
+      }
+      if (live) {
 #pragma unroll
-      for (int ks = 0; ks < GE::KC / 8; ++ks) {
-        const int kstep = ch * (GE::KC / 8) + ks;
-        if (kstep % SK != slice) continue;
-        AFrag a;
-        load_a(A, lda, mt * 16, kstep * 8, lane, a);
-        BFrag b[TPW];
+        for (int ks = 0; ks < GE::KC / 8; ++ks) {
+          const int kstep = ch * (GE::KC / 8) + ks;
+          if (kstep % SK != slice) continue;
+          AFrag a;
+          load_a(A, lda, mt * 16, kstep * 8, lane, a);
+          BFrag b[TPW];
 #pragma unroll
-        for (int j = 0; j < TPW; ++j) load_b(B, GE::LDB, ks * 8, ((tile0 + j) % TL::NTN) * 8, lane, b[j]);
-        zmma_tiles<TPW>(acc, a, b);
+          for (int j = 0; j < TPW; ++j) load_b(B, GE::LDB, ks * 8, ((tile0 + j) % TL::NTN) * 8, lane, b[j]);
+          zmma_tiles<TPW>(acc, a, b);
+        }
       }
       __syncwarp();
       if (lane == 0) mbar_arrive(&sm.empty[(int)((g0 + q) % GE::NST)]);
@@ -360,10 +373,21 @@ struct Rhs {
     const int tile0 = SK > 1 ? warp / SK : warp * TPW;
     const int slice = SK > 1 ? warp % SK : 0;
     const int mt = tile0 / TL::NTN;     // M = 32: 0 Qc rows, 1 Rc rows
+    static_assert(DP % 32 != 0 || (DP / 16) % TPW == 0, "a warp's tiles lie in one column half");
+    // packed Z2: Q X_c on rows of half hh lives in column half hh ^ p (p = 1 for odd channels)
+    // and takes K rows of half hh; R X_c lives in (1 - hh) ^ p and takes K rows of 1 - hh
+    bool zt = false;
+    int kn0 = -1;
+    if (zs && M == 32) {
+      const int p = (c % 2 == 0) ? 1 : 0;
+      const int colh = ((tile0 % TL::NTN) * 8) >= hz ? 1 : 0;
+      zt = colh != (mt == 0 ? (hh ^ p) : ((1 - hh) ^ p));
+      kn0 = mt == 0 ? hh : 1 - hh;
+    }
     ZFrag acc[TPW];
 #pragma unroll
     for (int j = 0; j < TPW; ++j) acc[j].zero();
-    stream_product<TL>(acc, sm.panel, GE::LDP, GE::CH1, q, g0, zb);
+    stream_product<TL>(acc, sm.panel, GE::LDP, GE::CH1, q, g0, zb, zt, kn0, -1);
     if (slice == 0 && warp < GE::NW) {
 #pragma unroll
       for (int j = 0; j < TPW; ++j) {
@@ -395,25 +419,45 @@ struct Rhs {
       const int c = first + r / 16;
       const int b = t.rsrc[c];
       const size_t off = (size_t)(row0 + (r & 15)) * DP + col;
-      const double2 x = __ldcg(zb + (size_t)c * GE::MAT + off);
-      double2 m = zscale(jac, __ldcg(st->P + (size_t)c * GE::MAT + off));
-      double2 ins = make_double2(0.0, 0.0);
-      if (b >= 0) ins = zscale(src * t.rcoef[c], __ldcg(zb + (size_t)b * GE::MAT + off));
-      sm.aprime[r * GE::LDA2 + col] = zscale(jac, x);
-      if constexpr (K3) {
-        sm.aprime[r * GE::LDA2 + DP + col] = m;
-        sm.aprime[r * GE::LDA2 + 2 * DP + col] = ins;
-      } else {
-        sm.aprime[r * GE::LDA2 + DP + col] = zadd(m, ins);
+      // packed Z2: X_c (row half hh) lives in column half hh ^ p, P_c and X_b in (1 - hh) ^ p;
+      // the products read only those parts of A'
+      bool need0 = true, need1 = true;
+      if (!K3 && zs) {
+        const int p = (c % 2 == 0) ? 1 : 0, colh = col >= hz ? 1 : 0;
+        need0 = colh == (hh ^ p);
+        need1 = !need0;
+      }
+      if (need0) sm.aprime[r * GE::LDA2 + col] = zscale(jac, __ldcg(zb + (size_t)c * GE::MAT + off));
+      if (need1) {
+        double2 m = zscale(jac, __ldcg(st->P + (size_t)c * GE::MAT + off));
+        double2 ins = make_double2(0.0, 0.0);
+        if (b >= 0) ins = zscale(src * t.rcoef[c], __ldcg(zb + (size_t)b * GE::MAT + off));
+        if constexpr (K3) {
+          sm.aprime[r * GE::LDA2 + DP + col] = m;
+          sm.aprime[r * GE::LDA2 + 2 * DP + col] = ins;
+        } else {
+          sm.aprime[r * GE::LDA2 + DP + col] = zadd(m, ins);
+        }
       }
     }
     __syncthreads();
     ZFrag acc[TPW];
 #pragma unroll
     for (int j = 0; j < TPW; ++j) acc[j].zero();
-    stream_product<TL>(acc, sm.aprime, GE::LDA2, (K3 ? 3 : 2) * GE::CH1, q, g0, zb);
     const int tile0 = SK > 1 ? warp / SK : warp * TPW;
     const int slice = SK > 1 ? warp % SK : 0;
+    static_assert(DP % 32 != 0 || (DP / 16) % TPW == 0, "a warp's tiles lie in one column half");
+    // packed Z2: channel c' of the warp's band (rows of half hh) lives in column half hh ^ p
+    bool zt = false;
+    int kn0 = -1, kn1 = -1;
+    if (!K3 && zs) {
+      const int cb = first + tile0 / TL::NTN;
+      const int p = (cb % 2 == 0) ? 1 : 0;
+      zt = (((tile0 % TL::NTN) * 8) >= hz ? 1 : 0) != (hh ^ p);
+      kn0 = hh ^ p;
+      kn1 = (1 - hh) ^ p;
+    }
+    stream_product<TL>(acc, sm.aprime, GE::LDA2, (K3 ? 3 : 2) * GE::CH1, q, g0, zb, zt, kn0, kn1);
     if (slice == 0 && warp < GE::NW) {
 #pragma unroll
       for (int j = 0; j < TPW; ++j) {
@@ -425,6 +469,10 @@ struct Rhs {
           const int a = t.lsrc[c];
           const size_t loc = (size_t)(row0 + (r & 15)) * DP + col;
           const size_t off = (size_t)c * GE::MAT + loc;
+          if (zt) {   // structurally zero: every term of the sum is an exact zero
+            kout[off] = make_double2(0.0, 0.0);
+            continue;
+          }
           double2 v = zadd(acc[j].value(i), kout[off]);
           if (a >= 0) v = zaxpy(src * t.lcoef[c], __ldcg((t.lkind[c] ? st->L : st->P) + (size_t)a * GE::MAT + loc), v);
           if (t.fixed[c] == 1) v = zaxpy(src, st->fixed0[loc], v);
@@ -517,6 +565,7 @@ trajectory_kernel(const TrajState* __restrict__ states, const double* __restrict
     if (rank == 0 && tid == 0) {
       TrajStats* o = st->stats;
       o->status = kInvalidInput;
+      o->packed = 0;
       o->attempts = o->accepted = o->rejected = o->dense_steps = o->next_point = 0;
       o->t = o->h = o->min_h = o->max_h = o->last_error = o->value = 0.0;
     }
@@ -546,6 +595,37 @@ trajectory_kernel(const TrajState* __restrict__ states, const double* __restrict
   }
   __syncthreads();
   Rhs<DP, SYS> rhs{st, sm, row0, tid, lane, warp, &gq, Rhs<DP, SYS>::total_chunks(), 0, 0};
+  // The packed Z2 route counts, per channel, the upper off-diagonal block of an odd channel
+  // (F1, F3, A2, A4: c even) and the two diagonal blocks of an even one, 10 (d/2)^2 entries plus
+  // the scalar (persistent_trajectory_backend.py:68, 115); the structural zeros and the lower
+  // blocks, the adjoints of the upper ones, stay out of the norm. When d = DP and d/2 is a
+  // multiple of 16 the structural zeros are also skipped in the products and stage sums: they
+  // stay exact zeros, written once below.
+  const bool packed = SYS == kSysQuartic && st->z2 > 0;
+  const int half = st->d / 2;
+  const bool zskip = packed && st->d == DP && DP % 32 == 0;
+  rhs.zs = zskip ? 1 : 0;
+  rhs.hz = half;
+  rhs.hh = zskip && row0 >= half ? 1 : 0;
+  // structurally zero element e of this CTA's rows (channel parity p: nonzero iff the row and
+  // column halves differ by p)
+  auto zero_elem = [&](int e) {
+    const int c = e / (16 * DP), row = row0 + (e % (16 * DP)) / DP, col = e % DP;
+    return (((row >= half) != (col >= half)) ? 1 : 0) != ((c % 2 == 0) ? 1 : 0);
+  };
+  if (zskip) {
+    // every work vector's own rows start at zero: the skipped parts are never written again
+    for (int e = tid; e < GE::OWN; e += GE::NT) {
+      const size_t off = own_offset<DP>(e, row0);
+      const double2 z0 = make_double2(0.0, 0.0);
+      st->y[off] = z0;
+      st->prop[off] = z0;
+      st->P[off] = z0;
+      for (int s = 0; s < 16; ++s) st->k[(size_t)s * GE::VEC + off] = z0;
+      st->z[off] = z0;
+      st->z[GE::VEC + off] = z0;
+    }
+  }
 
   // slot permutation: C.kslot[s] is the k buffer of stage s; y and proposed swap on acceptance
   if (tid < 16) C.kslot[tid] = tid;
@@ -574,12 +654,6 @@ trajectory_kernel(const TrajState* __restrict__ states, const double* __restrict
   rhs(zb(zcount), kb(0), C.jac[0], C.src[0]);
   ++zcount;
 
-  // The packed Z2 route counts, per channel, the upper off-diagonal block of an odd channel
-  // (F1, F3, A2, A4: c even) and the two diagonal blocks of an even one, 10 (d/2)^2 entries plus
-  // the scalar (persistent_trajectory_backend.py:68, 115); the structural zeros and the lower
-  // blocks, the adjoints of the upper ones, stay out of the norm.
-  const bool packed = SYS == kSysQuartic && st->z2 > 0;
-  const int half = st->d / 2;
   const double N = packed ? 10.0 * half * half + 1.0
                           : (double)GE::NCH * st->d * st->d + (GE::SCALAR ? 1.0 : 0.0);
   const double atol = st->atol, rtol = st->rtol;
@@ -624,6 +698,7 @@ trajectory_kernel(const TrajState* __restrict__ states, const double* __restrict
         ha[j] = j < terms ? h * w[j] : 0.0;
       }
       for (int e = tid; e < GE::OWN; e += GE::NT) {
+        if (zskip && zero_elem(e)) continue;
         const size_t off = own_offset<DP>(e, row0);
         double2 kv[12];
 #pragma unroll
@@ -831,6 +906,7 @@ trajectory_kernel(const TrajState* __restrict__ states, const double* __restrict
   if (rank == 0 && tid == 0) {
     TrajStats* o = st->stats;
     o->status = C.status;
+    o->packed = packed ? 1 : 0;
     o->attempts = C.attempts;
     o->accepted = C.accepted;
     o->rejected = C.rejected;

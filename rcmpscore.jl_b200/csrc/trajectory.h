@@ -8,7 +8,7 @@ namespace rcmps {
 // reference's diagnostics (device_control_backend.py:263-265 of rcmps_gpu).
 struct TrajStats {
   int status;
-  int pad_;
+  int packed;     // 1: the packed Z2 route was taken
   long long attempts, accepted, rejected, dense_steps, next_point;
   double t, h, min_h, max_h, last_error;
   double value;   // the scalar channel at the endpoint: the quartic density before g

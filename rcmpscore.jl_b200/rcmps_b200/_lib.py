@@ -39,7 +39,7 @@ class StateStats(C.Structure):
         ("t_end", C.c_double), ("last_step", C.c_double), ("min_step", C.c_double), ("max_step", C.c_double),
         ("quartic_value", C.c_double), ("kinetic_value", C.c_double),
         ("krylov_basis", C.c_int * 4), ("krylov_residual", C.c_double),
-        ("gmres_iterations", C.c_int), ("boundary_residual", C.c_double),
+        ("gmres_iterations", C.c_int), ("boundary_residual", C.c_double), ("packed_z2", C.c_int),
     ]
 
     def as_dict(self):

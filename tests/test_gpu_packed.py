@@ -78,6 +78,8 @@ def test_packed_bench_state_d64_matches_oracle(gpu_context):
     R, K = z2_state(64, 100)
     Q = O.left_canonical_q(R, K)
     rho = O.stationary_state(Q, R, tolerance=1e-13, method="krylov")
+    rho[:32, 32:] = 0.0          # exact block structure (the solver keeps it up to rounding)
+    rho[32:, :32] = 0.0
     rho = 0.5 * (rho + rho.conj().T)
     q = objective.evaluate_quartic_persistent_trajectory(R, Q, rho, 2.0)
     ref = O.evaluate_quartic(R, Q, rho, 2.0, packed_z2=True)
@@ -118,3 +120,49 @@ def test_packed_route_refuses_states_without_z2_structure(gpu_context):
     # the context stays usable, and the same states pass on the unpacked route
     out = objective.evaluate_quartic_persistent_trajectory(R, Q, rho, 1.0, n_quad=16, unpacked=True)
     assert out["stats"]["status"] == 0
+
+
+@pytest.mark.parametrize("d", [96, 128])
+def test_packed_quartic_large_d_matches_oracle(gpu_context, d):
+    """The skipped structural zeros at the other unpadded sizes with 16-row halves (dp 96, 128)."""
+    from rcmps_b200 import objective
+    from rcmps_b200.batch import z2_state
+    R, K = z2_state(d, 9100 + d)
+    Q = O.left_canonical_q(R, K)
+    rho = O.stationary_state(Q, R, tolerance=1e-13, method="krylov")
+    n = d // 2
+    rho[:n, n:] = 0.0
+    rho[n:, :n] = 0.0
+    rho = 0.5 * (rho + rho.conj().T)
+    q = objective.evaluate_quartic_persistent_trajectory(R, Q, rho, 2.0, half_window=1.0, n_quad=8)
+    ref = O.evaluate_quartic(R, Q, rho, 2.0, half_window=1.0, n_quad=8, packed_z2=True)
+    assert (q["stats"]["accepted"], q["stats"]["rejected"]) == (ref["stats"]["accepted"], ref["stats"]["rejected"])
+    assert abs(q["value"] - ref["value"]) <= ENERGY_TOL * max(1.0, abs(ref["value"]))
+    assert _rel(q["covector"], ref["covector"]) < 1e-10
+    assert _rel(q["environment"], ref["environment"]) < 1e-10
+
+
+def test_auto_route_d64_pair_in_one_launch(gpu_context):
+    """A random and a Z2 state of the bench workload in one launch: the random state takes the
+    unpacked route as when it runs alone, the Z2 state the packed one (structural zeros skipped)."""
+    from rcmps_b200 import objective
+    from rcmps_b200.batch import random_state, z2_state
+    states = [random_state(64, 0), z2_state(64, 100)]
+    rhos = []
+    for R, K in states:
+        Q = O.left_canonical_q(R, K)
+        rho, _ = objective.stationary_state(Q, R, tolerance=1e-13)
+        rhos.append(rho)
+    s = objective.settings_from_args(None, half_window=2.0, n_quad=32, kinetic_nodes=64,
+                                     symmetry=objective.SYMMETRY_AUTO)
+    E, G, st = objective.fg_phi4_batch([x[0] for x in states], [x[1] for x in states], rhos, [2.0, 2.0], s)
+    assert (st[0]["packed_z2"], st[1]["packed_z2"]) == (0, 1)
+    s0 = objective.settings_from_args(None, half_window=2.0, n_quad=32, kinetic_nodes=64)
+    E0, G0, st0 = objective.fg_phi4_batch([states[0][0]], [states[0][1]], [rhos[0]], [2.0], s0)
+    assert (st[0]["accepted"], st[0]["rejected"]) == (st0[0]["accepted"], st0[0]["rejected"])
+    assert abs(E[0] - E0[0]) <= 1e-12 * abs(E0[0])
+    R, K = states[1]
+    Q = O.left_canonical_q(R, K)
+    ref = O.evaluate_quartic(R, Q, rhos[1], 2.0, half_window=2.0, n_quad=32, packed_z2=True)
+    assert abs(st[1]["accepted"] - ref["stats"]["accepted"]) <= 1
+    assert abs(st[1]["quartic_value"] - ref["value"]) <= ENERGY_TOL * abs(ref["value"])
