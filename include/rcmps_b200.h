@@ -134,6 +134,15 @@ int rcmps_phi4_ode_batch(rcmps_context* context, int n_states, const int* dims, 
                          double* value, double* covector, double* environment, rcmps_state_stats* stats,
                          void* stream);
 
+/* The one-point function <phi> by the ODE of the first monomial: F0 = rho and
+ * dF1 = 2|t| L(F1) dt + j(t) (R F0 + F0 R^dag) dt with their adjoint channels, integrated by the
+ * same DOP853 controller; phi[i] = Re tr F1 at the endpoint (device, [n_states]). Replaces
+ * validate_sweep.phi_by_ode(r, k, rho, controls, xp) (optimizer/validate_sweep.py:23-32),
+ * RcmpsCore's phi_monomial(s, 1). stats[i].quartic_value holds the same value. */
+int rcmps_phi_ode_batch(rcmps_context* context, int n_states, const int* dims, const double* R, const double* K,
+                        const double* rho, const rcmps_settings* settings, double* phi, rcmps_state_stats* stats,
+                        void* stream);
+
 /* The trajectory alone, for one state: samples [2 n_quad + 1][7 d^2 + 1] complex (the seven
  * channels at every Gauss node and the endpoint, and the scalar channel, only filled at the
  * endpoint). Replaces PersistentTrajectoryDOP853.run() -> (samples, stats)

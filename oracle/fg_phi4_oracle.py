@@ -34,6 +34,7 @@ __all__ = [
     "QuarticSystem", "integrate", "quartic_pullback", "evaluate_quartic", "kinetic_raw",
     "stationary_state", "boundary_environment", "finish_gradient", "metric", "fg_phi4",
     "phi4_state", "z2_state", "left_canonical_q", "PackedZ2System", "z2_structure_ok",
+    "source_integral", "phi_expectation", "phi_by_ode",
 ]
 
 
@@ -564,6 +565,45 @@ def full_pullback(system, samples, points, weights, coefficients):
         total_cov += coefficient * (m + adj(nn)) / 2.0
         total_env += coefficient * (env + adj(env)) / 2.0
     return total_value, total_cov, total_env
+
+
+# The first monomial's spec, phi_monomial(s, 1) of RcmpsCore (validate_sweep.py:23-32): forward
+# F0 = rho, dF1 = 2|t| L(F1) dt + j(t) (R F0 + F0 R^dag) dt, with its adjoint channels.
+PHI1_SPECS = ((2, ((0, 1, "L", 1.0), (0, 1, "R", 1.0)), False),)
+
+
+def source_integral(half_window):
+    """Integral of the source over x in [-W, W] (ode_backend.py:782-790): 2^-1/2, its integral
+    over the line, minus twice the tail integral of K_{1/4}(x) x^{-1/4} beyond W, normalised by
+    2^{9/4} sqrt(pi) Gamma(5/4)."""
+    from scipy.integrate import quad
+    if not half_window > 0:
+        raise ValueError("positive half_window required")
+    tail = quad(lambda x: kv(0.25, x) / x ** 0.25, half_window, np.inf, epsabs=0, epsrel=1e-12, limit=200)[0]
+    return 2 ** -0.5 - 2.0 * tail / (2 ** 2.25 * math.sqrt(math.pi) * gamma(1.25))
+
+
+def phi_expectation(r, rho, half_window):
+    """<phi> on the window W in closed form (ode_backend.py:793-797): the first monomial's
+    tr F1(a) = source_integral(W) tr(R rho + rho R^dag), since the Lindbladian preserves the
+    trace."""
+    r, rho = np.asarray(r), np.asarray(rho)
+    return 2.0 * source_integral(half_window) * float(np.real(np.trace(rho @ r)))
+
+
+def phi_by_ode(r, k, rho, *, half_window, n_quad, atol=1e-13, rtol=1e-12, max_steps=1_000_000):
+    """<phi> as phi_monomial(s, 1) integrates it (validate_sweep.py:23-32): the four channels of
+    PHI1_SPECS by DOP853 with dense output at the Gauss nodes; the value is Re tr F1 at the
+    endpoint. Returns (value, stats)."""
+    r, k, rho = (np.asarray(x, complex) for x in (r, k, rho))
+    q = left_canonical_q(r, k)
+    system = FullSystem(q, r, rho, specs=PHI1_SPECS)
+    points, _ = quadrature(half_window, n_quad)
+    samples, stats = integrate(system, np.r_[points, math.sqrt(half_window)], atol=atol, rtol=rtol,
+                               max_steps=max_steps)
+    d = len(r)
+    end = samples[-1].reshape(system.channels, d, d)
+    return float(np.trace(end[1]).real), stats
 
 
 def evaluate_phi4(r, q, rho, g, *, half_window=20.0, n_quad=192, atol=1e-13, rtol=1e-12,

@@ -418,6 +418,33 @@ int rcmps_phi4_ode_batch(rcmps_context* ctx, int n, const int* dims, const doubl
   return quartic_run(ctx, job, s);
 }
 
+int rcmps_phi_ode_batch(rcmps_context* ctx, int n, const int* dims, const double* R, const double* K,
+                        const double* rho, const rcmps_settings* settings, double* phi, rcmps_state_stats* stats,
+                        void* stream) {
+  if (!ctx) return RCMPS_INVALID_ARGUMENT;
+  int rc = check_settings(ctx, settings);
+  if (rc) return rc;
+  rc = check_dims(ctx, n, dims);
+  if (rc) return rc;
+  if (n == 0) return RCMPS_OK;
+  if (!R || !K || !rho || !phi || !stats) return fail(ctx, RCMPS_INVALID_ARGUMENT, "NULL pointer");
+  cudaSetDevice(ctx->device);
+  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
+  for (int i = 0; i < n; ++i) std::memset(&stats[i], 0, sizeof(rcmps_state_stats));
+  QuarticJob job;
+  job.system = 2;
+  job.n = n;
+  job.dims = dims;
+  job.R = R;
+  job.K = K;
+  job.rho = rho;
+  job.settings = *settings;
+  job.settings.symmetry = 0;   // the packed route is the quartic term's only
+  job.value = phi;
+  job.stats = stats;
+  return quartic_run(ctx, job, s);
+}
+
 int rcmps_kinetic_batch(rcmps_context* ctx, int n, const int* dims, const double* R, const double* K,
                         const double* rho, const rcmps_settings* settings, double* value, double* covector,
                         double* environment, rcmps_state_stats* stats, void* stream) {

@@ -98,6 +98,26 @@ cudaError_t launch_commutator(double* ops, int dp, long long ops_stride, int nst
   return cudaGetLastError();
 }
 
+// One warp per state: the real part of the trace of one sample matrix.
+__global__ void endpoint_trace_kernel(const double2* __restrict__ samples, long long stride, long long offset,
+                                      int dp, const int* __restrict__ dims, double* __restrict__ out) {
+  const int s = blockIdx.x;
+  const int d = dims[s];
+  const double2* m = samples + (long long)s * stride + offset;
+  double v = 0.0;
+  for (int i = threadIdx.x; i < d; i += 32) v += m[(long long)i * dp + i].x;
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if (threadIdx.x == 0) out[s] = v;
+}
+
+cudaError_t launch_endpoint_trace(const double2* samples, long long stride, long long offset, int dp,
+                                  const int* d_dims, double* out, int nstates, cudaStream_t stream) {
+  if (nstates == 0) return cudaSuccess;
+  note_launch();
+  endpoint_trace_kernel<<<nstates, 32, 0, stream>>>(samples, stride, offset, dp, d_dims, out);
+  return cudaGetLastError();
+}
+
 // One CTA per state: the exact Z2 block structure test of the packed route
 // (ode_backend.py:246-256). K's off-diagonal blocks stand for Q's: with R's diagonal blocks zero,
 // R^dag R is block diagonal, so Q = -iK - R^dag R/2 has zero off-diagonal blocks iff K has.

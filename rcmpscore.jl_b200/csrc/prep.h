@@ -23,6 +23,9 @@ cudaError_t launch_scatter_values(const double* src, int n, const int* d_idx, do
 cudaError_t launch_export_samples(const double2* samples, int dp, int d, int npoints, const double* value,
                                   double* out, cudaStream_t stream);
 cudaError_t launch_commutator(double* ops, int dp, long long ops_stride, int nstates, cudaStream_t stream);
+// out[s] = Re tr of the leading d_s x d_s block of the dp x dp matrix at samples + s stride + offset
+cudaError_t launch_endpoint_trace(const double2* samples, long long stride, long long offset, int dp,
+                                  const int* d_dims, double* out, int nstates, cudaStream_t stream);
 // Exact Z2 block structure of each padded state (ode_backend.py:246-256): even d, R's diagonal
 // blocks, K's and rho's off-diagonal blocks exactly zero, ||rho - rho^dag||_F <= 1e-13 max(1,
 // ||rho||_F). Writes z2_flags[i] = 1 where the structure holds; mode 1 writes -1 elsewhere

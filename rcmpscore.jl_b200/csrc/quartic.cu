@@ -48,6 +48,10 @@ SysSizes sys_sizes(int system, int dp, int nblk) {
     z.wscr = (size_t)nblk * pullback_row_blocks(dp) * 3;
     z.part = (size_t)nblk * 4;
     z.fin = 8;
+  } else if (system == 2) {   // <phi>: the trajectory and its endpoint only
+    z.nops = kOps;
+    z.nwork = 21;
+    z.wscr = z.part = z.fin = 0;
   } else {
     z.nops = kOpsFull;
     z.nwork = 22;
@@ -339,6 +343,11 @@ int quartic_run(rcmps_context* ctx, QuarticJob& job, cudaStream_t stream) {
           }
         }
         if (e == cudaSuccess) e = pullback_launch(pa, nblk, stream);
+      } else if (system == 2) {
+        // <phi> = Re tr F1 at the endpoint (the last sample point, channel 1)
+        if (e == cudaSuccess)
+          e = launch_endpoint_trace(d_samp, (long long)npoints * vec, (long long)(npoints - 1) * vec + mat, dp,
+                                    (int*)P(o_dims), (double*)P(o_vout), n, stream);
       } else {
         FullPullbackArgs pa;
         pa.dp = dp;
@@ -375,7 +384,7 @@ int quartic_run(rcmps_context* ctx, QuarticJob& job, cudaStream_t stream) {
         e = launch_scatter_values((double*)P(o_vout), n, (int*)P(o_idx), job.value, job.accumulate, stream);
       if (e == cudaSuccess && job.samples_out && system == 0)
         e = launch_export_samples(d_samp, dp, h_dims[0], npoints, (double*)P(o_tval), job.samples_out, stream);
-      if (e == cudaSuccess && system == 1)   // the route's value comes from the pullback
+      if (e == cudaSuccess && system != 0)   // the value comes from the pullback or the endpoint
         e = cudaMemcpyAsync(h_vals, P(o_vout), n * 8, cudaMemcpyDeviceToHost, stream);
       if (e == cudaSuccess) e = cudaMemcpyAsync(h_tstats, P(o_tstats), n * sizeof(TrajStats), cudaMemcpyDeviceToHost, stream);
       if (e == cudaSuccess) e = cudaMemcpyAsync(h_flag, P(o_flag), n * sizeof(int), cudaMemcpyDeviceToHost, stream);

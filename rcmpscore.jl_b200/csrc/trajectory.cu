@@ -78,7 +78,7 @@ __device__ __forceinline__ double next_up(double t) {
 //   lsrc/lcoef/lkind: the left insertion c_l ol_a X_a (P_a for ol = R, L_a for the commutator);
 //   rsrc/rcoef: the right insertion c_r X_b ol_b^dag; fixed: 1 fixed0, 2 fixed6;
 //   init: initial value 0, rho (1) or the identity on the physical block (2).
-constexpr int kSysQuartic = 0, kSysFull = 1;
+constexpr int kSysQuartic = 0, kSysFull = 1, kSysPhi1 = 2;
 constexpr int kMaxChannels = 26;
 struct SysTab {
   int nch, ng1;
@@ -89,7 +89,7 @@ struct SysTab {
   int fixed[kMaxChannels], init[kMaxChannels];
   double lcoef[kMaxChannels], rcoef[kMaxChannels];
 };
-__constant__ SysTab c_sys[2];
+__constant__ SysTab c_sys[3];
 
 // Tiling of one product pass: M rows (a multiple of 16) by DP columns over NW warps; a warp owns
 // TPW consecutive 16x8 tiles of one band, or (when there are fewer tiles than warps) one tile and a
@@ -107,9 +107,9 @@ struct PassTiling {
 
 template <int DP, int SYS>
 struct Geo {
-  static constexpr int NCH = SYS == kSysQuartic ? 7 : 26;   // matrix channels
+  static constexpr int NCH = SYS == kSysQuartic ? 7 : SYS == kSysFull ? 26 : 4;   // matrix channels
   static constexpr bool SCALAR = SYS == kSysQuartic;       // the quartic system's scalar channel
-  static constexpr int KM = SYS == kSysQuartic ? 2 : 3;    // K blocks of the widest G2 pass
+  static constexpr int KM = SYS == kSysFull ? 3 : 2;       // K blocks of the widest G2 pass
   static constexpr int G = DP / 16;
   static constexpr int NW = (DP == 48 || DP == 96) ? 12 : (DP == 64 || DP == 128) ? 16 : 8;
   static constexpr int NWT = NW + 1;                  // + one producer warp that only streams B chunks
@@ -962,7 +962,7 @@ cudaError_t node_weights_launch(const double* d_points, const double* d_weights,
   return cudaGetLastError();
 }
 
-// The channel tables of the two systems (host side, copied to c_sys).
+// The channel tables of the systems (host side, copied to c_sys).
 static void quartic_table(SysTab& t) {
   std::memset(&t, 0, sizeof(t));
   t.nch = 7;
@@ -990,48 +990,43 @@ static void quartic_table(SysTab& t) {
   for (int p = 0; p < 4; ++p) { t.p_first[1][p] = pf[p]; t.p_count[1][p] = pc[p]; }
 }
 
-// Specs of the all-ODE route (ode_backend.py:60-73, 851-858): kinetic1 (4 channels, O = R),
-// kinetic2 (4 channels, O = [Q, R]) and phi^4 (5 channels, O = R); forward channels 0..12,
-// adjoint 13..25. A forward edge a -> b inserts forward a into forward b on its side; its trace
-// dual inserts adjoint b into adjoint a on the other side (ode_backend.py:108-113).
-static void full_table(SysTab& t) {
+struct SpecEdge { int a, b; bool left; double c; };
+struct SpecDef { int nch; const SpecEdge* edges; int nedge; bool comm; };
+
+// Table of forward and adjoint channels of a list of specs (ode_backend.py:76-167): forward
+// channels from 0, adjoint channels from half = sum of the specs' channels.
+static void spec_table(SysTab& t, const SpecDef* sp, int nsp) {
   std::memset(&t, 0, sizeof(t));
-  const int half = 13;
-  t.nch = 26;
-  struct Edge { int a, b; bool left; double c; };
-  const double r2 = 1.4142135623730951;
-  const Edge kin[4] = {{0, 1, true, r2}, {0, 2, false, r2}, {2, 3, true, r2}, {1, 3, false, r2}};
-  Edge quart[8];
-  for (int k = 0; k < 4; ++k) {
-    quart[2 * k] = {k, k + 1, true, (double)(k + 1)};
-    quart[2 * k + 1] = {k, k + 1, false, (double)(k + 1)};
+  int off[kMaxChannels], half = 0;
+  for (int s = 0; s < nsp; ++s) {
+    off[s] = half;
+    half += sp[s].nch;
   }
-  const int off[3] = {0, 4, 8}, nch[3] = {4, 4, 5};
-  const bool comm[3] = {false, true, false};
-  for (int c = 0; c < 26; ++c) {
+  const int nch = 2 * half;
+  t.nch = nch;
+  for (int c = 0; c < nch; ++c) {
     t.dir[c] = c < half ? 0 : 1;
     t.lsrc[c] = t.rsrc[c] = -1;
   }
-  bool is_comm[26] = {false}, lsource_comm[26] = {false};
-  for (int sp = 0; sp < 3; ++sp) {
-    const Edge* ed = sp == 2 ? quart : kin;
-    const int ne = sp == 2 ? 8 : 4;
-    for (int i = 0; i < nch[sp]; ++i) is_comm[off[sp] + i] = is_comm[half + off[sp] + i] = comm[sp];
-    t.init[off[sp]] = 1;                              // rho in the first forward channel
-    t.init[half + off[sp] + nch[sp] - 1] = 2;         // I in the last adjoint channel
-    for (int q = 0; q < ne; ++q) {
-      const int fa = off[sp] + ed[q].a, fb = off[sp] + ed[q].b;
-      const int aa = half + off[sp] + ed[q].a, ab = half + off[sp] + ed[q].b;
-      if (ed[q].left) {
-        t.lsrc[fb] = fa; t.lcoef[fb] = ed[q].c;       // forward b += c O X_a
-        t.rsrc[aa] = ab; t.rcoef[aa] = ed[q].c;       // adjoint a += c X_b O
+  bool is_comm[kMaxChannels] = {false}, lsource_comm[kMaxChannels] = {false};
+  for (int s = 0; s < nsp; ++s) {
+    for (int i = 0; i < sp[s].nch; ++i) is_comm[off[s] + i] = is_comm[half + off[s] + i] = sp[s].comm;
+    t.init[off[s]] = 1;                              // rho in the first forward channel
+    t.init[half + off[s] + sp[s].nch - 1] = 2;       // I in the last adjoint channel
+    for (int q = 0; q < sp[s].nedge; ++q) {
+      const SpecEdge& ed = sp[s].edges[q];
+      const int fa = off[s] + ed.a, fb = off[s] + ed.b;
+      const int aa = half + off[s] + ed.a, ab = half + off[s] + ed.b;
+      if (ed.left) {
+        t.lsrc[fb] = fa; t.lcoef[fb] = ed.c;       // forward b += c O X_a
+        t.rsrc[aa] = ab; t.rcoef[aa] = ed.c;       // adjoint a += c X_b O
       } else {
-        t.rsrc[fb] = fa; t.rcoef[fb] = ed[q].c;       // forward b += c X_a O^dag
-        t.lsrc[aa] = ab; t.lcoef[aa] = ed[q].c;       // adjoint a += c O^dag X_b
+        t.rsrc[fb] = fa; t.rcoef[fb] = ed.c;       // forward b += c X_a O^dag
+        t.lsrc[aa] = ab; t.lcoef[aa] = ed.c;       // adjoint a += c O^dag X_b
       }
     }
   }
-  for (int c = 0; c < 26; ++c)
+  for (int c = 0; c < nch; ++c)
     if (t.lsrc[c] >= 0 && is_comm[c]) {
       t.lkind[c] = 1;
       lsource_comm[t.lsrc[c]] = true;
@@ -1040,23 +1035,47 @@ static void full_table(SysTab& t) {
   int n = 0;
   for (int c = 0; c < half; ++c) { t.g1_ch[n] = c; t.g1_kind[n++] = 0; }
   for (int c = 0; c < half; ++c) if (lsource_comm[c]) { t.g1_ch[n] = c; t.g1_kind[n++] = 2; }
-  for (int c = half; c < 26; ++c) { t.g1_ch[n] = c; t.g1_kind[n++] = 1; }
-  for (int c = half; c < 26; ++c) if (lsource_comm[c]) { t.g1_ch[n] = c; t.g1_kind[n++] = 3; }
+  for (int c = half; c < nch; ++c) { t.g1_ch[n] = c; t.g1_kind[n++] = 1; }
+  for (int c = half; c < nch; ++c) if (lsource_comm[c]) { t.g1_ch[n] = c; t.g1_kind[n++] = 3; }
   t.ng1 = n;
   // G2 passes: one per channel, or pairs of consecutive channels of one spec
-  t.np[0] = 26;
-  for (int c = 0; c < 26; ++c) { t.p_first[0][c] = c; t.p_count[0][c] = 1; t.p_k3[0][c] = is_comm[c]; }
+  t.np[0] = nch;
+  for (int c = 0; c < nch; ++c) { t.p_first[0][c] = c; t.p_count[0][c] = 1; t.p_k3[0][c] = is_comm[c]; }
   int p = 0;
   for (int dir = 0; dir < 2; ++dir)
-    for (int sp = 0; sp < 3; ++sp)
-      for (int i = 0; i < nch[sp]; i += 2) {
-        const int c = dir * half + off[sp] + i;
+    for (int s = 0; s < nsp; ++s)
+      for (int i = 0; i < sp[s].nch; i += 2) {
+        const int c = dir * half + off[s] + i;
         t.p_first[1][p] = c;
-        t.p_count[1][p] = i + 1 < nch[sp] ? 2 : 1;
-        t.p_k3[1][p] = comm[sp];
+        t.p_count[1][p] = i + 1 < sp[s].nch ? 2 : 1;
+        t.p_k3[1][p] = sp[s].comm;
         ++p;
       }
   t.np[1] = p;
+}
+
+// Specs of the all-ODE route (ode_backend.py:60-73, 851-858): kinetic1 (4 channels, O = R),
+// kinetic2 (4 channels, O = [Q, R]) and phi^4 (5 channels, O = R); forward channels 0..12,
+// adjoint 13..25. A forward edge a -> b inserts forward a into forward b on its side; its trace
+// dual inserts adjoint b into adjoint a on the other side (ode_backend.py:108-113).
+static void full_table(SysTab& t) {
+  const double r2 = 1.4142135623730951;
+  const SpecEdge kin[4] = {{0, 1, true, r2}, {0, 2, false, r2}, {2, 3, true, r2}, {1, 3, false, r2}};
+  SpecEdge quart[8];
+  for (int k = 0; k < 4; ++k) {
+    quart[2 * k] = {k, k + 1, true, (double)(k + 1)};
+    quart[2 * k + 1] = {k, k + 1, false, (double)(k + 1)};
+  }
+  const SpecDef specs[3] = {{4, kin, 4, false}, {4, kin, 4, true}, {5, quart, 8, false}};
+  spec_table(t, specs, 3);
+}
+
+// The first monomial phi_monomial(s, 1) of RcmpsCore (validate_sweep.py:23-32): F0 = rho and
+// dF1 = 2|t| L(F1) dt + j(t) (R F0 + F0 R^dag) dt, with the two adjoint channels.
+static void phi1_table(SysTab& t) {
+  const SpecEdge phi[2] = {{0, 1, true, 1.0}, {0, 1, false, 1.0}};
+  const SpecDef spec = {2, phi, 2, false};
+  spec_table(t, &spec, 1);
 }
 
 cudaError_t trajectory_set_tables() {
@@ -1067,9 +1086,10 @@ cudaError_t trajectory_set_tables() {
   if ((e = cudaMemcpyToSymbol(c_dop_e5, rcmps_dop_e5, sizeof(rcmps_dop_e5))) != cudaSuccess) return e;
   if ((e = cudaMemcpyToSymbol(c_dop_e3, rcmps_dop_e3, sizeof(rcmps_dop_e3))) != cudaSuccess) return e;
   if ((e = cudaMemcpyToSymbol(c_dop_d, rcmps_dop_d, sizeof(rcmps_dop_d))) != cudaSuccess) return e;
-  SysTab tabs[2];
+  SysTab tabs[3];
   quartic_table(tabs[0]);
   full_table(tabs[1]);
+  phi1_table(tabs[2]);
   if ((e = cudaMemcpyToSymbol(c_sys, tabs, sizeof(tabs))) != cudaSuccess) return e;
   return cudaMemcpyToSymbol(c_source, rcmps_source_table, sizeof(rcmps_source_table));
 }
@@ -1092,9 +1112,10 @@ cudaError_t trajectory_launch(int system, int dp, const TrajState* d_states, int
                               int npoints, const TrajControls& ctl, cudaStream_t stream) {
   if (system == kSysQuartic) return launch_sys<kSysQuartic>(dp, d_states, nstates, d_points, npoints, ctl, stream);
   if (system == kSysFull) return launch_sys<kSysFull>(dp, d_states, nstates, d_points, npoints, ctl, stream);
+  if (system == kSysPhi1) return launch_sys<kSysPhi1>(dp, d_states, nstates, d_points, npoints, ctl, stream);
   return cudaErrorInvalidValue;
 }
 
-int trajectory_channels(int system) { return system == kSysFull ? 26 : 7; }
+int trajectory_channels(int system) { return system == kSysFull ? 26 : system == kSysPhi1 ? 4 : 7; }
 
 }  // namespace rcmps

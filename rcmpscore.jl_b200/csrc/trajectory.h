@@ -40,7 +40,8 @@ struct TrajControls {
 };
 
 cudaError_t trajectory_set_tables();
-// system: 0 the reduced quartic system (7 channels + scalar), 1 the all-ODE route (26 channels).
+// system: 0 the reduced quartic system (7 channels + scalar), 1 the all-ODE route (26 channels),
+// 2 the first monomial of <phi> (4 channels).
 cudaError_t trajectory_launch(int system, int dp, const TrajState* d_states, int nstates, const double* d_points,
                               int npoints, const TrajControls& ctl, cudaStream_t stream);
 int trajectory_channels(int system);

@@ -70,6 +70,8 @@ SIGNATURES = {
                                  _P, _P, _P, C.POINTER(StateStats), _P]),
     "rcmps_phi4_ode_batch": (_I, [_P, _I, C.POINTER(_I), C.POINTER(_D), _P, _P, _P, C.POINTER(Settings),
                                   _P, _P, _P, C.POINTER(StateStats), _P]),
+    "rcmps_phi_ode_batch": (_I, [_P, _I, C.POINTER(_I), _P, _P, _P, C.POINTER(Settings), _P,
+                                 C.POINTER(StateStats), _P]),
     "rcmps_quartic_samples": (_I, [_P, _I, _P, _P, _P, C.POINTER(Settings), _P, C.POINTER(StateStats), _P]),
     "rcmps_kinetic_batch": (_I, [_P, _I, C.POINTER(_I), _P, _P, _P, C.POINTER(Settings), _P, _P, _P,
                                  C.POINTER(StateStats), _P]),

@@ -6,6 +6,10 @@ This script imports the reference package rcmps_gpu read-only from a local check
   d16.npz       one D = 16 random state at the optimizer defaults (W = 30, n_quad = 512, 512 nodes)
   d64.npz       the seed-42 D = 64 random state at the optimizer defaults
   samples_d5.npz  trajectory samples of the reduced quartic system, D = 5, W = 2, n_quad = 16
+  phi.npz       <phi> in closed form (ode_backend.phi_expectation) and by the ODE of the first
+                monomial (validate_sweep.phi_by_ode, host NumPy integrator): D = 4 random (W = 6,
+                n_quad = 24), D = 8 Z2 (W = 20, n_quad = 64) and D = 16 random at the refined
+                validation settings (W = 40, n_quad = 1024, 1e-14/1e-13)
   packed.npz    the packed Z2 route (evaluate_quartic(..., packed_z2=True), the default of the
                 persistent trajectory) on Z2 states D = 4, 8 (W = 30, n_quad = 64), 16 and 32
                 (W = 30, n_quad = 512, 512 kinetic nodes: the optimizer defaults, with the
@@ -23,7 +27,7 @@ is the reference's test/fixtures/phi4_g2_D16_z2_portable (exported by RcmpsCore 
 States: NumPy PCG64 default_rng(seed); R and A with i.i.d. standard complex Gaussian entries
 times 0.2 (R drawn first), K = (A + A^dag)/2; Z2 states draw blocks in the order k1, k2, R12, R21.
 Run: python tests/golden/make_golden.py [name ...]  (all files by default, about a minute; the
-D = 64 record dominates; names: small d16 d64 samples ode packed)
+D = 64 record dominates; names: small d16 d64 samples ode packed phi)
 """
 from __future__ import annotations
 
@@ -110,6 +114,17 @@ def packed_samples():
                 accepted=stats["accepted_steps"], rejected=stats["rejected_steps"])
 
 
+def evaluate_phi(r, k, window, nq, atol=1e-13, rtol=1e-12):
+    q = -1j * k - r.conj().T @ r / 2
+    rho, _ = nm.stationary_state(q, r, tolerance=1e-13)
+    spec = ob._Spec(2, ((0, 1, True, 1.), (0, 1, False, 1.)))
+    out = ob._evaluate(r, q, rho, [spec], [1.], xp=np, half_window=window, n_quad=nq, atol=atol, rtol=rtol,
+                       initial_step=None, max_steps=1_000_000, use_graph=False, progress=None)
+    return dict(R=r, K=k, rho=rho, window=window, n_quad=nq, atol=atol, rtol=rtol,
+                phi_ode=float(out["value"]), phi=ob.phi_expectation(r, rho, window),
+                accepted=out["stats"]["accepted_steps"], rejected=out["stats"]["rejected_steps"])
+
+
 def evaluate_ode(r, k, g, window, nq):
     q = -1j * k - r.conj().T @ r / 2
     rho, _ = nm.stationary_state(q, r, tolerance=1e-13)
@@ -147,6 +162,10 @@ def main(names):
                          evaluate_ode(*random_state(16, 716), 2.0, 20.0, 192)])
     if "samples" in names:
         samples_d5()
+    if "phi" in names:
+        save("phi.npz", [evaluate_phi(*random_state(4, 904), 6.0, 24),
+                         evaluate_phi(*z2_state(8, 908), 20.0, 64),
+                         evaluate_phi(*random_state(16, 916), 40.0, 1024, 1e-14, 1e-13)])
     if "packed" in names:
         save("packed.npz", [evaluate_packed(*z2_state(4, 604), 1.5, 30.0, 64),
                             evaluate_packed(*z2_state(8, 508), 2.0, 30.0, 64),
@@ -170,4 +189,4 @@ def samples_d5():
 
 
 if __name__ == "__main__":
-    main(sys.argv[1:] or ["small", "d16", "d64", "ode", "samples", "packed"])
+    main(sys.argv[1:] or ["small", "d16", "d64", "ode", "samples", "packed", "phi"])

@@ -86,3 +86,17 @@ def test_packed_route_requires_exact_z2_structure():
     Q = O.left_canonical_q(R, rec["K"])
     assert O.z2_structure_ok(R, Q, rec["rho"])
     assert not O.z2_structure_ok(R[:7, :7], Q[:7, :7], rec["rho"][:7, :7])   # odd D
+
+
+@pytest.mark.parametrize("index", range(3))
+def test_phi_expectation_and_ode_match_reference(index):
+    """<phi> of the validation report (validate_sweep.py:23-32, 140-145; ode_backend.py:782-797):
+    the closed form and the ODE of the first monomial, against the reference's own routes."""
+    rec = load_records("phi.npz")[index]
+    phi = O.phi_expectation(rec["R"], rec["rho"], rec["window"])
+    assert abs(phi - rec["phi"]) <= 1e-13 * max(1.0, abs(rec["phi"]))
+    value, stats = O.phi_by_ode(rec["R"], rec["K"], rec["rho"], half_window=rec["window"], n_quad=int(rec["n_quad"]),
+                                atol=rec["atol"], rtol=rec["rtol"])
+    assert (stats["accepted"], stats["rejected"]) == (rec["accepted"], rec["rejected"])
+    assert abs(value - rec["phi_ode"]) <= 1e-12 * max(1.0, abs(rec["phi_ode"]))
+    assert abs(value - phi) <= 1e-9 * max(1.0, abs(phi))
