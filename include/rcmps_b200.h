@@ -191,6 +191,15 @@ int rcmps_stationary_state_batch(rcmps_context* context, int n_states, const int
                                  const double* K, double tolerance, double* rho, rcmps_state_stats* stats,
                                  void* stream);
 
+/* The same density started from a nearby one (a normalized Hermitian density of the previous
+ * state of an optimizer, device, packed): GMRES solves for the correction to an absolute
+ * residual of `tolerance`, and the result passes the same normalization, Hermiticity and
+ * stationarity checks. Replaces stationary_state_correction(q, r, rho_previous, tolerance)
+ * -> (rho, stats) (runtime/stationary_correction.py:19-96). */
+int rcmps_stationary_correction_batch(rcmps_context* context, int n_states, const int* dims, const double* R,
+                                      const double* K, const double* rho_previous, double tolerance,
+                                      double* rho, rcmps_state_stats* stats, void* stream);
+
 /* Number of kernel launches this library has issued in the process (all contexts). No
  * counterpart in the reference. */
 long long rcmps_launch_count(void);

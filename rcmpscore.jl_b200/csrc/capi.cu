@@ -523,6 +523,29 @@ int rcmps_stationary_state_batch(rcmps_context* ctx, int n, const int* dims, con
   return stationary_run(ctx, job, s);
 }
 
+int rcmps_stationary_correction_batch(rcmps_context* ctx, int n, const int* dims, const double* R,
+                                      const double* K, const double* rho_previous, double tolerance, double* rho,
+                                      rcmps_state_stats* stats, void* stream) {
+  if (!ctx) return RCMPS_INVALID_ARGUMENT;
+  int rc = check_dims(ctx, n, dims);
+  if (rc) return rc;
+  if (n == 0) return RCMPS_OK;
+  if (!R || !K || !rho_previous || !rho || !stats) return fail(ctx, RCMPS_INVALID_ARGUMENT, "NULL pointer");
+  cudaSetDevice(ctx->device);
+  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : ctx->slot[2].stream;
+  for (int i = 0; i < n; ++i) std::memset(&stats[i], 0, sizeof(rcmps_state_stats));
+  StationaryJob job;
+  job.n = n;
+  job.dims = dims;
+  job.R = R;
+  job.K = K;
+  job.tolerance = tolerance;
+  job.rho = rho;
+  job.rho_previous = rho_previous;
+  job.stats = stats;
+  return stationary_run(ctx, job, s);
+}
+
 // SMs the quartic pullback leaves free for the boundary solve that overlaps it
 constexpr int kBoundarySMs = 32;
 

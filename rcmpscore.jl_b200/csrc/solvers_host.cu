@@ -329,7 +329,11 @@ int stationary_run(rcmps_context* ctx, StationaryJob& job, cudaStream_t stream) 
     if (!e) e = cudaMemcpyAsync(P(o_b), hb, n * mat * 16, cudaMemcpyHostToDevice, stream);
     if (!e) e = cudaMemcpyAsync(P(o_trw), hb, n * mat * 16, cudaMemcpyHostToDevice, stream);
     if (!e) e = cudaMemsetAsync(P(o_status), 0, n * 4, stream);
-    if (!e) e = cudaMemsetAsync(P(gb.o_x), 0, (size_t)n * mat * 16, stream);
+    if (!e && job.rho_previous)   // warm start: x0 = rho_previous, GMRES corrects it
+      e = launch_pad(job.rho_previous, (long long*)P(o_off), (int*)P(o_dims), (double*)P(gb.o_x), dp, mat, n,
+                     stream);
+    else if (!e)
+      e = cudaMemsetAsync(P(gb.o_x), 0, (size_t)n * mat * 16, stream);
     if (!e) e = cudaMemsetAsync(d_in + 2 * n * mat, 0, n * mat * 16, stream);   // rho placeholder
     if (!e) e = launch_pad(job.R, (long long*)P(o_off), (int*)P(o_dims), dR, dp, mat, n, stream);
     if (!e) e = launch_pad(job.K, (long long*)P(o_off), (int*)P(o_dims), dK, dp, mat, n, stream);
@@ -345,6 +349,9 @@ int stationary_run(rcmps_context* ctx, StationaryJob& job, cudaStream_t stream) 
       A.A2h = ops + 3 * mat;
       A.trw = (double2*)P(o_trw) + (size_t)i * mat;   // + tr(X)/d I
       A.b = (double2*)P(o_b) + (size_t)i * mat;
+      // warm start: the target |b - A x| <= tolerance is absolute, as the reference's correction
+      // solve with rtol = atol = tolerance / max(1, |rhs|) (stationary_correction.py:60-66)
+      if (job.rho_previous) A.bnorm = 1.0;
     }
     e = gmres_run(hp, (ArnoldiProblem*)P(gb.o_probs), n, dp, m, maxrestart, (LindbladTask*)P(gb.o_tasks), stream);
     if (e) return fail(ctx, RCMPS_CUDA_ERROR, std::string("stationary GMRES: ") + cudaGetErrorString(e));

@@ -24,6 +24,10 @@ struct StationaryJob {
   const double *R = nullptr, *K = nullptr;    // device, packed
   double tolerance = 1e-11;
   double* rho = nullptr;                      // device, packed
+  // device, packed, optional: a nearby density to start from (the warm correction of
+  // stationary_correction.py:19-96); the GMRES then solves for the correction to an absolute
+  // residual of `tolerance`
+  const double* rho_previous = nullptr;
   rcmps_state_stats* stats = nullptr;
   int slot = 2;
 };

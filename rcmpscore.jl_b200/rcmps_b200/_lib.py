@@ -80,6 +80,8 @@ SIGNATURES = {
     "rcmps_finish_gradient_noalloc": (_I, [_P, _I, _P, _P, _P, _P, _P, C.POINTER(Settings), _P,
                                            C.POINTER(StateStats), _P]),
     "rcmps_stationary_state_batch": (_I, [_P, _I, C.POINTER(_I), _P, _P, _D, _P, C.POINTER(StateStats), _P]),
+    "rcmps_stationary_correction_batch": (_I, [_P, _I, C.POINTER(_I), _P, _P, _P, _D, _P, C.POINTER(StateStats),
+                                               _P]),
     "rcmps_fp64_peak_tflops": (_D, [_P]),
     "rcmps_launch_count": (C.c_longlong, []),
 }

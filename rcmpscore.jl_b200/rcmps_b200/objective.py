@@ -33,7 +33,7 @@ __all__ = ["SolverFailure", "KineticFailure", "DeviceControlFailure", "OverlapFa
            "settings_from_args", "fg_phi4_batch", "objective", "OverlapObjective",
            "evaluate_quartic_persistent_trajectory", "evaluate_phi4", "evaluate_phi4_batch", "kinetic_raw",
            "finish_gradient",
-           "stationary_state",
+           "stationary_state", "stationary_state_correction",
            "metric", "context"]
 
 
@@ -431,6 +431,43 @@ def stationary_state(q, r, *, tolerance=1e-11):
     if rc:
         raise SolverFailure(f"Invalid stationary density: {_lib.STATUS_NAMES.get(rc, rc)} ({ctx.error()})")
     return _unpack(rho, [d])[0], {"matvecs": stats[0].gmres_iterations, "stationary_residual": stats[0].boundary_residual}
+
+
+def stationary_state_correction(q, r, rho_previous, *, tolerance=1e-11, maxiter=200):
+    """Stationary density of (Q, R) started from a nearby density rho_previous, the previous
+    accepted state of an optimizer: GMRES on the GPU solves for the correction to an absolute
+    residual of `tolerance`, then the same checks as stationary_state apply
+    (stationary_correction.py:19-96). rho_previous must be finite, normalized, Hermitian and
+    positive (ValueError otherwise). The GPU solve restarts every 64 iterations, at most 200
+    times; maxiter is accepted for the reference's signature. Returns (rho, stats)."""
+    import torch
+    q, r, prev = (np.asarray(x) for x in (q, r, rho_previous))
+    if q.ndim != 2 or q.shape[0] != q.shape[1] or q.shape != r.shape or q.shape != prev.shape:
+        raise ValueError("q, r and rho_previous must be equally sized square matrices")
+    if any(x.dtype != np.complex128 for x in (q, r, prev)):
+        raise ValueError("stationary correction requires complex128 inputs")
+    if any(not np.isfinite(x).all() for x in (q, r, prev)):
+        raise ValueError("stationary correction inputs must be finite")
+    if not np.isfinite(tolerance) or tolerance <= 0 or maxiter < 1:
+        raise ValueError("tolerance and maxiter must be positive")
+    if abs(np.trace(prev) - 1) > 100 * tolerance or np.linalg.norm(prev - prev.conj().T) > 100 * tolerance:
+        raise ValueError("rho_previous must be normalized and Hermitian")
+    if np.linalg.eigvalsh(prev).min() < -10 * tolerance:
+        raise ValueError("rho_previous must be positive within the existing tolerance")
+    d = len(q)
+    ctx = context()
+    K = _k_from_q(q, r)
+    dR, dK, dP = _device([r]), _device([K]), _device([prev])
+    rho = torch.zeros(d * d, dtype=torch.complex128, device="cuda")
+    stats = (_lib.StateStats * 1)()
+    rc = ctx.lib.rcmps_stationary_correction_batch(ctx.handle, 1, (C.c_int * 1)(d), dR.data_ptr(), dK.data_ptr(),
+                                                   dP.data_ptr(), C.c_double(float(tolerance)), rho.data_ptr(),
+                                                   stats, _stream())
+    if rc:
+        raise SolverFailure(f"Invalid stationary density: {_lib.STATUS_NAMES.get(rc, rc)} ({ctx.error()})")
+    return _unpack(rho, [d])[0], {"matvecs": stats[0].gmres_iterations,
+                                  "stationary_residual": stats[0].boundary_residual,
+                                  "warm_start": True, "fallback_used": False}
 
 
 def metric(rho, x, y, metric_reg=1e-3):

@@ -10,6 +10,10 @@ This script imports the reference package rcmps_gpu read-only from a local check
                 monomial (validate_sweep.phi_by_ode, host NumPy integrator): D = 4 random (W = 6,
                 n_quad = 24), D = 8 Z2 (W = 20, n_quad = 64) and D = 16 random at the refined
                 validation settings (W = 40, n_quad = 1024, 1e-14/1e-13)
+  optim.npz     eight L-BFGS iterations of the reference's controller (runtime/optimizer.py) from a
+                D = 4 random state, objective = quartic (W = 6, n_quad = 24) + kinetic (32 nodes)
+                + finished gradient, stationary densities by numerics.stationary_state: per
+                accepted iteration the energy, step alpha, trials and gradient norm
   packed.npz    the packed Z2 route (evaluate_quartic(..., packed_z2=True), the default of the
                 persistent trajectory) on Z2 states D = 4, 8 (W = 30, n_quad = 64), 16 and 32
                 (W = 30, n_quad = 512, 512 kinetic nodes: the optimizer defaults, with the
@@ -27,7 +31,7 @@ is the reference's test/fixtures/phi4_g2_D16_z2_portable (exported by RcmpsCore 
 States: NumPy PCG64 default_rng(seed); R and A with i.i.d. standard complex Gaussian entries
 times 0.2 (R drawn first), K = (A + A^dag)/2; Z2 states draw blocks in the order k1, k2, R12, R21.
 Run: python tests/golden/make_golden.py [name ...]  (all files by default, about a minute; the
-D = 64 record dominates; names: small d16 d64 samples ode packed phi)
+D = 64 record dominates; names: small d16 d64 samples ode packed phi optim)
 """
 from __future__ import annotations
 
@@ -125,6 +129,36 @@ def evaluate_phi(r, k, window, nq, atol=1e-13, rtol=1e-12):
                 accepted=out["stats"]["accepted_steps"], rejected=out["stats"]["rejected_steps"])
 
 
+OPTIM = dict(seed=414, d=4, g=1.0, window=6.0, n_quad=24, nodes=32, iterations=8)
+
+
+def optim_run():
+    from rcmps_gpu.optimizer.runtime import optimizer as opt
+    c = OPTIM
+    r, k = random_state(c["d"], c["seed"])
+
+    def objective(rr, kk, rho):
+        q = -1j * kk - rr.conj().T @ rr / 2
+        quartic = ob.evaluate_quartic(rr, q, rho, c["g"], xp=np, half_window=c["window"], n_quad=c["n_quad"],
+                                      atol=1e-13, rtol=1e-12, reduced=True)
+        kinetic = kb.kinetic_raw(q, rr, rho, c["nodes"], xp=np, tolerance=1e-12, maxdim=1024)
+        grad, _ = nm.finish_gradient(q, rr, rho, quartic["covector"] + kinetic["covector"],
+                                     quartic["environment"] + kinetic["environment"], metric_reg=1e-3)
+        return quartic["value"] + kinetic["value"], grad, {}
+
+    q0 = -1j * k - r.conj().T @ r / 2
+    rho0, _ = nm.stationary_state(q0, r, tolerance=1e-13)
+    e0, g0, _ = objective(r, k, rho0)
+    accepted = [ev for ev in opt.optimize(r, k, rho0, e0, g0, objective,
+                                          dict(max_iterations=c["iterations"], gradient_tol=1e-9))
+                if ev["type"] == "accepted"]
+    last = accepted[-1]["state"]
+    return dict(R=r, K=k, rho=rho0, energy0=e0, gradient0=g0, **{key: value for key, value in c.items()},
+                energies=[ev["energy"] for ev in accepted], alphas=[ev["alpha"] for ev in accepted],
+                trials=[ev["trials"] for ev in accepted], gradient_norms=[ev["gradient_norm"] for ev in accepted],
+                R_final=last["R"], K_final=last["K"])
+
+
 def evaluate_ode(r, k, g, window, nq):
     q = -1j * k - r.conj().T @ r / 2
     rho, _ = nm.stationary_state(q, r, tolerance=1e-13)
@@ -166,6 +200,8 @@ def main(names):
         save("phi.npz", [evaluate_phi(*random_state(4, 904), 6.0, 24),
                          evaluate_phi(*z2_state(8, 908), 20.0, 64),
                          evaluate_phi(*random_state(16, 916), 40.0, 1024, 1e-14, 1e-13)])
+    if "optim" in names:
+        save("optim.npz", [optim_run()])
     if "packed" in names:
         save("packed.npz", [evaluate_packed(*z2_state(4, 604), 1.5, 30.0, 64),
                             evaluate_packed(*z2_state(8, 508), 2.0, 30.0, 64),
@@ -189,4 +225,4 @@ def samples_d5():
 
 
 if __name__ == "__main__":
-    main(sys.argv[1:] or ["small", "d16", "d64", "ode", "samples", "packed", "phi"])
+    main(sys.argv[1:] or ["small", "d16", "d64", "ode", "samples", "packed", "phi", "optim"])

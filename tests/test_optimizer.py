@@ -1,0 +1,96 @@
+"""The L-BFGS controller (rcmps_b200.optimizer) against eight iterations of the reference's own
+controller (runtime/optimizer.py; tests/golden/optim.npz): on the CPU with the oracle's
+objective and stationary densities, on the GPU with the library's."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import load_records
+from oracle import fg_phi4_oracle as O
+
+
+def _accepted(events):
+    return [ev for ev in events if ev["type"] == "accepted"]
+
+
+def _check(rec, accepted, tol):
+    assert len(accepted) == int(rec["iterations"])
+    assert [ev["trials"] for ev in accepted] == list(rec["trials"])
+    np.testing.assert_allclose([ev["alpha"] for ev in accepted], rec["alphas"], rtol=1e-8)
+    np.testing.assert_allclose([ev["energy"] for ev in accepted], rec["energies"], rtol=tol, atol=tol)
+    np.testing.assert_allclose(accepted[-1]["state"]["R"], rec["R_final"], atol=1e-8)
+
+
+def test_retraction_and_preconditioner():
+    from rcmps_b200 import optimizer
+    rng = np.random.default_rng(5)
+    R, K = O.phi4_state(6, 5)
+    X = rng.standard_normal((6, 6)) + 1j * rng.standard_normal((6, 6))
+    rr, kk = optimizer.retract(R, K, X, 1e-4)
+    assert np.abs(kk - kk.conj().T).max() == 0.0
+    q0, q1 = O.left_canonical_q(R, K), O.left_canonical_q(rr, kk)
+    # the left-canonical gauge Q + Q^dag + R^dag R = 0 holds by construction of Q
+    assert np.abs(q1 + q1.conj().T + rr.conj().T @ rr).max() < 1e-14
+    assert np.abs(q1 - q0).max() < 1e-2
+    rho = O.stationary_state(q0, R)
+    G = rng.standard_normal((6, 6)) + 1j * rng.standard_normal((6, 6))
+    P = optimizer.precondition(rho, G, 1e-3, 1e-4)
+    assert np.allclose(P @ (rho + 1e-4 * np.eye(6)), G @ (rho + 1e-3 * np.eye(6)), atol=1e-12)
+    with pytest.raises(ValueError):
+        optimizer._controls(dict(shrink=1.5))
+    assert optimizer._controls(dict(gradtol=1e-7, lbfgs_history=5)).gradient_tol == 1e-7
+
+
+def test_controller_matches_reference_with_oracle_components(monkeypatch):
+    from rcmps_b200 import optimizer
+    rec = load_records("optim.npz")[0]
+    monkeypatch.setattr(optimizer, "stationary_state",
+                        lambda q, r, tolerance: (O.stationary_state(q, r, tolerance=tolerance), {}))
+
+    def objective(r, k, rho):
+        e, g, _ = O.fg_phi4(r, k, rho, rec["g"], half_window=rec["window"], n_quad=int(rec["n_quad"]),
+                            nodes=int(rec["nodes"]))
+        return e, g, {}
+    events = list(optimizer.optimize(rec["R"], rec["K"], rec["rho"], rec["energy0"], rec["gradient0"], objective,
+                                     dict(max_iterations=int(rec["iterations"]), gradient_tol=1e-9)))
+    _check(rec, _accepted(events), 1e-10)
+    assert events[-1]["type"] == "stopped" and events[-1]["reason"] == "requested iteration limit reached"
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("warm", [False, True])
+def test_controller_matches_reference_on_the_gpu(gpu_context, warm):
+    """The library evaluates every trial (stationary density, energy, gradient); warm: the
+    density is corrected from the last accepted one."""
+    from rcmps_b200 import objective, optimizer
+    rec = load_records("optim.npz")[0]
+    args = objective.default_args(window=rec["window"], quadrature=int(rec["n_quad"]), nodes=int(rec["nodes"]))
+    call = lambda r, k, rho: objective.objective(r, k, rho, rec["g"], args)
+    events = list(optimizer.optimize(rec["R"], rec["K"], rec["rho"], rec["energy0"], rec["gradient0"], call,
+                                     dict(max_iterations=int(rec["iterations"]), gradient_tol=1e-9),
+                                     warm_stationary=warm))
+    _check(rec, _accepted(events), 1e-9)
+    if warm:
+        assert all(ev["stationary"]["warm_start"] for ev in events if ev["type"] == "accepted")
+
+
+@pytest.mark.gpu
+def test_warm_stationary_correction_matches_cold_solve(gpu_context):
+    """stationary_state_correction from a nearby density (the previous accepted state of an
+    optimizer) against the cold solve of the new state, and the reference's input checks."""
+    from rcmps_b200 import objective, optimizer
+    R, K = O.phi4_state(16, 17)
+    Q = O.left_canonical_q(R, K)
+    rho_prev, _ = objective.stationary_state(Q, R, tolerance=1e-13)
+    rng = np.random.default_rng(3)
+    X = 1e-3 * (rng.standard_normal((16, 16)) + 1j * rng.standard_normal((16, 16)))
+    rr, kk = optimizer.retract(R, K, X, 1.0)
+    qq = O.left_canonical_q(rr, kk)
+    cold, _ = objective.stationary_state(qq, rr, tolerance=1e-13)
+    warm, st = objective.stationary_state_correction(qq, rr, rho_prev, tolerance=1e-13)
+    assert np.abs(warm - cold).max() < 1e-11
+    assert st["warm_start"] and np.abs(warm - warm.conj().T).max() == 0.0
+    assert np.linalg.norm(O.lindblad(qq, rr, warm)) < 1e-11
+    with pytest.raises(ValueError):
+        objective.stationary_state_correction(qq, rr, 2.0 * rho_prev, tolerance=1e-13)
