@@ -30,3 +30,7 @@ emit("rcmps_dop_c", dop.C)
 emit("rcmps_dop_e5", e5)
 emit("rcmps_dop_e3", e3)
 emit("rcmps_dop_d", dd)
+# Stages the order-7 interpolation reads: k0 and k12 and every column of the dense matrix D with
+# a nonzero entry.
+dense = (1 << 0) | (1 << 12) | sum(1 << j for j in range(16) if np.any(dd[:, j] != 0.0))
+print(f"constexpr unsigned rcmps_dop_dense_mask = 0x{dense:04x}u;")

@@ -545,6 +545,14 @@ __device__ __forceinline__ size_t own_offset(int e, int row0) {
   return (size_t)c * DP * DP + (size_t)(row0 + rem / DP) * DP + (rem % DP);
 }
 
+// Structurally zero element e of a packed Z2 state's own rows (row0: the CTA's first row; half:
+// d/2): channel parity p (1 for c even), nonzero iff the row and column halves differ by p.
+template <int DP>
+__device__ __forceinline__ bool z2_zero_element(int e, int row0, int half) {
+  const int c = e / (16 * DP), row = row0 + (e % (16 * DP)) / DP, col = e % DP;
+  return (((row >= half) != (col >= half)) ? 1 : 0) != ((c % 2 == 0) ? 1 : 0);
+}
+
 template <int DP, int SYS>
 __global__ void __launch_bounds__(Geo<DP, SYS>::NT, 1)
 trajectory_kernel(const TrajState* __restrict__ states, const double* __restrict__ points, int npoints,
@@ -607,12 +615,6 @@ trajectory_kernel(const TrajState* __restrict__ states, const double* __restrict
   rhs.zs = zskip ? 1 : 0;
   rhs.hz = half;
   rhs.hh = zskip && row0 >= half ? 1 : 0;
-  // structurally zero element e of this CTA's rows (channel parity p: nonzero iff the row and
-  // column halves differ by p)
-  auto zero_elem = [&](int e) {
-    const int c = e / (16 * DP), row = row0 + (e % (16 * DP)) / DP, col = e % DP;
-    return (((row >= half) != (col >= half)) ? 1 : 0) != ((c % 2 == 0) ? 1 : 0);
-  };
   if (zskip) {
     // every work vector's own rows start at zero: the skipped parts are never written again
     for (int e = tid; e < GE::OWN; e += GE::NT) {
@@ -687,8 +689,8 @@ trajectory_kernel(const TrajState* __restrict__ states, const double* __restrict
     // ---------------------------------------------------------------- stages 1..12
     for (int s = 1; s <= 12; ++s) {
       const double* w = s == 12 ? c_dop_b : c_dop_a + 16 * s;
-      const int terms = s;   // a[s][0..s-1], b[0..11]
       double2* z = zb(zcount);
+      const int terms = s;   // a[s][0..s-1], b[0..11]
       double part = 0.0, dummy = 0.0;
       const double2* kp[12];
       double ha[12];
@@ -698,7 +700,7 @@ trajectory_kernel(const TrajState* __restrict__ states, const double* __restrict
         ha[j] = j < terms ? h * w[j] : 0.0;
       }
       for (int e = tid; e < GE::OWN; e += GE::NT) {
-        if (zskip && zero_elem(e)) continue;
+        if (zskip && z2_zero_element<DP>(e, row0, half)) continue;
         const size_t off = own_offset<DP>(e, row0);
         double2 kv[12];
 #pragma unroll
@@ -821,13 +823,22 @@ trajectory_kernel(const TrajState* __restrict__ states, const double* __restrict
         // dense stages 13..15
         for (int s = 13; s < 16; ++s) {
           double2* z = zb(zcount);
+          const double2* kp[15];
+          double ha[15];
+#pragma unroll
+          for (int j = 0; j < 15; ++j) {
+            kp[j] = kb(j);
+            ha[j] = j < s ? h * c_dop_a[16 * s + j] : 0.0;
+          }
           for (int e = tid; e < GE::OWN; e += GE::NT) {
             const size_t off = own_offset<DP>(e, row0);
+            double2 kv[15];
+#pragma unroll
+            for (int j = 0; j < 15; ++j) kv[j] = ha[j] != 0.0 ? __ldcg(kp[j] + off) : make_double2(0.0, 0.0);
             double2 v = ybuf[off];
-            for (int j = 0; j < s; ++j) {
-              const double a = c_dop_a[16 * s + j];
-              if (a != 0.0) v = zaxpy(h * a, kb(j)[off], v);
-            }
+#pragma unroll
+            for (int j = 0; j < 15; ++j)
+              if (ha[j] != 0.0) v = zaxpy(ha[j], kv[j], v);
             z[off] = v;
           }
           fence_proxy_async_global();
