@@ -34,6 +34,29 @@ struct RowGemmRing {
     int n;
   };
 
+  // Structural zeros of a product of two Z2 block-structured matrices (a packed Z2 state): with
+  // `half` = D/2 rows per parity half, the A block starting at row `row0` and parities pa (of A)
+  // and pout (of the product), output block (h, c) is zero unless c = h ^ pout, and a live
+  // block takes only the K rows of half h ^ pa. on = 0: a dense product.
+  struct ZSkip {
+    int on = 0, half = 0, row0 = 0, pa = 0, pout = 0;
+  };
+
+  // Whether this warp's tiles (one 16-row band, TPW tiles in one column half) are structurally
+  // zero; kh: the K half a live band takes (-1: every K row).
+  template <int MB>
+  __device__ static bool band_zero(const ZSkip& z, int& kh) {
+    constexpr int TN = Tiling<DP, MB, NW>::TN, TPW = Tiling<DP, MB, NW>::TPW;
+    kh = -1;
+    if (!z.on || (z.half % 16) != 0 || ((z.half / 8) % TPW) != 0) return false;
+    const int warp = threadIdx.x >> 5;
+    const int tile0 = warp * TPW;
+    const int h = (z.row0 + (tile0 / TN) * 16) >= z.half ? 1 : 0;
+    const int c = ((tile0 % TN) * 8) >= z.half ? 1 : 0;
+    kh = h ^ z.pa;
+    return c != (h ^ z.pout);
+  }
+
   __device__ static const double2* chunk_ptr(const Segs& s, int q) {
     int r = q * KC;
     for (int i = 0; i < s.n; ++i) {
@@ -60,9 +83,10 @@ struct RowGemmRing {
     for (int r = 0; r < KC; ++r) bulk_g2s(ring + slot * SLOT + r * LDB, src + r * DP, DP * 16, &full[slot]);
   }
 
-  // acc[TPW] += A * B. Call with all threads; ends with a __syncthreads.
+  // acc[TPW] += A * B. Call with all threads; ends with a __syncthreads. z: the product's
+  // structural zeros (packed Z2 states; a single K segment of DP rows), skipped.
   template <int MB>
-  __device__ void run(ZFrag* acc, const double2* A, int lda, const Segs& s) {
+  __device__ void run(ZFrag* acc, const double2* A, int lda, const Segs& s, const ZSkip& z = ZSkip()) {
     constexpr int TN = Tiling<DP, MB, NW>::TN, TPW = Tiling<DP, MB, NW>::TPW;
     int krows = 0;
     for (int i = 0; i < s.n; ++i) krows += s.rows[i];
@@ -70,6 +94,9 @@ struct RowGemmRing {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int tile0 = warp * TPW;
     const int mt = tile0 / TN;
+    int kh = -1;
+    const bool zt = (s.n == 1 && krows == DP) && band_zero<MB>(z, kh);
+    if (!(s.n == 1 && krows == DP)) kh = -1;
     if (threadIdx.x == 0) {
       fence_proxy_async_global();
       for (int q = 0; q < NST && q < nch; ++q) issue(s, q);
@@ -79,14 +106,19 @@ struct RowGemmRing {
       const int slot = (int)(g % NST);
       mbar_wait(&full[slot], (uint32_t)((g / NST) & 1), wait_flag);
       const double2* B = ring + slot * SLOT;
+      // every warp waits for every chunk (the slot is refilled after the barrier below); a
+      // chunk lies in one K half since the half is a multiple of KC
+      const bool live = !zt && (kh < 0 || ((q * KC >= z.half) ? 1 : 0) == kh);
+      if (live) {
 #pragma unroll
-      for (int ks = 0; ks < KC / 8; ++ks) {
-        AFrag a;
-        load_a(A, lda, mt * 16, q * KC + ks * 8, lane, a);
-        BFrag b[TPW];
+        for (int ks = 0; ks < KC / 8; ++ks) {
+          AFrag a;
+          load_a(A, lda, mt * 16, q * KC + ks * 8, lane, a);
+          BFrag b[TPW];
 #pragma unroll
-        for (int j = 0; j < TPW; ++j) load_b(B, LDB, ks * 8, ((tile0 + j) % TN) * 8, lane, b[j]);
-        zmma_tiles<TPW>(acc, a, b);
+          for (int j = 0; j < TPW; ++j) load_b(B, LDB, ks * 8, ((tile0 + j) % TN) * 8, lane, b[j]);
+          zmma_tiles<TPW>(acc, a, b);
+        }
       }
       __syncthreads();
       if (threadIdx.x == 0 && q + NST < nch) issue(s, q + NST);
@@ -119,8 +151,13 @@ template <int DP, int MB, int NW, int KC, int NST>
 struct RowGemm : RowGemmRing<DP, NW, KC, NST> {
   using Base = RowGemmRing<DP, NW, KC, NST>;
   static constexpr int TPW = Tiling<DP, MB, NW>::TPW;
-  __device__ void run(ZFrag* acc, const double2* A, int lda, const typename Base::Segs& s) {
-    Base::template run<MB>(acc, A, lda, s);
+  __device__ void run(ZFrag* acc, const double2* A, int lda, const typename Base::Segs& s,
+                      const typename Base::ZSkip& z = typename Base::ZSkip()) {
+    Base::template run<MB>(acc, A, lda, s, z);
+  }
+  __device__ static bool band_zero(const typename Base::ZSkip& z) {
+    int kh;
+    return Base::template band_zero<MB>(z, kh);
   }
   __device__ static void coord(int j, int i, int& row, int& col) { Base::template coord<MB>(j, i, row, col); }
 };

@@ -71,6 +71,18 @@ pullback_kernel(PullbackArgs a) {
     const double2* ops = a.ops + (size_t)state * a.ops_stride;
     const double2* R = ops + 2 * MAT;
     const double2* Rh = ops + 3 * MAT;
+    // packed Z2 state: f_k and b_k (k = 1..3) have parity 1 for odd k, 0 for k = 2; R is odd
+    const bool zs = a.packed && DP % 32 == 0 && a.dims[state] == DP &&
+                    *reinterpret_cast<const int*>(a.packed + (size_t)state * a.packed_stride + a.packed_offset) != 0;
+    auto zsk = [&](int row0, int pa, int pout) {
+      typename GM::ZSkip z;
+      z.on = zs ? 1 : 0;
+      z.half = DP / 2;
+      z.row0 = row0;
+      z.pa = pa;
+      z.pout = pout;
+      return z;
+    };
 
     auto fwd = [&](int i, int k) { return samples + (size_t)i * VEC + (size_t)(k - 1) * MAT; };       // f_k, k=1..3
     auto adj = [&](int i, int k) { return samples + (size_t)(n - 1 - i) * VEC + (size_t)(3 + k) * MAT; };  // b_k, k=0..3
@@ -106,31 +118,37 @@ pullback_kernel(PullbackArgs a) {
   #pragma unroll
               for (int j = 0; j < GM::TPW; ++j) tmp[j].zero();
               sb.ptr[0] = adj(i, k);
-              gm.run(tmp, bufX, PG::LDA, sb);
+              const int pk = k & 1;
+              const auto z0 = zsk(rbw * PG::MB, 1, 1 ^ pk);   // R^dag b_k
+              gm.run(tmp, bufX, PG::LDA, sb, z0);
+              // a structurally zero block of W_k is never read by the live tiles of the next
+              // product, so it is not written
+              if (!GM::band_zero(z0)) {
   #pragma unroll
-              for (int j = 0; j < GM::TPW; ++j)
+                for (int j = 0; j < GM::TPW; ++j)
   #pragma unroll
-                for (int e = 0; e < 4; ++e) {
-                  int row, col;
-                  GM::coord(j, e, row, col);
-                  row += rbw * PG::MB;
-                  double2 v = zscale(w, tmp[j].value(e));
-                  if (k < 3) v = zaxpy(c, adj(i, k + 1)[row * DP + col], v);
-                  else if (row == col) v.x += c;
-                  wscr[(k - 1) * MAT + row * DP + col] = v;
-                }
+                  for (int e = 0; e < 4; ++e) {
+                    int row, col;
+                    GM::coord(j, e, row, col);
+                    row += rbw * PG::MB;
+                    double2 v = zscale(w, tmp[j].value(e));
+                    if (k < 3) v = zaxpy(c, adj(i, k + 1)[row * DP + col], v);
+                    else if (row == col) v.x += c;
+                    wscr[(k - 1) * MAT + row * DP + col] = v;
+                  }
+              }
             }
             fence_proxy_async_global();   // W_k is read next by bulk copies
             __syncthreads();
             load_rows(bufY, fwd(i, k), rb * PG::MB, 1.0);
             __syncthreads();
             sb.ptr[0] = wscr + (k - 1) * MAT;
-            gm.run(acc, bufY, PG::LDA, sb);
+            gm.run(acc, bufY, PG::LDA, sb, zsk(rb * PG::MB, k & 1, 1));   // f_k W_k
           } else if (pass == 1) {
             load_rows(bufY, fwd(i, k), rb * PG::MB, w);   // P += w f_k b_k
             __syncthreads();
             sb.ptr[0] = adj(i, k);
-            gm.run(acc, bufY, PG::LDA, sb);
+            gm.run(acc, bufY, PG::LDA, sb, zsk(rb * PG::MB, k & 1, 0));
           } else if (pass == 2) {
             // W'_k rows = w b_k R + c b_{k+1} -> bufY; then nn += W'_k f_k
             load_rows(bufX, adj(i, k), rb * PG::MB, 1.0);
@@ -138,27 +156,30 @@ pullback_kernel(PullbackArgs a) {
   #pragma unroll
             for (int j = 0; j < GM::TPW; ++j) tmp[j].zero();
             sb.ptr[0] = R;
-            gm.run(tmp, bufX, PG::LDA, sb);
+            const auto z2 = zsk(rb * PG::MB, k & 1, 1 ^ (k & 1));   // b_k R
+            gm.run(tmp, bufX, PG::LDA, sb, z2);
+            if (!GM::band_zero(z2)) {   // zero blocks of W'_k are never read (as for W_k)
   #pragma unroll
-            for (int j = 0; j < GM::TPW; ++j)
+              for (int j = 0; j < GM::TPW; ++j)
   #pragma unroll
-              for (int e = 0; e < 4; ++e) {
-                int row, col;
-                GM::coord(j, e, row, col);
-                const int grow = row + rb * PG::MB;
-                double2 v = zscale(w, tmp[j].value(e));
-                if (k < 3) v = zaxpy(c, adj(i, k + 1)[grow * DP + col], v);
-                else if (grow == col) v.x += c;
-                bufY[row * PG::LDA + col] = v;
-              }
+                for (int e = 0; e < 4; ++e) {
+                  int row, col;
+                  GM::coord(j, e, row, col);
+                  const int grow = row + rb * PG::MB;
+                  double2 v = zscale(w, tmp[j].value(e));
+                  if (k < 3) v = zaxpy(c, adj(i, k + 1)[grow * DP + col], v);
+                  else if (grow == col) v.x += c;
+                  bufY[row * PG::LDA + col] = v;
+                }
+            }
             __syncthreads();
             sb.ptr[0] = fwd(i, k);
-            gm.run(acc, bufY, PG::LDA, sb);
+            gm.run(acc, bufY, PG::LDA, sb, zsk(rb * PG::MB, 1 ^ (k & 1), 1));   // W'_k f_k
           } else {
             load_rows(bufX, adj(i, k), rb * PG::MB, w);   // P' += w b_k f_k
             __syncthreads();
             sb.ptr[0] = fwd(i, k);
-            gm.run(acc, bufX, PG::LDA, sb);
+            gm.run(acc, bufX, PG::LDA, sb, zsk(rb * PG::MB, k & 1, 0));
           }
         }
       }

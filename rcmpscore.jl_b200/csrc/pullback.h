@@ -22,6 +22,12 @@ struct PullbackArgs {
   double2* env_out;            // [state][dp^2] (padded)
   double* value_out;           // [state]
   int* error_flag;             // [state]
+  // packed Z2 states (may be NULL): the trajectory's per-state route flag (int at byte offset
+  // packed_offset of each packed_stride-byte record) and the physical dimensions; a packed state
+  // with d = dp and d/2 a multiple of 16 skips the structural zeros of its products
+  const char* packed = nullptr;
+  int packed_stride = 0, packed_offset = 0;
+  const int* dims = nullptr;
 };
 
 cudaError_t pullback_launch(const PullbackArgs& a, int nblk, cudaStream_t s);

@@ -332,6 +332,10 @@ int quartic_run(rcmps_context* ctx, QuarticJob& job, cudaStream_t stream) {
         pa.env_out = (double2*)P(o_env);
         pa.value_out = (double*)P(o_vout);
         pa.error_flag = (int*)P(o_flag);
+        pa.packed = reinterpret_cast<const char*>(P(o_tstats));   // the route the trajectory took
+        pa.packed_stride = (int)sizeof(TrajStats);
+        pa.packed_offset = (int)offsetof(TrajStats, packed);
+        pa.dims = (int*)P(o_dims);
         if (early_env) {
           if (e == cudaSuccess) e = quartic_env_launch(pa, stream);
           if (e == cudaSuccess)
