@@ -8,9 +8,11 @@
 //   nn = sum_i sum_k (w b_k R + c_k b_{k+1}) f_k - R (sum_i sum_k w b_k f_k)
 // The k = 0 terms are linear in the adjoint samples (f_0 = rho is constant) and are formed
 // once from B0 = sum w b_0 and B1 = sum j b_1 in the finalize kernel, as are the deferred
-// products with R^dag and R. Per node and k >= 1 this leaves six D^3 products, run as four
-// accumulation passes on FP64 tensor cores (RowGemm), each CTA owning one block of output rows
-// and a range of nodes; partial sums are reduced in a fixed order.
+// products with R^dag and R. The samples are Hermitian and the weights real, so in exact
+// arithmetic nn = m^dag: the reference's covector (m + nn^dag)/2 equals m, and only m is formed
+// (the two differ by rounding, about 1e-15 relative). Per node and k >= 1 this leaves three D^3
+// products, run as two accumulation passes on FP64 tensor cores (RowGemm), each CTA owning one
+// block of output rows and a range of nodes; partial sums are reduced in a fixed order.
 #include <cuda_runtime.h>
 #include <algorithm>
 #include "common.cuh"
@@ -69,7 +71,6 @@ pullback_kernel(PullbackArgs a) {
     const int i0 = blk * a.nodes_per_block, i1 = min(n, i0 + a.nodes_per_block);
     const double2* samples = a.samples + (size_t)state * a.samples_stride;
     const double2* ops = a.ops + (size_t)state * a.ops_stride;
-    const double2* R = ops + 2 * MAT;
     const double2* Rh = ops + 3 * MAT;
     // packed Z2 state: f_k and b_k (k = 1..3) have parity 1 for odd k, 0 for k = 2; R is odd
     const bool zs = a.packed && DP % 32 == 0 && a.dims[state] == DP &&
@@ -94,7 +95,7 @@ pullback_kernel(PullbackArgs a) {
     };
 
     ZFrag acc[GM::TPW], tmp[GM::TPW];
-    for (int pass = 0; pass < 4; ++pass) {
+    for (int pass = 0; pass < 2; ++pass) {   // m, P (nn = m^dag and P' = P^dag are not formed)
   #pragma unroll
       for (int j = 0; j < GM::TPW; ++j) acc[j].zero();
       if (pass == 0 && PG::NRB == 1) {
@@ -144,46 +145,15 @@ pullback_kernel(PullbackArgs a) {
             __syncthreads();
             sb.ptr[0] = wscr + (k - 1) * MAT;
             gm.run(acc, bufY, PG::LDA, sb, zsk(rb * PG::MB, k & 1, 1));   // f_k W_k
-          } else if (pass == 1) {
+          } else {   // pass 1
             load_rows(bufY, fwd(i, k), rb * PG::MB, w);   // P += w f_k b_k
             __syncthreads();
             sb.ptr[0] = adj(i, k);
             gm.run(acc, bufY, PG::LDA, sb, zsk(rb * PG::MB, k & 1, 0));
-          } else if (pass == 2) {
-            // W'_k rows = w b_k R + c b_{k+1} -> bufY; then nn += W'_k f_k
-            load_rows(bufX, adj(i, k), rb * PG::MB, 1.0);
-            __syncthreads();
-  #pragma unroll
-            for (int j = 0; j < GM::TPW; ++j) tmp[j].zero();
-            sb.ptr[0] = R;
-            const auto z2 = zsk(rb * PG::MB, k & 1, 1 ^ (k & 1));   // b_k R
-            gm.run(tmp, bufX, PG::LDA, sb, z2);
-            if (!GM::band_zero(z2)) {   // zero blocks of W'_k are never read (as for W_k)
-  #pragma unroll
-              for (int j = 0; j < GM::TPW; ++j)
-  #pragma unroll
-                for (int e = 0; e < 4; ++e) {
-                  int row, col;
-                  GM::coord(j, e, row, col);
-                  const int grow = row + rb * PG::MB;
-                  double2 v = zscale(w, tmp[j].value(e));
-                  if (k < 3) v = zaxpy(c, adj(i, k + 1)[grow * DP + col], v);
-                  else if (grow == col) v.x += c;
-                  bufY[row * PG::LDA + col] = v;
-                }
-            }
-            __syncthreads();
-            sb.ptr[0] = fwd(i, k);
-            gm.run(acc, bufY, PG::LDA, sb, zsk(rb * PG::MB, 1 ^ (k & 1), 1));   // W'_k f_k
-          } else {
-            load_rows(bufX, adj(i, k), rb * PG::MB, w);   // P' += w b_k f_k
-            __syncthreads();
-            sb.ptr[0] = fwd(i, k);
-            gm.run(acc, bufX, PG::LDA, sb, zsk(rb * PG::MB, k & 1, 0));
           }
         }
       }
-      // store this CTA's partial of matrix `pass` (m, P, nn, P') on its rows
+      // store this CTA's partial of matrix `pass` (m, P) on its rows
       double2* out = a.partial + (((size_t)state * nblk + blk) * 4 + pass) * MAT;
   #pragma unroll
       for (int j = 0; j < GM::TPW; ++j)
@@ -239,7 +209,7 @@ __device__ void dmat_mul(double2* C, const double2* A, const double2* B, int dp,
 }
 
 // One CTA per state: reduce partials, add the k = 0 terms and the deferred products, and write
-// value, covector = g (m + nn^dag)/2 and environment = g Herm(b_0 at the endpoint).
+// value, covector = g m (= g (m + nn^dag)/2) and environment = g Herm(b_0 at the endpoint).
 __global__ void pullback_finalize(PullbackArgs a, int nblk) {
   const int state = blockIdx.x;
   const int dp = a.dp, MAT = dp * dp, VEC = 7 * MAT, n = a.nodes;
@@ -247,18 +217,15 @@ __global__ void pullback_finalize(PullbackArgs a, int nblk) {
   const double2* ops = a.ops + (size_t)state * a.ops_stride;
   const double2 *R = ops + 2 * MAT, *rho = ops + 7 * MAT;
   double2* t = a.fin + (size_t)state * 8 * MAT;
-  double2 *m = t, *P = t + MAT, *nn = t + 2 * MAT, *Pp = t + 3 * MAT, *B0 = t + 4 * MAT, *B1 = t + 5 * MAT,
-          *T1 = t + 6 * MAT, *T2 = t + 7 * MAT;
+  double2 *m = t, *P = t + MAT, *B0 = t + 4 * MAT, *B1 = t + 5 * MAT, *T1 = t + 6 * MAT;
   for (int e = threadIdx.x; e < MAT; e += blockDim.x) {
-    double2 s[4] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}};
+    double2 s[2] = {{0, 0}, {0, 0}};
     for (int b = 0; b < nblk; ++b) {
       const double2* p = a.partial + (((size_t)state * nblk + b) * 4) * MAT;
-      for (int q = 0; q < 4; ++q) s[q] = zadd(s[q], p[q * MAT + e]);
+      for (int q = 0; q < 2; ++q) s[q] = zadd(s[q], p[q * MAT + e]);
     }
     m[e] = s[0];
     P[e] = s[1];
-    nn[e] = s[2];
-    Pp[e] = s[3];
     double2 b0 = make_double2(0, 0), b1 = make_double2(0, 0);
     for (int i = 0; i < n; ++i) {
       const double2* bs = samples + (size_t)(n - 1 - i) * VEC;
@@ -275,20 +242,14 @@ __global__ void pullback_finalize(PullbackArgs a, int nblk) {
   dmat_mul(m, rho, B1, dp, false, false, 1.0, true);
   dmat_mul(P, rho, B0, dp, false, false, 1.0, true);      // P + rho B0
   dmat_mul(m, P, R, dp, false, true, -1.0, true);         // - (...) R^dag
-  // nn += B0 R rho + B1 rho - R (Pp + B0 rho)
-  dmat_mul(T2, B0, R, dp, false, false, 1.0, false);      // B0 R
-  dmat_mul(nn, T2, rho, dp, false, false, 1.0, true);
-  dmat_mul(nn, B1, rho, dp, false, false, 1.0, true);
-  dmat_mul(Pp, B0, rho, dp, false, false, 1.0, true);
-  dmat_mul(nn, R, Pp, dp, false, false, -1.0, true);
+  // nn = m^dag (B0, B1, rho Hermitian): the covector is g m
   const double g = a.coupling[state];
   const double2* env = samples + (size_t)(a.npoints - 1) * VEC + 3 * MAT;
   double2* cov_out = a.cov_out + (size_t)state * MAT;
   double2* env_out = a.env_out + (size_t)state * MAT;
   for (int e = threadIdx.x; e < MAT; e += blockDim.x) {
     const int i = e / dp, j = e % dp;
-    const double2 c = zadd(m[e], zconj(nn[j * dp + i]));
-    cov_out[e] = zscale(0.5 * g, c);
+    cov_out[e] = zscale(g, m[e]);
     const double2 h = zadd(env[e], zconj(env[j * dp + i]));
     env_out[e] = zscale(0.5 * g, h);
   }
