@@ -182,11 +182,30 @@ lindblad_kernel(const LindbladTask* __restrict__ tasks, int ntasks, int mode) {
 // One CTA per (chunk of CH rows, problem). Problem data: ArnoldiProblem.
 constexpr int CH = 512;
 
+// The second pass is run only when the first lost more than 1 - 1/sqrt(2) of the norm of w
+// (the criterion of Daniel, Gragg, Kaufman and Stewart): |w after pass 0|^2 < |w before|^2 / 2.
+// Otherwise w is orthogonal to the basis to working precision after one pass.
+__device__ __forceinline__ bool cgs_needs_second_pass(const ArnoldiProblem& P, int nchunk) {
+  double before = 0.0, after = 0.0;
+  for (int c = 0; c < nchunk; ++c) {
+    before += P.norms[c];
+    after += P.norms[nchunk + c];
+  }
+  return !(after > 0.5 * before);
+}
+
 // partial[p][chunk][i] = sum_{r in chunk} conj(V_i[r]) w[r], i = 0..j;  norms: |w|^2 partial (pass 0)
 __global__ void cgs_partial(ArnoldiProblem* __restrict__ probs, int nprob, int j, int nchunk, int pass) {
   const int p = blockIdx.y, ch = blockIdx.x;
   ArnoldiProblem& P = probs[p];
   if (!P.active || P.exhausted || j >= P.target) return;
+  if (pass == 1) {
+    // every CTA takes the same decision from the norms of pass 0; CTA 0 records it for the
+    // subtraction, which overwrites those norms
+    const bool again = cgs_needs_second_pass(P, nchunk);
+    if (ch == 0 && threadIdx.x == 0) P.reorth = again ? 1 : 0;
+    if (!again) return;
+  }
   const int n = P.n;
   const int r0 = ch * CH, r1 = min(n, r0 + CH);
   __shared__ double2 w[CH];
@@ -244,11 +263,12 @@ __global__ void cgs_partial(ArnoldiProblem* __restrict__ probs, int nprob, int j
   }
 }
 
-// h_i = sum_chunks partial; H[i][j] += h_i (chunk 0); w[r] -= sum_i V_i[r] h_i; pass 1: |w|^2 partial
+// h_i = sum_chunks partial; H[i][j] += h_i (chunk 0); w[r] -= sum_i V_i[r] h_i; |w|^2 partial
 __global__ void cgs_subtract(ArnoldiProblem* __restrict__ probs, int nprob, int j, int nchunk, int pass) {
   const int p = blockIdx.y, ch = blockIdx.x;
   ArnoldiProblem& P = probs[p];
   if (!P.active || P.exhausted || j >= P.target) return;
+  if (pass == 1 && !P.reorth) return;   // pass 0 left w orthogonal: its norms stand
   extern __shared__ double2 h[];
   for (int i = threadIdx.x; i <= j; i += blockDim.x) {
     double2 s = make_double2(0, 0);
@@ -284,7 +304,7 @@ __global__ void cgs_subtract(ArnoldiProblem* __restrict__ probs, int nprob, int 
     P.W[r] = acc;
     nrm += zabs2(acc);
   }
-  if (pass == 1) {
+  {
     __shared__ double red[32];
     nrm = warp_sum(nrm);
     if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = nrm;

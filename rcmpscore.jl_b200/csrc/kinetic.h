@@ -44,6 +44,7 @@ struct ArnoldiProblem {
   double beta, estimate, residual;
   int n, n_phys, dp, kmax, kmax1, target;
   int k, exhausted, nonfinite, active, solve, reconstruct, adjoint;
+  int reorth;                // the current Arnoldi step runs its second Gram-Schmidt pass
 };
 
 struct KineticSetup {

@@ -349,10 +349,14 @@ __global__ void stationary_finish_kernel(StationaryArgs a) {
   __syncthreads();
   const double den = zabs2(tr);
   double herm = 0.0;
+  // x / tr once per element (scratch), then (rho + rho^dag)/2 from that one copy: every pair
+  // (i, j), (j, i) is formed from the same two values, so the result is exactly Hermitian
+  double2* nx = a.tmp + (size_t)s * MAT;
+  for (int e = threadIdx.x; e < MAT; e += blockDim.x) nx[e] = zscale(1.0 / den, zmul(x[e], zconj(tr)));
+  __syncthreads();
   for (int e = threadIdx.x; e < MAT; e += blockDim.x) {
     const int i = e / dp, j = e % dp;
-    const double2 v = zscale(1.0 / den, zmul(x[e], zconj(tr)));
-    const double2 w = zscale(1.0 / den, zmul(x[j * dp + i], zconj(tr)));
+    const double2 v = nx[e], w = nx[j * dp + i];
     herm += zabs2(zsub(v, zconj(w)));
     rho[e] = zscale(0.5, zadd(v, zconj(w)));
   }
