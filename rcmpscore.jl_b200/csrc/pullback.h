@@ -16,7 +16,7 @@ struct PullbackArgs {
   const double* coupling;      // [state]
   const double* traj_value;    // [state] scalar channel at the endpoint
   double2* scratch;            // [CTAs][3 dp^2]
-  double2* partial;            // [state][nblk][4][dp^2]
+  double2* partial;            // [state][nblk][4][dp^2]: slots 0 (m) and 1 (P) are used
   double2* fin;                // [state][8 dp^2]
   double2* cov_out;            // [state][dp^2] (padded)
   double2* env_out;            // [state][dp^2] (padded)
