@@ -9,7 +9,7 @@
 // shifts: CGS2 with the breakdown test |v| <= 10 eps max(|v before projection|, eps); the basis
 // doubles (16, 32, ...) until the projected estimate max_c |c H[k,k-1] y_c[k-1]| / beta meets
 // the tolerance, then every shifted solution is reconstructed and its true residual checked.
-// Device organisation (this build): every phase is one launch over all active problems of a
+// Device organisation (this library): every phase is one launch over all active problems of a
 // batch (the Lindblad actions and the reconstruction on FP64 tensor cores, the Gram-Schmidt
 // passes as streaming reductions over the basis); the adjoint solutions are stored conjugate
 // transposed (a_c = A_c^dag, using (L* A)^dag = L*(A^dag)) as the contraction needs them.

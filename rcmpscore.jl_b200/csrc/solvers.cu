@@ -3,7 +3,7 @@
 //
 // Reference: rcmps_gpu numerics.py:55-126 (GMRES _right_solve, stationary_state,
 // boundary_environment, finish_gradient) and src/transfer.jl:33-153. The reference
-// right-preconditions GMRES with a Schur/trsyl no-jump inverse on the host; this build runs
+// right-preconditions GMRES with a Schur/trsyl no-jump inverse on the host; this library runs
 // unpreconditioned restarted GMRES(m) on the device for every state of a batch at once (the
 // Arnoldi steps reuse the Lindblad and Gram-Schmidt kernels of the kinetic term), stops on
 // |b - A x| <= tol max(1, |b|) and accepts with the reference's check |A x - b| <= 20 tol max(1, |b|).

@@ -1,7 +1,7 @@
 """Parity of the CUDA path (through the C ABI) with the reference and the oracle.
 
 Tolerances (written per test): integer outputs (DOP853 step counts, Krylov basis sizes) exactly;
-floating point at the north-star bar or tighter: energy |dE/E| <= 1e-10 and gradient <= 1e-8
+floating point at the parity bar or tighter: energy |dE/E| <= 1e-10 and gradient <= 1e-8
 relative in the metric norm, with max(|g|, 1) as the scale (near minima |g| itself is tiny).
 """
 import ctypes as C
