@@ -750,8 +750,9 @@ def _superop(f, d):
 
 def _solve(op, b, d, method, tolerance):
     """x with op(x) = b for a linear map op on D x D matrices: a dense LU of the D^2 x D^2
-    matrix ("dense"), or restarted GMRES on its action ("krylov", as numerics.py:55-71 does,
-    unpreconditioned) for sizes where the dense matrix is too costly."""
+    matrix ("dense"), or restarted GMRES on its action ("krylov") for sizes where the dense
+    matrix is too costly. The reference's GMRES (numerics.py:55-71) is right-preconditioned by
+    the no-jump inverse; the oracle's is not: only the solution is compared, not the iterates."""
     if method == "dense":
         return _mat(np.linalg.solve(_superop(op, d), _vec(b)), d)
     if method != "krylov":
