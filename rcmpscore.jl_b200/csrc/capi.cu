@@ -24,7 +24,14 @@
 namespace rcmps {
 
 static std::atomic<long long> g_launches{0};
-void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+// launches of this host thread (a graph capture counts the kernels it records)
+static thread_local long long t_launches = 0;
+void note_launch() {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  ++t_launches;
+}
+void note_launches(long long count) { g_launches.fetch_add(count, std::memory_order_relaxed); }
+long long thread_launch_count() { return t_launches; }
 
 cudaError_t arena_reserve(rcmps_slot& sl, size_t bytes) {
   if (bytes <= sl.arena_bytes) return cudaSuccess;
@@ -303,6 +310,8 @@ int rcmps_context_destroy(rcmps_context* ctx) {
   }
   if (ctx->aux) cudaFree(ctx->aux);
   if (ctx->host_io) cudaFree(ctx->host_io);
+  for (auto& g : ctx->gmres_graphs)
+    if (g.exec) cudaGraphExecDestroy(g.exec);
   delete ctx;
   return RCMPS_OK;
 }

@@ -18,6 +18,8 @@ namespace rcmps {
 
 // Kernel launches issued by the library in this process (every launch site calls note_launch).
 void note_launch();
+void note_launches(long long count);   // kernels replayed by one graph launch
+long long thread_launch_count();   // launches noted by the calling host thread
 
 // ------------------------------------------------------------------ status codes
 // The numbers of the reference's device controller (device_control_backend.py:23-27 of

@@ -16,6 +16,16 @@ struct rcmps_slot {
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
 };
 
+// One restart cycle of the batched GMRES captured as a CUDA graph, for the problems and tasks at
+// these device addresses and these sizes.
+struct rcmps_gmres_graph {
+  const void* probs = nullptr;
+  const void* tasks = nullptr;
+  int np = 0, dp = 0, m = 0;
+  long long kernels = 0;                // kernels the graph replays
+  cudaGraphExec_t exec = nullptr;
+};
+
 struct rcmps_context {
   int device = 0;
   int sms = 0;
@@ -25,6 +35,8 @@ struct rcmps_context {
   size_t aux_bytes = 0;
   void* host_io = nullptr;                // device copies of the host-buffer entry's inputs and outputs
   size_t host_io_bytes = 0;
+  rcmps_gmres_graph gmres_graphs[4];      // cached GMRES restart cycles (replaced in turn)
+  int gmres_graph_next = 0;
   std::string error;
   std::mutex mu;                          // guards `error` (the composite entry runs two host threads)
   bool tables = false;
@@ -39,6 +51,8 @@ cudaError_t pinned_reserve(rcmps_slot& slot, size_t bytes);
 cudaError_t aux_reserve(rcmps_context* ctx, size_t bytes);
 cudaError_t host_io_reserve(rcmps_context* ctx, size_t bytes);
 int fail(rcmps_context* ctx, int code, const std::string& message);
+void note_launches(long long count);   // kernels replayed by one graph launch
+long long thread_launch_count();   // launches noted by the calling host thread
 inline size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 int padded_dim(int d);   // 16, 32, 48, 64, 96, 128, or 0 if d is unsupported
 }  // namespace rcmps

@@ -30,10 +30,64 @@ struct Layout {
 constexpr int GCHROWS = 512;
 }  // namespace
 
+// The m Arnoldi steps of one restart cycle: launches that depend on nothing the host learns
+// between them (converged problems are skipped inside the kernels).
+static cudaError_t gmres_cycle_launches(ArnoldiProblem* d_probs, int NP, int dp, int m, LindbladTask* d_tasks,
+                                        cudaStream_t stream) {
+  const int nvec = dp * dp;
+  cudaError_t e = cudaSuccess;
+  for (int j = 0; j < m && !e; ++j) {
+    e = arnoldi_tasks_launch(d_probs, NP, j, d_tasks, stream);
+    if (!e) e = lindblad_launch(dp, d_tasks, NP, 0, stream);
+    if (!e) e = cgs_step_launch(d_probs, NP, j, nvec, stream);
+    if (!e) e = gmres_givens_launch(d_probs, NP, j, stream);
+  }
+  return e;
+}
+
+// One restart cycle, replayed from a CUDA graph that is captured on first use for these device
+// addresses and sizes and kept by the context (the cycle's several hundred launches then cost
+// one). If capture is not possible the cycle is launched directly.
+static cudaError_t gmres_cycle(rcmps_context* ctx, ArnoldiProblem* d_probs, int NP, int dp, int m,
+                               LindbladTask* d_tasks, cudaStream_t stream) {
+  for (auto& g : ctx->gmres_graphs)
+    if (g.exec && g.probs == d_probs && g.tasks == d_tasks && g.np == NP && g.dp == dp && g.m == m) {
+      note_launches(g.kernels);
+      return cudaGraphLaunch(g.exec, stream);
+    }
+  const long long before = thread_launch_count();
+  cudaGraph_t graph = nullptr;
+  if (cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+    cudaGetLastError();
+    return gmres_cycle_launches(d_probs, NP, dp, m, d_tasks, stream);
+  }
+  cudaError_t e = gmres_cycle_launches(d_probs, NP, dp, m, d_tasks, stream);
+  const cudaError_t ec = cudaStreamEndCapture(stream, &graph);
+  cudaGraphExec_t exec = nullptr;
+  if (!e && !ec && graph && cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess) {
+    if (graph) cudaGraphDestroy(graph);
+    rcmps_gmres_graph& g = ctx->gmres_graphs[ctx->gmres_graph_next];
+    ctx->gmres_graph_next = (ctx->gmres_graph_next + 1) % 4;
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+    g.probs = d_probs;
+    g.tasks = d_tasks;
+    g.np = NP;
+    g.dp = dp;
+    g.m = m;
+    g.kernels = thread_launch_count() - before;
+    g.exec = exec;
+    return cudaGraphLaunch(exec, stream);
+  }
+  // capture or instantiation failed: nothing was launched by the capture; launch directly
+  if (graph) cudaGraphDestroy(graph);
+  cudaGetLastError();
+  return gmres_cycle_launches(d_probs, NP, dp, m, d_tasks, stream);
+}
+
 // Restarted GMRES(m) over NP problems that share dp; hp/d_probs hold set-up problems with x = 0.
 // Returns 0, or a CUDA error code. Convergence per problem is in hp[p].converged / residual.
-static cudaError_t gmres_run(ArnoldiProblem* hp, ArnoldiProblem* d_probs, int NP, int dp, int m, int maxrestart,
-                             LindbladTask* d_tasks, cudaStream_t stream) {
+static cudaError_t gmres_run(rcmps_context* ctx, ArnoldiProblem* hp, ArnoldiProblem* d_probs, int NP, int dp,
+                             int m, int maxrestart, LindbladTask* d_tasks, cudaStream_t stream) {
   const int nvec = dp * dp;
   cudaError_t e = cudaMemcpyAsync(d_probs, hp, NP * sizeof(ArnoldiProblem), cudaMemcpyHostToDevice, stream);
   for (int it = 0; it <= maxrestart && !e; ++it) {
@@ -46,12 +100,7 @@ static cudaError_t gmres_run(ArnoldiProblem* hp, ArnoldiProblem* d_probs, int NP
     bool all = true;
     for (int p = 0; p < NP; ++p) all &= hp[p].converged != 0;
     if (all || it == maxrestart) break;
-    for (int j = 0; j < m && !e; ++j) {
-      e = arnoldi_tasks_launch(d_probs, NP, j, d_tasks, stream);
-      if (!e) e = lindblad_launch(dp, d_tasks, NP, 0, stream);
-      if (!e) e = cgs_step_launch(d_probs, NP, j, nvec, stream);
-      if (!e) e = gmres_givens_launch(d_probs, NP, j, stream);
-    }
+    e = gmres_cycle(ctx, d_probs, NP, dp, m, d_tasks, stream);
     if (!e) e = gmres_update_launch(d_probs, NP, nvec, m, stream);
   }
   return e;
@@ -219,7 +268,8 @@ int finish_solve(rcmps_context* ctx, FinishJob& job, cudaStream_t stream, Finish
       A.trw = ops + 7 * mat;  // + tr(rho X) I
       A.b = fa.b + (size_t)i * mat;
     }
-    e = gmres_run(hp, (ArnoldiProblem*)P(g.gb.o_probs), n, dp, m, maxrestart, (LindbladTask*)P(g.gb.o_tasks), stream);
+    e = gmres_run(ctx, hp, (ArnoldiProblem*)P(g.gb.o_probs), n, dp, m, maxrestart, (LindbladTask*)P(g.gb.o_tasks),
+                  stream);
     if (e) return fail(ctx, RCMPS_CUDA_ERROR, std::string("boundary GMRES: ") + cudaGetErrorString(e));
   }
   return RCMPS_OK;
@@ -353,7 +403,8 @@ int stationary_run(rcmps_context* ctx, StationaryJob& job, cudaStream_t stream) 
       // solve with rtol = atol = tolerance / max(1, |rhs|) (stationary_correction.py:60-66)
       if (job.rho_previous) A.bnorm = 1.0;
     }
-    e = gmres_run(hp, (ArnoldiProblem*)P(gb.o_probs), n, dp, m, maxrestart, (LindbladTask*)P(gb.o_tasks), stream);
+    e = gmres_run(ctx, hp, (ArnoldiProblem*)P(gb.o_probs), n, dp, m, maxrestart, (LindbladTask*)P(gb.o_tasks),
+                  stream);
     if (e) return fail(ctx, RCMPS_CUDA_ERROR, std::string("stationary GMRES: ") + cudaGetErrorString(e));
     StationaryArgs sa;
     sa.dp = dp;
