@@ -34,7 +34,8 @@ __all__ = [
     "QuarticSystem", "integrate", "quartic_pullback", "evaluate_quartic", "kinetic_raw",
     "stationary_state", "boundary_environment", "finish_gradient", "metric", "fg_phi4",
     "phi4_state", "z2_state", "left_canonical_q", "PackedZ2System", "z2_structure_ok",
-    "source_integral", "phi_expectation", "phi_by_ode",
+    "source_integral", "phi_expectation", "phi_by_ode", "NoJumpInverse",
+    "boundary_environment_preconditioned",
 ]
 
 
@@ -795,10 +796,75 @@ def boundary_environment(q, r, rho, environment, *, method="dense"):
     return _solve(lambda x: -lindblad_adjoint(q, r, x) + np.trace(rho @ x) * eye, b, d, method, 1e-13)
 
 
+class NoJumpInverse:
+    """The no-jump inverse of the reference's preconditioner (numerics.py:40-53): with the complex
+    Schur form Q = U T U^dag and T_s = T - (shift/2) I, y -> -U X U^dag where X solves the
+    triangular Sylvester equation T_s X + X T_s^dag = U^dag y U (T_s^dag X + X T_s for the adjoint
+    map). The shift is max(1, |Q|_2, |R|_2^2) when T has an eigenvalue with real part above
+    -100 eps times that scale, else 0."""
+
+    def __init__(self, q, r):
+        from scipy.linalg import get_lapack_funcs, schur
+        t, self.u = schur(np.asarray(q, complex), output="complex")
+        scale = max(1.0, np.linalg.norm(q, 2), np.linalg.norm(r, 2) ** 2)
+        self.shift = scale if np.real(np.diag(t)).max() >= -100 * np.finfo(float).eps * scale else 0.0
+        self.t = np.asfortranarray(t - self.shift / 2 * np.eye(len(q)))
+        self.trsyl = get_lapack_funcs("trsyl", (self.t,))
+
+    def __call__(self, y, adjoint=False):
+        c = np.asfortranarray(adj(self.u) @ y @ self.u)
+        x, scale, info = self.trsyl(self.t, self.t, c, trana="C" if adjoint else "N",
+                                    tranb="N" if adjoint else "C")
+        if info < 0 or not np.isfinite(scale) or scale <= 0:
+            raise OracleFailure(f"Sylvester inverse failed: info={info}, scale={scale}")
+        return self.u @ (-x / scale) @ adj(self.u)
+
+
+def boundary_environment_preconditioned(q, r, rho, environment, *, tolerance=1e-13):
+    """The reference's boundary solve itself (numerics.py:55-71, 103-117): GMRES(min(40, D^2))
+    with rtol = atol = tolerance on the column-major vectorization, right-preconditioned by the
+    adjoint no-jump inverse with the Sherman-Morrison correction for the tr(rho x) I term.
+    Returns (H, matvecs)."""
+    from scipy.sparse.linalg import LinearOperator, gmres
+    q, r, rho = (np.asarray(x, complex) for x in (q, r, rho))
+    d = len(q)
+    eye = np.eye(d, dtype=complex)
+    b = environment - np.trace(rho @ environment) * eye
+    inverse = NoJumpInverse(q, r)
+    z = inverse(eye, adjoint=True)
+    den = 1.0 + np.trace(rho @ z)
+
+    def pre(y):
+        x = inverse(y, adjoint=True)
+        return x - np.trace(rho @ x) / den * z
+
+    def op(x):
+        return -lindblad_adjoint(q, r, x) + np.trace(rho @ x) * eye
+
+    count = [0]
+
+    def matvec(v):
+        count[0] += 1
+        return op(pre(np.asarray(v).reshape((d, d), order="F"))).reshape(-1, order="F")
+
+    lin = LinearOperator((d * d, d * d), matvec=matvec, dtype=np.complex128)
+    y, info = gmres(lin, b.reshape(-1, order="F"), rtol=tolerance, atol=tolerance, restart=min(40, d * d),
+                    maxiter=200)
+    h = pre(y.reshape((d, d), order="F"))
+    residual = np.linalg.norm(op(h) - b)
+    if info != 0 or not np.isfinite(residual) or residual > 20 * tolerance * max(1.0, np.linalg.norm(b)):
+        raise OracleFailure(f"preconditioned boundary GMRES failed: info={info}, residual={residual:.3e}")
+    return h, count[0]
+
+
 def finish_gradient(q, r, rho, covector, environment, *, metric_reg=1e-3, method="dense"):
     """gradient = ((rho + reg I)^-1 (covector + rho R^dag H - rho H R^dag))^dag
-    (numerics.py:120-126, src/observables.jl:278-289)."""
-    h = boundary_environment(q, r, rho, environment, method=method)
+    (numerics.py:120-126, src/observables.jl:278-289). method "preconditioned" solves for H as
+    the reference does (boundary_environment_preconditioned)."""
+    if method == "preconditioned":
+        h, _ = boundary_environment_preconditioned(q, r, rho, environment)
+    else:
+        h = boundary_environment(q, r, rho, environment, method=method)
     c = covector + rho @ adj(r) @ h - rho @ h @ adj(r)
     return adj(np.linalg.solve(rho + metric_reg * np.eye(len(r)), c))
 

@@ -14,6 +14,9 @@ This script imports the reference package rcmps_gpu read-only from a local check
                 D = 4 random state, objective = quartic (W = 6, n_quad = 24) + kinetic (32 nodes)
                 + finished gradient, stationary densities by numerics.stationary_state: per
                 accepted iteration the energy, step alpha, trials and gradient norm
+  finish.npz    the reference's preconditioned boundary solve and finished gradient
+                (numerics.finish_gradient) with its GMRES matvec count, on random states D = 8, 16
+                and a Z2 state D = 16 with seeded covectors and environments
   packed.npz    the packed Z2 route (evaluate_quartic(..., packed_z2=True), the default of the
                 persistent trajectory) on Z2 states D = 4, 8 (W = 30, n_quad = 64), 16 and 32
                 (W = 30, n_quad = 512, 512 kinetic nodes: the optimizer defaults, with the
@@ -31,7 +34,7 @@ is the reference's test/fixtures/phi4_g2_D16_z2_portable (exported by RcmpsCore 
 States: NumPy PCG64 default_rng(seed); R and A with i.i.d. standard complex Gaussian entries
 times 0.2 (R drawn first), K = (A + A^dag)/2; Z2 states draw blocks in the order k1, k2, R12, R21.
 Run: python tests/golden/make_golden.py [name ...]  (all files by default, about a minute; the
-D = 64 record dominates; names: small d16 d64 samples ode packed phi optim)
+D = 64 record dominates; names: small d16 d64 samples ode packed phi optim finish)
 """
 from __future__ import annotations
 
@@ -159,6 +162,18 @@ def optim_run():
                 R_final=last["R"], K_final=last["K"])
 
 
+def finish_record(r, k, seed):
+    q = -1j * k - r.conj().T @ r / 2
+    rho, _ = nm.stationary_state(q, r, tolerance=1e-13)
+    rng = np.random.default_rng(seed)
+    d = len(r)
+    env = rng.standard_normal((d, d)) + 1j * rng.standard_normal((d, d))
+    env = (env + env.conj().T) / 2
+    cov = rng.standard_normal((d, d)) + 1j * rng.standard_normal((d, d))
+    grad, st = nm.finish_gradient(q, r, rho, cov, env, metric_reg=1e-3)
+    return dict(R=r, K=k, rho=rho, covector=cov, environment=env, gradient=grad, matvecs=st["matvecs"])
+
+
 def evaluate_ode(r, k, g, window, nq):
     q = -1j * k - r.conj().T @ r / 2
     rho, _ = nm.stationary_state(q, r, tolerance=1e-13)
@@ -200,6 +215,9 @@ def main(names):
         save("phi.npz", [evaluate_phi(*random_state(4, 904), 6.0, 24),
                          evaluate_phi(*z2_state(8, 908), 20.0, 64),
                          evaluate_phi(*random_state(16, 916), 40.0, 1024, 1e-14, 1e-13)])
+    if "finish" in names:
+        save("finish.npz", [finish_record(*random_state(8, 808), 1), finish_record(*random_state(16, 816), 2),
+                            finish_record(*z2_state(16, 826), 3)])
     if "optim" in names:
         save("optim.npz", [optim_run()])
     if "packed" in names:
@@ -225,4 +243,4 @@ def samples_d5():
 
 
 if __name__ == "__main__":
-    main(sys.argv[1:] or ["small", "d16", "d64", "ode", "samples", "packed", "phi", "optim"])
+    main(sys.argv[1:] or ["small", "d16", "d64", "ode", "samples", "packed", "phi", "optim", "finish"])

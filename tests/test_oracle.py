@@ -125,3 +125,21 @@ def test_coherent_state_known_answers():
     rho = np.eye(2, dtype=complex) / 2
     quartic = O.evaluate_quartic(R, Q, rho, 1.0, half_window=30.0, n_quad=64)
     assert abs(quartic["value"] - (math.sqrt(2) * a) ** 4) < 1e-10
+
+
+@pytest.mark.parametrize("index", range(3))
+def test_oracle_preconditioned_boundary_solve_matches_reference(index):
+    """The reference's boundary solve itself (numerics.py:55-126): the no-jump preconditioned
+    GMRES takes the same number of matrix-vector products, and the finished gradient agrees. The
+    unpreconditioned solves (the oracle's others, and the library's) need several times more."""
+    rec = load_records("finish.npz")[index]
+    R, K, rho = rec["R"], rec["K"], rec["rho"]
+    Q = O.left_canonical_q(R, K)
+    h, matvecs = O.boundary_environment_preconditioned(Q, R, rho, rec["environment"])
+    assert matvecs == int(rec["matvecs"])
+    grad = O.finish_gradient(Q, R, rho, rec["covector"], rec["environment"], method="preconditioned")
+    diff = grad - rec["gradient"]
+    assert math.sqrt(max(0.0, O.metric(rho, diff, diff))) < 1e-10 * max(1.0, math.sqrt(O.metric(rho, grad, grad)))
+    dense = O.finish_gradient(Q, R, rho, rec["covector"], rec["environment"], method="dense")
+    diff = dense - grad
+    assert math.sqrt(max(0.0, O.metric(rho, diff, diff))) < 1e-9 * max(1.0, math.sqrt(O.metric(rho, grad, grad)))
