@@ -80,7 +80,10 @@ void rcmps_default_settings(rcmps_settings* settings);
 
 /* Context of one device: streams, events and a device workspace that grows on demand.
  * Replaces the per-call solver objects of the reference (PersistentTrajectoryDOP853,
- * persistent_trajectory_backend.py:339-403; KineticContext, kinetic_backend.py:236-275). */
+ * persistent_trajectory_backend.py:339-403; KineticContext, kinetic_backend.py:236-275).
+ * A context serves one call at a time, as the reference's coordinator serves one state at a
+ * time (overlap_sweep_driver.py:132-135): its workspace, streams and cached GMRES graphs are
+ * shared by its calls. Use one context per host thread for concurrent calls. */
 int rcmps_context_create(int device, rcmps_context** context);
 int rcmps_context_destroy(rcmps_context* context);
 const char* rcmps_context_error(const rcmps_context* context);
