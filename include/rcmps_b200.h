@@ -110,6 +110,23 @@ int rcmps_fg_phi4_batch(rcmps_context* context, int n_states, const int* dims, c
                         double* energy, double* gradient, double* covector, double* environment,
                         rcmps_state_stats* stats, void* stream);
 
+/* Per-state integration controls of rcmps_fg_phi4_batch_controls. A value <= 0 takes the
+ * settings' value. No counterpart in the reference, whose objective integrates one state per
+ * call with one (atol, rtol) pair (runtime/sweep_driver.py:78-119): here a batch of states with
+ * mixed tolerance pairs shares one persistent trajectory launch. */
+typedef struct rcmps_state_controls {
+  double atol, rtol;           /* DOP853 tolerances of this state's quartic trajectory */
+} rcmps_state_controls;
+
+/* rcmps_fg_phi4_batch with per-state DOP853 tolerances: controls[i] (host, n_states entries)
+ * replaces settings->atol / rtol for state i; the same checks apply (atol > 0,
+ * rtol >= 100 eps). controls = NULL is rcmps_fg_phi4_batch. */
+int rcmps_fg_phi4_batch_controls(rcmps_context* context, int n_states, const int* dims, const double* couplings,
+                                 const double* R, const double* K, const double* rho,
+                                 const rcmps_settings* settings, const rcmps_state_controls* controls,
+                                 double* energy, double* gradient, double* covector, double* environment,
+                                 rcmps_state_stats* stats, void* stream);
+
 /* Same with every array in host memory (copies in and out inside the call, through a device
  * buffer the context keeps and grows on demand). */
 int rcmps_fg_phi4_batch_host(rcmps_context* context, int n_states, const int* dims, const double* couplings,
@@ -177,8 +194,11 @@ int rcmps_finish_gradient_batch(rcmps_context* context, int n_states, const int*
  * memory limit where an allocation in the middle of an optimizer step would fail or stall.
  * Its workspace is one fixed 2 MiB array in the library's device image, so it supports
  * 1 <= d <= 32 only; larger d returns RCMPS_INVALID_ARGUMENT with a message naming the limit.
- * The first call on each device looks up that array's device address (cudaGetSymbolAddress),
- * so make the first call before any stream capture begins. All calls share the one array:
+ * The first call on each device looks up that array's device address (cudaGetSymbolAddress)
+ * and keeps it for the life of the process, so do not use this entry on a device after a
+ * cudaDeviceReset of it. Every call copies GMRES state back to the host and synchronizes the
+ * stream once per GMRES restart and once at the end, so it must not be called on a capturing
+ * stream. All calls share the one array:
  * calls that overlap on the GPU (different streams or host threads) race on it, and the
  * caller must order them. Each call clears what must start at zero (the Poisson solution and
  * the status words). Arguments are those of rcmps_finish_gradient_batch with n_states = 1:

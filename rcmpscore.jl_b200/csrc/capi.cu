@@ -562,11 +562,27 @@ int rcmps_fg_phi4_batch(rcmps_context* ctx, int n, const int* dims, const double
                         const double* K, const double* rho, const rcmps_settings* settings, double* energy,
                         double* gradient, double* covector, double* environment, rcmps_state_stats* stats,
                         void* stream) {
+  return rcmps_fg_phi4_batch_controls(ctx, n, dims, couplings, R, K, rho, settings, nullptr, energy, gradient,
+                                      covector, environment, stats, stream);
+}
+
+int rcmps_fg_phi4_batch_controls(rcmps_context* ctx, int n, const int* dims, const double* couplings,
+                                 const double* R, const double* K, const double* rho,
+                                 const rcmps_settings* settings, const rcmps_state_controls* controls,
+                                 double* energy, double* gradient, double* covector, double* environment,
+                                 rcmps_state_stats* stats, void* stream) {
   if (!ctx) return RCMPS_INVALID_ARGUMENT;
   int rc = check_settings(ctx, settings);
   if (rc) return rc;
   rc = check_dims(ctx, n, dims);
   if (rc) return rc;
+  for (int i = 0; controls && i < n; ++i) {
+    const double at = controls[i].atol > 0.0 ? controls[i].atol : settings->atol;
+    const double rt = controls[i].rtol > 0.0 ? controls[i].rtol : settings->rtol;
+    if (!std::isfinite(at) || !std::isfinite(rt) || !(rt >= 100 * 2.220446049250313e-16))
+      return fail(ctx, RCMPS_INVALID_ARGUMENT,
+                  "controls[" + std::to_string(i) + "]: atol > 0 and rtol >= 100 eps, both finite");
+  }
   if (n == 0) return RCMPS_OK;
   if (!R || !K || !rho || !energy || !gradient || !stats || !couplings)
     return fail(ctx, RCMPS_INVALID_ARGUMENT, "NULL pointer");
@@ -603,6 +619,7 @@ int rcmps_fg_phi4_batch(rcmps_context* ctx, int n, const int* dims, const double
   qj.K = K;
   qj.rho = rho;
   qj.settings = *settings;
+  qj.controls = controls;
   qj.value = vq;
   qj.covector = cq;
   qj.environment = eq;

@@ -54,7 +54,9 @@ struct Bump {
 }  // namespace
 
 // Device address of the scratch array on the current device; looked up on the first call per
-// device (which therefore should not happen inside a stream capture).
+// device and kept for the life of the process (a cudaDeviceReset of that device would leave the
+// kept address stale, which the header rules out). Every call synchronizes its stream, so no call
+// may run inside a stream capture.
 static cudaError_t noalloc_scratch(int device, char** out) {
   std::lock_guard<std::mutex> lock(g_noalloc_mu);
   if (device < 0 || device >= 64) return cudaErrorInvalidDevice;

@@ -247,6 +247,11 @@ int quartic_run(rcmps_context* ctx, QuarticJob& job, cudaStream_t stream) {
         t.stats = reinterpret_cast<TrajStats*>(base + o_tstats) + i;
         t.atol = S.atol;
         t.rtol = S.rtol;
+        if (job.controls) {   // per-state tolerances (checked by the entry point)
+          const rcmps_state_controls& c = job.controls[idx[i]];
+          if (c.atol > 0.0) t.atol = c.atol;
+          if (c.rtol > 0.0) t.rtol = c.rtol;
+        }
         t.max_steps = S.max_steps;
         t.d = h_dims[i];
       }

@@ -14,6 +14,7 @@ struct QuarticJob {
   const double* couplings = nullptr;    // host, NULL: 1
   const double *R = nullptr, *K = nullptr, *rho = nullptr;   // device, packed
   rcmps_settings settings{};
+  const rcmps_state_controls* controls = nullptr;   // host [n], per-state tolerances, optional
   double* value = nullptr;              // device [n] (g * quartic density), optional
   double* covector = nullptr;           // device packed, optional
   double* environment = nullptr;        // device packed, optional

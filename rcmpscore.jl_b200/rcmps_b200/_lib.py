@@ -31,6 +31,11 @@ class Settings(C.Structure):
     ]
 
 
+class StateControls(C.Structure):
+    """Per-state DOP853 tolerances (rcmps_state_controls); a value <= 0 takes the settings'."""
+    _fields_ = [("atol", C.c_double), ("rtol", C.c_double)]
+
+
 class StateStats(C.Structure):
     _fields_ = [
         ("status", C.c_int), ("failed_component", C.c_int),
@@ -64,6 +69,8 @@ SIGNATURES = {
     "rcmps_workspace_bytes": (C.c_longlong, [_P, _I, C.POINTER(_I), C.POINTER(Settings)]),
     "rcmps_fg_phi4_batch": (_I, [_P, _I, C.POINTER(_I), C.POINTER(_D), _P, _P, _P, C.POINTER(Settings),
                                  _P, _P, _P, _P, C.POINTER(StateStats), _P]),
+    "rcmps_fg_phi4_batch_controls": (_I, [_P, _I, C.POINTER(_I), C.POINTER(_D), _P, _P, _P, C.POINTER(Settings),
+                                          C.POINTER(StateControls), _P, _P, _P, _P, C.POINTER(StateStats), _P]),
     "rcmps_fg_phi4_batch_host": (_I, [_P, _I, C.POINTER(_I), C.POINTER(_D), _P, _P, _P, C.POINTER(Settings),
                                       _P, _P, _P, _P, C.POINTER(StateStats)]),
     "rcmps_quartic_batch": (_I, [_P, _I, C.POINTER(_I), C.POINTER(_D), _P, _P, _P, C.POINTER(Settings),

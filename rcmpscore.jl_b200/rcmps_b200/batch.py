@@ -11,7 +11,7 @@ import math
 
 import numpy as np
 
-__all__ = ["random_state", "z2_state", "config_states", "shard"]
+__all__ = ["random_state", "z2_state", "config_states", "uneven_states", "shard"]
 
 
 def _draw(rng, n):
@@ -44,7 +44,12 @@ def config_states(name):
     """(R list, K list, couplings, description) of a named workload.
     d64_mixed: 16 random (seeds 0..15) + 16 Z2 (seeds 100..115) states at D = 64, g = 2;
     d32_batch: 64 random D = 32 states (seeds 0..63), g ~ U[0.5, 3] (seed 12345);
-    d64_pair: the first random and the first Z2 state of d64_mixed (a small profiling case)."""
+    d64_pair: the first random and the first Z2 state of d64_mixed (a small profiling case);
+    uneven200: 200 random states with D drawn from {16, 32, 48, 64, 96, 128}, g ~ U[0.5, 3] and
+    atol, rtol each drawn from {1e-10, 1e-12} (use uneven_states for the tolerances)."""
+    if name == "uneven200":
+        R, K, g, _ = uneven_states(200)
+        return R, K, g, "200 random states D in {16,32,48,64,96,128} (scaling 0.2), g~U[0.5,3], mixed atol/rtol"
     if name == "d64_mixed":
         R, K = [], []
         for s in range(16):
@@ -64,6 +69,27 @@ def config_states(name):
         g = np.random.default_rng(12345).uniform(0.5, 3.0, 64)
         return list(R), list(K), [float(x) for x in g], "64 random states D=32 (scaling 0.2), g~U[0.5,3]"
     raise ValueError(f"unknown workload {name!r}")
+
+
+UNEVEN_DIMS = (16, 32, 48, 64, 96, 128)
+UNEVEN_TOLERANCES = (1e-10, 1e-12)
+
+
+def uneven_states(count=200, seed=2024):
+    """The uneven workload: state i has D drawn from UNEVEN_DIMS, R, K from random_state(D,
+    4000 + i), a coupling g ~ U[0.5, 3] and a tolerance pair (atol, rtol) with both drawn from
+    UNEVEN_TOLERANCES; all draws come from one default_rng(seed) stream, state by state.
+    Returns (R list, K list, couplings, tolerances)."""
+    rng = np.random.default_rng(seed)
+    R, K, g, tol = [], [], [], []
+    for i in range(count):
+        d = int(rng.choice(UNEVEN_DIMS))
+        r, k = random_state(d, 4000 + i)
+        R.append(r)
+        K.append(k)
+        g.append(float(rng.uniform(0.5, 3.0)))
+        tol.append((float(rng.choice(UNEVEN_TOLERANCES)), float(rng.choice(UNEVEN_TOLERANCES))))
+    return R, K, g, tol
 
 
 def shard(dims, rank, world):

@@ -1,22 +1,30 @@
-"""State files shared with RcmpsCore.jl: the portable directory format and JLD2 checkpoints.
+"""State files exchanged with RcmpsCore.jl: portable directories and JLD2 checkpoints.
 
-Same API and semantics as rcmps_gpu.io (gpu/src/rcmps_gpu/io.py:94-471 of RcmpsCore.jl):
-StateRecord, Integration, Manifold, read_portable, write_portable, read_jld2.
+Public names follow rcmps_gpu.io (gpu/src/rcmps_gpu/io.py of RcmpsCore.jl): StateRecord,
+Integration, Manifold, read_portable, write_portable, read_jld2, FORMAT, FORMAT_VERSION,
+SYMMETRIES. The implementation here is table-driven: every metadata key of the format is one
+row of a schema (`_FORMAT1`), and reading, checking and writing all walk that table.
 
-Portable state directory, "rcmps-portable-state" format 1:
-    metadata.toml   format, format_version = 1, D, model, coupling (required); mass, symmetry
-                    ("Z2" | "none"), energy, gradient_norm, phi, validation_passed, producer,
-                    source, info (optional); [integration] n_quad, max_point, atol, rtol,
-                    maxiters; [manifold] metric_reg, precond_reg, precond_reg_prefactor
-    R.bin, K.bin    required; rho.bin, gradient.bin optional
-Every .bin is a headerless D x D complex128 matrix, little-endian, column-major (16 D^2 bytes).
-Readers ignore unknown keys and files. Research directories without `format` (the GPU
-optimizer's initial/ and optimized_state/, the Julia exports) are read too: they describe phi4
-with mass 1; energy, gradient and gradient norm fall back to the saved_* keys (their settings to
-[saved_integration]).
+The on-disk format ("rcmps-portable-state", format 1; the format description of
+gpu/src/rcmps_gpu/io.py:15-61 and gpu/julia/portable.jl:141-260):
+  * metadata.toml: required format, format_version (= 1), D, model, coupling; optional mass
+    (1.0 when absent; phi4 only admits 1.0), symmetry ("Z2" or "none"), energy, gradient_norm,
+    phi, validation_passed, producer, source, info, a table [integration] (n_quad, max_point,
+    atol, rtol, optional maxiters) and a table [manifold] (metric_reg, precond_reg, optional
+    precond_reg_prefactor). Unknown keys are kept in StateRecord.metadata and otherwise ignored.
+  * R.bin and K.bin (required), rho.bin and gradient.bin (optional): each a headerless D x D
+    complex128 matrix, little-endian, column-major (Julia's memory order), exactly 16 D^2 bytes.
+    In memory every matrix is a C-ordered (D, D) complex128 array.
+Research directories without a `format` key (the earlier GPU optimizer's initial/ and
+optimized_state/, Julia exports of the research tree) are read as the "legacy" dialect: they
+describe phi4 with mass 1, and a value missing under its format-1 name is taken from its saved_*
+counterpart unless the matching saved_*_available flag is false; the integration settings of
+such saved values are [saved_integration], and otherwise come from the top-level window /
+quadrature style keys.
 
-JLD2 schema 1 (RcmpsCore's rcmps_store): read with h5py, which this environment may lack; the
-reader then raises ImportError. Matrices are stored column-major, so the HDF5 view is transposed.
+JLD2 checkpoints (RcmpsCore's rcmps_store, schema_version 1) are read with h5py, which is an
+optional dependency: without it read_jld2 raises ImportError. JLD2 stores column-major matrices,
+so their HDF5 view is the transpose.
 """
 from __future__ import annotations
 
@@ -35,15 +43,13 @@ __all__ = ["FORMAT", "FORMAT_VERSION", "SYMMETRIES", "Integration", "Manifold", 
 FORMAT = "rcmps-portable-state"
 FORMAT_VERSION = 1
 SYMMETRIES = ("Z2", "none")
-MATRICES = ("R", "K", "rho", "gradient")
-# top-level keys of format 1, in written order
-KEYS = ("format", "format_version", "D", "model", "coupling", "mass", "symmetry", "energy",
-        "gradient_norm", "phi", "validation_passed", "producer", "source", "info", "integration", "manifold")
+_BIN = "<c16"                       # element type of every .bin file
+_NAME = re.compile(r"[A-Za-z0-9_]+\Z")
 
 
 @dataclass(frozen=True)
 class Integration:
-    """IntegratorParameters: max_point is the physical half-window, n_quad the nodes per half."""
+    """RcmpsCore IntegratorParameters: Gauss nodes per half window and the half window x_max."""
     n_quad: int
     max_point: float
     atol: float
@@ -53,7 +59,7 @@ class Integration:
 
 @dataclass(frozen=True)
 class Manifold:
-    """ManifoldParameters."""
+    """RcmpsCore ManifoldParameters."""
     metric_reg: float
     precond_reg: float
     precond_reg_prefactor: float | None = None
@@ -61,7 +67,9 @@ class Manifold:
 
 @dataclass(frozen=True, eq=False)
 class StateRecord:
-    """A state as stored; matrices are C-ordered complex128 (D, D) arrays or None."""
+    """One stored state. Matrices are C-ordered complex128 (D, D) arrays, or None when absent
+    (or not read). `origin` says what was read ("portable", "portable-legacy", "jld2"), `files`
+    which files of the directory hold the record, `metadata` the raw TOML table."""
     D: int
     model: str
     coupling: float
@@ -85,297 +93,350 @@ class StateRecord:
     metadata: dict = field(default_factory=dict)
 
 
-# ---------------------------------------------------------------------------- value checks
+# ------------------------------------------------------------------------------- value kinds
+# A kind turns a TOML value into its Python value or raises ValueError naming `where`.
 
-def _int(v, name, minimum=1):
-    if isinstance(v, (bool, np.bool_)) or not isinstance(v, (int, np.integer)) or v < minimum:
-        raise ValueError(f"{name} must be an integer >= {minimum}, not {v!r}")
+def _is_bool(v):
+    return isinstance(v, (bool, np.bool_))
+
+
+def _kind_count(v, where):
+    """A positive integer (booleans are not integers here)."""
+    if _is_bool(v) or not isinstance(v, (int, np.integer)) or v <= 0:
+        raise ValueError(f"{where}: expected a positive integer, got {v!r}")
     return int(v)
 
 
-def _real(v, name, *, positive=False, nonnegative=False):
-    if isinstance(v, (bool, np.bool_)) or not isinstance(v, (int, float, np.integer, np.floating)):
-        raise ValueError(f"{name} must be a real number, not {v!r}")
-    v = float(v)
-    if not math.isfinite(v) or (positive and v <= 0) or (nonnegative and v < 0):
-        qual = " and positive" if positive else " and nonnegative" if nonnegative else ""
-        raise ValueError(f"{name} must be finite{qual}, not {v!r}")
-    return v
+def _finite(v, where):
+    if _is_bool(v) or not isinstance(v, (int, float, np.integer, np.floating)) or not math.isfinite(float(v)):
+        raise ValueError(f"{where}: expected a finite real number, got {v!r}")
+    return float(v)
 
 
-def _str(v, name):
-    if not isinstance(v, str):
-        raise ValueError(f"{name} must be a string, not {v!r}")
-    return v
+def _kind_real(v, where):
+    return _finite(v, where)
 
 
-def _bool(v, name):
-    if not isinstance(v, (bool, np.bool_)):
-        raise ValueError(f"{name} must be true or false, not {v!r}")
-    return bool(v)
-
-
-def _sym(v, name):
-    if v not in SYMMETRIES:
-        raise ValueError(f"{name} must be one of {SYMMETRIES}, not {v!r}")
-    return v
-
-
-def _opt(conv, v, name, **kw):
-    return None if v is None else conv(v, name, **kw)
-
-
-def _model_check(model, mass):
-    if not model:
-        raise ValueError("the model name is empty")
-    if model == "phi4" and mass != 1.0:
-        raise ValueError(f"model phi4 has no mass parameter (its normal-ordering mass is 1); mass = {mass!r} refused")
-
-
-def _integration(t, name):
-    if not isinstance(t, dict):
-        raise ValueError(f"{name} must be a table")
-    try:
-        return Integration(_int(t["n_quad"], f"{name}.n_quad"),
-                           _real(t["max_point"], f"{name}.max_point", positive=True),
-                           _real(t["atol"], f"{name}.atol", positive=True),
-                           _real(t["rtol"], f"{name}.rtol", positive=True),
-                           _opt(_int, t.get("maxiters"), f"{name}.maxiters"))
-    except KeyError as err:
-        raise ValueError(f"{name} has no {err.args[0]}") from None
-
-
-def _manifold(t, name):
-    if not isinstance(t, dict):
-        raise ValueError(f"{name} must be a table")
-    try:
-        return Manifold(_real(t["metric_reg"], f"{name}.metric_reg", nonnegative=True),
-                        _real(t["precond_reg"], f"{name}.precond_reg", nonnegative=True),
-                        _opt(_real, t.get("precond_reg_prefactor"), f"{name}.precond_reg_prefactor",
-                             nonnegative=True))
-    except KeyError as err:
-        raise ValueError(f"{name} has no {err.args[0]}") from None
-
-
-def _matrix(v, name, d):
-    x = np.asarray(v)
-    if x.shape != (d, d) or not np.issubdtype(x.dtype, np.number):
-        raise ValueError(f"{name} must be a {d}x{d} matrix, not of shape {x.shape} and type {x.dtype}")
-    x = np.ascontiguousarray(x, dtype=np.complex128)
-    if not np.isfinite(x).all():
-        raise ValueError(f"{name} holds nonfinite values")
+def _kind_positive(v, where):
+    x = _finite(v, where)
+    if x <= 0.0:
+        raise ValueError(f"{where}: expected a real number > 0, got {v!r}")
     return x
 
 
-# ---------------------------------------------------------------------------- JLD2
+def _kind_nonneg(v, where):
+    x = _finite(v, where)
+    if x < 0.0:
+        raise ValueError(f"{where}: expected a real number >= 0, got {v!r}")
+    return x
 
-def _jld2_complex(ds):
-    raw = ds[()]
-    out = np.empty(np.shape(raw), dtype=np.complex128)
-    out.real, out.imag = raw["re"], raw["im"]
+
+def _kind_text(v, where):
+    if not isinstance(v, str):
+        raise ValueError(f"{where}: expected a string, got {v!r}")
+    return v
+
+
+def _kind_flag(v, where):
+    if not _is_bool(v):
+        raise ValueError(f"{where}: expected true or false, got {v!r}")
+    return bool(v)
+
+
+def _kind_symmetry(v, where):
+    if v not in SYMMETRIES:
+        raise ValueError(f"{where}: expected one of {', '.join(SYMMETRIES)}, got {v!r}")
+    return v
+
+
+# ------------------------------------------------------------------------------- the schema
+# (key, kind, required); the order is the order in which write_portable writes the keys.
+_INTEGRATION = (("n_quad", _kind_count, True), ("max_point", _kind_positive, True),
+                ("atol", _kind_positive, True), ("rtol", _kind_positive, True),
+                ("maxiters", _kind_count, False))
+_MANIFOLD = (("metric_reg", _kind_nonneg, True), ("precond_reg", _kind_nonneg, True),
+             ("precond_reg_prefactor", _kind_nonneg, False))
+_FORMAT1 = (("D", _kind_count, True), ("model", _kind_text, True), ("coupling", _kind_real, True),
+            ("mass", _kind_real, False), ("symmetry", _kind_symmetry, False), ("energy", _kind_real, False),
+            ("gradient_norm", _kind_nonneg, False), ("phi", _kind_real, False),
+            ("validation_passed", _kind_flag, False), ("producer", _kind_text, False),
+            ("source", _kind_text, False), ("info", _kind_text, False))
+_TABLES = {"integration": (_INTEGRATION, Integration), "manifold": (_MANIFOLD, Manifold)}
+_RESERVED = {"format", "format_version", *(k for k, _, _ in _FORMAT1), *_TABLES}
+
+
+def _parse(schema, table, where):
+    """Checked values of `schema`'s keys found in `table` (absent optional keys are None)."""
+    if not isinstance(table, dict):
+        raise ValueError(f"{where}: expected a table")
+    out = {}
+    for key, kind, required in schema:
+        if key in table:
+            out[key] = kind(table[key], f"{where} {key}")
+        elif required:
+            raise ValueError(f"{where}: the required key {key!r} is absent")
+        else:
+            out[key] = None
     return out
 
 
-def _jld2_string(f, name):
-    try:
-        v = f[name][()]
-    except (KeyError, OSError):
-        if name not in f:
-            raise
-        return ""
-    return v.decode() if isinstance(v, (bytes, np.bytes_)) else str(v)
+def _parse_table(name, table, where):
+    schema, cls = _TABLES[name]
+    return cls(**_parse(schema, table, where))
 
 
-def read_jld2(path):
-    """Read an rcmps_store checkpoint (JLD2 schema 1). rho is not stored (None)."""
-    import h5py   # optional dependency
-
-    with h5py.File(path, "r") as f:
-        if int(f["schema_version"][()]) != 1:
-            raise ValueError("unsupported schema")
-        R, K = _jld2_complex(f["R"]).T, _jld2_complex(f["K"]).T
-        coupling = _jld2_complex(f["coupling"])
-        model = _jld2_string(f, "model")
-        mass = float(f["mass"][()]) if "mass" in f else 1.0
-        e0 = float(f["e0"][()])
-        grad = _jld2_complex(f["grad"]).T if "grad" in f else None
-        info = _jld2_string(f, "info") if "info" in f else None
-        row = f["integration"][()]
-        integ = Integration(int(row["n_quad"]), float(row["max_point"]), float(row["atol"]), float(row["rtol"]),
-                            int(row["maxiters"]) if "maxiters" in row.dtype.names else None)
-        mrow = f["manifold"][()] if "manifold" in f else None
-        man = None if mrow is None else Manifold(
-            float(mrow["metric_reg"]), float(mrow["precond_reg"]),
-            float(mrow["precond_reg_prefactor"]) if "precond_reg_prefactor" in mrow.dtype.names else None)
-    if coupling.imag != 0:
-        raise ValueError("model coupling must be real")
-    _model_check(model, mass)
-    if R.ndim != 2 or R.shape[0] != R.shape[1] or R.shape[0] == 0:
-        raise ValueError("R must be nonempty and square")
-    d = R.shape[0]
-    evaluated = math.isfinite(e0)
-    return StateRecord(D=d, model=model, coupling=float(coupling.real), R=_matrix(R, "R", d), K=_matrix(K, "K", d),
-                       mass=mass, gradient=_matrix(grad, "grad", d) if evaluated and grad is not None else None,
-                       energy=e0 if evaluated else None, integration=integ, manifold=man, info=info, origin="jld2")
+def _check_model(model, mass):
+    if not model:
+        raise ValueError("model: the name is empty")
+    if model == "phi4" and mass != 1.0:
+        raise ValueError(f"mass: model phi4 is normal-ordered at mass 1 and takes no other mass (got {mass!r})")
 
 
-# ---------------------------------------------------------------------------- portable
-
-def _fields_format1(md):
-    if md["format"] != FORMAT:
-        raise ValueError(f"metadata.toml: format {md['format']!r} is not {FORMAT!r}")
-    ver = md.get("format_version")
-    if type(ver) is not int or ver != FORMAT_VERSION:
-        raise ValueError(f"metadata.toml: unsupported {FORMAT} format_version {ver!r} (this reader knows {FORMAT_VERSION})")
-    for key in ("D", "model", "coupling"):
-        if key not in md:
-            raise ValueError(f"metadata.toml: required key {key} is missing")
-    g = md.get
-    return dict(
-        D=_int(g("D"), "D"), model=_str(g("model"), "model"), coupling=_real(g("coupling"), "coupling"),
-        mass=_real(g("mass", 1.0), "mass"), energy=_opt(_real, g("energy"), "energy"),
-        gradient_norm=_opt(_real, g("gradient_norm"), "gradient_norm", nonnegative=True),
-        symmetry=_opt(_sym, g("symmetry"), "symmetry"), phi=_opt(_real, g("phi"), "phi"),
-        validation_passed=_opt(_bool, g("validation_passed"), "validation_passed"),
-        producer=_opt(_str, g("producer"), "producer"), source=_opt(_str, g("source"), "source"),
-        info=_opt(_str, g("info"), "info"),
-        integration=_opt(_integration, g("integration"), "[integration]"),
-        manifold=_opt(_manifold, g("manifold"), "[manifold]"), origin="portable"), "gradient.bin"
+def _square(m, where, d):
+    """A finite (d, d) complex128 C-ordered copy of `m`."""
+    a = np.asarray(m)
+    if a.shape != (d, d) or not (np.issubdtype(a.dtype, np.number) and not np.issubdtype(a.dtype, np.bool_)):
+        raise ValueError(f"{where}: expected a numeric {d}x{d} matrix, got shape {a.shape} of {a.dtype}")
+    a = np.ascontiguousarray(a, dtype=np.complex128)
+    if not np.isfinite(a).all():
+        raise ValueError(f"{where}: contains a NaN or infinite entry")
+    return a
 
 
-def _fields_legacy(md, directory):
-    g = md.get
-    for key in ("D", "coupling"):
-        if key not in md:
-            raise ValueError(f"metadata.toml: required key {key} is missing")
-    from_saved = False
+# ------------------------------------------------------------------------------- .bin files
 
-    def available(flag, default=True):
-        return g(flag, default) is not False
-
-    energy = g("energy")
-    if energy is None and "saved_energy" in md and available("saved_energy_available"):
-        energy, from_saved = g("saved_energy"), True
-    gname = "gradient.bin"
-    if not (directory / gname).exists():
-        gname = "saved_gradient.bin"
-        if (directory / gname).exists() and available("saved_gradient_available"):
-            from_saved = True
-        else:
-            gname = None
-    norm = g("gradient_norm")
-    if norm is None and "saved_gradient_norm" in md and available(
-            "saved_gradient_norm_available", available("saved_gradient_available")):
-        norm, from_saved = g("saved_gradient_norm"), True
-    if from_saved:
-        integ = _integration(g("saved_integration"), "[saved_integration]") if "saved_integration" in md else None
-    else:
-        n_quad = g("quadrature", g("n_quad"))
-        max_point = g("window", g("half_window", g("max_point")))
-        integ = None if n_quad is None and max_point is None else _integration(
-            dict(n_quad=n_quad, max_point=max_point, atol=g("atol"), rtol=g("rtol"), maxiters=g("maxiters")),
-            "metadata.toml (integration keys)")
-    man = (_manifold(md, "metadata.toml (metric_reg, precond_reg)")
-           if "metric_reg" in md and "precond_reg" in md else None)
-    return dict(D=_int(g("D"), "D"), model="phi4", coupling=_real(g("coupling"), "coupling"), mass=1.0,
-                energy=_opt(_real, energy, "energy"),
-                gradient_norm=_opt(_real, norm, "gradient_norm", nonnegative=True),
-                validation_passed=_opt(_bool, g("validation_passed"), "validation_passed"),
-                source=_opt(_str, g("source"), "source"), integration=integ, manifold=man,
-                origin="portable-legacy"), gname
+def _load_bin(path, d):
+    expect = 16 * d * d
+    have = path.stat().st_size
+    if have != expect:
+        raise ValueError(f"{path.name}: a {d}x{d} complex128 matrix takes {expect} bytes, the file has {have} bytes")
+    return _square(np.fromfile(path, dtype=_BIN).reshape(d, d, order="F"), path.name, d)
 
 
-def _read_bin(path, d):
-    size = path.stat().st_size
-    if size != 16 * d * d:
-        raise ValueError(f"{path.name} has {size} bytes, not the {16 * d * d} of a {d}x{d} complex128 matrix")
-    return _matrix(np.fromfile(path, dtype="<c16").reshape((d, d), order="F"), path.name, d)
+def _store_bin(path, m):
+    np.asfortranarray(m).ravel(order="K").astype(_BIN).tofile(path)
+
+
+# ------------------------------------------------------------------------------- dialects
+
+def _format1(md, directory):
+    """Fields of a format-1 metadata table, and the name of its gradient file."""
+    if md.get("format") != FORMAT:
+        raise ValueError(f"metadata.toml: format is {md.get('format')!r}; this reader reads {FORMAT!r}")
+    version = md.get("format_version")
+    if type(version) is not int or version != FORMAT_VERSION:
+        raise ValueError(f"metadata.toml: format_version {version!r} is not supported "
+                         f"(known: {FORMAT_VERSION})")
+    fields = _parse(_FORMAT1, md, "metadata.toml")
+    if fields["mass"] is None:
+        fields["mass"] = 1.0
+    for name in _TABLES:
+        fields[name] = _parse_table(name, md[name], f"[{name}]") if name in md else None
+    fields["origin"] = "portable"
+    return fields, "gradient.bin"
+
+
+class _Legacy:
+    """The research dialect: metadata without `format`. A value is read under its format-1 name
+    first; otherwise, when a saved_* copy exists and its availability flag is not false, the
+    saved copy is used and the record's integration settings become [saved_integration]."""
+
+    def __init__(self, md, directory):
+        self.md, self.dir, self.saved = md, directory, False
+
+    def _available(self, flag, default=True):
+        return self.md.get(flag, default) is not False
+
+    def _scalar(self, name, flag, flag_default=True):
+        if name in self.md:
+            return self.md[name]
+        if f"saved_{name}" in self.md and self._available(flag, flag_default):
+            self.saved = True
+            return self.md[f"saved_{name}"]
+        return None
+
+    def _gradient_file(self):
+        if (self.dir / "gradient.bin").exists():
+            return "gradient.bin"
+        if (self.dir / "saved_gradient.bin").exists() and self._available("saved_gradient_available"):
+            self.saved = True
+            return "saved_gradient.bin"
+        return None
+
+    def _integration(self):
+        md = self.md
+        if self.saved:
+            return _parse_table("integration", md["saved_integration"], "[saved_integration]") \
+                if "saved_integration" in md else None
+        n_quad = next((md[k] for k in ("quadrature", "n_quad") if k in md), None)
+        window = next((md[k] for k in ("window", "half_window", "max_point") if k in md), None)
+        if n_quad is None and window is None:
+            return None
+        table = {"n_quad": n_quad, "max_point": window, **{k: md[k] for k in ("atol", "rtol", "maxiters") if k in md}}
+        return _parse_table("integration", {k: v for k, v in table.items() if v is not None},
+                            "metadata.toml integration keys")
+
+    def fields(self):
+        md = self.md
+        for key in ("D", "coupling"):
+            if key not in md:
+                raise ValueError(f"metadata.toml: the required key {key!r} is absent")
+        energy = self._scalar("energy", "saved_energy_available")
+        gradient_file = self._gradient_file()
+        norm = self._scalar("gradient_norm", "saved_gradient_norm_available",
+                            self._available("saved_gradient_available"))
+        manifold = (_parse_table("manifold", md, "metadata.toml manifold keys")
+                    if "metric_reg" in md and "precond_reg" in md else None)
+        opt = lambda kind, v, where: None if v is None else kind(v, where)
+        fields = dict(D=_kind_count(md["D"], "metadata.toml D"), model="phi4",
+                      coupling=_kind_real(md["coupling"], "metadata.toml coupling"), mass=1.0,
+                      energy=opt(_kind_real, energy, "metadata.toml energy"),
+                      gradient_norm=opt(_kind_nonneg, norm, "metadata.toml gradient_norm"),
+                      validation_passed=opt(_kind_flag, md.get("validation_passed"), "metadata.toml validation_passed"),
+                      source=opt(_kind_text, md.get("source"), "metadata.toml source"),
+                      integration=self._integration(), manifold=manifold, origin="portable-legacy")
+        return fields, gradient_file
 
 
 def read_portable(directory, *, arrays=True):
-    """Read a portable state directory (format 1 or a research dialect). With arrays=False only
-    metadata.toml is read and checked."""
+    """Read a portable state directory (format 1, or the research dialect when metadata.toml
+    has no `format`). With arrays=False only metadata.toml is read and checked, and the
+    matrices stay None."""
     directory = Path(directory)
-    with (directory / "metadata.toml").open("rb") as stream:
-        md = tomllib.load(stream)
-    fields, gname = _fields_format1(md) if "format" in md else _fields_legacy(md, directory)
-    _model_check(fields["model"], fields["mass"])
-    names = dict(R="R.bin", K="K.bin", rho="rho.bin", gradient=gname)
-    names = {k: v for k, v in names.items() if v is not None and (k in ("R", "K") or (directory / v).exists())}
-    files = ("metadata.toml", *names.values())
+    with open(directory / "metadata.toml", "rb") as fh:
+        md = tomllib.load(fh)
+    fields, gradient_file = _format1(md, directory) if "format" in md else _Legacy(md, directory).fields()
+    _check_model(fields["model"], fields["mass"])
+    matrix_files = {"R": "R.bin", "K": "K.bin"}
+    for name, fname in (("rho", "rho.bin"), ("gradient", gradient_file)):
+        if fname is not None and (directory / fname).exists():
+            matrix_files[name] = fname
     if arrays:
-        fields.update({k: _read_bin(directory / v, fields["D"]) for k, v in names.items()})
-    return StateRecord(**fields, files=files, metadata=md)
+        for name, fname in matrix_files.items():
+            fields[name] = _load_bin(directory / fname, fields["D"])
+    return StateRecord(**fields, files=("metadata.toml", *matrix_files.values()), metadata=md)
 
 
-def _toml_str(text):
-    esc = {'"': '\\"', "\\": "\\\\", "\b": "\\b", "\t": "\\t", "\n": "\\n", "\f": "\\f", "\r": "\\r"}
-    return '"' + "".join(esc.get(c, f"\\u{ord(c):04X}" if ord(c) < 0x20 or ord(c) == 0x7F else c) for c in text) + '"'
+# ------------------------------------------------------------------------------- writing
 
-
-def _toml_val(v, name):
-    if isinstance(v, (bool, np.bool_)):
+def _toml_scalar(v, where):
+    if _is_bool(v):
         return "true" if v else "false"
     if isinstance(v, (int, np.integer)):
         return str(int(v))
     if isinstance(v, (float, np.floating)):
-        return repr(_real(v, name))
+        return repr(_kind_real(v, where))
     if isinstance(v, str):
-        return _toml_str(v)
-    raise TypeError(f"{name}: a metadata value must be a string, boolean, integer or real, not {v!r}")
+        out = ['"']
+        for ch in v:
+            if ch in '"\\':
+                out.append("\\" + ch)
+            elif ord(ch) < 0x20 or ord(ch) == 0x7F:
+                out.append({"\n": "\\n", "\t": "\\t", "\r": "\\r"}.get(ch, f"\\u{ord(ch):04X}"))
+            else:
+                out.append(ch)
+        return "".join(out) + '"'
+    raise TypeError(f"{where}: metadata values are strings, booleans, integers or reals, not {type(v).__name__}")
 
 
-def _toml_table(name, values):
-    rows = [f"{k} = {_toml_val(v, f'{name}.{k}')}" for k, v in values.items() if v is not None]
-    return f"\n[{name}]\n" + "".join(r + "\n" for r in rows)
+def _render(schema, values, where):
+    """`key = value` lines of the non-None values, checked by the schema's kinds."""
+    lines = []
+    for key, kind, required in schema:
+        v = values.get(key)
+        if v is None:
+            if required:
+                raise ValueError(f"{where}: {key} is required")
+            continue
+        lines.append(f"{key} = {_toml_scalar(kind(v, f'{where} {key}'), f'{where} {key}')}")
+    return lines
 
 
 def write_portable(directory, record, *, extra=None, extra_matrices=None):
-    """Write `record` as a new format-1 directory (refused if it exists); .bin files first,
-    metadata.toml last by rename. Returns the directory."""
+    """Write `record` as a new format-1 directory; an existing directory is refused
+    (FileExistsError). `extra` adds top-level keys and `extra_matrices` further D x D .bin
+    files. The .bin files are written first and metadata.toml last, by an atomic rename, so a
+    reader never sees a metadata file without its matrices. Returns the directory."""
     directory = Path(directory)
-    d = _int(record.D, "D")
+    d = _kind_count(record.D, "D")
     if record.R is None or record.K is None:
-        raise ValueError("R and K are required")
-    mats = {n: _matrix(getattr(record, n), n, d) for n in MATRICES if getattr(record, n) is not None}
-    for n, m in (extra_matrices or {}).items():
-        if n in MATRICES or not re.fullmatch(r"[A-Za-z0-9_]+", n):
-            raise ValueError(f"extra matrix name {n!r} is not allowed")
-        mats[n] = _matrix(m, n, d)
-    model, mass = _str(record.model, "model"), _real(record.mass, "mass")
-    _model_check(model, mass)
-    head = dict(format=FORMAT, format_version=FORMAT_VERSION, D=d, model=model,
-                coupling=_real(record.coupling, "coupling"), mass=mass,
-                symmetry=_opt(_sym, record.symmetry, "symmetry"), energy=_opt(_real, record.energy, "energy"),
-                gradient_norm=_opt(_real, record.gradient_norm, "gradient_norm", nonnegative=True),
-                phi=_opt(_real, record.phi, "phi"),
-                validation_passed=_opt(_bool, record.validation_passed, "validation_passed"),
-                producer=_opt(_str, record.producer, "producer"), source=_opt(_str, record.source, "source"),
-                info=_opt(_str, record.info, "info"))
-    for key in extra or {}:
-        if key in KEYS or not re.fullmatch(r"[A-Za-z0-9_-]+", key):
-            raise ValueError(f"extra metadata key {key!r} is not allowed")
-    text = "".join(f"{k} = {_toml_val(v, k)}\n" for k, v in {**head, **(extra or {})}.items() if v is not None)
-    if record.integration is not None:
-        i = record.integration
-        text += _toml_table("integration", dict(
-            n_quad=_int(i.n_quad, "integration.n_quad"),
-            max_point=_real(i.max_point, "integration.max_point", positive=True),
-            atol=_real(i.atol, "integration.atol", positive=True),
-            rtol=_real(i.rtol, "integration.rtol", positive=True),
-            maxiters=_opt(_int, i.maxiters, "integration.maxiters")))
-    if record.manifold is not None:
-        m = record.manifold
-        text += _toml_table("manifold", dict(
-            metric_reg=_real(m.metric_reg, "manifold.metric_reg", nonnegative=True),
-            precond_reg=_real(m.precond_reg, "manifold.precond_reg", nonnegative=True),
-            precond_reg_prefactor=_opt(_real, m.precond_reg_prefactor, "manifold.precond_reg_prefactor",
-                                       nonnegative=True)))
-    tomllib.loads(text)
+        raise ValueError("write_portable: R and K are required")
+    matrices = {}
+    for name in ("R", "K", "rho", "gradient"):
+        if getattr(record, name) is not None:
+            matrices[name] = _square(getattr(record, name), name, d)
+    for name, m in (extra_matrices or {}).items():
+        if name in matrices or name in ("R", "K", "rho", "gradient") or not _NAME.match(name):
+            raise ValueError(f"write_portable: {name!r} cannot name an extra matrix")
+        matrices[name] = _square(m, name, d)
+    values = {key: getattr(record, key) for key, _, _ in _FORMAT1}
+    values["mass"] = 1.0 if record.mass is None else record.mass
+    _check_model(_kind_text(values["model"], "model"), _kind_real(values["mass"], "mass"))
+    lines = [f'format = "{FORMAT}"', f"format_version = {FORMAT_VERSION}"]
+    lines += _render(_FORMAT1, values, "metadata")
+    for key, v in (extra or {}).items():
+        if key in _RESERVED or not re.fullmatch(r"[A-Za-z0-9_-]+", key):
+            raise ValueError(f"write_portable: {key!r} cannot be an extra metadata key")
+        lines.append(f"{key} = {_toml_scalar(v, key)}")
+    for name, (schema, _) in _TABLES.items():
+        obj = getattr(record, name)
+        if obj is not None:
+            lines += ["", f"[{name}]"] + _render(schema, obj.__dict__, f"[{name}]")
+    text = "\n".join(lines) + "\n"
+    tomllib.loads(text)                     # what is written must read back
     directory.mkdir(parents=True, exist_ok=False)
-    for n, m in mats.items():
-        m.ravel(order="F").astype("<c16").tofile(directory / f"{n}.bin")
-    tmp = directory / ".metadata.toml.tmp"
-    tmp.write_bytes(text.encode("utf-8"))
-    os.replace(tmp, directory / "metadata.toml")
+    for name, m in matrices.items():
+        _store_bin(directory / f"{name}.bin", m)
+    staging = directory / ".metadata.toml.partial"
+    staging.write_text(text, encoding="utf-8")
+    os.replace(staging, directory / "metadata.toml")
     return directory
+
+
+# ------------------------------------------------------------------------------- JLD2
+
+def read_jld2(path):
+    """Read an rcmps_store checkpoint (JLD2 schema_version 1) with h5py. rho is not stored
+    (rcmps_load recomputes it), so the record's rho is None; energy and gradient are None for a
+    state that was never evaluated (e0 not finite)."""
+    import h5py                             # optional dependency
+
+    def cplx(node):
+        raw = node[()]
+        return np.asarray(raw["re"]) + 1j * np.asarray(raw["im"])
+
+    def text(f, key):
+        if key not in f:
+            return None
+        raw = f[key][()]
+        return raw.decode() if isinstance(raw, (bytes, np.bytes_)) else str(raw)
+
+    def row_table(raw, schema, cls):
+        names = raw.dtype.names
+        return cls(**{key: (None if key not in names else
+                            int(raw[key]) if kind is _kind_count else float(raw[key]))
+                      for key, kind, _ in schema})
+
+    with h5py.File(path, "r") as f:
+        if int(f["schema_version"][()]) != 1:
+            raise ValueError(f"{path}: only schema_version 1 checkpoints are read")
+        R, K = cplx(f["R"]).T, cplx(f["K"]).T
+        coupling = complex(cplx(f["coupling"]))
+        model = text(f, "model") or ""
+        mass = float(f["mass"][()]) if "mass" in f else 1.0
+        e0 = float(f["e0"][()])
+        grad = cplx(f["grad"]).T if "grad" in f else None
+        info = text(f, "info")
+        integration = row_table(f["integration"][()], _INTEGRATION, Integration)
+        manifold = row_table(f["manifold"][()], _MANIFOLD, Manifold) if "manifold" in f else None
+    if coupling.imag != 0.0:
+        raise ValueError(f"{path}: the coupling is not real ({coupling})")
+    _check_model(model, mass)
+    if R.ndim != 2 or R.shape[0] != R.shape[1] or R.shape[0] == 0:
+        raise ValueError(f"{path}: R is not a nonempty square matrix")
+    d = R.shape[0]
+    evaluated = math.isfinite(e0)
+    return StateRecord(D=d, model=model, coupling=coupling.real, R=_square(R, "R", d), K=_square(K, "K", d), mass=mass,
+                       gradient=_square(grad, "grad", d) if evaluated and grad is not None else None,
+                       energy=e0 if evaluated else None, integration=integration, manifold=manifold, info=info,
+                       origin="jld2")

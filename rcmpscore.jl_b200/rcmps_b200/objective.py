@@ -155,14 +155,18 @@ def _raise_for(status, ctx, stats, what):
     raise SolverFailure(msg)
 
 
-def fg_phi4_batch(R, K, rho, couplings, settings=None, *, device=None, return_parts=False):
+def fg_phi4_batch(R, K, rho, couplings, settings=None, *, device=None, return_parts=False, tolerances=None):
     """phi^4 energies and finished gradients of a batch of states (lists of D_i x D_i matrices,
     uneven D allowed). Returns (energies [n], gradients [n matrices], stats [n dicts]); with
-    return_parts also the raw covectors and environments."""
+    return_parts also the raw covectors and environments. `tolerances`: optional per-state
+    (atol, rtol) pairs of the quartic trajectories (rcmps_fg_phi4_batch_controls), so that states
+    with mixed tolerance pairs share one launch."""
     import torch
     n = len(R)
     if not (len(K) == len(rho) == len(couplings) == n):
         raise ValueError("R, K, rho and couplings must have the same length")
+    if tolerances is not None and len(tolerances) != n:
+        raise ValueError("tolerances must hold one (atol, rtol) pair per state")
     dims = [_check_matrices(R[i], K[i], rho[i]) for i in range(n)]
     ctx = context(device)
     s = settings if settings is not None else _lib.default_settings()
@@ -173,10 +177,14 @@ def fg_phi4_batch(R, K, rho, couplings, settings=None, *, device=None, return_pa
     cov = torch.zeros(total, dtype=torch.complex128, device="cuda") if return_parts else None
     env = torch.zeros(total, dtype=torch.complex128, device="cuda") if return_parts else None
     stats = (_lib.StateStats * n)()
-    rc = ctx.lib.rcmps_fg_phi4_batch(ctx.handle, n, (C.c_int * n)(*dims), (C.c_double * n)(*map(float, couplings)),
-                                     dR.data_ptr(), dK.data_ptr(), dP.data_ptr(), C.byref(s), energy.data_ptr(),
-                                     grad.data_ptr(), cov.data_ptr() if cov is not None else None,
-                                     env.data_ptr() if env is not None else None, stats, _stream())
+    controls = None
+    if tolerances is not None:
+        controls = (_lib.StateControls * n)(*(_lib.StateControls(float(a), float(r)) for a, r in tolerances))
+    rc = ctx.lib.rcmps_fg_phi4_batch_controls(ctx.handle, n, (C.c_int * n)(*dims),
+                                              (C.c_double * n)(*map(float, couplings)), dR.data_ptr(), dK.data_ptr(),
+                                              dP.data_ptr(), C.byref(s), controls, energy.data_ptr(),
+                                              grad.data_ptr(), cov.data_ptr() if cov is not None else None,
+                                              env.data_ptr() if env is not None else None, stats, _stream())
     if rc:
         bad = next((i for i in range(n) if stats[i].status), 0)
         _raise_for(rc, ctx, stats[bad], "fg_phi4")

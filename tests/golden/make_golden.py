@@ -1,7 +1,8 @@
 """Generate the golden vectors of tests/golden/ by running RcmpsCore.jl's own NumPy path.
 
-This script imports the reference package rcmps_gpu read-only from a local checkout
-(default /root/reference/gpu/src; override with RCMPS_REFERENCE_SRC) and writes .npz files:
+This script imports the reference package rcmps_gpu read-only from a local checkout of the
+reference (its gpu/src directory, given as --reference PATH or in the environment variable
+RCMPS_REFERENCE_SRC; there is no default) and writes .npz files:
   small.npz     D = 4, 6, 8 random and D = 8 Z2 states at W = 30, n_quad = 64, 128 kinetic nodes
   d16.npz       one D = 16 random state at the optimizer defaults (W = 30, n_quad = 512, 512 nodes)
   d64.npz       the seed-42 D = 64 random state at the optimizer defaults
@@ -22,6 +23,14 @@ This script imports the reference package rcmps_gpu read-only from a local check
                 (W = 30, n_quad = 512, 512 kinetic nodes: the optimizer defaults, with the
                 kinetic term and the finished gradient), and the packed trajectory samples of a
                 D = 4 Z2 state at W = 2, n_quad = 16
+  d32batch.npz  the first 8 states of the 64-state D = 32 batch workload (random seeds 0..7,
+                couplings g ~ U[0.5, 3] from default_rng(12345)) at the optimizer defaults
+  bench.npz     four states of the 32-state D = 64 benchmark workload at the optimizer defaults:
+                random seeds 0 and 1 (unpacked reduced route) and Z2 seeds 100 and 101 (the
+                packed route, with the reference's own stationary density), each with the kinetic
+                term and the finished gradient
+  uneven.npz    states 0, 1, 2, 4, 5, 6 (D = 16, 32, 48) of the uneven 200-state workload, each at
+                its own drawn (atol, rtol) pair, W = 30, n_quad = 512, 512 kinetic nodes
   ode.npz       the all-ODE route (evaluate_phi4: kinetic1 + kinetic2 + g phi^4 as 26 channels):
                 D = 3 (W = 6, n_quad = 24), D = 8 random and Z2 (W = 20, n_quad = 64) and
                 D = 16 (W = 20, n_quad = 192, the Julia defaults of the fixture)
@@ -33,8 +42,9 @@ is the reference's test/fixtures/phi4_g2_D16_z2_portable (exported by RcmpsCore 
 
 States: NumPy PCG64 default_rng(seed); R and A with i.i.d. standard complex Gaussian entries
 times 0.2 (R drawn first), K = (A + A^dag)/2; Z2 states draw blocks in the order k1, k2, R12, R21.
-Run: python tests/golden/make_golden.py [name ...]  (all files by default, about a minute; the
-D = 64 record dominates; names: small d16 d64 samples ode packed phi optim finish)
+Run: python tests/golden/make_golden.py --reference PATH/gpu/src [name ...]  (all files by
+default; names: small d16 d64 samples ode packed phi optim finish d32batch bench uneven; the D = 64
+records dominate, about a minute each on one core)
 """
 from __future__ import annotations
 
@@ -47,10 +57,19 @@ from pathlib import Path
 import numpy as np
 
 HERE = Path(__file__).resolve().parent
-sys.path.insert(0, os.environ.get("RCMPS_REFERENCE_SRC", "/root/reference/gpu/src"))
-from rcmps_gpu.optimizer.runtime import kinetic_backend as kb  # noqa: E402
-from rcmps_gpu.optimizer.runtime import numerics as nm  # noqa: E402
-from rcmps_gpu.optimizer.runtime import ode_backend as ob  # noqa: E402
+kb = nm = ob = None     # the reference's runtime modules, imported by _import_reference
+
+
+def _import_reference(path):
+    """Import rcmps_gpu's runtime modules from the reference checkout at `path` (gpu/src)."""
+    global kb, nm, ob
+    if not path:
+        raise SystemExit("give the reference's gpu/src directory: --reference PATH or RCMPS_REFERENCE_SRC")
+    if not (Path(path) / "rcmps_gpu").is_dir():
+        raise SystemExit(f"{path} holds no rcmps_gpu package")
+    sys.path.insert(0, str(path))
+    from rcmps_gpu.optimizer.runtime import kinetic_backend, numerics, ode_backend
+    kb, nm, ob = kinetic_backend, numerics, ode_backend
 
 
 def draw(rng, n):
@@ -74,16 +93,16 @@ def z2_state(d, seed, scale=0.2):
     return r, k
 
 
-def evaluate(r, k, g, window, nq, nodes):
+def evaluate(r, k, g, window, nq, nodes, atol=1e-13, rtol=1e-12):
     q = -1j * k - r.conj().T @ r / 2
     rho, _ = nm.stationary_state(q, r, tolerance=1e-13)
-    quartic = ob.evaluate_quartic(r, q, rho, g, xp=np, half_window=window, n_quad=nq, atol=1e-13, rtol=1e-12,
+    quartic = ob.evaluate_quartic(r, q, rho, g, xp=np, half_window=window, n_quad=nq, atol=atol, rtol=rtol,
                                   reduced=True)
     kinetic = kb.kinetic_raw(q, r, rho, nodes, xp=np, tolerance=1e-12, maxdim=1024)
     cov = quartic["covector"] + kinetic["covector"]
     env = quartic["environment"] + kinetic["environment"]
     grad, _ = nm.finish_gradient(q, r, rho, cov, env, metric_reg=1e-3)
-    return dict(R=r, K=k, rho=rho, g=g, window=window, n_quad=nq, nodes=nodes,
+    return dict(R=r, K=k, rho=rho, g=g, window=window, n_quad=nq, nodes=nodes, atol=atol, rtol=rtol,
                 quartic_value=quartic["value"], quartic_covector=quartic["covector"],
                 quartic_environment=quartic["environment"],
                 accepted=quartic["stats"]["accepted_steps"], rejected=quartic["stats"]["rejected_steps"],
@@ -220,6 +239,18 @@ def main(names):
                             finish_record(*z2_state(16, 826), 3)])
     if "optim" in names:
         save("optim.npz", [optim_run()])
+    if "d32batch" in names:
+        gs = np.random.default_rng(12345).uniform(0.5, 3.0, 64)
+        save("d32batch.npz", [evaluate(*random_state(32, seed), float(gs[seed]), 30.0, 512, 512) for seed in range(8)])
+    if "uneven" in names:
+        draws = uneven_draws(20)
+        save("uneven.npz", [dict(evaluate(*random_state(d, seed), g, 30.0, 512, 512, atol, rtol), index=i)
+                            for i, (d, seed, g, atol, rtol) in enumerate(draws) if i in UNEVEN_PINNED])
+    if "bench" in names:
+        save("bench.npz", [evaluate(*random_state(64, 0), 2.0, 30.0, 512, 512),
+                           evaluate(*random_state(64, 1), 2.0, 30.0, 512, 512),
+                           evaluate_packed(*z2_state(64, 100), 2.0, 30.0, 512, 512),
+                           evaluate_packed(*z2_state(64, 101), 2.0, 30.0, 512, 512)])
     if "packed" in names:
         save("packed.npz", [evaluate_packed(*z2_state(4, 604), 1.5, 30.0, 64),
                             evaluate_packed(*z2_state(8, 508), 2.0, 30.0, 64),
@@ -242,5 +273,31 @@ def samples_d5():
                         accepted=stats["accepted_steps"], rejected=stats["rejected_steps"])
 
 
+UNEVEN_PINNED = (0, 1, 2, 4, 5, 6)
+
+
+def uneven_draws(count, seed=2024):
+    """(D, state seed, g, atol, rtol) of the uneven workload's first `count` states: one
+    default_rng(seed) stream draws, state by state, D from {16, 32, 48, 64, 96, 128}, g ~ U[0.5, 3]
+    and atol, rtol from {1e-10, 1e-12}; state i is random_state(D, 4000 + i)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        d = int(rng.choice((16, 32, 48, 64, 96, 128)))
+        g = float(rng.uniform(0.5, 3.0))
+        atol, rtol = float(rng.choice((1e-10, 1e-12))), float(rng.choice((1e-10, 1e-12)))
+        out.append((d, 4000 + i, g, atol, rtol))
+    return out
+
+
+ALL = ["small", "d16", "d64", "ode", "samples", "packed", "phi", "optim", "finish", "d32batch", "bench", "uneven"]
+
 if __name__ == "__main__":
-    main(sys.argv[1:] or ["small", "d16", "d64", "ode", "samples", "packed", "phi", "optim", "finish"])
+    import argparse
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--reference", default=os.environ.get("RCMPS_REFERENCE_SRC"),
+                    help="the reference's gpu/src directory (default: $RCMPS_REFERENCE_SRC)")
+    ap.add_argument("names", nargs="*", choices=ALL + [[]], default=[])
+    a = ap.parse_args()
+    _import_reference(a.reference)
+    main(a.names or ALL)

@@ -194,7 +194,7 @@ def test_ode_route_matches_reference(gpu_context, index):
     R, K, rho, g = rec["R"], rec["K"], rec["rho"], rec["g"]
     Q = O.left_canonical_q(R, K)
     out = objective.evaluate_phi4(R, Q, rho, g, half_window=rec["window"], n_quad=int(rec["n_quad"]))
-    assert abs(out["stats"]["accepted"] - rec["accepted"]) <= 2 and abs(out["stats"]["rejected"] - rec["rejected"]) <= 2
+    assert (out["stats"]["accepted"], out["stats"]["rejected"]) == (rec["accepted"], rec["rejected"])
     assert abs(out["value"] - rec["value"]) <= ENERGY_TOL * abs(rec["value"])
     assert np.abs(out["covector"] - rec["covector"]).max() <= 1e-10 * max(1.0, np.abs(rec["covector"]).max())
     assert np.abs(out["environment"] - rec["environment"]).max() <= 1e-10 * max(1.0, np.abs(rec["environment"]).max())

@@ -26,12 +26,8 @@ def test_phi_by_ode_matches_reference(gpu_context, index):
     controls = SimpleNamespace(window=rec["window"], quadrature=int(rec["n_quad"]), atol=rec["atol"],
                                rtol=rec["rtol"], max_steps=1_000_000)
     value, stats = validate.phi_by_ode(rec["R"], rec["K"], rec["rho"], controls)
-    # as on the all-ODE route, a step-size decision taken at rounding level may add or drop a
-    # step; the value then differs by the integration error, within the energy parity bar
-    same = (stats["accepted_steps"], stats["rejected_steps"]) == (rec["accepted"], rec["rejected"])
-    assert abs(stats["accepted_steps"] - rec["accepted"]) <= 2
-    tol = 1e-12 if same else 1e-10
-    assert abs(value - rec["phi_ode"]) <= tol * max(1.0, abs(rec["phi_ode"]))
+    assert (stats["accepted_steps"], stats["rejected_steps"]) == (rec["accepted"], rec["rejected"])
+    assert abs(value - rec["phi_ode"]) <= 1e-12 * max(1.0, abs(rec["phi_ode"]))
 
 
 @pytest.mark.gpu

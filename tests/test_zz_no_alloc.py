@@ -2,8 +2,13 @@
 
 Both are called through the C ABI on the same device inputs; the no-alloc entry is called twice
 in a row (its fixed device scratch is reused, so the second call checks that nothing carries
-over). This file is collected last so that it also runs after every other entry has used the
-device.
+over). It is also checked directly against the reference's own finished gradients
+(tests/golden/finish.npz: numerics.finish_gradient, metric_reg 1e-3, tolerance 1e-13). This
+file is collected last so that it also runs after every other entry has used the device.
+
+Every call runs on a dedicated non-default stream, and the device is synchronized after the
+inputs and outputs are created, so no fill kernel on torch's stream can land after a library
+write.
 """
 from __future__ import annotations
 
@@ -61,9 +66,11 @@ def test_noalloc_matches_batched_twice(gpu_context, case):
     lib = ctx.lib
     s = _lib.default_settings(metric_reg=1e-3, boundary_tolerance=1e-13)
     dR, dK, dP, dC, dE = (_dev(torch, x) for x in (R, K, rho, cov, env))
-    stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    side = torch.cuda.Stream()
+    stream = C.c_void_p(side.cuda_stream)
 
     ref = torch.zeros(d * d, dtype=torch.complex128, device="cuda")
+    torch.cuda.synchronize()
     st_ref = (_lib.StateStats * 1)()
     rc = lib.rcmps_finish_gradient_batch(ctx.handle, 1, (C.c_int * 1)(d), dR.data_ptr(), dK.data_ptr(),
                                          dP.data_ptr(), dC.data_ptr(), dE.data_ptr(), C.byref(s), ref.data_ptr(),
@@ -73,6 +80,7 @@ def test_noalloc_matches_batched_twice(gpu_context, case):
     scale = max(1.0, _metric_norm(rho, ref_h))
     for call in range(2):
         got = torch.full((d * d,), float("nan"), dtype=torch.complex128, device="cuda")
+        torch.cuda.synchronize()
         st = _lib.StateStats()
         rc = lib.rcmps_finish_gradient_noalloc(ctx.handle, d, dR.data_ptr(), dK.data_ptr(), dP.data_ptr(),
                                                dC.data_ptr(), dE.data_ptr(), C.byref(s), got.data_ptr(),
@@ -82,6 +90,33 @@ def test_noalloc_matches_batched_twice(gpu_context, case):
         assert _metric_norm(rho, got_h - ref_h) <= GRAD_TOL * scale, call
         assert st.gmres_iterations == st_ref[0].gmres_iterations
         assert abs(st.boundary_residual - st_ref[0].boundary_residual) <= 1e-3 * st_ref[0].boundary_residual + 1e-300
+
+
+@pytest.mark.parametrize("index", range(3))
+def test_noalloc_matches_reference_finish(gpu_context, index):
+    """The reference's finished gradient (numerics.finish_gradient: the no-jump preconditioned
+    boundary GMRES and the metric solve) on random states D = 8, 16 and a Z2 state D = 16, twice
+    in a row."""
+    import torch
+    from rcmps_b200 import _lib
+    rec = load_records("finish.npz")[index]
+    R, K, rho = rec["R"], rec["K"], rec["rho"]
+    d = len(R)
+    ctx = gpu_context
+    s = _lib.default_settings(metric_reg=1e-3, boundary_tolerance=1e-13)
+    dR, dK, dP, dC, dE = (_dev(torch, x) for x in (R, K, rho, rec["covector"], rec["environment"]))
+    side = torch.cuda.Stream()
+    scale = max(1.0, _metric_norm(rho, rec["gradient"]))
+    for call in range(2):
+        got = torch.full((d * d,), float("nan"), dtype=torch.complex128, device="cuda")
+        torch.cuda.synchronize()
+        st = _lib.StateStats()
+        rc = ctx.lib.rcmps_finish_gradient_noalloc(ctx.handle, d, dR.data_ptr(), dK.data_ptr(), dP.data_ptr(),
+                                                   dC.data_ptr(), dE.data_ptr(), C.byref(s), got.data_ptr(),
+                                                   C.byref(st), C.c_void_p(side.cuda_stream))
+        assert rc == 0 and st.status == 0, (call, rc, ctx.error())
+        got_h = got.cpu().numpy().reshape(d, d)
+        assert _metric_norm(rho, got_h - rec["gradient"]) <= GRAD_TOL * scale, call
 
 
 def test_noalloc_rejects_sizes_beyond_its_scratch(gpu_context):
