@@ -1,32 +1,52 @@
-"""L-BFGS controller of rcmps_gpu's optimizer around the B200 objective.
+"""L-BFGS optimizer of an RCMPS around the B200 objective.
 
-Mirrors gpu/src/rcmps_gpu/optimizer/runtime/optimizer.py (the controller that follows
-RcmpsCore/OptimKit 0.5): the metric <x, y> = 2 Re tr(x^dag y (rho + reg I)), the canonical
-retraction of (R, K), the rho-preconditioner, the first direction of fixed metric norm, the
-two-loop L-BFGS direction rescaled to the latest secant pair, cautious history updates and
-bounded Armijo backtracking. It yields the same trial / accepted / stopped events with the same
-resumable state, so the reference's drivers and checkpoint code consume it unchanged.
+The interface is that of rcmps_gpu's controller (gpu/src/rcmps_gpu/optimizer/runtime/
+optimizer.py:24-259, which follows RcmpsCore/OptimKit 0.5): the same controls and aliases, the
+same "trial", "accepted" and "stopped" events, and a resumable state with the same fields, so
+the reference's sweep drivers and checkpoint code consume this module unchanged. The algorithm
+it implements, stated here in full:
 
-The GPU does the evaluation: every trial's stationary density comes from the library
-(stationary_state, or with warm_stationary=True the correction started from the last accepted
-density, stationary_correction.py:19-96) and objective_callable is normally
-rcmps_b200.objective.objective. The L-BFGS algebra is on D x D host matrices.
+  * tangent vectors are D x D matrices X (the variation of R; K follows from the retraction),
+    with the metric <X, Y> = 2 Re tr(X^dag Y M), M = rho + metric_reg I;
+  * the preconditioner is P(X) = (N^-1 (X M)^dag)^dag, N = rho + precond_reg I; precond_reg
+    starts at initial_precond_reg and becomes max(10 eps, precond_prefactor min(|g|^2, 1)) after
+    every accepted step;
+  * with no curvature pairs the direction is -P(g) scaled to metric norm initial_direction_norm;
+    otherwise the two-loop recursion over the pairs (s_j, y_j, 1/<s_j, y_j>), with the middle
+    preconditioner scaled by gamma = <s, y> / <y, P(y)> of the newest pair (no direction when
+    gamma is not positive); a direction that is not a descent direction clears the history and
+    falls back to the first kind;
+  * bounded Armijo backtracking along the canonical retraction R + a X,
+    K + i a/2 (X^dag R - R^dag X) (Hermitized), from a = min(next step, max_relative_step
+    max(1, |R|) / |X|), shrinking by `shrink`, at most line_search_trials trials; every trial
+    solves its stationary density first (on the GPU) and then calls the objective;
+  * after an accepted step the pair (s, y) = (a X, g_new - g) is kept only when the cautious
+    test <s, y> / <s, s> > |g_new| / 10^4 holds (norms in the new state's metric), normalized by
+    |s|, in a history of at most `history` pairs.
+
+Every trial's stationary density comes from the library: rcmps_stationary_state_batch, or with
+warm_stationary=True the correction started from the last accepted density
+(rcmps_stationary_correction_batch). objective_callable is normally
+rcmps_b200.objective.objective.
 """
 from __future__ import annotations
 
+from collections import deque
 from dataclasses import dataclass, fields
 from time import perf_counter
 
 import numpy as np
 
-from .objective import SolverFailure, metric, stationary_state, stationary_state_correction
+from .objective import SolverFailure, stationary_state, stationary_state_correction
 
 __all__ = ["OptimizationControls", "retract", "precondition", "optimize"]
+
+_EPS = np.finfo(float).eps
 
 
 @dataclass(frozen=True)
 class OptimizationControls:
-    """The reference's controls (optimizer.py:24-41), same names and defaults."""
+    """Controls of the optimizer; names and defaults are the reference's (optimizer.py:24-41)."""
     max_iterations: int = 3000
     gradient_tol: float = 3e-5
     max_seconds: float | None = None
@@ -45,214 +65,303 @@ class OptimizationControls:
     energy_atol: float = 0.0
     refresh_curvatures: bool = False
 
+    def validated(self):
+        """Self, or ValueError naming the first control outside its domain."""
+        finite = lambda v: v is not None and np.isfinite(v)
+        rules = (("max_iterations", self.max_iterations >= 0), ("history", self.history >= 1),
+                 ("line_search_trials", self.line_search_trials >= 1),
+                 ("gradient_tol", finite(self.gradient_tol) and self.gradient_tol > 0),
+                 ("metric_reg", finite(self.metric_reg) and self.metric_reg >= 0),
+                 ("stationary_tolerance", finite(self.stationary_tolerance) and self.stationary_tolerance > 0),
+                 ("initial_precond_reg", finite(self.initial_precond_reg) and self.initial_precond_reg > 0),
+                 ("precond_prefactor", finite(self.precond_prefactor) and self.precond_prefactor > 0),
+                 ("initial_step", finite(self.initial_step) and self.initial_step > 0),
+                 ("initial_direction_norm", finite(self.initial_direction_norm) and self.initial_direction_norm > 0),
+                 ("max_relative_step", finite(self.max_relative_step) and self.max_relative_step > 0),
+                 ("armijo_c1", 0 < self.armijo_c1 < 1), ("shrink", 0 < self.shrink < 1),
+                 ("energy_atol", finite(self.energy_atol) and self.energy_atol >= 0),
+                 ("max_seconds", self.max_seconds is None or (finite(self.max_seconds) and self.max_seconds > 0)))
+        bad = [name for name, ok in rules if not ok]
+        if bad:
+            raise ValueError(f"invalid optimization controls: {', '.join(bad)}")
+        return self
 
-_ALIASES = {"iterations": "max_iterations", "gradtol": "gradient_tol", "gradient_tolerance": "gradient_tol",
-            "lbfgs_history": "history", "max_trials": "line_search_trials", "armijo_energy_atol": "energy_atol"}
+
+# Alternative spellings that drivers pass (the reference's aliases, optimizer.py:48-53).
+CONTROL_ALIASES = {"iterations": "max_iterations", "gradtol": "gradient_tol", "gradient_tolerance": "gradient_tol",
+                   "lbfgs_history": "history", "max_trials": "line_search_trials",
+                   "armijo_energy_atol": "energy_atol"}
 
 
 def _controls(controls):
-    """OptimizationControls from a dataclass, dict or namespace (aliases of optimizer.py:44-70)."""
+    """OptimizationControls from a dataclass, a dict or a namespace; unknown names are ignored."""
     if isinstance(controls, OptimizationControls):
-        c = controls
-    else:
-        values = dict(controls) if isinstance(controls, dict) else dict(vars(controls))
-        for alias, name in _ALIASES.items():
-            if alias in values and name not in values:
-                values[name] = values[alias]
-        names = {f.name for f in fields(OptimizationControls)}
-        c = OptimizationControls(**{key: value for key, value in values.items() if key in names})
-    positive = (c.gradient_tol, c.stationary_tolerance, c.initial_precond_reg, c.precond_prefactor, c.initial_step,
-                c.initial_direction_norm, c.max_relative_step)
-    ok = (c.max_iterations >= 0 and c.history >= 1 and c.line_search_trials >= 1 and
-          all(np.isfinite(x) and x > 0 for x in positive) and
-          np.isfinite(c.metric_reg) and c.metric_reg >= 0 and 0 < c.armijo_c1 < 1 and 0 < c.shrink < 1 and
-          np.isfinite(c.energy_atol) and c.energy_atol >= 0 and
-          (c.max_seconds is None or (np.isfinite(c.max_seconds) and c.max_seconds > 0)))
-    if not ok:
-        raise ValueError("invalid optimization controls")
-    return c
+        return controls.validated()
+    given = dict(controls) if isinstance(controls, dict) else dict(vars(controls))
+    names = {f.name for f in fields(OptimizationControls)}
+    chosen = {}
+    for key, value in given.items():
+        target = key if key in names else CONTROL_ALIASES.get(key)
+        if target is not None and (target == key or target not in given):
+            chosen[target] = value
+    return OptimizationControls(**chosen).validated()
 
 
 def retract(r, k, direction, alpha):
-    """The canonical retraction (numerics.py:133-136): R + alpha X, and K moved so that
-    Q = -iK - R^dag R / 2 stays left-canonical to first order, then made Hermitian."""
-    rr = r + alpha * direction
-    kk = k + 0.5j * alpha * (direction.conj().T @ r - r.conj().T @ direction)
-    return rr, 0.5 * (kk + kk.conj().T)
+    """The canonical retraction of (R, K) along the tangent `direction` by `alpha`
+    (numerics.py:133-136): R' = R + a X, K' = Herm(K + i a/2 (X^dag R - R^dag X))."""
+    x = np.asarray(direction)
+    r_new = r + alpha * x
+    k_new = k + 0.5j * alpha * (x.conj().T @ r - r.conj().T @ x)
+    return r_new, 0.5 * (k_new + k_new.conj().T)
 
 
 def precondition(rho, gradient, metric_reg=1e-3, precond_reg=1e-4):
-    """(rho + precond_reg I)^-1 applied from the right to G (rho + metric_reg I)
+    """P(X) = (N^-1 (X M)^dag)^dag with M = rho + metric_reg I and N = rho + precond_reg I
     (numerics.py:139-142)."""
     eye = np.eye(len(rho))
-    lhs = (gradient @ (rho + metric_reg * eye)).conj().T
-    return np.linalg.solve(rho + precond_reg * eye, lhs).conj().T
+    rhs = (gradient @ (rho + metric_reg * eye)).conj().T
+    return np.linalg.solve(rho + precond_reg * eye, rhs).conj().T
 
 
-def _norm(rho, x, reg):
-    sq = metric(rho, x, x, reg)
-    if not np.isfinite(sq) or sq < 0:
-        raise SolverFailure(f"invalid tangent metric norm squared: {sq}")
-    return float(np.sqrt(sq))
+class _Tangent:
+    """The metric of the tangent space at one state (its density rho)."""
+
+    def __init__(self, rho, metric_reg):
+        self.rho, self.reg = rho, metric_reg
+        self.m = rho + metric_reg * np.eye(len(rho))
+
+    def inner(self, x, y):
+        return float(2.0 * np.real(np.vdot(x, y @ self.m)))
+
+    def norm(self, x):
+        sq = self.inner(x, x)
+        if not (np.isfinite(sq) and sq >= 0):
+            raise SolverFailure(f"the metric norm of a tangent vector is invalid (squared {sq})")
+        return float(np.sqrt(sq))
+
+    def precondition(self, x, precond_reg):
+        return precondition(self.rho, x, self.reg, precond_reg)
 
 
-def _first_direction(rho, gradient, reg, preg, length):
-    p = precondition(rho, gradient, reg, preg)
-    n = _norm(rho, p, reg)
-    if n == 0:
-        raise SolverFailure("preconditioned direction vanished before convergence")
-    return -(length / n) * p
+class _History:
+    """Curvature pairs (s, y, 1/<s, y>) with |s| = 1, at most `size` of them (oldest dropped)."""
+
+    def __init__(self, size, pairs=()):
+        self.pairs = deque(pairs, maxlen=size)
+
+    def __len__(self):
+        return len(self.pairs)
+
+    def clear(self):
+        self.pairs.clear()
+
+    def push(self, s, y, inv_sy):
+        self.pairs.append((s, y, inv_sy))
+
+    def refresh(self, tangent, gnorm):
+        """Recompute every pair's curvature in the current metric and drop those that fail the
+        cautious test."""
+        kept = []
+        for s, y, _ in self.pairs:
+            sy, ss = tangent.inner(s, y), tangent.inner(s, s)
+            if ss > 0 and sy / ss > gnorm / 1e4:
+                kept.append((s, y, 1.0 / sy))
+        self.pairs = deque(kept, maxlen=self.pairs.maxlen)
+
+    def direction(self, tangent, gradient, precond_reg):
+        """(-H g, gamma) by the two-loop recursion; (None, gamma) when the scaling of the
+        newest pair is not positive."""
+        q = gradient.copy()
+        alphas = []
+        for s, y, inv in reversed(self.pairs):
+            a = inv * tangent.inner(s, q)
+            alphas.append(a)
+            q = q - a * y
+        s_new, y_new, _ = self.pairs[-1]
+        denom = tangent.inner(y_new, tangent.precondition(y_new, precond_reg))
+        gamma = tangent.inner(s_new, y_new) / denom if denom > 0 else np.nan
+        if not (np.isfinite(gamma) and gamma > 0):
+            return None, gamma
+        z = gamma * tangent.precondition(q, precond_reg)
+        for (s, y, inv), a in zip(self.pairs, reversed(alphas)):
+            z = z + (a - inv * tangent.inner(y, z)) * s
+        return -z, float(gamma)
 
 
-def _two_loop(rho, gradient, pairs, reg, preg):
-    """L-BFGS direction from normalized pairs (s, y, 1/<s, y>), the preconditioner rescaled by
-    <s, y> / <y, P y> of the newest pair (optimizer.py:88-107). (None, gamma) if that scale is
-    not positive."""
-    q = gradient.copy()
-    alphas = []
-    for s, y, rs in reversed(pairs):
-        a = rs * metric(rho, s, q, reg)
-        alphas.append(a)
-        q -= a * y
-    s, y, _ = pairs[-1]
-    py = precondition(rho, y, reg, preg)
-    num, den = metric(rho, s, y, reg), metric(rho, y, py, reg)
-    gamma = num / den if den > 0 else np.nan
-    if not np.isfinite(gamma) or gamma <= 0:
-        return None, gamma
-    z = gamma * precondition(rho, q, reg, preg)
-    for (s, y, rs), a in zip(pairs, reversed(alphas)):
-        z += s * (a - rs * metric(rho, y, z, reg))
-    return -z, float(gamma)
+def _first_direction(tangent, gradient, precond_reg, length):
+    pg = tangent.precondition(gradient, precond_reg)
+    n = tangent.norm(pg)
+    if n == 0.0:
+        raise SolverFailure("the preconditioned gradient vanished before convergence")
+    return -(length / n) * pg
 
 
-def optimize(r, k, rho, energy, gradient, objective_callable, controls, resume_state=None, *,
-             warm_stationary=False):
-    """Yield trial, accepted and stopped events from an evaluated initial state
-    (optimizer.py:110-259). objective_callable(r, k, rho) -> (energy, gradient, stats). Accepted
-    and stopped events carry `state` (R, K, rho, gradient, energy, pairs, precond_reg, next_step,
-    iteration, evaluations, elapsed_seconds) from which resume_state continues exactly.
-    warm_stationary: each trial's density is corrected from the last accepted one instead of
-    solved cold (the reference's plain controller solves cold)."""
-    p = _controls(controls)
-    res = resume_state or {}
-    as_c = lambda x: np.array(x, dtype=np.complex128, copy=True)
-    r = as_c(res.get("R", res.get("r", r)))
-    k = as_c(res.get("K", res.get("k", k)))
-    rho = as_c(res.get("rho", rho))
-    gradient = as_c(res.get("gradient", res.get("g", gradient)))
-    energy = float(res.get("energy", energy))
-    if (r.ndim != 2 or r.shape[0] != r.shape[1] or any(x.shape != r.shape for x in (k, rho, gradient)) or
-            not np.isfinite(energy) or not all(np.isfinite(x).all() for x in (r, k, rho, gradient))):
-        raise ValueError("invalid accepted optimization state")
-    pairs = [(as_c(s), as_c(y), float(rs)) for s, y, rs in res.get("pairs", [])][-p.history:]
-    if any(s.shape != r.shape or y.shape != r.shape or not np.isfinite(rs) or rs <= 0 or
-           not np.isfinite(s).all() or not np.isfinite(y).all() for s, y, rs in pairs):
-        raise ValueError("invalid resumed LBFGS history")
-    iteration = int(res.get("iteration", 0))
-    evaluations = int(res.get("evaluations", 0))
-    precond_reg = float(res.get("precond_reg", p.initial_precond_reg))
-    next_step = float(res.get("next_step", p.initial_step))
-    elapsed_before = float(res.get("elapsed_seconds", 0.0))
-    if (iteration < 0 or evaluations < 0 or not np.isfinite(precond_reg) or precond_reg <= 0 or
-            not np.isfinite(next_step) or next_step <= 0 or not np.isfinite(elapsed_before) or elapsed_before < 0):
-        raise ValueError("invalid resumed optimizer controls or counters")
-    last_stats = res.get("stats")
-    t0 = perf_counter()
-    reg = p.metric_reg
+class _Run:
+    """One invocation of the optimizer: the accepted state, its history and counters."""
 
-    def snapshot():
-        return dict(R=r, K=k, rho=rho, gradient=gradient, g=gradient, energy=energy, pairs=list(pairs),
-                    precond_reg=precond_reg, next_step=next_step, iteration=iteration, evaluations=evaluations,
-                    elapsed_seconds=elapsed_before + perf_counter() - t0,
-                    gradient_norm=_norm(rho, gradient, reg), stats=last_stats)
+    def __init__(self, r, k, rho, energy, gradient, objective_callable, controls, resume_state, warm):
+        self.c = _controls(controls)
+        self.objective = objective_callable
+        self.warm = bool(warm)
+        res = resume_state or {}
+        pick = lambda *names_and_default: next((res[n] for n in names_and_default[:-1] if n in res),
+                                               names_and_default[-1])
+        as_c = lambda a: np.array(a, dtype=np.complex128, copy=True)
+        self.r, self.k = as_c(pick("R", "r", r)), as_c(pick("K", "k", k))
+        self.rho, self.g = as_c(pick("rho", rho)), as_c(pick("gradient", "g", gradient))
+        self.energy = float(pick("energy", energy))
+        shape = self.r.shape
+        if (self.r.ndim != 2 or shape[0] != shape[1] or any(a.shape != shape for a in (self.k, self.rho, self.g))
+                or not np.isfinite(self.energy) or not all(np.isfinite(a).all() for a in (self.r, self.k, self.rho, self.g))):
+            raise ValueError("the accepted state to optimize from is invalid (shapes or nonfinite values)")
+        pairs = [(as_c(s), as_c(y), float(inv)) for s, y, inv in res.get("pairs", [])][-self.c.history:]
+        for s, y, inv in pairs:
+            if s.shape != shape or y.shape != shape or not (np.isfinite(inv) and inv > 0) \
+                    or not (np.isfinite(s).all() and np.isfinite(y).all()):
+                raise ValueError("the resumed L-BFGS history is invalid")
+        self.history = _History(self.c.history, pairs)
+        self.iteration = int(res.get("iteration", 0))
+        self.evaluations = int(res.get("evaluations", 0))
+        self.precond_reg = float(res.get("precond_reg", self.c.initial_precond_reg))
+        self.next_step = float(res.get("next_step", self.c.initial_step))
+        self.elapsed_before = float(res.get("elapsed_seconds", 0.0))
+        if (min(self.iteration, self.evaluations) < 0 or not (np.isfinite(self.precond_reg) and self.precond_reg > 0)
+                or not (np.isfinite(self.next_step) and self.next_step > 0)
+                or not (np.isfinite(self.elapsed_before) and self.elapsed_before >= 0)):
+            raise ValueError("the resumed optimizer counters or controls are invalid")
+        self.last_stats = res.get("stats")
+        self.start = perf_counter()
 
-    def stop(reason, converged=False, **extra):
-        return dict(type="stopped", event="stopped", reason=reason, converged=converged, state=snapshot(), **extra)
+    # ---------------------------------------------------------------- state and events
+    def tangent(self):
+        return _Tangent(self.rho, self.c.metric_reg)
 
-    def out_of_time():
-        return p.max_seconds is not None and perf_counter() - t0 >= p.max_seconds
+    def state(self):
+        return dict(R=self.r, K=self.k, rho=self.rho, gradient=self.g, g=self.g, energy=self.energy,
+                    pairs=list(self.history.pairs), precond_reg=self.precond_reg, next_step=self.next_step,
+                    iteration=self.iteration, evaluations=self.evaluations,
+                    elapsed_seconds=self.elapsed_before + perf_counter() - self.start,
+                    gradient_norm=self.tangent().norm(self.g), stats=self.last_stats)
 
-    while True:
-        gn = _norm(rho, gradient, reg)
-        if gn <= p.gradient_tol:
-            yield stop("gradient tolerance reached", converged=True)
-            return
-        if iteration >= p.max_iterations:
-            yield stop("requested iteration limit reached")
-            return
-        if out_of_time():
-            yield stop("optimization time budget reached")
-            return
-        it0 = perf_counter()
-        if p.refresh_curvatures:
-            kept = []
-            for s, y, _ in pairs:
-                sy, ss = metric(rho, s, y, reg), metric(rho, s, s, reg)
-                if ss > 0 and sy / ss > gn / 10000:
-                    kept.append((s, y, 1 / sy))
-            pairs = kept
+    def stopped(self, reason, converged=False, **extra):
+        return dict(type="stopped", event="stopped", reason=reason, converged=converged, state=self.state(), **extra)
+
+    def out_of_time(self):
+        return self.c.max_seconds is not None and perf_counter() - self.start >= self.c.max_seconds
+
+    # ---------------------------------------------------------------- one iteration
+    def search_direction(self, tangent, gnorm):
+        if self.c.refresh_curvatures:
+            self.history.refresh(tangent, gnorm)
         gamma = None
-        if pairs:
-            direction, gamma = _two_loop(rho, gradient, pairs, reg, precond_reg)
+        direction = None
+        if len(self.history):
+            direction, gamma = self.history.direction(tangent, self.g, self.precond_reg)
         else:
-            direction = _first_direction(rho, gradient, reg, precond_reg, p.initial_direction_norm)
-        slope = metric(rho, gradient, direction, reg) if direction is not None else np.nan
-        if not np.isfinite(slope) or slope >= 0:   # not a descent direction: restart the history
-            pairs = []
-            direction = _first_direction(rho, gradient, reg, precond_reg, p.initial_direction_norm)
-            slope = metric(rho, gradient, direction, reg)
-        if not np.isfinite(slope) or slope >= 0:
-            raise SolverFailure("preconditioned direction is not a descent direction")
-        alpha = min(next_step, p.max_relative_step * max(1.0, np.linalg.norm(r)) /
-                    max(np.linalg.norm(direction), np.finfo(float).eps))
-        accepted = False
-        failures = []
-        for trial in range(1, p.line_search_trials + 1):
-            if out_of_time():
-                yield stop("optimization time budget reached during line search", numerical_failures=failures)
-                return
-            rr, kk = retract(r, k, direction, alpha)
-            qq = -1j * kk - rr.conj().T @ rr / 2
-            try:
-                if warm_stationary:
-                    rhonew, sstats = stationary_state_correction(qq, rr, rho, tolerance=p.stationary_tolerance)
-                else:
-                    rhonew, sstats = stationary_state(qq, rr, tolerance=p.stationary_tolerance)
-                evaluations += 1
-                enew, gnew, newstats = objective_callable(rr, kk, rhonew)
-                enew = float(enew)
-                gnew = np.asarray(gnew, dtype=np.complex128)
-                if not np.isfinite(enew) or not np.isfinite(gnew).all() or gnew.shape != r.shape:
-                    raise SolverFailure("trial returned nonfinite or invalid objective/gradient")
-                bound = energy + p.armijo_c1 * alpha * slope + p.energy_atol
-                accepted = bool(enew <= bound)
-                yield dict(type="trial", event="trial", iteration=iteration + 1, trial=trial, alpha=float(alpha),
-                           energy=enew, armijo_bound=float(bound), accepted=accepted, stats=newstats,
-                           stationary=sstats, evaluations=evaluations)
-                if accepted:
-                    break
-            except (SolverFailure, RuntimeError) as err:
-                failures.append(str(err))
-                yield dict(type="trial", event="trial", iteration=iteration + 1, trial=trial, alpha=float(alpha),
-                           accepted=False, error=str(err), evaluations=evaluations)
-            alpha *= p.shrink
-        if not accepted:
-            yield stop("Armijo line search exhausted; last accepted state retained", numerical_failures=failures)
-            return
-        step, change = alpha * direction, gnew - gradient
-        new_gn = _norm(rhonew, gnew, reg)
-        sy, ss = metric(rhonew, step, change, reg), metric(rhonew, step, step, reg)
-        cautious = bool(np.isfinite(sy) and np.isfinite(ss) and ss > 0 and sy / ss > new_gn / 10000)
+            direction = _first_direction(tangent, self.g, self.precond_reg, self.c.initial_direction_norm)
+        slope = tangent.inner(self.g, direction) if direction is not None else np.nan
+        if not (np.isfinite(slope) and slope < 0):
+            self.history.clear()
+            direction = _first_direction(tangent, self.g, self.precond_reg, self.c.initial_direction_norm)
+            slope = tangent.inner(self.g, direction)
+            if not (np.isfinite(slope) and slope < 0):
+                raise SolverFailure("the preconditioned direction does not descend")
+        return direction, slope, gamma
+
+    def trial_density(self, r, q):
+        if self.warm:
+            return stationary_state_correction(q, r, self.rho, tolerance=self.c.stationary_tolerance)
+        return stationary_state(q, r, tolerance=self.c.stationary_tolerance)
+
+    def evaluate(self, r, k):
+        q = -1j * k - r.conj().T @ r / 2
+        rho, stationary = self.trial_density(r, q)
+        self.evaluations += 1
+        e, g, stats = self.objective(r, k, rho)
+        e, g = float(e), np.asarray(g, dtype=np.complex128)
+        if not np.isfinite(e) or g.shape != self.r.shape or not np.isfinite(g).all():
+            raise SolverFailure("the objective returned a nonfinite or misshapen energy or gradient")
+        return rho, e, g, stats, stationary
+
+    def accept(self, alpha, direction, r, k, rho, e, g, stats):
+        step, change = alpha * direction, g - self.g
+        new = _Tangent(rho, self.c.metric_reg)
+        gnorm = new.norm(g)
+        sy, ss = new.inner(step, change), new.inner(step, step)
+        cautious = bool(np.isfinite(sy) and np.isfinite(ss) and ss > 0 and sy / ss > gnorm / 1e4)
         if cautious:
             length = np.sqrt(ss)
-            pairs = (pairs + [(step / length, change / length, ss / sy)])[-p.history:]
-        r, k, rho, energy, gradient = rr, kk, rhonew, enew, gnew
-        last_stats = newstats
-        iteration += 1
-        next_step = min(1.0, 2 * alpha) if p.warm_start_line_search else p.initial_step
-        precond_reg = max(10 * np.finfo(float).eps, p.precond_prefactor * min(new_gn * new_gn, 1.0))
-        yield dict(type="accepted", event="accepted", state=snapshot(), iteration=iteration, energy=energy,
-                   gradient_norm=new_gn, alpha=float(alpha), trials=trial, seconds=perf_counter() - it0,
-                   stats=newstats, stationary=sstats, gamma=gamma, cautious_update=cautious,
-                   history_size=len(pairs), evaluations=evaluations)
+            self.history.push(step / length, change / length, ss / sy)
+        self.r, self.k, self.rho, self.energy, self.g = r, k, rho, e, g
+        self.last_stats = stats
+        self.iteration += 1
+        self.next_step = min(1.0, 2.0 * alpha) if self.c.warm_start_line_search else self.c.initial_step
+        self.precond_reg = max(10 * _EPS, self.c.precond_prefactor * min(gnorm * gnorm, 1.0))
+        return gnorm, cautious
+
+    def events(self):
+        c = self.c
+        while True:
+            tangent = self.tangent()
+            gnorm = tangent.norm(self.g)
+            if gnorm <= c.gradient_tol:
+                yield self.stopped("gradient tolerance reached", converged=True)
+                return
+            if self.iteration >= c.max_iterations:
+                yield self.stopped("requested iteration limit reached")
+                return
+            if self.out_of_time():
+                yield self.stopped("optimization time budget reached")
+                return
+            began = perf_counter()
+            direction, slope, gamma = self.search_direction(tangent, gnorm)
+            alpha = min(self.next_step,
+                        c.max_relative_step * max(1.0, np.linalg.norm(self.r)) / max(np.linalg.norm(direction), _EPS))
+            failures, found = [], None
+            for trial in range(1, c.line_search_trials + 1):
+                if self.out_of_time():
+                    yield self.stopped("optimization time budget reached during line search",
+                                       numerical_failures=failures)
+                    return
+                r_t, k_t = retract(self.r, self.k, direction, alpha)
+                try:
+                    rho_t, e_t, g_t, stats_t, stationary_t = self.evaluate(r_t, k_t)
+                except (SolverFailure, RuntimeError) as err:
+                    failures.append(str(err))
+                    yield dict(type="trial", event="trial", iteration=self.iteration + 1, trial=trial,
+                               alpha=float(alpha), accepted=False, error=str(err), evaluations=self.evaluations)
+                else:
+                    bound = self.energy + c.armijo_c1 * alpha * slope + c.energy_atol
+                    ok = bool(e_t <= bound)
+                    yield dict(type="trial", event="trial", iteration=self.iteration + 1, trial=trial,
+                               alpha=float(alpha), energy=e_t, armijo_bound=float(bound), accepted=ok,
+                               stats=stats_t, stationary=stationary_t, evaluations=self.evaluations)
+                    if ok:
+                        found = (trial, r_t, k_t, rho_t, e_t, g_t, stats_t, stationary_t)
+                        break
+                alpha *= c.shrink
+            if found is None:
+                yield self.stopped("Armijo line search exhausted; last accepted state retained",
+                                   numerical_failures=failures)
+                return
+            trial, r_t, k_t, rho_t, e_t, g_t, stats_t, stationary_t = found
+            gnorm_new, cautious = self.accept(alpha, direction, r_t, k_t, rho_t, e_t, g_t, stats_t)
+            yield dict(type="accepted", event="accepted", state=self.state(), iteration=self.iteration,
+                       energy=self.energy, gradient_norm=gnorm_new, alpha=float(alpha), trials=trial,
+                       seconds=perf_counter() - began, stats=stats_t, stationary=stationary_t, gamma=gamma,
+                       cautious_update=cautious, history_size=len(self.history), evaluations=self.evaluations)
+
+
+def optimize(r, k, rho, energy, gradient, objective_callable, controls, resume_state=None, *, warm_stationary=False):
+    """Yield the optimizer's events from an accepted, already evaluated state (r, k, rho,
+    energy, gradient). objective_callable(r, k, rho) -> (energy, gradient, stats).
+
+    "trial" events report each line-search evaluation; "accepted" events carry the complete
+    resumable `state` (R, K, rho, gradient, energy, the normalized pairs, precond_reg,
+    next_step, iteration, evaluations, elapsed_seconds); the single "stopped" event ends the
+    stream with its reason. resume_state continues a run from such a state without a new
+    initial evaluation; max_iterations counts accepted iterations across resumes, max_seconds
+    this invocation only. warm_stationary=True starts each trial's stationary solve from the
+    last accepted density."""
+    return _Run(r, k, rho, energy, gradient, objective_callable, controls, resume_state, warm_stationary).events()
