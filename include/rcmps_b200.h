@@ -223,6 +223,15 @@ int rcmps_stationary_correction_batch(rcmps_context* context, int n_states, cons
                                       const double* K, const double* rho_previous, double tolerance,
                                       double* rho, rcmps_state_stats* stats, void* stream);
 
+/* C_b = A_b B_b for n_states pairs of d x d complex matrices (1 <= d <= 64; device, packed
+ * row-major like every batch of this header) by the split-precision tensor-core engine of the
+ * trajectory: FP64 values cut into six 7-bit BF16 slices per operand (per-row scales of A,
+ * per-column scales of B), the slice products on tcgen05 with FP32 accumulation in TMEM,
+ * recombined in FP64 (error about 2^-42 of row scale x column scale x d). No counterpart in
+ * the reference; the engine's unit-level check. */
+int rcmps_split_product_batch(rcmps_context* context, int n_states, int d, const double* A, const double* B,
+                              double* C, void* stream);
+
 /* Number of kernel launches this library has issued in the process (all contexts). No
  * counterpart in the reference. */
 long long rcmps_launch_count(void);

@@ -89,6 +89,7 @@ SIGNATURES = {
     "rcmps_stationary_state_batch": (_I, [_P, _I, C.POINTER(_I), _P, _P, _D, _P, C.POINTER(StateStats), _P]),
     "rcmps_stationary_correction_batch": (_I, [_P, _I, C.POINTER(_I), _P, _P, _P, _D, _P, C.POINTER(StateStats),
                                                _P]),
+    "rcmps_split_product_batch": (_I, [_P, _I, _I, _P, _P, _P, _P]),
     "rcmps_fp64_peak_tflops": (_D, [_P]),
     "rcmps_launch_count": (C.c_longlong, []),
 }
