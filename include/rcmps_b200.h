@@ -59,6 +59,13 @@ typedef struct rcmps_settings {
                                   RCMPS_INVALID_ARGUMENT (--packed-z2, the default of
                                   evaluate_quartic_persistent_trajectory); 2 packed for the states
                                   with that structure, unpacked for the others */
+  int precision;               /* quartic trajectory products: 0 FP64 tensor cores (DMMA); 1 split
+                                  precision on the 5th-generation tensor cores (each FP64 operand cut
+                                  into six 7-bit BF16 slices, slice products accumulated in FP32 in
+                                  tensor memory, recombined in FP64; error about 2^-43 of the row and
+                                  column scales per term) for the states of padded dimension 64, FP64
+                                  for the others. The DOP853 error estimate and step control, the
+                                  stage sums and every solve stay FP64. */
 } rcmps_settings;
 
 /* Per-state diagnostics. */

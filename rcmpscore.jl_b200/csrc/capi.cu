@@ -200,6 +200,8 @@ int check_settings(rcmps_context* ctx, const rcmps_settings* s) {
   if (!(s->max_device_seconds >= 0.0)) return fail(ctx, RCMPS_INVALID_ARGUMENT, "max_device_seconds must be >= 0");
   if (s->symmetry < 0 || s->symmetry > 2)
     return fail(ctx, RCMPS_INVALID_ARGUMENT, "symmetry must be 0 (unpacked), 1 (packed Z2) or 2 (packed where Z2)");
+  if (s->precision < 0 || s->precision > 1)
+    return fail(ctx, RCMPS_INVALID_ARGUMENT, "precision must be 0 (FP64 tensor cores) or 1 (split BF16 slices)");
   return RCMPS_OK;
 }
 
@@ -266,6 +268,7 @@ void rcmps_default_settings(rcmps_settings* s) {
   s->metric_reg = 1e-3;
   s->boundary_tolerance = 1e-13;
   s->symmetry = 0;
+  s->precision = 0;
 }
 
 int rcmps_context_create(int device, rcmps_context** out) {

@@ -62,7 +62,11 @@ SysSizes sys_sizes(int system, int dp, int nblk) {
   return z;
 }
 
-size_t state_bytes(int system, int dp, int npoints, int nodes) {
+// The split-precision engine runs the quartic trajectory of the states of padded dimension 64
+// when the settings ask for it.
+bool split_engine_for(const rcmps_settings& S, int system, int dp) { return S.precision == 1 && system == 0 && dp == 64; }
+
+size_t state_bytes(int system, int dp, int npoints, int nodes, bool split = false) {
   const size_t mat = (size_t)dp * dp * 16;
   const int nblk = (nodes + kNodesPerBlock - 1) / kNodesPerBlock;
   const SysSizes z = sys_sizes(system, dp, nblk);
@@ -73,6 +77,7 @@ size_t state_bytes(int system, int dp, int npoints, int nodes) {
   b += (size_t)npoints * z.nch * mat;           // samples
   b += (z.wscr + z.part + z.fin + 2) * mat;     // pullback scratch, partials, finalize, cov/env
   b += 1024;                                    // small per-state records
+  if (split) b += split_state_bytes();          // BF16 slices of the constant operands
   return b;
 }
 
@@ -143,7 +148,8 @@ int quartic_run(rcmps_context* ctx, QuarticJob& job, cudaStream_t stream) {
   for (auto& kv : groups) {
     const int dp = kv.first;
     const std::vector<int>& all = kv.second;
-    const size_t per = state_bytes(system, dp, npoints, nodes);
+    const bool split = split_engine_for(S, system, dp);
+    const size_t per = state_bytes(system, dp, npoints, nodes, split);
     const SysSizes zs = sys_sizes(system, dp, nblk);
     const int NCH = zs.nch;
     const size_t fixed = (size_t)(npoints + 3 * nodes) * 8 + 4096;
@@ -176,6 +182,7 @@ int quartic_run(rcmps_context* ctx, QuarticJob& job, cudaStream_t stream) {
       const size_t o_fin = L.add((size_t)n * zs.fin * mat * 16);
       const size_t o_cov = L.add((size_t)n * mat * 16);
       const size_t o_env = L.add((size_t)n * mat * 16);
+      const size_t o_split = L.add(split ? (size_t)n * split_state_bytes() : 0);
       cudaError_t e = arena_reserve(SL, L.total);
       if (e != cudaSuccess)
         return fail(ctx, RCMPS_OUT_OF_MEMORY, "quartic workspace: " + std::to_string(L.total) + " bytes");
@@ -245,6 +252,7 @@ int quartic_run(rcmps_context* ctx, QuarticJob& job, cudaStream_t stream) {
         t.L = system == 1 ? w + 21 * vec : nullptr;
         t.samples = d_samp + (size_t)i * npoints * vec;
         t.stats = reinterpret_cast<TrajStats*>(base + o_tstats) + i;
+        if (split) split_state_pointers(reinterpret_cast<unsigned char*>(base + o_split) + (size_t)i * split_state_bytes(), t);
         t.atol = S.atol;
         t.rtol = S.rtol;
         if (job.controls) {   // per-state tolerances (checked by the entry point)
@@ -276,6 +284,7 @@ int quartic_run(rcmps_context* ctx, QuarticJob& job, cudaStream_t stream) {
                            stream);
       if (e == cudaSuccess && system == 1)
         e = launch_commutator(reinterpret_cast<double*>(d_ops), dp, (long long)zs.nops * mat, n, stream);
+      if (e == cudaSuccess && split) e = split_prep_launch((TrajState*)P(o_states), n, stream);
       // the packed Z2 route: each state's flag in its TrajState (the dense route keeps 0)
       if (e == cudaSuccess && system == 0 && S.symmetry != 0)
         e = launch_z2_check(dR, dK, dP, (int*)P(o_dims), dp, in_stride, n, S.symmetry,
@@ -307,7 +316,8 @@ int quartic_run(rcmps_context* ctx, QuarticJob& job, cudaStream_t stream) {
       tc.max_ns = (unsigned long long)(S.max_device_seconds * 1e9);
       if (e == cudaSuccess) e = cudaEventRecord(e0, stream);
       if (e == cudaSuccess)
-        e = trajectory_launch(system, dp, (TrajState*)P(o_states), n, (double*)P(o_points), npoints, tc, stream);
+        e = trajectory_launch(system, dp, (TrajState*)P(o_states), n, (double*)P(o_points), npoints, tc, stream,
+                              split ? 1 : 0);
       if (e == cudaSuccess) e = cudaEventRecord(e1, stream);
       if (e != cudaSuccess) return fail(ctx, RCMPS_CUDA_ERROR, std::string("trajectory launch: ") + cudaGetErrorString(e));
       // copy the trajectory values into a plain array for the finalize step

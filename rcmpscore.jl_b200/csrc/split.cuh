@@ -8,23 +8,24 @@
 // cut is unbiased and |r| <= 2^-7kSlices / 2). The slices are stored pre-weighted,
 // w_i = u_i 2^-7i, which BF16 holds exactly. Then
 //     C[m][n] = s_m t_n 2^-14 sum_{i,l} (sum_k wA_i[m][k] wB_l[k][n]),
-// and the pairs with i + l <= kSlices - 1 are kept (error about 2^-43 of s_m t_n per term).
+// and the pairs with i + l <= kSlices - 1 are kept: with seven slices the error is about 2^-50
+// of s_m t_n per term. (Six slices, 2^-43, meet a 1e-10 energy bar but not the DOP853 step
+// control at rtol 1e-12, whose error estimate cancels to about 1e-12 of the stage values: the
+// product rounding then dominates it and the controller takes about ten times the steps.)
 // The pair products accumulate in FP32 in TMEM, one accumulator per group s = i + l for
-// s = 0 .. 3 (exact: every group sum is an integer times 2^-7s, of magnitude at most
-// 128^2 K + 2 s 128 64 K < 2^24 for K <= 256) and one shared accumulator for s >= 4, whose terms
-// are at most 2^-28 of the leading group, so that its FP32 rounding stays below 2^-50 of the
-// result. (With one shared accumulator from s = 3 on, its rounding, about 2^-38 of the result,
-// was measured to match the truncation error itself.) The five accumulators are summed in FP64
-// and rescaled.
+// s = 0 .. 4 (exact: every group sum is an integer times 2^-7s, of magnitude at most
+// 128^2 K + 2 128 64 K + (s - 1) 64^2 K < 2^24 for K <= 256) and one shared accumulator for
+// s >= 5, whose terms are at most 2^-35 of the leading group, so that its FP32 rounding stays
+// below 2^-57 of the result. The accumulators are summed in FP64 and rescaled.
 //
 // Complex arithmetic is folded into K: with A_cat = [Ar | Ai] (M x 2K) and
 // B_cat = [[Br, Bi], [-Bi, Br]] (2K x 2N), A_cat B_cat = [Re C | Im C].
 //
-// Shared-memory operand layout (K-major, no swizzle): an operand block of MN rows and 64 K
-// elements (BF16) is a grid of 8 x 8 core matrices of 128 bytes (8 rows of 16 bytes); core
-// matrix (mn / 8, k / 8) sits at ((k / 8) (MN / 8) + mn / 8) 128 bytes, so the descriptor's
-// stride byte offset (between core matrices adjacent in MN) is 128 and its leading byte offset
-// (adjacent in K) is MN / 8 * 128. One MMA instruction covers K = 16, i.e. two core matrices.
+// Shared-memory operand layout (K-major, no swizzle): an operand block of MN rows and kChunkK K
+// elements (BF16) is a grid of core matrices of 128 bytes (8 rows of 16 bytes); core matrix
+// (mn / 8, k / 8) sits at ((k / 8) (MN / 8) + mn / 8) 128 bytes, so the descriptor's stride byte
+// offset (between core matrices adjacent in MN) is 128 and its leading byte offset (adjacent in
+// K) is MN / 8 * 128. One MMA instruction covers K = 16, i.e. two core matrices.
 //
 // Accumulators (M = 64, cta_group::1): row m of a 64-row accumulator based at lane b (0 or 16)
 // lives in TMEM lane b + (m % 16) + 32 (m / 16), so two accumulators share the same columns in
@@ -39,18 +40,18 @@
 namespace rcmps {
 namespace split {
 
-constexpr int kSlices = 6;      // slices per operand: 42 bits
+constexpr int kSlices = 7;      // slices per operand: 49 bits
 constexpr int kBits = 7;        // bits per slice
-constexpr int kGroups = 5;      // accumulators: s = 0, 1, 2, 3 and s >= 4
+constexpr int kGroups = 6;      // accumulators: s = 0 .. 4 and s >= 5
 constexpr int kM = 64;          // rows of every product (the MMA's M)
-constexpr int kChunkK = 64;     // K elements (BF16) of one staged chunk
+constexpr int kChunkK = 32;     // K elements (BF16) of one staged chunk
 constexpr int kPairs = kSlices * (kSlices + 1) / 2;
 
-// Byte offset of element (mn, k) in a K-major operand block of MN rows x 64 K.
+// Byte offset of element (mn, k) in a K-major operand block of MN rows x kChunkK K.
 RCMPS_DEVICE_INLINE uint32_t kmajor_offset(int mn, int k, int MN) {
   return (uint32_t)((((k >> 3) * (MN >> 3)) + (mn >> 3)) * 128 + (mn & 7) * 16 + (k & 7) * 2);
 }
-// Bytes of one slice of an operand block of MN rows x 64 K.
+// Bytes of one slice of an operand block of MN rows x kChunkK K.
 __host__ __device__ constexpr uint32_t block_bytes(int MN) { return (uint32_t)MN * kChunkK * 2; }
 
 // Shared-memory matrix descriptor (sm_100 format, version 1, no swizzle).
@@ -144,8 +145,8 @@ RCMPS_DEVICE_INLINE void slice8(const double* v, unsigned char* dst, uint32_t st
   double r[8];
 #pragma unroll
   for (int e = 0; e < 8; ++e) r[e] = v[e];
-  constexpr float kWeight[6] = {1.0f, 0x1p-7f, 0x1p-14f, 0x1p-21f, 0x1p-28f, 0x1p-35f};
-  static_assert(kSlices <= 6 && kBits == 7, "slice weights");
+  constexpr float kWeight[8] = {1.0f, 0x1p-7f, 0x1p-14f, 0x1p-21f, 0x1p-28f, 0x1p-35f, 0x1p-42f, 0x1p-49f};
+  static_assert(kSlices <= 8 && kBits == 7, "slice weights");
 #pragma unroll
   for (int i = 0; i < kSlices; ++i) {
     const float w = kWeight[i];
@@ -165,14 +166,14 @@ RCMPS_DEVICE_INLINE void slice8(const double* v, unsigned char* dst, uint32_t st
 }
 
 // ------------------------------------------------------------------ MMAs of one staged chunk
-// Every kept pair (i, l) of the chunk's slices, K = 64 in four MMAs of K = 16, into the
+// Every kept pair (i, l) of the chunk's slices, K = kChunkK in MMAs of K = 16, into the
 // kGroups group accumulators at tmem_acc + g * NCAT columns. first_chunk: the unit's first chunk (each
 // group's first MMA overwrites its accumulator). a_base / b_base: shared addresses of slice 0.
 template <int NCAT>
 RCMPS_DEVICE_INLINE void chunk_mmas(uint32_t tmem_acc, uint32_t a_base, uint32_t b_base, bool first_chunk) {
   constexpr uint32_t a_lbo = (kM / 8) * 128, b_lbo = (NCAT / 8) * 128;
   constexpr uint32_t idesc = idesc_bf16_m64(NCAT);
-  bool written[kGroups] = {false, false, false, false, false};
+  bool written[kGroups] = {};
 #pragma unroll
   for (int s = 0; s < kSlices; ++s) {
 #pragma unroll

@@ -2,8 +2,9 @@
 // (split.cuh): C_b = A_b B_b for every b, each product on one CTA.
 //
 // Each product is two units (the column halves of C, 32 complex columns each), accumulated in the
-// two lane halves of TMEM (kGroups accumulators of 64 FP32 columns each); each unit is two
-// staged chunks (the real and the imaginary part of A with the matching blocks of B_cat), so a
+// two lane halves of TMEM (kGroups accumulators of 64 FP32 columns each); each unit is four
+// staged chunks (K_cat = 128 in chunks of 32: the real, then the imaginary part of A with the
+// matching row blocks of B_cat), so a
 // CTA runs the same pipeline as the trajectory's split right-hand side: chunk q is sliced into
 // shared-memory buffer q % 2 while the MMAs of chunk q - 1 run, and the epilogue of unit u - 1
 // (TMEM -> FP64 recombination) runs while the MMAs of unit u do.
@@ -18,7 +19,7 @@ namespace rcmps {
 namespace {
 
 constexpr int kProdThreads = 512;
-constexpr uint32_t kBufBytes = split::kSlices * (split::block_bytes(64) + split::block_bytes(64));   // 96 KB
+constexpr uint32_t kBufBytes = split::kSlices * (split::block_bytes(64) + split::block_bytes(64));
 constexpr size_t kProdSmem = 2 * (size_t)kBufBytes + (64 + 2 * 32) * 8 + 4 * 8 + 16;
 
 __global__ void __launch_bounds__(kProdThreads, 1)
@@ -104,32 +105,35 @@ split_product_kernel(const double2* __restrict__ A, const double2* __restrict__ 
       sB[ab * 32 + tid] = pow2_above(mx);
     }
     __syncthreads();
-    for (int kc = 0; kc < 2; ++kc, ++q) {
-      const int buf = q & 1;
+    // K_cat = [Re A | Im A] = 128 columns, in chunks of kChunkK: chunk kc holds part kc / 2 (0 the
+    // real part of A with the rows [Br, Bi] of B_cat, 1 the imaginary part with [-Bi, Br]) at
+    // complex columns koff = 32 (kc % 2) ..
+    constexpr int kChunks = 128 / kChunkK, kGroupsK = kChunkK / 8;
+    for (int kc = 0; kc < kChunks; ++kc, ++q) {
+      const int buf = q & 1, part = kc / 2, koff = kChunkK * (kc % 2);
       if (q >= 2) mbar_wait(&mma_done[buf], (uint32_t)(((q >> 1) - 1) & 1), &wait_flag);
       unsigned char* bA = bufs + (size_t)buf * kBufBytes;
       unsigned char* bB = bA + kSlices * block_bytes(64);
-      // 512 A items (row m, 8 consecutive k) then 512 B items (column n of B_cat, 8 consecutive k)
-      for (int it = tid; it < 1024; it += kProdThreads) {
+      // A items (row m, 8 consecutive k), then B items (column n of B_cat, 8 consecutive k)
+      for (int it = tid; it < 2 * 64 * kGroupsK; it += kProdThreads) {
         double v[8];
-        if (it < 512) {
-          const int m = it >> 3, k0 = (it & 7) * 8;
+        if (it < 64 * kGroupsK) {
+          const int m = it / kGroupsK, k0 = (it % kGroupsK) * 8;
           const double inv = 1.0 / sA[m];
 #pragma unroll
           for (int e = 0; e < 8; ++e) {
-            const double2 x = load(a, m, k0 + e);
-            v[e] = (kc == 0 ? x.x : x.y) * inv;
+            const double2 x = load(a, m, koff + k0 + e);
+            v[e] = (part == 0 ? x.x : x.y) * inv;
           }
           slice8(v, bA + kmajor_offset(m, k0, 64), block_bytes(64));
         } else {
-          const int j = it - 512, n = j >> 3, k0 = (j & 7) * 8;
+          const int j = it - 64 * kGroupsK, n = j / kGroupsK, k0 = (j % kGroupsK) * 8;
           const int col = 32 * u + (n & 31);
           const double inv = 1.0 / sB[ab * 32 + (n & 31)];
 #pragma unroll
           for (int e = 0; e < 8; ++e) {
-            const double2 x = load(b, k0 + e, col);
-            // B_cat = [[Br, Bi], [-Bi, Br]]: chunk 0 holds the rows of Ar, chunk 1 those of Ai
-            const double val = kc == 0 ? (n < 32 ? x.x : x.y) : (n < 32 ? -x.y : x.x);
+            const double2 x = load(b, koff + k0 + e, col);
+            const double val = part == 0 ? (n < 32 ? x.x : x.y) : (n < 32 ? -x.y : x.x);
             v[e] = val * inv;
           }
           slice8(v, bB + kmajor_offset(n, k0, 64), block_bytes(64));
@@ -142,7 +146,7 @@ split_product_kernel(const double2* __restrict__ A, const double2* __restrict__ 
         tc_fence_after();
         chunk_mmas<64>(acc_addr(tmem, ab, 0), smem_u32(bA), smem_u32(bB), kc == 0);
         mma_commit(&mma_done[buf]);
-        if (kc == 1) mma_commit(&acc_full[ab]);
+        if (kc == kChunks - 1) mma_commit(&acc_full[ab]);
       }
     }
     if (u >= 1) epilogue(u - 1);

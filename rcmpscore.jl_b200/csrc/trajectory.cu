@@ -29,10 +29,12 @@
 //     G1 product C X and a third K block [.. | src c_r X_b] * C^dag to G2.
 #include <cuda_runtime.h>
 #include <cstdint>
+#include <type_traits>
 #include <cstdio>
 #include <cstring>
 #include "common.cuh"
 #include "dop853_tables.h"
+#include "split.cuh"
 #include "source_table.h"
 #include "trajectory.h"
 
@@ -538,6 +540,8 @@ struct Rhs {
   }
 };
 
+#include "trajectory_split.cuh"
+
 // Element e of this CTA's rows -> offset in a stage vector.
 template <int DP>
 __device__ __forceinline__ size_t own_offset(int e, int row0) {
@@ -553,13 +557,34 @@ __device__ __forceinline__ bool z2_zero_element(int e, int row0, int half) {
   return (((row >= half) != (col >= half)) ? 1 : 0) != ((c % 2 == 0) ? 1 : 0);
 }
 
-template <int DP, int SYS>
+// Shared memory of the kernel: the FP64 engine's panels and ring (Geo::SMEM), or the split
+// engine's chunk buffers followed by the controller's tail (2048 bytes).
+template <int DP, int SYS, int ENG>
+constexpr size_t kernel_smem() {
+  return ENG == 0 ? Geo<DP, SYS>::SMEM : ((split_engine::kEnd + 127) / 128) * 128 + 2048;
+}
+
+template <int DP, int SYS, int ENG>
+__device__ __forceinline__ Smem<DP, SYS> carve_engine(unsigned char* base) {
+  if constexpr (ENG == 0) {
+    return carve<DP, SYS>(base);
+  } else {
+    // the controller's scalars after the split engine's region, at the offsets carve uses
+    constexpr size_t tail = ((split_engine::kEnd + 127) / 128) * 128;
+    Smem<DP, SYS> s = carve<DP, SYS>(base + tail - (size_t)Geo<DP, SYS>::END2 * 16);
+    s.panel = s.aprime = s.ring = s.split = nullptr;
+    return s;
+  }
+}
+
+template <int DP, int SYS, int ENG>
 __global__ void __launch_bounds__(Geo<DP, SYS>::NT, 1)
 trajectory_kernel(const TrajState* __restrict__ states, const double* __restrict__ points, int npoints,
                   TrajControls ctl_in) {
   using GE = Geo<DP, SYS>;
+  static_assert(ENG == 0 || (SYS == kSysQuartic && DP == 64), "the split engine covers the quartic system at dp 64");
   extern __shared__ __align__(128) unsigned char smem_raw[];
-  Smem<DP, SYS> sm = carve<DP, SYS>(smem_raw);
+  Smem<DP, SYS> sm = carve_engine<DP, SYS, ENG>(smem_raw);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const uint32_t rank = cluster_rank();
   const int sidx = (int)cluster_id_x();
@@ -580,10 +605,16 @@ trajectory_kernel(const TrajState* __restrict__ states, const double* __restrict
     return;
   }
 
+  SplitSmem ssm{};
+  if constexpr (ENG == 1) ssm = split_carve(smem_raw);
   if (tid == 0) {
-    for (int i = 0; i < GE::NST; ++i) {
-      mbar_init(&sm.full[i], 1);
-      mbar_init(&sm.empty[i], GE::NW);
+    if constexpr (ENG == 0) {
+      for (int i = 0; i < GE::NST; ++i) {
+        mbar_init(&sm.full[i], 1);
+        mbar_init(&sm.empty[i], GE::NW);
+      }
+    } else {
+      for (int i = 0; i < 6; ++i) mbar_init(&ssm.mma_done[i], 1);   // mma_done, acc_full, copy_full
     }
     fence_mbar_init();
     C.t = -ctl_in.endpoint;
@@ -601,8 +632,32 @@ trajectory_kernel(const TrajState* __restrict__ states, const double* __restrict
     C.src[0] = source_value(-ctl_in.endpoint);
     for (int i = 0; i < 16; ++i) { C.ksc[i] = 0.0; sm.kscp[i] = 0.0; }
   }
+  uint32_t tmem = 0;
+  if constexpr (ENG == 1) {
+    if (warp == 0) split::tmem_alloc(ssm.tslot, split_engine::kTmemCols);
+    split::tc_fence_before();
+    __syncthreads();
+    split::tc_fence_after();
+    tmem = *ssm.tslot;
+  }
   __syncthreads();
-  Rhs<DP, SYS> rhs{st, sm, row0, tid, lane, warp, &gq, Rhs<DP, SYS>::total_chunks(), 0, 0};
+  using RhsT = std::conditional_t<ENG == 0, Rhs<DP, SYS>, RhsSplit<DP>>;
+  RhsT rhs;
+  if constexpr (ENG == 0) {
+    rhs = Rhs<DP, SYS>{st, sm, row0, tid, lane, warp, &gq, Rhs<DP, SYS>::total_chunks(), 0, 0};
+  } else {
+    rhs.st = st;
+    rhs.ss = ssm;
+    rhs.row0 = row0;
+    rhs.rank = (int)rank;
+    rhs.tid = tid;
+    rhs.lane = lane;
+    rhs.warp = warp;
+    rhs.tmem = tmem;
+    rhs.q = 0;
+    rhs.u = 0;
+    rhs.wait_flag = &C.wait_flag;
+  }
   // The packed Z2 route counts, per channel, the upper off-diagonal block of an odd channel
   // (F1, F3, A2, A4: c even) and the two diagonal blocks of an even one, 10 (d/2)^2 entries plus
   // the scalar (persistent_trajectory_backend.py:68, 115); the structural zeros and the lower
@@ -612,9 +667,11 @@ trajectory_kernel(const TrajState* __restrict__ states, const double* __restrict
   const bool packed = SYS == kSysQuartic && st->z2 > 0;
   const int half = st->d / 2;
   const bool zskip = packed && st->d == DP && DP % 32 == 0;
-  rhs.zs = zskip ? 1 : 0;
-  rhs.hz = half;
-  rhs.hh = zskip && row0 >= half ? 1 : 0;
+  if constexpr (ENG == 0) {
+    rhs.zs = zskip ? 1 : 0;
+    rhs.hz = half;
+    rhs.hh = zskip && row0 >= half ? 1 : 0;
+  }
   if (zskip) {
     // every work vector's own rows start at zero: the skipped parts are never written again
     for (int e = tid; e < GE::OWN; e += GE::NT) {
@@ -908,11 +965,26 @@ trajectory_kernel(const TrajState* __restrict__ states, const double* __restrict
 
   // wait (bounded) for any copies still in flight before the CTA's shared memory goes away
   __syncthreads();
-  if (tid == 0 && C.wait_flag) {
-    // a copy whose wait gave up may still be in flight: wait for each slot's last use, bounded
-    for (long long g = gq - 1; g >= 0 && g >= gq - GE::NST; --g) {
-      mbar_wait(&sm.full[g % GE::NST], (uint32_t)((g / GE::NST) & 1), nullptr);
+  if constexpr (ENG == 0) {
+    if (tid == 0 && C.wait_flag) {
+      // a copy whose wait gave up may still be in flight: wait for each slot's last use, bounded
+      for (long long g = gq - 1; g >= 0 && g >= gq - GE::NST; --g) {
+        mbar_wait(&sm.full[g % GE::NST], (uint32_t)((g / GE::NST) & 1), nullptr);
+      }
     }
+  } else {
+    // every unit's epilogue waited for its MMAs; after a wait that gave up, wait (bounded) once
+    // more for the last unit's and the last copies' barriers, then release TMEM
+    if (tid == 0 && C.wait_flag && rhs.u > 0) {
+      const long long uu = rhs.u - 1;
+      mbar_wait(&ssm.acc_full[uu & 1], (uint32_t)((uu >> 1) & 1), nullptr);
+      for (long long g = rhs.q - 1; g >= 0 && g >= rhs.q - 2; --g)
+        mbar_wait(&ssm.copy_full[g & 1], (uint32_t)((g >> 1) & 1), nullptr);
+    }
+    split::tc_fence_before();
+    __syncthreads();
+    split::tc_fence_after();
+    if (warp == 0) split::tmem_dealloc(tmem, split_engine::kTmemCols);
   }
   if (rank == 0 && tid == 0) {
     TrajStats* o = st->stats;
@@ -934,17 +1006,19 @@ trajectory_kernel(const TrajState* __restrict__ states, const double* __restrict
   cluster_sync();
 }
 
-template <int DP, int SYS>
+template <int DP, int SYS, int ENG = 0>
 static cudaError_t launch_dp(const TrajState* d_states, int nstates, const double* d_points, int npoints,
                              const TrajControls& ctl, cudaStream_t stream) {
   using GE = Geo<DP, SYS>;
-  auto kern = trajectory_kernel<DP, SYS>;
-  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GE::SMEM);
+  constexpr size_t smem = kernel_smem<DP, SYS, ENG>();
+  static_assert(smem <= 232448, "shared memory per CTA");
+  auto kern = trajectory_kernel<DP, SYS, ENG>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(nstates * GE::G, 1, 1);
   cfg.blockDim = dim3(GE::NT, 1, 1);
-  cfg.dynamicSmemBytes = GE::SMEM;
+  cfg.dynamicSmemBytes = smem;
   cfg.stream = stream;
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -1119,8 +1193,28 @@ static cudaError_t launch_sys(int dp, const TrajState* d_states, int nstates, co
   }
 }
 
+size_t split_state_bytes() { return split_engine::kStateBytes; }
+
+void split_state_pointers(unsigned char* block, TrajState& t) {
+  using namespace split_engine;
+  t.split_g1 = block;
+  t.split_g2 = block + kG1Bytes;
+  t.split_g1_scale = reinterpret_cast<const double*>(block + kG1Bytes + kG2Bytes);
+  t.split_g2_scale = reinterpret_cast<const double*>(block + kG1Bytes + kG2Bytes + kG1ScaleBytes);
+}
+
+cudaError_t split_prep_launch(const TrajState* d_states, int nstates, cudaStream_t stream) {
+  note_launch();
+  split_prep_kernel<<<dim3(nstates, 10), 256, 0, stream>>>(d_states);
+  return cudaGetLastError();
+}
+
 cudaError_t trajectory_launch(int system, int dp, const TrajState* d_states, int nstates, const double* d_points,
-                              int npoints, const TrajControls& ctl, cudaStream_t stream) {
+                              int npoints, const TrajControls& ctl, cudaStream_t stream, int engine) {
+  if (engine == 1) {
+    if (system != kSysQuartic || dp != 64) return cudaErrorInvalidValue;
+    return launch_dp<64, kSysQuartic, 1>(d_states, nstates, d_points, npoints, ctl, stream);
+  }
   if (system == kSysQuartic) return launch_sys<kSysQuartic>(dp, d_states, nstates, d_points, npoints, ctl, stream);
   if (system == kSysFull) return launch_sys<kSysFull>(dp, d_states, nstates, d_points, npoints, ctl, stream);
   if (system == kSysPhi1) return launch_sys<kSysPhi1>(dp, d_states, nstates, d_points, npoints, ctl, stream);

@@ -31,6 +31,12 @@ struct TrajState {
   int d;                              // physical bond dimension (d <= dp)
   int z2;                             // quartic system: 1 the packed Z2 error norm (10 (d/2)^2 + 1
                                       // entries), 0 the dense one, -1 refused (no exact Z2 structure)
+  // split-precision engine (dp = 64): BF16 slices of the constant operands and their scales,
+  // written by split_prep_launch (split_state_bytes() per state)
+  const unsigned char* split_g1;      // [rank 4][direction 2][chunk 2] panel^T slices, 48 KB each
+  const unsigned char* split_g2;      // [direction 2][chunk 4] [F1^T | F2^T] slices, 48 KB each
+  const double* split_g1_scale;       // [rank][direction][32]
+  const double* split_g2_scale;       // [direction][64]
 };
 
 struct TrajControls {
@@ -41,9 +47,14 @@ struct TrajControls {
 
 cudaError_t trajectory_set_tables();
 // system: 0 the reduced quartic system (7 channels + scalar), 1 the all-ODE route (26 channels),
-// 2 the first monomial of <phi> (4 channels).
+// 2 the first monomial of <phi> (4 channels). engine: 0 FP64 tensor cores (mma.sync), 1 the
+// split-precision BF16 engine on tcgen05 (system 0 and dp = 64 only; needs split_prep_launch).
 cudaError_t trajectory_launch(int system, int dp, const TrajState* d_states, int nstates, const double* d_points,
-                              int npoints, const TrajControls& ctl, cudaStream_t stream);
+                              int npoints, const TrajControls& ctl, cudaStream_t stream, int engine = 0);
+// Bytes of split-engine constants per state, and the kernel that writes them (dp = 64).
+size_t split_state_bytes();
+void split_state_pointers(unsigned char* block, TrajState& t);   // t.split_* inside `block`
+cudaError_t split_prep_launch(const TrajState* d_states, int nstates, cudaStream_t stream);
 int trajectory_channels(int system);
 cudaError_t node_weights_launch(const double* d_points, const double* d_weights, int n, double* d_wj,
                                 cudaStream_t stream);

@@ -27,7 +27,7 @@ class Settings(C.Structure):
         ("initial_step", C.c_double), ("max_steps", C.c_longlong), ("max_device_seconds", C.c_double),
         ("kinetic_nodes", C.c_int), ("krylov_tolerance", C.c_double), ("krylov_initialdim", C.c_int),
         ("krylov_maxdim", C.c_int), ("metric_reg", C.c_double), ("boundary_tolerance", C.c_double),
-        ("symmetry", C.c_int),
+        ("symmetry", C.c_int), ("precision", C.c_int),
     ]
 
 

@@ -264,18 +264,20 @@ def _k_from_q(q, r):
 def evaluate_quartic_persistent_trajectory(R, Q, rho, g=1.0, *, xp=None, half_window=30.0, n_quad=512,
                                            atol=1e-13, rtol=1e-12, initial_step=None, max_steps=1_000_000,
                                            max_device_seconds=30.0, return_samples=False, unpacked=False,
-                                           **ignored):
+                                           precision=0, **ignored):
     """g times the quartic value, raw covector and environment:
     dict(value, energy, covector, environment, stats[, samples]). As the reference
     (persistent_trajectory_backend.py:439-461), the packed Z2 route is the default and a state
     without the exact Z2 block structure raises ValueError; unpacked=True takes the seven
-    unpacked channels (any state). Packed samples have 10 (D/2)^2 + 1 entries per point."""
+    unpacked channels (any state). Packed samples have 10 (D/2)^2 + 1 entries per point.
+    precision=1 runs the trajectory products of a padded-64 state on the split-precision
+    tensor-core engine (rcmps_settings.precision)."""
     import torch
     d = _check_matrices(R, Q, rho)
     ctx = context()
     s = _lib.default_settings(half_window=float(half_window), n_quad=int(n_quad), atol=float(atol), rtol=float(rtol),
                               max_steps=int(max_steps), max_device_seconds=float(max_device_seconds),
-                              symmetry=SYMMETRY_NONE if unpacked else SYMMETRY_Z2)
+                              symmetry=SYMMETRY_NONE if unpacked else SYMMETRY_Z2, precision=int(precision))
     if initial_step is not None:
         s.initial_step = float(initial_step)
     K = _k_from_q(Q, R)
