@@ -32,7 +32,13 @@ sys.path[:0] = [str(ROOT), str(ROOT / "rcmpscore.jl_b200")]
 import numpy as np  # noqa: E402
 
 METRIC = "fg_phi4 evals/s at D=64 (energy + finished gradient), FP64"
+METRIC_SPLIT = ("fg_phi4 evals/s at D=64 (energy + finished gradient), split-precision trajectory products "
+                "(BF16 slices on tcgen05) vs FP64, |dE/E|<=1e-10")
 FLOPS_PER_RHS_D3 = 224      # 28 complex D^3 products (8 flops per complex multiply-add) per right-hand side
+# BF16 tensor flops the split engine executes per right-hand side of one D = 64 state (4 CTAs):
+# per CTA and chunk 28 slice pairs x 2 MMAs of M = 64, K = 16 and N = N_cat; chunks: 7 G1 units x 4
+# (N_cat 64), 3 paired G2 units x 8 (N_cat 64), 1 single G2 unit x 8 (N_cat 32)
+SPLIT_FLOPS_PER_RHS = 4 * 28 * 2 * 2 * 64 * 16 * (7 * 4 * 64 + 3 * 8 * 64 + 1 * 8 * 32)
 
 
 # ----------------------------------------------------------------------------- clocks
@@ -176,7 +182,9 @@ def run_b200(args, rank, world, local_rank):
     total = sum(d * d for d in dims)
     # the quartic route of each state as the reference takes it: packed Z2 for the Z2 states,
     # the unpacked channels for the others
-    s = _lib.default_settings(symmetry=2 if args.quartic_route == "auto" else 0)
+    split = args.precision == "split"
+    s = _lib.default_settings(symmetry=2 if args.quartic_route == "auto" else 0, precision=1 if split else 0,
+                              half_window=args.half_window, n_quad=args.n_quad)
     cdims = (C.c_int * n)(*dims)
     cg = (C.c_double * n)(*g)
     pack = lambda L: torch.from_numpy(np.concatenate([np.ascontiguousarray(x).ravel() for x in L])).cuda()
@@ -247,6 +255,26 @@ def run_b200(args, rank, world, local_rank):
     traj = statistics.mean(traj_ms)
     achieved = flops / (traj / 1000.0) / 1e12
     peak = lib.rcmps_fp64_peak_tflops(ctx.handle)
+    split_roofline = None
+    if split:
+        # the split engine runs on the BF16 tensor pipe: executed BF16 flops against the measured
+        # sustained cuBLAS BF16 throughput (the kernel runs inside a long step)
+        bf16 = sum(SPLIT_FLOPS_PER_RHS * rhs_calls[i] for i in range(n) if dims[i] == 64)
+        peaks = {}
+        pf = ROOT / "MEASURED_PEAKS.json"
+        if pf.exists():
+            try:
+                peaks = json.loads(pf.read_text())
+            except (OSError, ValueError):
+                peaks = {}
+        bpeak = peaks.get("bf16_tflops_sustained") or 1400.0
+        split_roofline = {"bound": "tensor", "achieved": bf16 / (traj / 1000.0) / 1e12, "peak": bpeak,
+                          "unit": "TFLOP/s", "frac": bf16 / (traj / 1000.0) / 1e12 / bpeak, "traffic": None,
+                          "kernel": "trajectory_kernel<64, quartic, split> (tcgen05.mma kind::f16, BF16 slices)",
+                          "peak_source": ("MEASURED_PEAKS.json bf16_tflops_sustained (of measured)"
+                                          if peaks.get("bf16_tflops_sustained") else "fallback 1.4 PFLOP/s"),
+                          "flops_per_launch": bf16, "launch_ms": traj,
+                          "fp64_equivalent_tflops": achieved}
     # DRAM traffic of one launch: bytes per right-hand side of one state from an ncu capture of a
     # smaller case at the same D, times this launch's right-hand sides (traffic grows with them)
     traffic = None
@@ -290,6 +318,32 @@ def run_b200(args, rank, world, local_rank):
         e2e = {"value": total_states * e2e_steps / wall, "unit": "evals/s",
                "h2d_bytes_per_step": 3 * total * 16 * world, "d2h_bytes_per_step": (n * 8 + total * 16) * world}
 
+    # per-state error of the split arm against the FP64 form on the same states (untimed)
+    split_error = None
+    if split and not quartic_only:
+        E_s, G_s = energy.cpu().numpy().copy(), grad.cpu().numpy().copy()
+        s64 = _lib.default_settings(symmetry=s.symmetry, precision=0)
+        rc = lib.rcmps_fg_phi4_batch(ctx.handle, n, cdims, cg, dR.data_ptr(), dK.data_ptr(), drho.data_ptr(),
+                                     C.byref(s64), energy.data_ptr(), grad.data_ptr(), None, None, stats, sptr)
+        if rc:
+            raise RuntimeError(f"fg_phi4 (FP64 comparison) failed: {ctx.error()}")
+        E_f, G_f = energy.cpu().numpy(), grad.cpu().numpy()
+        rho_h = drho.cpu().numpy()
+        rows, o = [], 0
+        for i in range(n):
+            d = dims[i]
+            rho_i = rho_h[o:o + d * d].reshape(d, d)
+            m = rho_i + 1e-3 * np.eye(d)
+            dg = (G_s[o:o + d * d] - G_f[o:o + d * d]).reshape(d, d)
+            gf = G_f[o:o + d * d].reshape(d, d)
+            metric = lambda x: float(np.sqrt(max(0.0, 2.0 * np.real(np.vdot(x, x @ m)))))
+            rows.append({"state": mine[i], "rel_energy": abs(E_s[i] - E_f[i]) / abs(E_f[i]),
+                         "rel_gradient": metric(dg) / max(1.0, metric(gf))})
+            o += d * d
+        split_error = {"against": "the FP64 tensor-core form of this library on the same states",
+                       "max_rel_energy": max(r["rel_energy"] for r in rows),
+                       "max_rel_gradient": max(r["rel_gradient"] for r in rows), "per_state": rows}
+
     cpu = None
     plan = cpu_eval_plan(args.workload)
     if rank == 0 and world == 1 and not args.no_cpu_baseline and plan:
@@ -298,11 +352,14 @@ def run_b200(args, rank, world, local_rank):
                "sample": (f"one complete fg_phi4 evaluation of workload state 0 (D={plan[0][0]}, random, seed "
                           f"{plan[0][1]}) with the oracle on one core: {t_eval:.1f} s")}
     if rank == 0:
-        metric = METRIC if not quartic_only else "quartic term (trajectory + pullback) evals/s at D=64, FP64"
+        metric = METRIC_SPLIT if split else METRIC
+        if quartic_only:
+            metric = "quartic term (trajectory + pullback) evals/s at D=64, " + ("split" if split else "FP64")
         line = {"metric": metric, "value": value, "unit": "evals/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": elapsed / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-                "config": {"workload": desc, "states_per_gpu": n, "half_window": 30.0, "n_quad": 512,
+                "config": {"workload": desc, "states_per_gpu": n, "half_window": args.half_window,
+                           "n_quad": args.n_quad,
                            "kinetic_nodes": 512, "atol": 1e-13, "rtol": 1e-12, "krylov_tolerance": 1e-12,
                            "l2": "inputs and workspaces exceed L2 (126 MB); no flush needed", "parallelism":
                            f"state shards over {world} GPU(s)",
@@ -330,6 +387,14 @@ def run_b200(args, rank, world, local_rank):
                 "gpu_launches": None, "gpu_launches_note": "library kernel launches per step (rcmps_launch_count)", "clocks": clocks.summary(), "e2e": e2e, "cpu_baseline": cpu}
         line["gpu_launches"] = launches
         line["launches_before_timed"] = launches0
+        line["config"]["precision"] = ("split: trajectory products of the D=64 states on tcgen05 BF16 slices "
+                                       "(7 x 7 bits), FP64 step control, sums and solves" if split else
+                                       "FP64 tensor cores (DMMA)")
+        if split:
+            line["dtype"] = "f64 (split bf16 trajectory products)"
+            line["roofline_fp64_form"] = line["roofline"]
+            line["roofline"] = split_roofline
+            line["split_error"] = split_error
         print(json.dumps(line), flush=True)
 
 
@@ -344,6 +409,12 @@ def main():
     p.add_argument("--quartic-route", choices=("auto", "unpacked"), default="auto",
                    help="auto: the packed Z2 route for the Z2 states (the reference's default for them); "
                         "unpacked: the seven unpacked channels for every state")
+    p.add_argument("--half-window", type=float, default=30.0,
+                   help="window W of the integration (profiling cases only; the benchmark uses 30)")
+    p.add_argument("--n-quad", type=int, default=512,
+                   help="Gauss nodes per half window (profiling cases only; the benchmark uses 512)")
+    p.add_argument("--precision", choices=("fp64", "split"), default="fp64",
+                   help="trajectory products: FP64 tensor cores, or split BF16 slices on tcgen05 (D = 64)")
     p.add_argument("--component", choices=("fg", "quartic"), default="fg",
                    help="time the whole evaluation (default) or the quartic term alone")
     args = p.parse_args()

@@ -145,11 +145,11 @@ RCMPS_DEVICE_INLINE void slice8(const double* v, unsigned char* dst, uint32_t st
   double r[8];
 #pragma unroll
   for (int e = 0; e < 8; ++e) r[e] = v[e];
-  constexpr float kWeight[8] = {1.0f, 0x1p-7f, 0x1p-14f, 0x1p-21f, 0x1p-28f, 0x1p-35f, 0x1p-42f, 0x1p-49f};
+  constexpr double kWeight[8] = {1.0, 0x1p-7, 0x1p-14, 0x1p-21, 0x1p-28, 0x1p-35, 0x1p-42, 0x1p-49};
   static_assert(kSlices <= 8 && kBits == 7, "slice weights");
 #pragma unroll
   for (int i = 0; i < kSlices; ++i) {
-    const float w = kWeight[i];
+    const double w = kWeight[i];
     uint32_t packed[4];
 #pragma unroll
     for (int e = 0; e < 8; e += 2) {
@@ -158,7 +158,8 @@ RCMPS_DEVICE_INLINE void slice8(const double* v, unsigned char* dst, uint32_t st
       const double t0 = rint(r[e]), t1 = rint(r[e + 1]);
       r[e] -= t0;
       r[e + 1] -= t1;
-      const __nv_bfloat16 b0 = __float2bfloat16_rn((float)t0 * w), b1 = __float2bfloat16_rn((float)t1 * w);
+      // t w has at most 8 significant bits: one exact conversion
+      const __nv_bfloat16 b0 = __double2bfloat16(t0 * w), b1 = __double2bfloat16(t1 * w);
       packed[e / 2] = (uint32_t)__bfloat16_as_ushort(b0) | ((uint32_t)__bfloat16_as_ushort(b1) << 16);
     }
     *reinterpret_cast<uint4*>(dst + (size_t)i * stride) = make_uint4(packed[0], packed[1], packed[2], packed[3]);

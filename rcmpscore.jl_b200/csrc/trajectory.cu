@@ -614,7 +614,7 @@ trajectory_kernel(const TrajState* __restrict__ states, const double* __restrict
         mbar_init(&sm.empty[i], GE::NW);
       }
     } else {
-      for (int i = 0; i < 6; ++i) mbar_init(&ssm.mma_done[i], 1);   // mma_done, acc_full, copy_full
+      split_barriers_init(ssm);
     }
     fence_mbar_init();
     C.t = -ctl_in.endpoint;
@@ -976,10 +976,13 @@ trajectory_kernel(const TrajState* __restrict__ states, const double* __restrict
     // every unit's epilogue waited for its MMAs; after a wait that gave up, wait (bounded) once
     // more for the last unit's and the last copies' barriers, then release TMEM
     if (tid == 0 && C.wait_flag && rhs.u > 0) {
+      using split_engine::kBufs;
       const long long uu = rhs.u - 1;
-      mbar_wait(&ssm.acc_full[uu & 1], (uint32_t)((uu >> 1) & 1), nullptr);
-      for (long long g = rhs.q - 1; g >= 0 && g >= rhs.q - 2; --g)
-        mbar_wait(&ssm.copy_full[g & 1], (uint32_t)((g >> 1) & 1), nullptr);
+      mbar_wait(&ssm.acc[uu & 1], (uint32_t)((uu >> 1) & 1), nullptr);
+      for (long long g = rhs.q - 1; g >= 0 && g >= rhs.q - kBufs; --g) {
+        mbar_wait(&ssm.copy[g % kBufs], (uint32_t)((g / kBufs) & 1), nullptr);
+        mbar_wait(&ssm.free[g % kBufs], (uint32_t)((g / kBufs) & 1), nullptr);
+      }
     }
     split::tc_fence_before();
     __syncthreads();

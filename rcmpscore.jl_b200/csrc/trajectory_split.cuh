@@ -17,30 +17,42 @@
 //     Re F2^T, Im F1^T, Im F2^T with the matching rows of B_cat.
 //     The epilogue adds k_c (jac Qc X_c from G1), the left insertion src coef P_a and the fixed
 //     terms, as the FP64 kernel does.
-// A unit is 4 (G1) or 8 (G2) chunks; chunk q is staged in shared-memory buffer q % 2 (A half and
-// B half, 28 KB each: seven slices of 4 KB) while the MMAs of chunk q - 1 run; the constant half
-// arrives by bulk copy (cp.async.bulk) on the buffer's copy barrier, the sliced half is written by
-// all threads. Unit u accumulates in the lane half u % 2 of TMEM (6 accumulators of 64 columns),
-// so the epilogue of unit u - 1 runs while the MMAs of unit u do. One thread issues every MMA and
-// copy; every wait on a barrier is bounded and sets the controller's wait flag.
+// A unit is 4 (G1) or 8 (G2) chunks. The work is split between warps:
+//   * builder warps 0-15 slice the per-stage operand of chunk q into shared-memory buffer q % 3
+//     (A half and B half, 28 KB each: seven slices of 4 KB) once the MMAs of chunk q - 3 released
+//     it, and arrive on the buffer's "full" barrier; they also run the epilogues;
+//   * the issuer (lane 0 of warp 16) bulk-copies (cp.async.bulk) the constant half of chunk q + 1
+//     ahead, waits for chunk q's full and copy barriers, issues its MMAs and commits them to the
+//     buffer's "free" barrier (and, after a unit's last chunk, to the unit's accumulator barrier).
+// Unit u accumulates in the lane half u % 2 of TMEM (6 accumulators of 64 columns). Its epilogue
+// runs in the builders' program order during unit u + 1, two chunks in, when its MMAs have long
+// completed, so the tensor pipe is not drained at unit boundaries; the builders' arrival on the
+// full barrier of unit u + 2's first chunk comes after that epilogue, which orders its TMEM reads
+// before the MMAs that overwrite the lane half. The epilogue's results (k_c and P_c rows) are
+// ordered for the later builds and epilogues by a named barrier of the builder warps. Every wait
+// on a barrier is bounded and sets the controller's wait flag.
 
 namespace split_engine {
 
 constexpr uint32_t kHalf = split::kSlices * split::block_bytes(64);   // one operand half
 constexpr uint32_t kBuf = 2 * kHalf;                                   // A half + B half
+constexpr int kBufs = 3;                                               // chunk buffers
 constexpr int kG1Chunks = 128 / split::kChunkK, kG2Chunks = 256 / split::kChunkK;
 constexpr int kKGroups = split::kChunkK / 8;                           // 8-element K groups per chunk
+constexpr int kBuilders = 512;                                         // threads of warps 0-15
+constexpr int kEpilogueChunk = 2;                                      // chunk of unit u + 1 after which unit u's epilogue runs
 constexpr size_t kG1Bytes = (size_t)4 * 2 * kG1Chunks * kHalf;         // [rank][dir][chunk] panel^T slices
 constexpr size_t kG2Bytes = (size_t)2 * kG2Chunks * kHalf;             // [dir][chunk] [F1^T | F2^T] slices
 constexpr size_t kG1ScaleBytes = (size_t)4 * 2 * 32 * 8;               // [rank][dir][32] column scales
 constexpr size_t kG2ScaleBytes = (size_t)2 * 64 * 8;                   // [dir][64] row scales
 constexpr size_t kStateBytes = kG1Bytes + kG2Bytes + kG1ScaleBytes + kG2ScaleBytes;
-// shared memory: two chunk buffers, scales [2][64] x 2, partial maxima [8][64], 6 barriers, TMEM slot
-constexpr size_t kOffRow = 2 * (size_t)kBuf;
-constexpr size_t kOffCol = kOffRow + 2 * 64 * 8;
-constexpr size_t kOffRed = kOffCol + 2 * 64 * 8;
+// shared memory: chunk buffers, G1 scales [7][64], G2 scales [4][32], partial maxima [8][64],
+// barriers (full, free, copy per buffer; accumulator per lane half), TMEM slot
+constexpr size_t kOffG1 = kBufs * (size_t)kBuf;
+constexpr size_t kOffG2 = kOffG1 + 7 * 64 * 8;
+constexpr size_t kOffRed = kOffG2 + 4 * 32 * 8;
 constexpr size_t kOffBar = kOffRed + 8 * 64 * 8;
-constexpr size_t kOffSlot = kOffBar + 6 * 8;
+constexpr size_t kOffSlot = kOffBar + (3 * kBufs + 2) * 8;
 constexpr size_t kEnd = kOffSlot + 16;
 constexpr uint32_t kTmemCols = 512;
 
@@ -48,12 +60,13 @@ constexpr uint32_t kTmemCols = 512;
 
 struct SplitSmem {
   unsigned char* buf;
-  double* srow;        // [2][64] scales of the M index (columns of the product's output matrix)
-  double* scol;        // [2][64] scales of the N index
+  double* g1scale;     // [7][64] per column of X_c (the G1 products' M index)
+  double* g2scale;     // [4][32] per own row of X', Y' of each G2 unit (its N index)
   double* red;         // [8][64] partial maxima
-  uint64_t* mma_done;  // [2] chunk buffer free again
-  uint64_t* acc_full;  // [2] accumulator lane half complete
-  uint64_t* copy_full; // [2] constant half landed
+  uint64_t* full;      // [kBufs] sliced half written (one arrival per builder warp)
+  uint64_t* free;      // [kBufs] MMAs of the buffer's chunk completed
+  uint64_t* copy;      // [kBufs] constant half landed
+  uint64_t* acc;       // [2] accumulator lane half complete
   uint32_t* tslot;     // TMEM base address written by tcgen05.alloc
 };
 
@@ -61,20 +74,39 @@ __device__ __forceinline__ SplitSmem split_carve(unsigned char* base) {
   using namespace split_engine;
   SplitSmem s;
   s.buf = base;
-  s.srow = reinterpret_cast<double*>(base + kOffRow);
-  s.scol = reinterpret_cast<double*>(base + kOffCol);
+  s.g1scale = reinterpret_cast<double*>(base + kOffG1);
+  s.g2scale = reinterpret_cast<double*>(base + kOffG2);
   s.red = reinterpret_cast<double*>(base + kOffRed);
-  s.mma_done = reinterpret_cast<uint64_t*>(base + kOffBar);
-  s.acc_full = s.mma_done + 2;
-  s.copy_full = s.mma_done + 4;
+  s.full = reinterpret_cast<uint64_t*>(base + kOffBar);
+  s.free = s.full + kBufs;
+  s.copy = s.free + kBufs;
+  s.acc = s.copy + kBufs;
   s.tslot = reinterpret_cast<uint32_t*>(base + kOffSlot);
   return s;
+}
+
+// Barrier initialization (thread 0): full counts one arrival per builder warp.
+__device__ __forceinline__ void split_barriers_init(const SplitSmem& s) {
+  using namespace split_engine;
+  for (int b = 0; b < kBufs; ++b) {
+    mbar_init(&s.full[b], kBuilders / 32);
+    mbar_init(&s.free[b], 1);
+    mbar_init(&s.copy[b], 1);
+  }
+  mbar_init(&s.acc[0], 1);
+  mbar_init(&s.acc[1], 1);
+}
+
+// Named barrier of the builder warps only (the issuer warp keeps issuing).
+__device__ __forceinline__ void builders_sync() {
+  asm volatile("bar.sync 1, %0;" ::"n"(split_engine::kBuilders) : "memory");
 }
 
 // One product unit of a right-hand side.
 struct SplitUnit {
   int g2;      // 0: G1 of channel c; 1: G2 of channels c .. c + nc - 1
   int c, nc, dir;
+  int g2i;     // index of the G2 unit (0..3)
 };
 
 template <int DP>
@@ -97,14 +129,17 @@ struct RhsSplit {
       U.g2 = 0;
       U.c = k;
       U.nc = 1;
+      U.g2i = 0;
     } else {
       U.g2 = 1;
       U.c = t.p_first[1][k - 7];
       U.nc = t.p_count[1][k - 7];
+      U.g2i = k - 7;
     }
     U.dir = t.dir[U.c];
     return U;
   }
+  __device__ static int chunks(const SplitUnit& U) { return U.g2 ? split_engine::kG2Chunks : split_engine::kG1Chunks; }
 
   // Y' = jac P_c + src coef_c X_b of own row r, column k (the same expression in the scale and
   // the slicing passes, so that every sliced value lies below its scale).
@@ -116,60 +151,49 @@ struct RhsSplit {
     return m;
   }
 
-  // Scales of unit U into srow[ab], scol[ab]; ends with a block barrier.
-  __device__ void scales(const SplitUnit& U, const double2* zb, double jac, double src, int ab) {
-    double* srow = ss.srow + ab * 64;
-    double* scol = ss.scol + ab * 64;
-    if (!U.g2) {
-      const double2* X = zb + (size_t)U.c * GE::MAT;
-      if (tid < 512) {
-        const int j = tid & 63, g = tid >> 6;
-        double mx = 0.0;
-#pragma unroll
-        for (int e = 0; e < 8; ++e) {
-          const double2 v = __ldcg(X + (size_t)(8 * g + e) * DP + j);
-          mx = fmax(mx, fmax(fabs(v.x), fabs(v.y)));
-        }
-        ss.red[g * 64 + j] = mx;
+  // Builders: scales of every column of the 7 channels of the stage vector (the G1 products'
+  // A rows), one column per thread.
+  __device__ void g1_scales(const double2* zb) {
+    for (int col = tid; col < 7 * 64; col += split_engine::kBuilders) {
+      const double2* X = zb + (size_t)(col / 64) * GE::MAT + (col % 64);
+      double mx = 0.0;
+#pragma unroll 8
+      for (int k = 0; k < 64; ++k) {
+        const double2 v = __ldcg(X + (size_t)k * DP);
+        mx = fmax(mx, fmax(fabs(v.x), fabs(v.y)));
       }
-      __syncthreads();
-      if (tid < 64) {
-        double mx = 0.0;
-        for (int g = 0; g < 8; ++g) mx = fmax(mx, ss.red[g * 64 + tid]);
-        srow[tid] = split::pow2_above(mx);
-      } else if (tid < 96) {
-        scol[tid - 64] = st->split_g1_scale[(rank * 2 + U.dir) * 32 + (tid - 64)];
-      }
-    } else {
-      const int rows = 16 * U.nc;
-      if (tid < rows * 8) {
-        const int n = tid >> 3, g = tid & 7, cc = U.c + n / 16, r = n % 16;
-        const double2* X = zb + (size_t)cc * GE::MAT + (size_t)(row0 + r) * DP;
-        double mx = 0.0;
-#pragma unroll
-        for (int e = 0; e < 8; ++e) {
-          const int k = 8 * g + e;
-          const double2 x = zscale(jac, __ldcg(X + k));
-          const double2 y = yprime(cc, r, k, zb, jac, src);
-          mx = fmax(mx, fmax(fmax(fabs(x.x), fabs(x.y)), fmax(fabs(y.x), fabs(y.y))));
-        }
-        ss.red[g * 64 + n] = mx;
-      }
-      __syncthreads();
-      if (tid < rows) {
-        double mx = 0.0;
-        for (int g = 0; g < 8; ++g) mx = fmax(mx, ss.red[g * 64 + tid]);
-        scol[tid] = split::pow2_above(mx);
-      } else if (tid >= 64 && tid < 128) {
-        srow[tid - 64] = st->split_g2_scale[U.dir * 64 + (tid - 64)];
-      }
+      ss.g1scale[col] = split::pow2_above(mx);
     }
-    __syncthreads();
+    builders_sync();
   }
 
-  // The sliced half of chunk kc of unit U into dst.
-  __device__ void build(const SplitUnit& U, int kc, const double2* zb, double jac, double src, int ab,
-                        unsigned char* dst) {
+  // Builders: scales of the own rows of X' and Y' of G2 unit U (its B columns).
+  __device__ void g2_scales(const SplitUnit& U, const double2* zb, double jac, double src) {
+    const int rows = 16 * U.nc;
+    if (tid < rows * 8) {
+      const int n = tid >> 3, g = tid & 7, cc = U.c + n / 16, r = n % 16;
+      const double2* X = zb + (size_t)cc * GE::MAT + (size_t)(row0 + r) * DP;
+      double mx = 0.0;
+#pragma unroll
+      for (int e = 0; e < 8; ++e) {
+        const int k = 8 * g + e;
+        const double2 x = zscale(jac, __ldcg(X + k));
+        const double2 y = yprime(cc, r, k, zb, jac, src);
+        mx = fmax(mx, fmax(fmax(fabs(x.x), fabs(x.y)), fmax(fabs(y.x), fabs(y.y))));
+      }
+      ss.red[g * 64 + n] = mx;
+    }
+    builders_sync();
+    if (tid < rows) {
+      double mx = 0.0;
+      for (int g = 0; g < 8; ++g) mx = fmax(mx, ss.red[g * 64 + tid]);
+      ss.g2scale[U.g2i * 32 + tid] = split::pow2_above(mx);
+    }
+    builders_sync();
+  }
+
+  // Builders: the sliced half of chunk kc of unit U into dst.
+  __device__ void build(const SplitUnit& U, int kc, const double2* zb, double jac, double src, unsigned char* dst) {
     using split_engine::kKGroups;
     const int koff = split::kChunkK * (kc % 2);   // complex K offset of the chunk within its block
     if (!U.g2) {
@@ -177,7 +201,7 @@ struct RhsSplit {
       const double2* X = zb + (size_t)U.c * GE::MAT;
       if (tid < 64 * kKGroups) {
         const int j = tid & 63, k8 = tid >> 6;
-        const double inv = 1.0 / ss.srow[ab * 64 + j];
+        const double inv = 1.0 / ss.g1scale[U.c * 64 + j];
         double v[8];
 #pragma unroll
         for (int e = 0; e < 8; ++e) {
@@ -194,7 +218,7 @@ struct RhsSplit {
         const int n_cat = tid % ncat, k8 = tid / ncat;
         const int n = n_cat % rows, cc = U.c + n / 16, r = n % 16;
         const bool second = n_cat >= rows;
-        const double inv = 1.0 / ss.scol[ab * 64 + n];
+        const double inv = 1.0 / ss.g2scale[U.g2i * 32 + n];
         const double2* X = zb + (size_t)cc * GE::MAT + (size_t)(row0 + r) * DP;
         double v[8];
 #pragma unroll
@@ -209,10 +233,11 @@ struct RhsSplit {
     }
   }
 
-  // Results of unit U (issued as unit number uu) from its TMEM lane half into k and P.
+  // Builders: results of unit U (issued as unit number uu) from its TMEM lane half into k and P;
+  // ends with a named barrier of the builders.
   __device__ void epilogue(const SplitUnit& U, long long uu, double2* kout, double jac, double src) {
     const int ab = (int)(uu & 1);
-    mbar_wait(&ss.acc_full[ab], (uint32_t)((uu >> 1) & 1), wait_flag);
+    mbar_wait(&ss.acc[ab], (uint32_t)((uu >> 1) & 1), wait_flag);
     split::tc_fence_after();
     const bool narrow = U.g2 && U.nc == 1;   // N_cat = 32: real columns 0..15, imaginary 16..31
     const int ncat = narrow ? 32 : 64;
@@ -223,12 +248,13 @@ struct RhsSplit {
                         (uint32_t)ncat, sum);
       const int j = 16 * quarter + (lane & 15);       // output column (the M index)
       const int part = narrow ? (lane >> 4) : h;       // 0 real, 1 imaginary
-      const double sj = ss.srow[ab * 64 + j] * 0x1p-14;
       const SysTab& t = T();
+      const double sj = (U.g2 ? st->split_g2_scale[U.dir * 64 + j] : ss.g1scale[U.c * 64 + j]) * 0x1p-14;
 #pragma unroll 4
       for (int i = 0; i < 16; ++i) {
         const int n = narrow ? i : 16 * (lane >> 4) + i;   // the N index
-        const double val = sum[i] * sj * ss.scol[ab * 64 + n];
+        const double sn = U.g2 ? ss.g2scale[U.g2i * 32 + n] : st->split_g1_scale[(rank * 2 + U.dir) * 32 + n];
+        const double val = sum[i] * sj * sn;
         if (!U.g2) {
           const int r = n & 15;
           const size_t off = (size_t)U.c * GE::MAT + (size_t)(row0 + r) * DP + j;
@@ -247,54 +273,90 @@ struct RhsSplit {
       }
     }
     split::tc_fence_before();
-    __syncthreads();
+    builders_sync();
+  }
+
+  // Issuer: the constant half of chunk (unit k, chunk kc), numbered qq, into its buffer.
+  __device__ void issue_copy(const SplitUnit& U, int kc, long long qq) {
+    using namespace split_engine;
+    const int b = (int)(qq % kBufs);
+    if (qq >= kBufs) mbar_wait(&ss.free[b], (uint32_t)((qq / kBufs - 1) & 1), wait_flag);
+    const unsigned char* srcp = U.g2 ? st->split_g2 + (size_t)(U.dir * kG2Chunks + kc) * kHalf
+                                     : st->split_g1 + (size_t)((rank * 2 + U.dir) * kG1Chunks + kc) * kHalf;
+    unsigned char* dst = ss.buf + (size_t)b * kBuf + (U.g2 ? 0 : kHalf);
+    mbar_expect_tx(&ss.copy[b], kHalf);
+#pragma unroll
+    for (int i = 0; i < split::kSlices; ++i)
+      bulk_g2s(dst + i * split::block_bytes(64), srcp + i * split::block_bytes(64), split::block_bytes(64), &ss.copy[b]);
   }
 
   // One right-hand side: k_out = f(t, z) on this CTA's rows (the FP64 kernel's contract).
   __device__ void operator()(const double2* zb, double2* kout, double jac, double src) {
     using namespace split_engine;
     const int nu = units();
-    SplitUnit prev{};
-    for (int k = 0; k < nu; ++k) {
-      const SplitUnit U = unit(k);
-      const int ab = (int)(u & 1);
-      const int nchunk = U.g2 ? kG2Chunks : kG1Chunks;
-      for (int kc = 0; kc < nchunk; ++kc) {
-        const int buf = (int)(q & 1);
-        unsigned char* bA = ss.buf + (size_t)buf * kBuf;
-        unsigned char* bB = bA + kHalf;
-        if (q >= 2) mbar_wait(&ss.mma_done[buf], (uint32_t)(((q >> 1) - 1) & 1), wait_flag);
-        if (tid == 0) {
-          const unsigned char* srcp = U.g2 ? st->split_g2 + (size_t)(U.dir * kG2Chunks + kc) * kHalf
-                                           : st->split_g1 + (size_t)((rank * 2 + U.dir) * kG1Chunks + kc) * kHalf;
-          unsigned char* dst = U.g2 ? bA : bB;
-          mbar_expect_tx(&ss.copy_full[buf], kHalf);
-#pragma unroll
-          for (int i = 0; i < split::kSlices; ++i)
-            bulk_g2s(dst + i * split::block_bytes(64), srcp + i * split::block_bytes(64), split::block_bytes(64),
-                     &ss.copy_full[buf]);
+    if (warp == kBuilders / 32) {
+      // ------------------------------------------------ issuer warp
+      if (lane == 0) {
+        long long qq = q, uu = u;
+        int nk = 0, nkc = 0;          // the next chunk whose copy is to be issued
+        auto advance = [&](int& k, int& kc) {
+          if (++kc == chunks(unit(k))) {
+            kc = 0;
+            ++k;
+          }
+        };
+        issue_copy(unit(0), 0, qq);
+        advance(nk, nkc);
+        for (int k = 0; k < nu; ++k, ++uu) {
+          const SplitUnit U = unit(k);
+          const int ab = (int)(uu & 1);
+          for (int kc = 0; kc < chunks(U); ++kc, ++qq) {
+            if (nk < nu) {             // the next chunk's constant half, one chunk ahead
+              issue_copy(unit(nk), nkc, qq + 1);
+              advance(nk, nkc);
+            }
+            const int b = (int)(qq % kBufs);
+            const uint32_t ph = (uint32_t)((qq / kBufs) & 1);
+            mbar_wait(&ss.full[b], ph, wait_flag);
+            mbar_wait(&ss.copy[b], ph, wait_flag);
+            split::tc_fence_after();
+            const uint32_t bA = smem_u32(ss.buf + (size_t)b * kBuf), bB = bA + kHalf;
+            const uint32_t acc = split::acc_addr(tmem, ab, 0);
+            if (U.g2 && U.nc == 1) split::chunk_mmas<32>(acc, bA, bB, kc == 0);
+            else split::chunk_mmas<64>(acc, bA, bB, kc == 0);
+            split::mma_commit(&ss.free[b]);
+            if (kc == chunks(U) - 1) split::mma_commit(&ss.acc[ab]);
+          }
         }
-        if (kc == 0) scales(U, zb, jac, src, ab);
-        build(U, kc, zb, jac, src, ab, U.g2 ? bB : bA);
-        split::fence_proxy_async_smem();
-        split::tc_fence_before();
-        __syncthreads();
-        if (tid == 0) {
-          mbar_wait(&ss.copy_full[buf], (uint32_t)((q >> 1) & 1), wait_flag);
-          split::tc_fence_after();
-          const uint32_t acc = split::acc_addr(tmem, ab, 0);
-          if (U.g2 && U.nc == 1) split::chunk_mmas<32>(acc, smem_u32(bA), smem_u32(bB), kc == 0);
-          else split::chunk_mmas<64>(acc, smem_u32(bA), smem_u32(bB), kc == 0);
-          split::mma_commit(&ss.mma_done[buf]);
-          if (kc == nchunk - 1) split::mma_commit(&ss.acc_full[ab]);
-        }
-        ++q;
-        if (kc == 0 && k > 0) epilogue(prev, u - 1, kout, jac, src);
       }
-      prev = U;
-      ++u;
+      __syncwarp();
+    } else {
+      // ------------------------------------------------ builder warps
+      g1_scales(zb);
+      long long qq = q, uu = u;
+      SplitUnit prev{};
+      for (int k = 0; k < nu; ++k, ++uu) {
+        const SplitUnit U = unit(k);
+        if (U.g2) g2_scales(U, zb, jac, src);
+        for (int kc = 0; kc < chunks(U); ++kc, ++qq) {
+          const int b = (int)(qq % kBufs);
+          if (qq >= kBufs) mbar_wait(&ss.free[b], (uint32_t)((qq / kBufs - 1) & 1), wait_flag);
+          unsigned char* bufp = ss.buf + (size_t)b * kBuf;
+          build(U, kc, zb, jac, src, U.g2 ? bufp + kHalf : bufp);
+          split::fence_proxy_async_smem();
+          split::tc_fence_before();
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&ss.full[b]);
+          if (kc == kEpilogueChunk && k > 0) epilogue(prev, uu - 1, kout, jac, src);
+        }
+        prev = U;
+      }
+      epilogue(prev, uu - 1, kout, jac, src);
     }
-    epilogue(prev, u - 1, kout, jac, src);
+    // every thread leaves with the same counters
+    for (int k = 0; k < nu; ++k) q += chunks(unit(k));
+    u += nu;
+    __syncthreads();
   }
 };
 
