@@ -204,13 +204,14 @@ def run_b200(args, rank, world, local_rank):
     quartic_only = args.component == "quartic"
     cov = torch.zeros(total, dtype=torch.complex128, device="cuda") if quartic_only else None
 
-    def step():
+    def step(settings=s):
         if quartic_only:   # the quartic term alone (trajectory + pullback): the small profiling case
             rc = lib.rcmps_quartic_batch(ctx.handle, n, cdims, cg, dR.data_ptr(), dK.data_ptr(), drho.data_ptr(),
-                                         C.byref(s), energy.data_ptr(), cov.data_ptr(), grad.data_ptr(), stats, sptr)
+                                         C.byref(settings), energy.data_ptr(), cov.data_ptr(), grad.data_ptr(), stats,
+                                         sptr)
         else:
             rc = lib.rcmps_fg_phi4_batch(ctx.handle, n, cdims, cg, dR.data_ptr(), dK.data_ptr(), drho.data_ptr(),
-                                         C.byref(s), energy.data_ptr(), grad.data_ptr(), None, None, stats, sptr)
+                                         C.byref(settings), energy.data_ptr(), grad.data_ptr(), None, None, stats, sptr)
         if rc:
             raise RuntimeError(f"{args.component} failed: {_lib.STATUS_NAMES.get(rc)} {ctx.error()}")
 
@@ -255,11 +256,11 @@ def run_b200(args, rank, world, local_rank):
     traj = statistics.mean(traj_ms)
     achieved = flops / (traj / 1000.0) / 1e12
     peak = lib.rcmps_fp64_peak_tflops(ctx.handle)
-    split_roofline = None
-    if split:
+    def split_roofline_of(traj_ms_split, rhs):
         # the split engine runs on the BF16 tensor pipe: executed BF16 flops against the measured
         # sustained cuBLAS BF16 throughput (the kernel runs inside a long step)
-        bf16 = sum(SPLIT_FLOPS_PER_RHS * rhs_calls[i] for i in range(n) if dims[i] == 64)
+        bf16 = sum(SPLIT_FLOPS_PER_RHS * rhs[i] for i in range(n) if dims[i] == 64)
+        fp64eq = sum(FLOPS_PER_RHS_D3 * rhs[i] * dims[i] ** 3 * (0.25 if packed[i] else 1.0) for i in range(n))
         peaks = {}
         pf = ROOT / "MEASURED_PEAKS.json"
         if pf.exists():
@@ -268,13 +269,16 @@ def run_b200(args, rank, world, local_rank):
             except (OSError, ValueError):
                 peaks = {}
         bpeak = peaks.get("bf16_tflops_sustained") or 1400.0
-        split_roofline = {"bound": "tensor", "achieved": bf16 / (traj / 1000.0) / 1e12, "peak": bpeak,
-                          "unit": "TFLOP/s", "frac": bf16 / (traj / 1000.0) / 1e12 / bpeak, "traffic": None,
-                          "kernel": "trajectory_kernel<64, quartic, split> (tcgen05.mma kind::f16, BF16 slices)",
-                          "peak_source": ("MEASURED_PEAKS.json bf16_tflops_sustained (of measured)"
-                                          if peaks.get("bf16_tflops_sustained") else "fallback 1.4 PFLOP/s"),
-                          "flops_per_launch": bf16, "launch_ms": traj,
-                          "fp64_equivalent_tflops": achieved}
+        rate = bf16 / (traj_ms_split / 1000.0) / 1e12
+        return {"bound": "tensor", "achieved": rate, "peak": bpeak, "unit": "TFLOP/s", "frac": rate / bpeak,
+                "traffic": None,
+                "kernel": "trajectory_kernel<64, quartic, split> (tcgen05.mma kind::f16, BF16 slices)",
+                "peak_source": ("MEASURED_PEAKS.json bf16_tflops_sustained (of measured)"
+                                if peaks.get("bf16_tflops_sustained") else "fallback 1.4 PFLOP/s"),
+                "flops_per_launch": bf16, "launch_ms": traj_ms_split,
+                "fp64_equivalent_tflops": fp64eq / (traj_ms_split / 1000.0) / 1e12}
+
+    split_roofline = split_roofline_of(traj, rhs_calls) if split else None
     # DRAM traffic of one launch: bytes per right-hand side of one state from an ncu capture of a
     # smaller case at the same D, times this launch's right-hand sides (traffic grows with them)
     traffic = None
@@ -318,16 +322,16 @@ def run_b200(args, rank, world, local_rank):
         e2e = {"value": total_states * e2e_steps / wall, "unit": "evals/s",
                "h2d_bytes_per_step": 3 * total * 16 * world, "d2h_bytes_per_step": (n * 8 + total * 16) * world}
 
-    # per-state error of the split arm against the FP64 form on the same states (untimed)
-    split_error = None
-    if split and not quartic_only:
+    def split_error_of():
+        """Per-state error of the split form against the FP64 form on the same states (untimed)."""
+        s_split = _lib.default_settings(symmetry=s.symmetry, precision=1, half_window=s.half_window, n_quad=s.n_quad)
+        s64 = _lib.default_settings(symmetry=s.symmetry, precision=0, half_window=s.half_window, n_quad=s.n_quad)
+        step(s_split)
         E_s, G_s = energy.cpu().numpy().copy(), grad.cpu().numpy().copy()
-        s64 = _lib.default_settings(symmetry=s.symmetry, precision=0)
-        rc = lib.rcmps_fg_phi4_batch(ctx.handle, n, cdims, cg, dR.data_ptr(), dK.data_ptr(), drho.data_ptr(),
-                                     C.byref(s64), energy.data_ptr(), grad.data_ptr(), None, None, stats, sptr)
-        if rc:
-            raise RuntimeError(f"fg_phi4 (FP64 comparison) failed: {ctx.error()}")
+        acc_s = [stats[i].accepted for i in range(n)]
+        step(s64)
         E_f, G_f = energy.cpu().numpy(), grad.cpu().numpy()
+        acc_f = [stats[i].accepted for i in range(n)]
         rho_h = drho.cpu().numpy()
         rows, o = [], 0
         for i in range(n):
@@ -338,11 +342,40 @@ def run_b200(args, rank, world, local_rank):
             gf = G_f[o:o + d * d].reshape(d, d)
             metric = lambda x: float(np.sqrt(max(0.0, 2.0 * np.real(np.vdot(x, x @ m)))))
             rows.append({"state": mine[i], "rel_energy": abs(E_s[i] - E_f[i]) / abs(E_f[i]),
-                         "rel_gradient": metric(dg) / max(1.0, metric(gf))})
+                         "rel_gradient": metric(dg) / max(1.0, metric(gf)),
+                         "accepted_split": acc_s[i], "accepted_fp64": acc_f[i]})
             o += d * d
-        split_error = {"against": "the FP64 tensor-core form of this library on the same states",
-                       "max_rel_energy": max(r["rel_energy"] for r in rows),
-                       "max_rel_gradient": max(r["rel_gradient"] for r in rows), "per_state": rows}
+        return {"against": "the FP64 tensor-core form of this library on the same states",
+                "max_rel_energy": max(r["rel_energy"] for r in rows),
+                "max_rel_gradient": max(r["rel_gradient"] for r in rows), "per_state": rows}
+
+    split_error = split_error_of() if split and not quartic_only else None
+
+    # the split-precision arm beside the FP64 one in the default run: the same workload and timing
+    split_arm = None
+    if not split and not quartic_only and args.split_arm_steps > 0 and any(d == 64 for d in dims):
+        s_split = _lib.default_settings(symmetry=s.symmetry, precision=1, half_window=s.half_window, n_quad=s.n_quad)
+        step(s_split)                          # warm-up
+        barrier()
+        t_ms = []
+        st0, st1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        st0.record(stream)
+        for _ in range(args.split_arm_steps):
+            step(s_split)
+            t_ms.append(ctx.timings()[0])
+        st1.record(stream)
+        barrier()
+        el = st0.elapsed_time(st1)
+        if dist is not None:
+            t = torch.tensor([el], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            el = float(t.item())
+        rhs_s = [stats[i].rhs_calls for i in range(n)]
+        v_split = total_states * args.split_arm_steps / (el / 1000.0)
+        split_arm = {"metric": METRIC_SPLIT, "value": v_split, "unit": "evals/s",
+                     "steps": args.split_arm_steps, "warmup": 1, "ms_per_step": el / args.split_arm_steps,
+                     "ratio_to_fp64": v_split / value, "trajectory_ms": statistics.mean(t_ms),
+                     "roofline": split_roofline_of(statistics.mean(t_ms), rhs_s), "split_error": split_error_of()}
 
     cpu = None
     plan = cpu_eval_plan(args.workload)
@@ -390,6 +423,8 @@ def run_b200(args, rank, world, local_rank):
         line["config"]["precision"] = ("split: trajectory products of the D=64 states on tcgen05 BF16 slices "
                                        "(7 x 7 bits), FP64 step control, sums and solves" if split else
                                        "FP64 tensor cores (DMMA)")
+        if split_arm is not None:
+            line["split_precision_arm"] = split_arm
         if split:
             line["dtype"] = "f64 (split bf16 trajectory products)"
             line["roofline_fp64_form"] = line["roofline"]
@@ -415,6 +450,8 @@ def main():
                    help="Gauss nodes per half window (profiling cases only; the benchmark uses 512)")
     p.add_argument("--precision", choices=("fp64", "split"), default="fp64",
                    help="trajectory products: FP64 tensor cores, or split BF16 slices on tcgen05 (D = 64)")
+    p.add_argument("--split-arm-steps", type=int, default=3,
+                   help="steps of the split-precision arm timed after the FP64 one (0: none)")
     p.add_argument("--component", choices=("fg", "quartic"), default="fg",
                    help="time the whole evaluation (default) or the quartic term alone")
     args = p.parse_args()

@@ -193,6 +193,17 @@ int rcmps_finish_gradient_batch(rcmps_context* context, int n_states, const int*
                                 const double* environment, const rcmps_settings* settings, double* gradient,
                                 rcmps_state_stats* stats, void* stream);
 
+/* The boundary Poisson solve alone: H with (-L*(H) + tr(rho H) I) = environment - tr(rho environment) I,
+ * by restarted GMRES(64) to |r| <= boundary_tolerance max(1, |b|), on device memory. x0 (packed, or
+ * NULL) is an initial guess of H for each state (a warm start, e.g. the learned one of
+ * rcmps_b200.warmstart); the target and the acceptance test do not depend on it. H is written
+ * packed; stats[i].gmres_iterations and boundary_residual report the solve. Replaces
+ * boundary_environment(q, r, rho, environment, tolerance) -> (H, stats) (runtime/numerics.py:103-117). */
+int rcmps_boundary_environment_batch(rcmps_context* context, int n_states, const int* dims, const double* R,
+                                     const double* K, const double* rho, const double* environment, const double* x0,
+                                     const rcmps_settings* settings, double* H, rcmps_state_stats* stats,
+                                     void* stream);
+
 /* rcmps_finish_gradient_batch for ONE state, without allocating anything: no cudaMalloc, no
  * cudaFree, no pinned host buffer. No counterpart in the reference. It serves callers that may
  * not allocate at the moment they need the finished gradient: a host whose memory planner
@@ -238,6 +249,21 @@ int rcmps_stationary_correction_batch(rcmps_context* context, int n_states, cons
  * the reference; the engine's unit-level check. */
 int rcmps_split_product_batch(rcmps_context* context, int n_states, int d, const double* A, const double* B,
                               double* C, void* stream);
+
+/* Kernels of the learned GMRES warm start (rcmps_b200.warmstart), FP32, device memory, row-major.
+ * No counterpart in the reference. The network maps n = 2 d^2 reals of a right-hand side of the
+ * boundary solve to an approximate solution: H = W1 X (W1: rank x n, X: n x batch, one sample per
+ * column), Y = W2 H (W2: n x rank). */
+int rcmps_warmstart_forward(rcmps_context* context, int n, int rank, int batch, const float* W1, const float* W2,
+                            const float* X, float* H, float* Y, void* stream);
+/* Gradients of loss = sum (Y - T)^2 / batch: dY = 2 (Y - T) / batch, dW2 = dY H^T, dH = W2^T dY,
+ * dW1 = dH X^T (dY: n x batch and dH: rank x batch are caller scratch); *loss (device double). */
+int rcmps_warmstart_backward(rcmps_context* context, int n, int rank, int batch, const float* W2, const float* X,
+                             const float* H, const float* Y, const float* T, float* dY, float* dH, float* dW1,
+                             float* dW2, double* loss, void* stream);
+/* One Adam step (step >= 1, bias-corrected) of `count` parameters with gradients and moments m, v. */
+int rcmps_warmstart_adam(rcmps_context* context, long long count, float* param, const float* grad, float* m, float* v,
+                         float lr, float beta1, float beta2, float eps, int step, void* stream);
 
 /* Number of kernel launches this library has issued in the process (all contexts). No
  * counterpart in the reference. */

@@ -514,6 +514,41 @@ int rcmps_finish_gradient_batch(rcmps_context* ctx, int n, const int* dims, cons
   return finish_run(ctx, job, s);
 }
 
+int rcmps_boundary_environment_batch(rcmps_context* ctx, int n, const int* dims, const double* R, const double* K,
+                                     const double* rho, const double* environment, const double* x0,
+                                     const rcmps_settings* settings, double* H, rcmps_state_stats* stats,
+                                     void* stream) {
+  if (!ctx) return RCMPS_INVALID_ARGUMENT;
+  int rc = check_settings(ctx, settings);
+  if (rc) return rc;
+  rc = check_dims(ctx, n, dims);
+  if (rc) return rc;
+  if (n == 0) return RCMPS_OK;
+  if (!R || !K || !rho || !environment || !H || !stats) return fail(ctx, RCMPS_INVALID_ARGUMENT, "NULL pointer");
+  cudaSetDevice(ctx->device);
+  for (int i = 0; i < n; ++i) std::memset(&stats[i], 0, sizeof(rcmps_state_stats));
+  FinishJob job;
+  job.n = n;
+  job.dims = dims;
+  job.R = R;
+  job.K = K;
+  job.rho = rho;
+  job.environment = environment;
+  job.x0 = x0;
+  job.settings = *settings;
+  job.stats = stats;
+  job.slot = 2;
+  cudaStream_t cs = stream ? static_cast<cudaStream_t>(stream) : nullptr;
+  cudaStream_t s2 = ctx->slot[2].stream;
+  cudaEvent_t ready = ctx->slot[2].ev[3];
+  cudaEventRecord(ready, cs);
+  cudaStreamWaitEvent(s2, ready, 0);
+  rc = boundary_run(ctx, job, H, s2);
+  cudaEventRecord(ready, s2);
+  cudaStreamWaitEvent(cs, ready, 0);
+  return rc;
+}
+
 int rcmps_stationary_state_batch(rcmps_context* ctx, int n, const int* dims, const double* R, const double* K,
                                  double tolerance, double* rho, rcmps_state_stats* stats, void* stream) {
   if (!ctx) return RCMPS_INVALID_ARGUMENT;

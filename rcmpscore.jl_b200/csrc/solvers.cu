@@ -40,6 +40,28 @@ __global__ void gmres_residual(ArnoldiProblem* __restrict__ probs, int nprob, in
   }
 }
 
+// bnorm = |b| of every problem (one CTA per problem): the stopping target of a warm-started solve
+__global__ void gmres_bnorm(ArnoldiProblem* __restrict__ probs, int nprob) {
+  ArnoldiProblem& P = probs[blockIdx.x];
+  double s = 0.0;
+  for (int r = threadIdx.x; r < P.n; r += blockDim.x) s += zabs2(P.b[r]);
+  __shared__ double red[32];
+  s = warp_sum(s);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
+    P.bnorm = sqrt(t);
+  }
+}
+
+cudaError_t gmres_bnorm_launch(ArnoldiProblem* probs, int nprob, cudaStream_t stream) {
+  note_launch();
+  gmres_bnorm<<<nprob, 256, 0, stream>>>(probs, nprob);
+  return cudaGetLastError();
+}
+
 // beta = |r|; converged if beta <= gtarget; V_0 /= beta; g = beta e1; H = 0
 __global__ void gmres_start(ArnoldiProblem* __restrict__ probs, int nprob, int nchunk) {
   const int p = blockIdx.y, ch = blockIdx.x;

@@ -34,6 +34,7 @@ struct StationaryArgs {
 };
 
 cudaError_t gmres_residual_launch(ArnoldiProblem* d, int nprob, int n, cudaStream_t s);
+cudaError_t gmres_bnorm_launch(ArnoldiProblem* d, int nprob, cudaStream_t s);
 cudaError_t gmres_givens_launch(ArnoldiProblem* d, int nprob, int j, cudaStream_t s);
 cudaError_t gmres_update_launch(ArnoldiProblem* d, int nprob, int n, int kmax, cudaStream_t s);
 cudaError_t gmres_x_tasks_launch(const ArnoldiProblem* d, int nprob, LindbladTask* tasks, cudaStream_t s);

@@ -87,9 +87,12 @@ static cudaError_t gmres_cycle(rcmps_context* ctx, ArnoldiProblem* d_probs, int 
 // Restarted GMRES(m) over NP problems that share dp; hp/d_probs hold set-up problems with x = 0.
 // Returns 0, or a CUDA error code. Convergence per problem is in hp[p].converged / residual.
 static cudaError_t gmres_run(rcmps_context* ctx, ArnoldiProblem* hp, ArnoldiProblem* d_probs, int NP, int dp,
-                             int m, int maxrestart, LindbladTask* d_tasks, cudaStream_t stream) {
+                             int m, int maxrestart, LindbladTask* d_tasks, cudaStream_t stream,
+                             bool bnorm_from_b = false) {
   const int nvec = dp * dp;
   cudaError_t e = cudaMemcpyAsync(d_probs, hp, NP * sizeof(ArnoldiProblem), cudaMemcpyHostToDevice, stream);
+  // a warm start: the first residual is not |b|, so |b| is measured for the stopping target
+  if (!e && bnorm_from_b) e = gmres_bnorm_launch(d_probs, NP, stream);
   for (int it = 0; it <= maxrestart && !e; ++it) {
     e = gmres_x_tasks_launch(d_probs, NP, d_tasks, stream);
     if (!e) e = lindblad_launch(dp, d_tasks, NP, 0, stream);
@@ -249,6 +252,8 @@ int finish_solve(rcmps_context* ctx, FinishJob& job, cudaStream_t stream, Finish
     if (!e) e = cudaMemcpyAsync(P(g.o_off), ho, n * 8, cudaMemcpyHostToDevice, stream);
     if (!e) e = cudaMemsetAsync(P(g.o_status), 0, n * 4, stream);
     if (!e) e = cudaMemsetAsync(P(g.gb.o_x), 0, (size_t)n * mat * 16, stream);
+    if (!e && job.x0)
+      e = launch_pad(job.x0, (long long*)P(g.o_off), (int*)P(g.o_dims), (double*)P(g.gb.o_x), dp, mat, n, stream);
     if (!e) e = launch_pad(job.R, (long long*)P(g.o_off), (int*)P(g.o_dims), dR, dp, mat, n, stream);
     if (!e) e = launch_pad(job.K, (long long*)P(g.o_off), (int*)P(g.o_dims), dK, dp, mat, n, stream);
     if (!e) e = launch_pad(job.rho, (long long*)P(g.o_off), (int*)P(g.o_dims), dP, dp, mat, n, stream);
@@ -269,9 +274,46 @@ int finish_solve(rcmps_context* ctx, FinishJob& job, cudaStream_t stream, Finish
       A.b = fa.b + (size_t)i * mat;
     }
     e = gmres_run(ctx, hp, (ArnoldiProblem*)P(g.gb.o_probs), n, dp, m, maxrestart, (LindbladTask*)P(g.gb.o_tasks),
-                  stream);
+                  stream, job.x0 != nullptr);
     if (e) return fail(ctx, RCMPS_CUDA_ERROR, std::string("boundary GMRES: ") + cudaGetErrorString(e));
   }
+  return RCMPS_OK;
+}
+
+int boundary_run(rcmps_context* ctx, FinishJob& job, double* H, cudaStream_t stream) {
+  FinishPlan plan;
+  int rc = finish_solve(ctx, job, stream, plan);
+  if (rc) return rc;
+  const double tol = job.settings.boundary_tolerance;
+  rcmps_slot& SL = ctx->slot[job.slot];
+  char* base = static_cast<char*>(SL.arena);
+  char* h = static_cast<char*>(SL.pinned);
+  cudaError_t e = cudaSuccess;
+  for (auto& g : plan.groups) {
+    const size_t mat = (size_t)g.dp * g.dp;
+    e = launch_unpad_acc(reinterpret_cast<double*>(base + g.gb.o_x), (long long)mat, g.dp,
+                         reinterpret_cast<long long*>(base + g.o_off), reinterpret_cast<int*>(base + g.o_dims), H, g.n,
+                         false, stream);
+    if (e) break;
+  }
+  if (!e) e = cudaStreamSynchronize(stream);
+  if (e) return fail(ctx, RCMPS_CUDA_ERROR, std::string("boundary solution: ") + cudaGetErrorString(e));
+  for (auto& g : plan.groups) {
+    const ArnoldiProblem* hp = reinterpret_cast<const ArnoldiProblem*>(h + g.h_probs);
+    for (int i = 0; i < g.n; ++i) {
+      rcmps_state_stats& st = job.stats[g.idx[i]];
+      const ArnoldiProblem& A = hp[i];
+      st.gmres_iterations = A.iters;
+      st.boundary_residual = A.residual;
+      const bool ok = A.converged || A.residual <= 20.0 * tol * std::max(1.0, A.bnorm);
+      if (!st.status && (A.nonfinite || !std::isfinite(A.residual) || !ok)) {
+        st.status = RCMPS_SOLVE_FAILURE;
+        st.failed_component = 4;
+      }
+    }
+  }
+  for (int i = 0; i < job.n; ++i)
+    if (job.stats[i].status) return job.stats[i].status;
   return RCMPS_OK;
 }
 

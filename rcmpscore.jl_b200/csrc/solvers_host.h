@@ -16,6 +16,9 @@ struct FinishJob {
   double* gradient = nullptr;                 // device, packed
   rcmps_state_stats* stats = nullptr;         // host [n]
   int slot = 2;
+  // device, packed, optional: initial guesses of the boundary Poisson solutions (a warm start);
+  // the stopping target stays tol max(1, |b|)
+  const double* x0 = nullptr;
 };
 
 struct StationaryJob {
@@ -48,5 +51,7 @@ struct FinishPlan {
 int finish_solve(rcmps_context* ctx, FinishJob& job, cudaStream_t stream, FinishPlan& plan);
 int finish_complete(rcmps_context* ctx, FinishJob& job, cudaStream_t stream, FinishPlan& plan);
 int stationary_run(rcmps_context* ctx, StationaryJob& job, cudaStream_t stream);
+// The boundary Poisson solve alone: H (device, packed) and the per-state GMRES statistics.
+int boundary_run(rcmps_context* ctx, FinishJob& job, double* H, cudaStream_t stream);
 
 }  // namespace rcmps

@@ -84,12 +84,18 @@ SIGNATURES = {
                                  C.POINTER(StateStats), _P]),
     "rcmps_finish_gradient_batch": (_I, [_P, _I, C.POINTER(_I), _P, _P, _P, _P, _P, C.POINTER(Settings), _P,
                                          C.POINTER(StateStats), _P]),
+    "rcmps_boundary_environment_batch": (_I, [_P, _I, C.POINTER(_I), _P, _P, _P, _P, _P, C.POINTER(Settings), _P,
+                                              C.POINTER(StateStats), _P]),
     "rcmps_finish_gradient_noalloc": (_I, [_P, _I, _P, _P, _P, _P, _P, C.POINTER(Settings), _P,
                                            C.POINTER(StateStats), _P]),
     "rcmps_stationary_state_batch": (_I, [_P, _I, C.POINTER(_I), _P, _P, _D, _P, C.POINTER(StateStats), _P]),
     "rcmps_stationary_correction_batch": (_I, [_P, _I, C.POINTER(_I), _P, _P, _P, _D, _P, C.POINTER(StateStats),
                                                _P]),
     "rcmps_split_product_batch": (_I, [_P, _I, _I, _P, _P, _P, _P]),
+    "rcmps_warmstart_forward": (_I, [_P, _I, _I, _I, _P, _P, _P, _P, _P, _P]),
+    "rcmps_warmstart_backward": (_I, [_P, _I, _I, _I, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
+    "rcmps_warmstart_adam": (_I, [_P, C.c_longlong, _P, _P, _P, _P, C.c_float, C.c_float, C.c_float, C.c_float, _I,
+                                  _P]),
     "rcmps_fp64_peak_tflops": (_D, [_P]),
     "rcmps_launch_count": (C.c_longlong, []),
 }

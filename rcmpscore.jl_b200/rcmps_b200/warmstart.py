@@ -1,0 +1,163 @@
+"""Learned warm start of the boundary Poisson GMRES (the solve behind every finished gradient).
+
+The boundary solve (-L*(H) + tr(rho H) I) = b, b = E - tr(rho E) I, is linear in b: its solution
+map is the inverse of a d^2 x d^2 operator that changes slowly along an optimizer run. Restarted
+GMRES spends most of its iterations on the few slowly converging directions of that operator.
+WarmStartNet learns them: a small network y = W2 (W1 x) (two linear layers, x the 2 d^2 real
+entries of b scaled to unit norm, rank r hidden units) is trained on (state, right-hand side,
+solution) triples that the plain GPU solver emits for the states an optimizer visits, and then
+proposes the initial guess H0 = |b| W2 W1 (b / |b|) of a later solve. Its training and
+inference run on the GPU through the library's own kernels (rcmps_warmstart_forward / _backward
+/ _adam: FP32 tiled GEMMs, the mean-squared-error gradient, Adam); the gradients are checked
+against a NumPy restatement (oracle/warmstart_oracle.py).
+
+The GMRES residual judges every answer: a warm-started solve stops at the same target,
+|b - A H| <= tol max(1, |b|), as the cold one, and unpreconditioned GMRES from zero remains the
+fallback (a guess worse than zero only costs iterations, never accuracy).
+
+No counterpart in the reference (its solves are preconditioned by the no-jump inverse,
+numerics.py:37-71, and start from zero).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+
+import numpy as np
+
+from . import _lib
+from .objective import _stream, boundary_environment_batch, context
+
+__all__ = ["WarmStartNet", "random_environments", "solve_triples", "gmres_gain"]
+
+
+def random_environments(rho, count, rng):
+    """`count` right-hand sides of the boundary solve for a state with density rho: i.i.d.
+    standard complex Gaussian d x d matrices, projected so that tr(rho E) = 0 (then b = E)."""
+    d = len(rho)
+    out = []
+    for _ in range(count):
+        g = (rng.standard_normal((d, d)) + 1j * rng.standard_normal((d, d))) / math.sqrt(2.0)
+        out.append(g - np.trace(rho @ g) * np.eye(d))
+    return out
+
+
+def solve_triples(R, K, rho, environments, *, tolerance=1e-13):
+    """(b, H) pairs of one state by the plain solver (GMRES from zero): the training data."""
+    H, stats = boundary_environment_batch([R] * len(environments), [K] * len(environments),
+                                          [rho] * len(environments), environments, tolerance=tolerance)
+    eye = np.eye(len(rho))
+    return [np.asarray(e) - np.trace(rho @ e) * eye for e in environments], H, stats
+
+
+def _to_real(mats):
+    """Samples as columns: (n = 2 d^2, count) float32, each column (Re, Im) interleaved."""
+    return np.ascontiguousarray(np.stack([np.asarray(m, np.complex128).view(np.float64).ravel() for m in mats],
+                                         axis=1).astype(np.float32))
+
+
+def _from_real(cols, d):
+    cols = np.asarray(cols, np.float64)
+    return [cols[:, j].copy().view(np.complex128).reshape(d, d) for j in range(cols.shape[1])]
+
+
+class WarmStartNet:
+    """Two linear layers, W1 (rank x n) and W2 (n x rank), FP32 on the GPU; n = 2 d^2."""
+
+    def __init__(self, d, rank=128, seed=0, device=None):
+        import torch
+        self.d, self.rank, self.n = int(d), int(rank), 2 * int(d) * int(d)
+        self.ctx = context(device)
+        g = np.random.default_rng(seed)
+        w1 = g.standard_normal((self.rank, self.n)) / math.sqrt(self.n)
+        w2 = g.standard_normal((self.n, self.rank)) * (0.1 / math.sqrt(self.rank))
+        self.W1 = torch.from_numpy(w1.astype(np.float32)).cuda()
+        self.W2 = torch.from_numpy(w2.astype(np.float32)).cuda()
+        self._m = [torch.zeros_like(self.W1), torch.zeros_like(self.W2)]
+        self._v = [torch.zeros_like(self.W1), torch.zeros_like(self.W2)]
+        self.step = 0
+
+    def _check(self, rc, what):
+        if rc:
+            raise RuntimeError(f"{what}: {_lib.STATUS_NAMES.get(rc, rc)} ({self.ctx.error()})")
+
+    def forward_device(self, X):
+        """H = W1 X, Y = W2 H for device float32 X of shape (n, batch)."""
+        import torch
+        batch = X.shape[1]
+        H = torch.empty((self.rank, batch), dtype=torch.float32, device="cuda")
+        Y = torch.empty((self.n, batch), dtype=torch.float32, device="cuda")
+        self._check(self.ctx.lib.rcmps_warmstart_forward(self.ctx.handle, self.n, self.rank, batch,
+                                                         self.W1.data_ptr(), self.W2.data_ptr(), X.data_ptr(),
+                                                         H.data_ptr(), Y.data_ptr(), _stream()), "forward")
+        return H, Y
+
+    def loss_and_grads(self, X, T):
+        """(loss, dW1, dW2) of loss = sum (Y - T)^2 / batch on device float32 samples."""
+        import torch
+        batch = X.shape[1]
+        H, Y = self.forward_device(X)
+        dY = torch.empty_like(Y)
+        dH = torch.empty_like(H)
+        dW1 = torch.empty_like(self.W1)
+        dW2 = torch.empty_like(self.W2)
+        loss = torch.zeros(1, dtype=torch.float64, device="cuda")
+        self._check(self.ctx.lib.rcmps_warmstart_backward(self.ctx.handle, self.n, self.rank, batch,
+                                                          self.W2.data_ptr(), X.data_ptr(), H.data_ptr(),
+                                                          Y.data_ptr(), T.data_ptr(), dY.data_ptr(), dH.data_ptr(),
+                                                          dW1.data_ptr(), dW2.data_ptr(), loss.data_ptr(),
+                                                          _stream()), "backward")
+        return float(loss.item()), dW1, dW2
+
+    def _adam(self, grads, lr):
+        self.step += 1
+        for p, g, m, v in zip((self.W1, self.W2), grads, self._m, self._v):
+            self._check(self.ctx.lib.rcmps_warmstart_adam(self.ctx.handle, p.numel(), p.data_ptr(), g.data_ptr(),
+                                                          m.data_ptr(), v.data_ptr(), C.c_float(lr),
+                                                          C.c_float(0.9), C.c_float(0.999), C.c_float(1e-8),
+                                                          self.step, _stream()), "adam")
+
+    def fit(self, rhs, solutions, *, epochs=200, batch=128, lr=2e-3, seed=0):
+        """Train on (b, H) pairs (lists of d x d complex matrices): each pair scaled by 1/|b| (the
+        map is linear), Adam on the mean squared error. Returns the loss of every epoch."""
+        import torch
+        scale = np.array([np.linalg.norm(b) for b in rhs])
+        X = torch.from_numpy(_to_real([b / s for b, s in zip(rhs, scale)])).cuda()
+        T = torch.from_numpy(_to_real([h / s for h, s in zip(solutions, scale)])).cuda()
+        count = X.shape[1]
+        g = np.random.default_rng(seed)
+        losses = []
+        for _ in range(epochs):
+            order = torch.from_numpy(g.permutation(count)).cuda()
+            total = 0.0
+            for s0 in range(0, count, batch):
+                idx = order[s0:s0 + batch]
+                xb, tb = X[:, idx].contiguous(), T[:, idx].contiguous()
+                loss, dW1, dW2 = self.loss_and_grads(xb, tb)
+                self._adam((dW1, dW2), lr)
+                total += loss * xb.shape[1]
+            losses.append(total / count)
+        return losses
+
+    def predict(self, rhs):
+        """Initial guesses |b| W2 W1 (b / |b|) for a list of right-hand sides."""
+        import torch
+        scale = np.array([max(np.linalg.norm(b), 1e-300) for b in rhs])
+        X = torch.from_numpy(_to_real([b / s for b, s in zip(rhs, scale)])).cuda()
+        _, Y = self.forward_device(X)
+        return [h * s for h, s in zip(_from_real(Y.cpu().numpy(), self.d), scale)]
+
+
+def gmres_gain(net, R, K, rho, environments, *, tolerance=1e-13):
+    """GMRES matrix-vector products and residuals of the same solves started from zero (the
+    fallback) and from the network's guess: dict(cold, warm, cold_residual, warm_residual,
+    solution_difference)."""
+    rhs = [e - np.trace(rho @ e) * np.eye(len(rho)) for e in environments]
+    n = len(environments)
+    H0, st0 = boundary_environment_batch([R] * n, [K] * n, [rho] * n, environments, tolerance=tolerance)
+    H1, st1 = boundary_environment_batch([R] * n, [K] * n, [rho] * n, environments, tolerance=tolerance,
+                                         x0=net.predict(rhs))
+    diff = max(np.abs(a - b).max() / max(1.0, np.abs(a).max()) for a, b in zip(H0, H1))
+    return {"cold": [s["matvecs"] for s in st0], "warm": [s["matvecs"] for s in st1],
+            "cold_residual": [s["residual"] for s in st0], "warm_residual": [s["residual"] for s in st1],
+            "target": [tolerance * max(1.0, float(np.linalg.norm(b))) for b in rhs], "solution_difference": diff}
