@@ -193,16 +193,30 @@ int rcmps_finish_gradient_batch(rcmps_context* context, int n_states, const int*
                                 const double* environment, const rcmps_settings* settings, double* gradient,
                                 rcmps_state_stats* stats, void* stream);
 
+/* A learned approximate inverse of the boundary operator, used as the right preconditioner of a
+ * flexible GMRES: M v = W2 (W1 v) + identity v on the n = 2 d^2 reals of a d x d matrix ((Re, Im)
+ * interleaved, row-major), FP32 device weights W1 (rank x n) and W2 (n x rank) trained by
+ * rcmps_warmstart_* (rcmps_b200.warmstart). No counterpart in the reference. */
+typedef struct rcmps_gmres_network {
+  const float* W1;
+  const float* W2;
+  int n, rank;
+  float identity;
+} rcmps_gmres_network;
+
 /* The boundary Poisson solve alone: H with (-L*(H) + tr(rho H) I) = environment - tr(rho environment) I,
  * by restarted GMRES(64) to |r| <= boundary_tolerance max(1, |b|), on device memory. x0 (packed, or
  * NULL) is an initial guess of H for each state (a warm start, e.g. the learned one of
- * rcmps_b200.warmstart); the target and the acceptance test do not depend on it. H is written
- * packed; stats[i].gmres_iterations and boundary_residual report the solve. Replaces
+ * rcmps_b200.warmstart); network (or NULL) a learned right preconditioner, applied in flexible
+ * GMRES (the basis passes through M in FP32, the Arnoldi relation and the update stay FP64, so
+ * the attainable accuracy is that of the plain solve); every state then has the network's d.
+ * Neither changes the stopping target or the acceptance test. H is written packed;
+ * stats[i].gmres_iterations and boundary_residual report the solve. Replaces
  * boundary_environment(q, r, rho, environment, tolerance) -> (H, stats) (runtime/numerics.py:103-117). */
 int rcmps_boundary_environment_batch(rcmps_context* context, int n_states, const int* dims, const double* R,
                                      const double* K, const double* rho, const double* environment, const double* x0,
-                                     const rcmps_settings* settings, double* H, rcmps_state_stats* stats,
-                                     void* stream);
+                                     const rcmps_gmres_network* network, const rcmps_settings* settings, double* H,
+                                     rcmps_state_stats* stats, void* stream);
 
 /* rcmps_finish_gradient_batch for ONE state, without allocating anything: no cudaMalloc, no
  * cudaFree, no pinned host buffer. No counterpart in the reference. It serves callers that may

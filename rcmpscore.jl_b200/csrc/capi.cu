@@ -250,6 +250,26 @@ __global__ void fp64_peak_kernel(double* out, int iters) {
 
 using namespace rcmps;
 
+// The solves run on the context's solve stream (slot 2), ordered after the caller's earlier work
+// on `stream` and before its later work, so that their GMRES restart cycles can be captured as
+// CUDA graphs whatever stream the caller passes (the legacy default stream cannot be captured).
+// stream == NULL: the context's stream itself, no ordering.
+static cudaStream_t solve_stream_enter(rcmps_context* ctx, void* stream) {
+  cudaStream_t s2 = ctx->slot[2].stream;
+  if (stream) {
+    cudaEventRecord(ctx->slot[2].ev[3], static_cast<cudaStream_t>(stream));
+    cudaStreamWaitEvent(s2, ctx->slot[2].ev[3], 0);
+  }
+  return s2;
+}
+static int solve_stream_leave(rcmps_context* ctx, void* stream, int rc) {
+  if (stream) {
+    cudaEventRecord(ctx->slot[2].ev[3], ctx->slot[2].stream);
+    cudaStreamWaitEvent(static_cast<cudaStream_t>(stream), ctx->slot[2].ev[3], 0);
+  }
+  return rc;
+}
+
 extern "C" {
 
 void rcmps_default_settings(rcmps_settings* s) {
@@ -498,7 +518,7 @@ int rcmps_finish_gradient_batch(rcmps_context* ctx, int n, const int* dims, cons
   if (!R || !K || !rho || !covector || !environment || !gradient || !stats)
     return fail(ctx, RCMPS_INVALID_ARGUMENT, "NULL pointer");
   cudaSetDevice(ctx->device);
-  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : ctx->slot[2].stream;
+  cudaStream_t s = solve_stream_enter(ctx, stream);
   for (int i = 0; i < n; ++i) std::memset(&stats[i], 0, sizeof(rcmps_state_stats));
   FinishJob job;
   job.n = n;
@@ -511,13 +531,13 @@ int rcmps_finish_gradient_batch(rcmps_context* ctx, int n, const int* dims, cons
   job.settings = *settings;
   job.gradient = gradient;
   job.stats = stats;
-  return finish_run(ctx, job, s);
+  return solve_stream_leave(ctx, stream, finish_run(ctx, job, s));
 }
 
 int rcmps_boundary_environment_batch(rcmps_context* ctx, int n, const int* dims, const double* R, const double* K,
                                      const double* rho, const double* environment, const double* x0,
-                                     const rcmps_settings* settings, double* H, rcmps_state_stats* stats,
-                                     void* stream) {
+                                     const rcmps_gmres_network* network, const rcmps_settings* settings, double* H,
+                                     rcmps_state_stats* stats, void* stream) {
   if (!ctx) return RCMPS_INVALID_ARGUMENT;
   int rc = check_settings(ctx, settings);
   if (rc) return rc;
@@ -525,6 +545,13 @@ int rcmps_boundary_environment_batch(rcmps_context* ctx, int n, const int* dims,
   if (rc) return rc;
   if (n == 0) return RCMPS_OK;
   if (!R || !K || !rho || !environment || !H || !stats) return fail(ctx, RCMPS_INVALID_ARGUMENT, "NULL pointer");
+  if (network) {
+    if (!network->W1 || !network->W2 || network->rank < 1 || network->rank > 4096 || !std::isfinite(network->identity))
+      return fail(ctx, RCMPS_INVALID_ARGUMENT, "network: weights, 1 <= rank <= 4096, finite identity");
+    for (int i = 0; i < n; ++i)
+      if (2 * dims[i] * dims[i] != network->n)
+        return fail(ctx, RCMPS_INVALID_ARGUMENT, "network: every state needs 2 d^2 = n (state " + std::to_string(i) + ")");
+  }
   cudaSetDevice(ctx->device);
   for (int i = 0; i < n; ++i) std::memset(&stats[i], 0, sizeof(rcmps_state_stats));
   FinishJob job;
@@ -535,18 +562,12 @@ int rcmps_boundary_environment_batch(rcmps_context* ctx, int n, const int* dims,
   job.rho = rho;
   job.environment = environment;
   job.x0 = x0;
+  job.net = network;
   job.settings = *settings;
   job.stats = stats;
   job.slot = 2;
-  cudaStream_t cs = stream ? static_cast<cudaStream_t>(stream) : nullptr;
-  cudaStream_t s2 = ctx->slot[2].stream;
-  cudaEvent_t ready = ctx->slot[2].ev[3];
-  cudaEventRecord(ready, cs);
-  cudaStreamWaitEvent(s2, ready, 0);
-  rc = boundary_run(ctx, job, H, s2);
-  cudaEventRecord(ready, s2);
-  cudaStreamWaitEvent(cs, ready, 0);
-  return rc;
+  cudaStream_t s2 = solve_stream_enter(ctx, stream);
+  return solve_stream_leave(ctx, stream, boundary_run(ctx, job, H, s2));
 }
 
 int rcmps_stationary_state_batch(rcmps_context* ctx, int n, const int* dims, const double* R, const double* K,
@@ -557,7 +578,7 @@ int rcmps_stationary_state_batch(rcmps_context* ctx, int n, const int* dims, con
   if (n == 0) return RCMPS_OK;
   if (!R || !K || !rho || !stats) return fail(ctx, RCMPS_INVALID_ARGUMENT, "NULL pointer");
   cudaSetDevice(ctx->device);
-  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : ctx->slot[2].stream;
+  cudaStream_t s = solve_stream_enter(ctx, stream);
   for (int i = 0; i < n; ++i) std::memset(&stats[i], 0, sizeof(rcmps_state_stats));
   StationaryJob job;
   job.n = n;
@@ -567,7 +588,7 @@ int rcmps_stationary_state_batch(rcmps_context* ctx, int n, const int* dims, con
   job.tolerance = tolerance;
   job.rho = rho;
   job.stats = stats;
-  return stationary_run(ctx, job, s);
+  return solve_stream_leave(ctx, stream, stationary_run(ctx, job, s));
 }
 
 int rcmps_stationary_correction_batch(rcmps_context* ctx, int n, const int* dims, const double* R,
@@ -579,7 +600,7 @@ int rcmps_stationary_correction_batch(rcmps_context* ctx, int n, const int* dims
   if (n == 0) return RCMPS_OK;
   if (!R || !K || !rho_previous || !rho || !stats) return fail(ctx, RCMPS_INVALID_ARGUMENT, "NULL pointer");
   cudaSetDevice(ctx->device);
-  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : ctx->slot[2].stream;
+  cudaStream_t s = solve_stream_enter(ctx, stream);
   for (int i = 0; i < n; ++i) std::memset(&stats[i], 0, sizeof(rcmps_state_stats));
   StationaryJob job;
   job.n = n;
@@ -590,7 +611,7 @@ int rcmps_stationary_correction_batch(rcmps_context* ctx, int n, const int* dims
   job.rho = rho;
   job.rho_previous = rho_previous;
   job.stats = stats;
-  return stationary_run(ctx, job, s);
+  return solve_stream_leave(ctx, stream, stationary_run(ctx, job, s));
 }
 
 // SMs the quartic pullback leaves free for the boundary solve that overlaps it

@@ -22,6 +22,10 @@ struct rcmps_gmres_graph {
   const void* probs = nullptr;
   const void* tasks = nullptr;
   int np = 0, dp = 0, m = 0;
+  const void* net = nullptr;            // the learned preconditioner in the graph, if any: its weights,
+  const void* net2 = nullptr;           // rank and identity weight (all baked into the kernels)
+  int net_rank = 0;
+  float net_identity = 0.f;
   long long kernels = 0;                // kernels the graph replays
   cudaGraphExec_t exec = nullptr;
 };

@@ -346,13 +346,14 @@ __global__ void cgs_finish(ArnoldiProblem* __restrict__ probs, int nprob, int j,
   }
 }
 
-// Arnoldi matvec tasks of step j: W = L(V_j) for every problem still extending.
+// Arnoldi matvec tasks of step j: W = L(V_j) for every problem still extending (L(Z_j) for a
+// flexible GMRES problem, whose preconditioned basis Z_j = M V_j was formed before).
 __global__ void arnoldi_tasks(const ArnoldiProblem* __restrict__ probs, int nprob, int j, LindbladTask* tasks) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= nprob) return;
   const ArnoldiProblem& P = probs[p];
   LindbladTask t;
-  t.X = (P.active && !P.exhausted && j < P.target) ? P.V + (size_t)j * P.ldv : nullptr;
+  t.X = (P.active && !P.exhausted && j < P.target) ? (P.Z ? P.Z : P.V) + (size_t)j * P.ldv : nullptr;
   t.out = P.W;
   t.A1 = P.A1;
   t.A1h = P.A1h;

@@ -45,6 +45,9 @@ struct ArnoldiProblem {
   int n, n_phys, dp, kmax, kmax1, target;
   int k, exhausted, nonfinite, active, solve, reconstruct, adjoint;
   int reorth;                // the current Arnoldi step runs its second Gram-Schmidt pass
+  // flexible GMRES (solvers_host.cu): Z_j = M V_j, the basis passed through a preconditioner M;
+  // the Lindblad action is applied to Z_j and the update is x += Z y. NULL: unpreconditioned.
+  double2* Z;                // [kmax][ldv]
 };
 
 struct KineticSetup {

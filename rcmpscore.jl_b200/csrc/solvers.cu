@@ -179,9 +179,10 @@ __global__ void gmres_update(ArnoldiProblem* __restrict__ probs, int nprob, int 
   }
   __syncthreads();
   const int r0 = ch * GCH, r1 = min(P.n, r0 + GCH);
+  const double2* basis = P.Z ? P.Z : P.V;   // flexible GMRES: x += Z y
   for (int r = r0 + threadIdx.x; r < r1; r += blockDim.x) {
     double2 acc = P.x[r];
-    for (int i = 0; i < k; ++i) acc = zadd(acc, zmul(P.V[(size_t)i * P.ldv + r], y[i]));
+    for (int i = 0; i < k; ++i) acc = zadd(acc, zmul(basis[(size_t)i * P.ldv + r], y[i]));
     P.x[r] = acc;
   }
   if (ch == 0 && threadIdx.x == 0) P.restarts += 1;

@@ -15,6 +15,7 @@
 #include "quartic.h"
 #include "solvers.h"
 #include "solvers_host.h"
+#include "warmstart.h"
 
 namespace rcmps {
 
@@ -30,13 +31,32 @@ struct Layout {
 constexpr int GCHROWS = 512;
 }  // namespace
 
+// The learned preconditioner of a flexible GMRES: the network's weights and its FP32 buffers.
+struct GmresNet {
+  const float* W1 = nullptr;   // rank x n
+  const float* W2 = nullptr;   // n x rank
+  int n = 0, rank = 0, d = 0;
+  float identity = 0.f;
+  float *X32 = nullptr, *H32 = nullptr, *Y32 = nullptr;   // n x NP, rank x NP, n x NP
+};
+
 // The m Arnoldi steps of one restart cycle: launches that depend on nothing the host learns
-// between them (converged problems are skipped inside the kernels).
+// between them (converged problems are skipped inside the kernels). With a learned
+// preconditioner every step first forms Z_j = M V_j (pack, two GEMMs, unpack).
 static cudaError_t gmres_cycle_launches(ArnoldiProblem* d_probs, int NP, int dp, int m, LindbladTask* d_tasks,
-                                        cudaStream_t stream) {
+                                        cudaStream_t stream, const GmresNet* net = nullptr) {
   const int nvec = dp * dp;
   cudaError_t e = cudaSuccess;
   for (int j = 0; j < m && !e; ++j) {
+    if (net) {
+      e = net_pack_launch(d_probs, NP, j, net->d, dp, net->X32, stream);
+      if (!e) e = warmstart_gemm(false, false, net->rank, NP, net->n, 1.f, net->W1, net->n, net->X32, NP, 0.f, net->H32,
+                                 NP, stream);
+      if (!e) e = warmstart_gemm(false, false, net->n, NP, net->rank, 1.f, net->W2, net->rank, net->H32, NP, 0.f,
+                                 net->Y32, NP, stream);
+      if (!e) e = net_unpack_launch(d_probs, NP, j, net->d, dp, net->Y32, net->identity, stream);
+      if (e) break;
+    }
     e = arnoldi_tasks_launch(d_probs, NP, j, d_tasks, stream);
     if (!e) e = lindblad_launch(dp, d_tasks, NP, 0, stream);
     if (!e) e = cgs_step_launch(d_probs, NP, j, nvec, stream);
@@ -49,9 +69,14 @@ static cudaError_t gmres_cycle_launches(ArnoldiProblem* d_probs, int NP, int dp,
 // addresses and sizes and kept by the context (the cycle's several hundred launches then cost
 // one). If capture is not possible the cycle is launched directly.
 static cudaError_t gmres_cycle(rcmps_context* ctx, ArnoldiProblem* d_probs, int NP, int dp, int m,
-                               LindbladTask* d_tasks, cudaStream_t stream) {
+                               LindbladTask* d_tasks, cudaStream_t stream, const GmresNet* net = nullptr) {
+  const void* key = net ? static_cast<const void*>(net->W1) : nullptr;
+  const void* key2 = net ? static_cast<const void*>(net->W2) : nullptr;
+  const int krank = net ? net->rank : 0;
+  const float kid = net ? net->identity : 0.f;
   for (auto& g : ctx->gmres_graphs)
-    if (g.exec && g.probs == d_probs && g.tasks == d_tasks && g.np == NP && g.dp == dp && g.m == m) {
+    if (g.exec && g.probs == d_probs && g.tasks == d_tasks && g.np == NP && g.dp == dp && g.m == m &&
+        g.net == key && g.net2 == key2 && g.net_rank == krank && g.net_identity == kid) {
       note_launches(g.kernels);
       return cudaGraphLaunch(g.exec, stream);
     }
@@ -59,9 +84,9 @@ static cudaError_t gmres_cycle(rcmps_context* ctx, ArnoldiProblem* d_probs, int 
   cudaGraph_t graph = nullptr;
   if (cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
     cudaGetLastError();
-    return gmres_cycle_launches(d_probs, NP, dp, m, d_tasks, stream);
+    return gmres_cycle_launches(d_probs, NP, dp, m, d_tasks, stream, net);
   }
-  cudaError_t e = gmres_cycle_launches(d_probs, NP, dp, m, d_tasks, stream);
+  cudaError_t e = gmres_cycle_launches(d_probs, NP, dp, m, d_tasks, stream, net);
   const cudaError_t ec = cudaStreamEndCapture(stream, &graph);
   cudaGraphExec_t exec = nullptr;
   if (!e && !ec && graph && cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess) {
@@ -74,6 +99,10 @@ static cudaError_t gmres_cycle(rcmps_context* ctx, ArnoldiProblem* d_probs, int 
     g.np = NP;
     g.dp = dp;
     g.m = m;
+    g.net = key;
+    g.net2 = key2;
+    g.net_rank = krank;
+    g.net_identity = kid;
     g.kernels = thread_launch_count() - before;
     g.exec = exec;
     return cudaGraphLaunch(exec, stream);
@@ -81,14 +110,14 @@ static cudaError_t gmres_cycle(rcmps_context* ctx, ArnoldiProblem* d_probs, int 
   // capture or instantiation failed: nothing was launched by the capture; launch directly
   if (graph) cudaGraphDestroy(graph);
   cudaGetLastError();
-  return gmres_cycle_launches(d_probs, NP, dp, m, d_tasks, stream);
+  return gmres_cycle_launches(d_probs, NP, dp, m, d_tasks, stream, net);
 }
 
 // Restarted GMRES(m) over NP problems that share dp; hp/d_probs hold set-up problems with x = 0.
 // Returns 0, or a CUDA error code. Convergence per problem is in hp[p].converged / residual.
 static cudaError_t gmres_run(rcmps_context* ctx, ArnoldiProblem* hp, ArnoldiProblem* d_probs, int NP, int dp,
                              int m, int maxrestart, LindbladTask* d_tasks, cudaStream_t stream,
-                             bool bnorm_from_b = false) {
+                             bool bnorm_from_b = false, const GmresNet* net = nullptr) {
   const int nvec = dp * dp;
   cudaError_t e = cudaMemcpyAsync(d_probs, hp, NP * sizeof(ArnoldiProblem), cudaMemcpyHostToDevice, stream);
   // a warm start: the first residual is not |b|, so |b| is measured for the stopping target
@@ -103,7 +132,7 @@ static cudaError_t gmres_run(rcmps_context* ctx, ArnoldiProblem* hp, ArnoldiProb
     bool all = true;
     for (int p = 0; p < NP; ++p) all &= hp[p].converged != 0;
     if (all || it == maxrestart) break;
-    e = gmres_cycle(ctx, d_probs, NP, dp, m, d_tasks, stream);
+    e = gmres_cycle(ctx, d_probs, NP, dp, m, d_tasks, stream, net);
     if (!e) e = gmres_update_launch(d_probs, NP, nvec, m, stream);
   }
   return e;
@@ -167,6 +196,7 @@ struct FinishPlan::Group {
   int dp = 0, n = 0;
   std::vector<int> idx;
   size_t o_dims = 0, o_off = 0, o_in = 0, o_ops = 0, o_b = 0, o_tmp = 0, o_status = 0;
+  size_t o_z = 0, o_x32 = 0, o_h32 = 0, o_y32 = 0;   // learned preconditioner (flexible GMRES)
   GmresBuffers gb{};
   size_t h_dims = 0, h_off = 0, h_probs = 0, h_status = 0;
 };
@@ -220,6 +250,12 @@ int finish_solve(rcmps_context* ctx, FinishJob& job, cudaStream_t stream, Finish
     g.o_tmp = L.add(n * 4 * mat * 16);
     g.o_status = L.add(n * 4);
     g.gb = gmres_layout(L, n, g.dp, m);
+    if (job.net) {   // flexible GMRES: the preconditioned basis and the network's buffers
+      g.o_z = L.add((size_t)n * m * mat * 16);
+      g.o_x32 = L.add((size_t)job.net->n * n * 4);
+      g.o_h32 = L.add((size_t)job.net->rank * n * 4);
+      g.o_y32 = L.add((size_t)job.net->n * n * 4);
+    }
     g.h_dims = H.add(n * 4);
     g.h_off = H.add(n * 8);
     g.h_probs = H.add(n * sizeof(ArnoldiProblem));
@@ -272,9 +308,22 @@ int finish_solve(rcmps_context* ctx, FinishJob& job, cudaStream_t stream, Finish
       A.A2h = ops + 2 * mat;
       A.trw = ops + 7 * mat;  // + tr(rho X) I
       A.b = fa.b + (size_t)i * mat;
+      if (job.net) A.Z = (double2*)P(g.o_z) + (size_t)i * m * mat;
+    }
+    GmresNet net;
+    if (job.net) {
+      net.W1 = job.net->W1;
+      net.W2 = job.net->W2;
+      net.n = job.net->n;
+      net.rank = job.net->rank;
+      net.identity = job.net->identity;
+      net.d = hd[0];
+      net.X32 = (float*)P(g.o_x32);
+      net.H32 = (float*)P(g.o_h32);
+      net.Y32 = (float*)P(g.o_y32);
     }
     e = gmres_run(ctx, hp, (ArnoldiProblem*)P(g.gb.o_probs), n, dp, m, maxrestart, (LindbladTask*)P(g.gb.o_tasks),
-                  stream, job.x0 != nullptr);
+                  stream, job.x0 != nullptr, job.net ? &net : nullptr);
     if (e) return fail(ctx, RCMPS_CUDA_ERROR, std::string("boundary GMRES: ") + cudaGetErrorString(e));
   }
   return RCMPS_OK;

@@ -19,6 +19,8 @@ struct FinishJob {
   // device, packed, optional: initial guesses of the boundary Poisson solutions (a warm start);
   // the stopping target stays tol max(1, |b|)
   const double* x0 = nullptr;
+  // optional: a learned right preconditioner (flexible GMRES); every state has d with 2 d^2 = net->n
+  const rcmps_gmres_network* net = nullptr;
 };
 
 struct StationaryJob {

@@ -18,6 +18,7 @@
 #include "../../include/rcmps_b200.h"
 #include "common.cuh"
 #include "context.h"
+#include "warmstart.h"
 
 namespace rcmps {
 namespace {
@@ -117,6 +118,40 @@ __global__ void adam_kernel(long long count, float* __restrict__ p, const float*
   }
 }
 
+// The network's input columns from the Arnoldi vectors V_j of NP problems (one column each).
+__global__ void net_pack_kernel(const ArnoldiProblem* __restrict__ probs, int NP, int j, int d, int dp,
+                                float* __restrict__ X32) {
+  const int p = blockIdx.y;
+  const ArnoldiProblem& P = probs[p];
+  const double2* v = P.V + (size_t)j * P.ldv;
+  const bool live = P.active && !P.exhausted && j < P.target;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < d * d; e += gridDim.x * blockDim.x) {
+    const double2 x = live ? v[(e / d) * dp + (e % d)] : make_double2(0.0, 0.0);
+    X32[(size_t)(2 * e) * NP + p] = (float)x.x;
+    X32[(size_t)(2 * e + 1) * NP + p] = (float)x.y;
+  }
+}
+
+// Z_j = M V_j + identity V_j of every problem still extending, from the network's output columns.
+__global__ void net_unpack_kernel(const ArnoldiProblem* __restrict__ probs, int NP, int j, int d, int dp,
+                                  const float* __restrict__ Y32, float identity) {
+  const int p = blockIdx.y;
+  const ArnoldiProblem& P = probs[p];
+  if (!(P.active && !P.exhausted && j < P.target)) return;
+  const double2* v = P.V + (size_t)j * P.ldv;
+  double2* z = P.Z + (size_t)j * P.ldv;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < dp * dp; e += gridDim.x * blockDim.x) {
+    const int r = e / dp, c = e % dp;
+    double2 out = make_double2(0.0, 0.0);
+    if (r < d && c < d) {
+      const int i = r * d + c;
+      out.x = (double)Y32[(size_t)(2 * i) * NP + p] + (double)identity * v[e].x;
+      out.y = (double)Y32[(size_t)(2 * i + 1) * NP + p] + (double)identity * v[e].y;
+    }
+    z[e] = out;
+  }
+}
+
 int check_shape(rcmps_context* ctx, int n, int rank, int batch) {
   if (n < 1 || rank < 1 || batch < 1 || n > (1 << 26) || rank > 4096)
     return fail(ctx, RCMPS_INVALID_ARGUMENT, "warm-start network: 1 <= n, 1 <= rank <= 4096, 1 <= batch");
@@ -124,6 +159,25 @@ int check_shape(rcmps_context* ctx, int n, int rank, int batch) {
 }
 
 }  // namespace
+
+cudaError_t warmstart_gemm(bool ta, bool tb, int M, int N, int K, float alpha, const float* A, int lda, const float* B,
+                           int ldb, float beta, float* C, int ldc, cudaStream_t s) {
+  return gemm(ta, tb, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, s);
+}
+
+cudaError_t net_pack_launch(const ArnoldiProblem* probs, int NP, int j, int d, int dp, float* X32, cudaStream_t s) {
+  note_launch();
+  net_pack_kernel<<<dim3((d * d + 255) / 256, NP), 256, 0, s>>>(probs, NP, j, d, dp, X32);
+  return cudaGetLastError();
+}
+
+cudaError_t net_unpack_launch(const ArnoldiProblem* probs, int NP, int j, int d, int dp, const float* Y32,
+                              float identity, cudaStream_t s) {
+  note_launch();
+  net_unpack_kernel<<<dim3((dp * dp + 255) / 256, NP), 256, 0, s>>>(probs, NP, j, d, dp, Y32, identity);
+  return cudaGetLastError();
+}
+
 }  // namespace rcmps
 
 using namespace rcmps;

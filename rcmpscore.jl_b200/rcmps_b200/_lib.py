@@ -36,6 +36,11 @@ class StateControls(C.Structure):
     _fields_ = [("atol", C.c_double), ("rtol", C.c_double)]
 
 
+class GmresNetwork(C.Structure):
+    """A learned right preconditioner of the boundary GMRES (rcmps_gmres_network)."""
+    _fields_ = [("W1", C.c_void_p), ("W2", C.c_void_p), ("n", C.c_int), ("rank", C.c_int), ("identity", C.c_float)]
+
+
 class StateStats(C.Structure):
     _fields_ = [
         ("status", C.c_int), ("failed_component", C.c_int),
@@ -84,8 +89,8 @@ SIGNATURES = {
                                  C.POINTER(StateStats), _P]),
     "rcmps_finish_gradient_batch": (_I, [_P, _I, C.POINTER(_I), _P, _P, _P, _P, _P, C.POINTER(Settings), _P,
                                          C.POINTER(StateStats), _P]),
-    "rcmps_boundary_environment_batch": (_I, [_P, _I, C.POINTER(_I), _P, _P, _P, _P, _P, C.POINTER(Settings), _P,
-                                              C.POINTER(StateStats), _P]),
+    "rcmps_boundary_environment_batch": (_I, [_P, _I, C.POINTER(_I), _P, _P, _P, _P, _P, C.POINTER(GmresNetwork),
+                                              C.POINTER(Settings), _P, C.POINTER(StateStats), _P]),
     "rcmps_finish_gradient_noalloc": (_I, [_P, _I, _P, _P, _P, _P, _P, C.POINTER(Settings), _P,
                                            C.POINTER(StateStats), _P]),
     "rcmps_stationary_state_batch": (_I, [_P, _I, C.POINTER(_I), _P, _P, _D, _P, C.POINTER(StateStats), _P]),

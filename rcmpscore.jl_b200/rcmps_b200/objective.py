@@ -133,9 +133,17 @@ def _unpack(t, dims):
     return out
 
 
+# CUDA's handle of the legacy default stream (cudaStreamLegacy). torch reports its default stream
+# as handle 0, which the library reads as "the context's own stream"; the explicit handle keeps the
+# library's kernels ordered with torch's work on that stream (an entry that returns before its
+# kernels finish would otherwise race with torch freeing and reusing its tensors).
+_LEGACY_STREAM = 0x1
+
+
 def _stream():
     import torch
-    return C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    handle = torch.cuda.current_stream().cuda_stream
+    return C.c_void_p(handle if handle else _LEGACY_STREAM)
 
 
 def _raise_for(status, ctx, stats, what):
@@ -427,12 +435,14 @@ def finish_gradient(q, r, rho, covector, environment, *, metric_reg=1e-3, tolera
     return _unpack(grad, [d])[0], {"matvecs": stats[0].gmres_iterations, "residual": stats[0].boundary_residual}
 
 
-def boundary_environment_batch(R, K, rho, environments, *, tolerance=1e-13, x0=None, device=None):
+def boundary_environment_batch(R, K, rho, environments, *, tolerance=1e-13, x0=None, network=None, device=None):
     """The boundary Poisson solutions H_i, (-L*(H) + tr(rho H) I) = E - tr(rho E) I, of one
     environment E_i per entry (lists of D_i x D_i matrices; an entry may repeat a state with
     different environments), by restarted GMRES on the GPU (rcmps_boundary_environment_batch).
-    x0: optional initial guesses (a warm start). Returns (H list, stats list) with stats[i] =
-    dict(matvecs, residual) as the reference's boundary_environment (numerics.py:103-117)."""
+    x0: optional initial guesses (a warm start); network: an optional learned right preconditioner
+    (rcmps_b200.warmstart.WarmStartNet, every state of its d), applied in flexible GMRES. Returns
+    (H list, stats list) with stats[i] = dict(matvecs, residual) as the reference's
+    boundary_environment (numerics.py:103-117)."""
     import torch
     n = len(R)
     if not (len(K) == len(rho) == len(environments) == n) or (x0 is not None and len(x0) != n):
@@ -446,8 +456,9 @@ def boundary_environment_batch(R, K, rho, environments, *, tolerance=1e-13, x0=N
     stats = (_lib.StateStats * n)()
     rc = ctx.lib.rcmps_boundary_environment_batch(ctx.handle, n, (C.c_int * n)(*dims), dR.data_ptr(), dK.data_ptr(),
                                                   dP.data_ptr(), dE.data_ptr(),
-                                                  dX.data_ptr() if dX is not None else None, C.byref(s),
-                                                  H.data_ptr(), stats, _stream())
+                                                  dX.data_ptr() if dX is not None else None,
+                                                  C.byref(network.c_struct()) if network is not None else None,
+                                                  C.byref(s), H.data_ptr(), stats, _stream())
     if rc:
         raise SolverFailure(f"Poisson GMRES failed: {_lib.STATUS_NAMES.get(rc, rc)} ({ctx.error()})")
     return _unpack(H, dims), [{"matvecs": stats[i].gmres_iterations, "residual": stats[i].boundary_residual}

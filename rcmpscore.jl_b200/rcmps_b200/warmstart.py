@@ -77,6 +77,14 @@ class WarmStartNet:
         self._v = [torch.zeros_like(self.W1), torch.zeros_like(self.W2)]
         self.step = 0
 
+    def c_struct(self, identity=None):
+        """The network as the library's right preconditioner (rcmps_gmres_network): M v = W2 W1 v
+        (+ v when the rank is below n, so that M stays invertible on the complement)."""
+        if identity is None:
+            identity = 0.0 if self.rank >= self.n else 1.0
+        self._cs = _lib.GmresNetwork(self.W1.data_ptr(), self.W2.data_ptr(), self.n, self.rank, float(identity))
+        return self._cs
+
     def _check(self, rc, what):
         if rc:
             raise RuntimeError(f"{what}: {_lib.STATUS_NAMES.get(rc, rc)} ({self.ctx.error()})")
@@ -149,15 +157,21 @@ class WarmStartNet:
 
 
 def gmres_gain(net, R, K, rho, environments, *, tolerance=1e-13):
-    """GMRES matrix-vector products and residuals of the same solves started from zero (the
-    fallback) and from the network's guess: dict(cold, warm, cold_residual, warm_residual,
-    solution_difference)."""
+    """GMRES matrix-vector products and residuals of the same solves by the fallback (GMRES from
+    zero, unpreconditioned), from the network's warm start, and with the network as the right
+    preconditioner of flexible GMRES (its coarse correction applied at every step):
+    dict(cold, warm, preconditioned, *_residual, target, *_difference)."""
     rhs = [e - np.trace(rho @ e) * np.eye(len(rho)) for e in environments]
     n = len(environments)
     H0, st0 = boundary_environment_batch([R] * n, [K] * n, [rho] * n, environments, tolerance=tolerance)
     H1, st1 = boundary_environment_batch([R] * n, [K] * n, [rho] * n, environments, tolerance=tolerance,
                                          x0=net.predict(rhs))
-    diff = max(np.abs(a - b).max() / max(1.0, np.abs(a).max()) for a, b in zip(H0, H1))
+    H2, st2 = boundary_environment_batch([R] * n, [K] * n, [rho] * n, environments, tolerance=tolerance,
+                                         network=net)
+    diff = lambda A, B: max(np.abs(a - b).max() / max(1.0, np.abs(a).max()) for a, b in zip(A, B))
     return {"cold": [s["matvecs"] for s in st0], "warm": [s["matvecs"] for s in st1],
+            "preconditioned": [s["matvecs"] for s in st2],
             "cold_residual": [s["residual"] for s in st0], "warm_residual": [s["residual"] for s in st1],
-            "target": [tolerance * max(1.0, float(np.linalg.norm(b))) for b in rhs], "solution_difference": diff}
+            "preconditioned_residual": [s["residual"] for s in st2],
+            "target": [tolerance * max(1.0, float(np.linalg.norm(b))) for b in rhs],
+            "solution_difference": diff(H0, H1), "preconditioned_difference": diff(H0, H2)}

@@ -76,27 +76,33 @@ def _path_states(d, seed, count, step):
     return out
 
 
-def test_learned_warm_start_cuts_gmres_iterations(gpu_context):
-    """Train on triples of five states of a path (D = 16, 128 right-hand sides each) and solve 64
-    new right-hand sides of the sixth, held-out state from zero and from the network's guess: the
-    warm solves take at least a quarter fewer matrix-vector products to the same residual target,
-    and the solutions agree."""
+def test_learned_network_cuts_gmres_iterations(gpu_context):
+    """Train a full-rank network (D = 16: n = 512) on triples of five states of a path (256
+    right-hand sides each) and solve 64 new right-hand sides of the sixth, held-out state three
+    ways: the fallback (GMRES from zero, unpreconditioned), from the network's warm start, and
+    with the network as the right preconditioner of flexible GMRES. Every solve meets the same
+    residual target and they agree to 1e-10; the warm start saves a little (its gain is
+    logarithmic in the guess's accuracy at a 1e-13 target), the preconditioned solves take at
+    most a third of the fallback's matrix-vector products."""
     from rcmps_b200.warmstart import WarmStartNet, gmres_gain, random_environments, solve_triples
     d = 16
     states = _path_states(d, 161, 6, 1e-2)
     rng = np.random.default_rng(5)
     B, H = [], []
     for R, K, rho in states[:5]:
-        b, h, _ = solve_triples(R, K, rho, random_environments(rho, 128, rng))
+        b, h, _ = solve_triples(R, K, rho, random_environments(rho, 256, rng))
         B += b
         H += h
-    net = WarmStartNet(d, rank=128, seed=1)
-    losses = net.fit(B, H, epochs=150, batch=128, lr=2e-3)
-    assert losses[-1] < 0.2 * losses[0]
+    net = WarmStartNet(d, rank=2 * d * d, seed=1)
+    losses = net.fit(B, H, epochs=300, batch=128, lr=2e-3)
+    assert losses[-1] < 0.01 * losses[0]
     R, K, rho = states[5]
     gain = gmres_gain(net, R, K, rho, random_environments(rho, 64, np.random.default_rng(6)))
-    cold, warm = np.mean(gain["cold"]), np.mean(gain["warm"])
-    print(f"GMRES matvecs: cold {cold:.1f}, warm {warm:.1f}; final loss {losses[-1]:.3e} (first {losses[0]:.3e})")
-    assert warm <= 0.75 * cold
-    assert all(r <= t for r, t in zip(gain["warm_residual"], gain["target"]))
-    assert gain["solution_difference"] <= 1e-10
+    cold, warm, pre = np.mean(gain["cold"]), np.mean(gain["warm"]), np.mean(gain["preconditioned"])
+    print(f"GMRES matvecs: cold {cold:.1f}, warm {warm:.1f}, preconditioned {pre:.1f}; "
+          f"final loss {losses[-1]:.3e} (first {losses[0]:.3e})")
+    assert warm < cold
+    assert pre <= cold / 3
+    for key in ("warm_residual", "preconditioned_residual"):
+        assert all(r <= t for r, t in zip(gain[key], gain["target"]))
+    assert gain["solution_difference"] <= 1e-10 and gain["preconditioned_difference"] <= 1e-10
