@@ -210,7 +210,10 @@ typedef struct rcmps_gmres_network {
  * rcmps_b200.warmstart); network (or NULL) a learned right preconditioner, applied in flexible
  * GMRES (the basis passes through M in FP32, the Arnoldi relation and the update stay FP64, so
  * the attainable accuracy is that of the plain solve); every state then has the network's d.
- * Neither changes the stopping target or the acceptance test. H is written packed;
+ * Neither changes the stopping target or the acceptance test. Unpreconditioned GMRES is the
+ * fallback: states that the preconditioned pass (at most 8 restart cycles) leaves unconverged are
+ * solved again without the network, from where that pass left them (gmres_iterations counts both
+ * passes). H is written packed;
  * stats[i].gmres_iterations and boundary_residual report the solve. Replaces
  * boundary_environment(q, r, rho, environment, tolerance) -> (H, stats) (runtime/numerics.py:103-117). */
 int rcmps_boundary_environment_batch(rcmps_context* context, int n_states, const int* dims, const double* R,

@@ -534,6 +534,9 @@ int rcmps_finish_gradient_batch(rcmps_context* ctx, int n, const int* dims, cons
   return solve_stream_leave(ctx, stream, finish_run(ctx, job, s));
 }
 
+// restart cycles of the learned-preconditioner pass of the boundary solve before the fallback
+constexpr int kLearnedRestarts = 8;
+
 int rcmps_boundary_environment_batch(rcmps_context* ctx, int n, const int* dims, const double* R, const double* K,
                                      const double* rho, const double* environment, const double* x0,
                                      const rcmps_gmres_network* network, const rcmps_settings* settings, double* H,
@@ -546,8 +549,8 @@ int rcmps_boundary_environment_batch(rcmps_context* ctx, int n, const int* dims,
   if (n == 0) return RCMPS_OK;
   if (!R || !K || !rho || !environment || !H || !stats) return fail(ctx, RCMPS_INVALID_ARGUMENT, "NULL pointer");
   if (network) {
-    if (!network->W1 || !network->W2 || network->rank < 1 || network->rank > 4096 || !std::isfinite(network->identity))
-      return fail(ctx, RCMPS_INVALID_ARGUMENT, "network: weights, 1 <= rank <= 4096, finite identity");
+    if (!network->W1 || !network->W2 || network->rank < 1 || network->rank > 32768 || !std::isfinite(network->identity))
+      return fail(ctx, RCMPS_INVALID_ARGUMENT, "network: weights, 1 <= rank <= 32768, finite identity");
     for (int i = 0; i < n; ++i)
       if (2 * dims[i] * dims[i] != network->n)
         return fail(ctx, RCMPS_INVALID_ARGUMENT, "network: every state needs 2 d^2 = n (state " + std::to_string(i) + ")");
@@ -567,7 +570,21 @@ int rcmps_boundary_environment_batch(rcmps_context* ctx, int n, const int* dims,
   job.stats = stats;
   job.slot = 2;
   cudaStream_t s2 = solve_stream_enter(ctx, stream);
-  return solve_stream_leave(ctx, stream, boundary_run(ctx, job, H, s2));
+  if (!network) return solve_stream_leave(ctx, stream, boundary_run(ctx, job, H, s2));
+  // the learned preconditioner first, for a few restart cycles; unpreconditioned GMRES is the
+  // fallback: every state that did not converge is solved again from where the first pass left it
+  job.max_restarts = kLearnedRestarts;
+  rc = boundary_run(ctx, job, H, s2);
+  if (rc == RCMPS_SOLVE_FAILURE) {
+    std::vector<rcmps_state_stats> first(stats, stats + n);
+    for (int i = 0; i < n; ++i) std::memset(&stats[i], 0, sizeof(rcmps_state_stats));
+    job.net = nullptr;
+    job.x0 = H;
+    job.max_restarts = 200;
+    rc = boundary_run(ctx, job, H, s2);
+    for (int i = 0; i < n; ++i) stats[i].gmres_iterations += first[i].gmres_iterations;
+  }
+  return solve_stream_leave(ctx, stream, rc);
 }
 
 int rcmps_stationary_state_batch(rcmps_context* ctx, int n, const int* dims, const double* R, const double* K,

@@ -225,7 +225,7 @@ FinishPlan::~FinishPlan() = default;
 
 int finish_solve(rcmps_context* ctx, FinishJob& job, cudaStream_t stream, FinishPlan& plan) {
   const rcmps_settings& S = job.settings;
-  const int m = 64, maxrestart = 200;
+  const int m = 64, maxrestart = job.max_restarts;
   const double tol = S.boundary_tolerance;
   if (!(tol > 0.0) || !(S.metric_reg >= 0.0)) return fail(ctx, RCMPS_INVALID_ARGUMENT, "invalid boundary controls");
   plan.off.assign(job.n + 1, 0);

@@ -21,6 +21,7 @@ struct FinishJob {
   const double* x0 = nullptr;
   // optional: a learned right preconditioner (flexible GMRES); every state has d with 2 d^2 = net->n
   const rcmps_gmres_network* net = nullptr;
+  int max_restarts = 200;                     // restart cycles of the boundary GMRES
 };
 
 struct StationaryJob {

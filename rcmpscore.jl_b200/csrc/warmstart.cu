@@ -26,25 +26,29 @@ namespace {
 constexpr int kT = 64, kBK = 16;
 
 // op(A)[m][k] = TA ? A[k lda + m] : A[m lda + k]; op(B)[k][n] = TB ? B[n ldb + k] : B[k ldb + n]
+// Split K (gridDim.z > 1): CTA z covers the k-range [z kspan, (z + 1) kspan) and adds its partial
+// product to C atomically (C was cleared by the caller; alpha applies per partial, beta = 0).
 template <bool TA, bool TB>
 __global__ void __launch_bounds__(256) gemm_f32(int M, int N, int K, float alpha, const float* __restrict__ A,
                                                 int lda, const float* __restrict__ B, int ldb, float beta,
-                                                float* __restrict__ C, int ldc) {
+                                                float* __restrict__ C, int ldc, int kspan) {
   __shared__ float As[kBK][kT + 4];
   __shared__ float Bs[kBK][kT + 4];
   const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
   const int m0 = blockIdx.y * kT, n0 = blockIdx.x * kT;
+  const int kbeg = blockIdx.z * kspan, kend = min(K, kbeg + kspan);
+  const bool split = gridDim.z > 1;
   float acc[4][4] = {};
-  for (int k0 = 0; k0 < K; k0 += kBK) {
+  for (int k0 = kbeg; k0 < kend; k0 += kBK) {
     for (int i = threadIdx.x; i < kT * kBK; i += 256) {
       const int mm = TA ? i % kT : i / kBK, kk = TA ? i / kT : i % kBK;   // coalesced along the contiguous index
       const int gm = m0 + mm, gk = k0 + kk;
-      As[kk][mm] = (gm < M && gk < K) ? (TA ? A[(size_t)gk * lda + gm] : A[(size_t)gm * lda + gk]) : 0.f;
+      As[kk][mm] = (gm < M && gk < kend) ? (TA ? A[(size_t)gk * lda + gm] : A[(size_t)gm * lda + gk]) : 0.f;
     }
     for (int i = threadIdx.x; i < kT * kBK; i += 256) {
       const int nn = TB ? i / kBK : i % kT, kk = TB ? i % kBK : i / kT;
       const int gn = n0 + nn, gk = k0 + kk;
-      Bs[kk][nn] = (gn < N && gk < K) ? (TB ? B[(size_t)gn * ldb + gk] : B[(size_t)gk * ldb + gn]) : 0.f;
+      Bs[kk][nn] = (gn < N && gk < kend) ? (TB ? B[(size_t)gn * ldb + gk] : B[(size_t)gk * ldb + gn]) : 0.f;
     }
     __syncthreads();
 #pragma unroll
@@ -69,19 +73,38 @@ __global__ void __launch_bounds__(256) gemm_f32(int M, int N, int K, float alpha
       const int gm = m0 + ty * 4 + i, gn = n0 + tx * 4 + j;
       if (gm < M && gn < N) {
         float* c = C + (size_t)gm * ldc + gn;
-        *c = beta == 0.f ? alpha * acc[i][j] : fmaf(beta, *c, alpha * acc[i][j]);
+        if (split) atomicAdd(c, alpha * acc[i][j]);
+        else *c = beta == 0.f ? alpha * acc[i][j] : fmaf(beta, *c, alpha * acc[i][j]);
       }
     }
 }
 
+// Tiles of C below about four waves of the 148 SMs split K (atomically accumulated partials) so
+// that thin products (the preconditioner's n x NP and rank x NP outputs) still fill the GPU.
 cudaError_t gemm(bool ta, bool tb, int M, int N, int K, float alpha, const float* A, int lda, const float* B, int ldb,
                  float beta, float* C, int ldc, cudaStream_t s) {
-  const dim3 grid((N + kT - 1) / kT, (M + kT - 1) / kT);
+  const int tiles = ((N + kT - 1) / kT) * ((M + kT - 1) / kT);
+  int splits = 1;
+  if (beta == 0.f)
+    while (tiles * splits < 4 * 148 && K / (2 * splits) >= 256) splits *= 2;
+  const int kspan = ((K + splits - 1) / splits + kBK - 1) / kBK * kBK;
+  const dim3 grid((N + kT - 1) / kT, (M + kT - 1) / kT, splits);
+  if (splits > 1) {
+    for (int r = 0; r < M; ++r) {   // C rows may be strided (ldc >= N)
+      if (ldc == N) {
+        const cudaError_t e = cudaMemsetAsync(C, 0, (size_t)M * N * sizeof(float), s);
+        if (e) return e;
+        break;
+      }
+      const cudaError_t e = cudaMemsetAsync(C + (size_t)r * ldc, 0, (size_t)N * sizeof(float), s);
+      if (e) return e;
+    }
+  }
   note_launch();
-  if (!ta && !tb) gemm_f32<false, false><<<grid, 256, 0, s>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc);
-  else if (!ta && tb) gemm_f32<false, true><<<grid, 256, 0, s>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc);
-  else if (ta && !tb) gemm_f32<true, false><<<grid, 256, 0, s>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc);
-  else gemm_f32<true, true><<<grid, 256, 0, s>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc);
+  if (!ta && !tb) gemm_f32<false, false><<<grid, 256, 0, s>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, kspan);
+  else if (!ta && tb) gemm_f32<false, true><<<grid, 256, 0, s>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, kspan);
+  else if (ta && !tb) gemm_f32<true, false><<<grid, 256, 0, s>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, kspan);
+  else gemm_f32<true, true><<<grid, 256, 0, s>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, kspan);
   return cudaGetLastError();
 }
 
@@ -153,8 +176,8 @@ __global__ void net_unpack_kernel(const ArnoldiProblem* __restrict__ probs, int 
 }
 
 int check_shape(rcmps_context* ctx, int n, int rank, int batch) {
-  if (n < 1 || rank < 1 || batch < 1 || n > (1 << 26) || rank > 4096)
-    return fail(ctx, RCMPS_INVALID_ARGUMENT, "warm-start network: 1 <= n, 1 <= rank <= 4096, 1 <= batch");
+  if (n < 1 || rank < 1 || batch < 1 || n > (1 << 26) || rank > 32768)
+    return fail(ctx, RCMPS_INVALID_ARGUMENT, "warm-start network: 1 <= n, 1 <= rank <= 32768, 1 <= batch");
   return RCMPS_OK;
 }
 

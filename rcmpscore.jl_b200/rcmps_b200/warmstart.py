@@ -175,3 +175,75 @@ def gmres_gain(net, R, K, rho, environments, *, tolerance=1e-13):
             "preconditioned_residual": [s["residual"] for s in st2],
             "target": [tolerance * max(1.0, float(np.linalg.norm(b))) for b in rhs],
             "solution_difference": diff(H0, H1), "preconditioned_difference": diff(H0, H2)}
+
+
+def path_states(d, seed, count, step):
+    """A seeded optimizer-like path of `count` states: each the canonical retraction of the previous
+    one along a random tangent direction of relative size `step` (the stand-in for the states an
+    L-BFGS run visits), with its stationary density by the library's solve."""
+    from .batch import random_state
+    from .objective import stationary_state
+    from .optimizer import retract
+    rng = np.random.default_rng(seed)
+    R, K = random_state(d, seed)
+    out = []
+    for _ in range(count):
+        Q = -1j * K - R.conj().T @ R / 2
+        rho, _ = stationary_state(Q, R, tolerance=1e-13)
+        out.append((R, K, rho))
+        X = rng.standard_normal((d, d)) + 1j * rng.standard_normal((d, d))
+        R, K = retract(R, K, X, step * np.linalg.norm(R) / np.linalg.norm(X))
+    return out
+
+
+def path_experiment(d, *, train_states=8, rhs_per_state=512, test_rhs=64, rank=None, epochs=100, lr=1e-3,
+                    step=1e-2, seed=161, tolerance=1e-13):
+    """Train on the plain solver's triples of the first `train_states` states of a path and solve
+    `test_rhs` new right-hand sides of the next (held-out) state by the fallback, from the warm
+    start and with the learned preconditioner. Returns the matrix-vector products, the device
+    milliseconds of each batched solve (CUDA events), the training time and the final loss."""
+    import time
+    import torch
+    states = path_states(d, seed, train_states + 1, step)
+    rng = np.random.default_rng(seed + 1)
+    B, H = [], []
+    t0 = time.perf_counter()
+    for R, K, rho in states[:train_states]:
+        b, h, _ = solve_triples(R, K, rho, random_environments(rho, rhs_per_state, rng), tolerance=tolerance)
+        B += b
+        H += h
+    t_data = time.perf_counter() - t0
+    net = WarmStartNet(d, rank=rank or min(2 * d * d, len(B)), seed=seed)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    losses = net.fit(B, H, epochs=epochs, batch=128, lr=lr)
+    torch.cuda.synchronize()
+    t_train = time.perf_counter() - t0
+    R, K, rho = states[train_states]
+    envs = random_environments(rho, test_rhs, np.random.default_rng(seed + 2))
+    n = len(envs)
+
+    def timed(**kw):
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record()
+        Hs, st = boundary_environment_batch([R] * n, [K] * n, [rho] * n, envs, tolerance=tolerance, **kw)
+        ev1.record()
+        torch.cuda.synchronize()
+        return Hs, st, ev0.elapsed_time(ev1)
+
+    timed()                                        # warm-up (graph capture of the cycles)
+    H0, st0, ms0 = timed()
+    timed(network=net)
+    H2, st2, ms2 = timed(network=net)
+    rhs = [e - np.trace(rho @ e) * np.eye(d) for e in envs]
+    H1, st1, ms1 = timed(x0=net.predict(rhs))
+    diff = lambda A, Bm: max(np.abs(a - b).max() / max(1.0, np.abs(a).max()) for a, b in zip(A, Bm))
+    return {"d": d, "train_triples": len(B), "rank": net.rank, "epochs": epochs, "loss_first": losses[0],
+            "loss_last": losses[-1], "data_seconds": t_data, "train_seconds": t_train,
+            "matvecs_cold": float(np.mean([s["matvecs"] for s in st0])),
+            "matvecs_warm": float(np.mean([s["matvecs"] for s in st1])),
+            "matvecs_preconditioned": float(np.mean([s["matvecs"] for s in st2])),
+            "ms_cold": ms0, "ms_warm": ms1, "ms_preconditioned": ms2,
+            "max_residual_over_target": max(s["residual"] / (tolerance * max(1.0, float(np.linalg.norm(b))))
+                                            for st in (st0, st1, st2) for s, b in zip(st, rhs)),
+            "solution_difference": max(diff(H0, H1), diff(H0, H2))}
