@@ -172,11 +172,18 @@ def run_b200(args, rank, world, local_rank):
     ctx = _lib.Context(local_rank)
     lib = ctx.lib
     R, K, g, desc = config_states(args.workload)
+    tolerances = None
+    if args.workload == "uneven200":      # per-state (atol, rtol) pairs in the same launch
+        from rcmps_b200.batch import uneven_states
+        tolerances = uneven_states(len(R))[3]
     dims_all = [len(r) for r in R]
     mine = shard(dims_all, rank, world)
     R = [R[i] for i in mine]
     K = [K[i] for i in mine]
     g = [g[i] for i in mine]
+    controls = None
+    if tolerances is not None:
+        controls = (_lib.StateControls * len(mine))(*(_lib.StateControls(*tolerances[i]) for i in mine))
     dims = [len(r) for r in R]
     n = len(dims)
     total = sum(d * d for d in dims)
@@ -210,8 +217,9 @@ def run_b200(args, rank, world, local_rank):
                                          C.byref(settings), energy.data_ptr(), cov.data_ptr(), grad.data_ptr(), stats,
                                          sptr)
         else:
-            rc = lib.rcmps_fg_phi4_batch(ctx.handle, n, cdims, cg, dR.data_ptr(), dK.data_ptr(), drho.data_ptr(),
-                                         C.byref(settings), energy.data_ptr(), grad.data_ptr(), None, None, stats, sptr)
+            rc = lib.rcmps_fg_phi4_batch_controls(ctx.handle, n, cdims, cg, dR.data_ptr(), dK.data_ptr(),
+                                                  drho.data_ptr(), C.byref(settings), controls, energy.data_ptr(),
+                                                  grad.data_ptr(), None, None, stats, sptr)
         if rc:
             raise RuntimeError(f"{args.component} failed: {_lib.STATUS_NAMES.get(rc)} {ctx.error()}")
 
@@ -302,7 +310,17 @@ def run_b200(args, rank, world, local_rank):
         hG = torch.zeros(total, dtype=torch.complex128).pin_memory()
         e2e_steps = args.steps
 
+        rho_host = None
+        if tolerances is not None:
+            from rcmps_b200 import objective
+            rho_np = hP.numpy()
+            offs = np.cumsum([0] + [d * d for d in dims])
+            rho_host = [rho_np[offs[i]:offs[i + 1]].reshape(dims[i], dims[i]) for i in range(n)]
+
         def host_step():
+            if tolerances is not None:   # per-state tolerances: the Python entry on host arrays
+                objective.fg_phi4_batch(R, K, rho_host, g, s, tolerances=[tolerances[i] for i in mine])
+                return
             rc = lib.rcmps_fg_phi4_batch_host(ctx.handle, n, cdims, cg, hR.data_ptr(), hK.data_ptr(), hP.data_ptr(),
                                               C.byref(s), hE.data_ptr(), hG.data_ptr(), None, None, stats)
             if rc:
@@ -353,7 +371,8 @@ def run_b200(args, rank, world, local_rank):
 
     # the split-precision arm beside the FP64 one in the default run: the same workload and timing
     split_arm = None
-    if not split and not quartic_only and args.split_arm_steps > 0 and any(d == 64 for d in dims):
+    if (not split and not quartic_only and args.split_arm_steps > 0 and args.workload == "d64_mixed"
+            and any(d == 64 for d in dims)):
         s_split = _lib.default_settings(symmetry=s.symmetry, precision=1, half_window=s.half_window, n_quad=s.n_quad)
         step(s_split)                          # warm-up
         barrier()
@@ -377,6 +396,17 @@ def run_b200(args, rank, world, local_rank):
                      "ratio_to_fp64": v_split / value, "trajectory_ms": statistics.mean(t_ms),
                      "roofline": split_roofline_of(statistics.mean(t_ms), rhs_s), "split_error": split_error_of()}
 
+    # the learned GMRES preconditioner of the boundary solve: trained on the plain solver's triples
+    # along a seeded optimizer-like path, measured on a held-out state of it against the fallback
+    learned = None
+    if not quartic_only and args.learned_d > 0 and world == 1 and args.workload == "d64_mixed":
+        from rcmps_b200.warmstart import path_experiment
+        learned = path_experiment(args.learned_d, train_states=args.learned_states, rhs_per_state=512, test_rhs=64,
+                                  epochs=args.learned_epochs)
+        learned["config"] = (f"D={args.learned_d}: {args.learned_states} states of a seeded path (relative steps "
+                             "1e-2), 512 traceless Gaussian right-hand sides each, 64 held-out right-hand sides of the "
+                             "next state; target |r| <= 1e-13 max(1, |b|)")
+
     cpu = None
     plan = cpu_eval_plan(args.workload)
     if rank == 0 and world == 1 and not args.no_cpu_baseline and plan:
@@ -386,6 +416,9 @@ def run_b200(args, rank, world, local_rank):
                           f"{plan[0][1]}) with the oracle on one core: {t_eval:.1f} s")}
     if rank == 0:
         metric = METRIC_SPLIT if split else METRIC
+        if args.workload == "uneven200":
+            metric = ("fg_phi4 evals/s, 200 states D in {16..128} with per-state atol/rtol in one batched call, "
+                      + ("split" if split else "FP64"))
         if quartic_only:
             metric = "quartic term (trajectory + pullback) evals/s at D=64, " + ("split" if split else "FP64")
         line = {"metric": metric, "value": value, "unit": "evals/s", "n_gpus": world, "steps": args.steps,
@@ -420,11 +453,19 @@ def run_b200(args, rank, world, local_rank):
                 "gpu_launches": None, "gpu_launches_note": "library kernel launches per step (rcmps_launch_count)", "clocks": clocks.summary(), "e2e": e2e, "cpu_baseline": cpu}
         line["gpu_launches"] = launches
         line["launches_before_timed"] = launches0
+        tuning = {}
+        for dp in sorted(set(((d + 15) // 16) * 16 if d <= 64 else (96 if d <= 96 else 128) for d in dims)):
+            ring, ms = C.c_int(0), (C.c_float * 3)()
+            if lib.rcmps_trajectory_tuning(ctx.handle, 0, dp, C.byref(ring), ms) == 0 and ring.value:
+                tuning[str(dp)] = {"ring_stages": ring.value, "calibration_ms": [round(x, 3) for x in ms]}
+        line["config"]["autotuned_tiles"] = tuning
         line["config"]["precision"] = ("split: trajectory products of the D=64 states on tcgen05 BF16 slices "
                                        "(7 x 7 bits), FP64 step control, sums and solves" if split else
                                        "FP64 tensor cores (DMMA)")
         if split_arm is not None:
             line["split_precision_arm"] = split_arm
+        if learned is not None:
+            line["learned_gmres"] = learned
         if split:
             line["dtype"] = "f64 (split bf16 trajectory products)"
             line["roofline_fp64_form"] = line["roofline"]
@@ -450,6 +491,10 @@ def main():
                    help="Gauss nodes per half window (profiling cases only; the benchmark uses 512)")
     p.add_argument("--precision", choices=("fp64", "split"), default="fp64",
                    help="trajectory products: FP64 tensor cores, or split BF16 slices on tcgen05 (D = 64)")
+    p.add_argument("--learned-d", type=int, default=32,
+                   help="bond dimension of the learned-preconditioner measurement (0: none)")
+    p.add_argument("--learned-states", type=int, default=8, help="training states of that measurement")
+    p.add_argument("--learned-epochs", type=int, default=100, help="training epochs of that measurement")
     p.add_argument("--split-arm-steps", type=int, default=3,
                    help="steps of the split-precision arm timed after the FP64 one (0: none)")
     p.add_argument("--component", choices=("fg", "quartic"), default="fg",

@@ -282,6 +282,14 @@ int rcmps_warmstart_backward(rcmps_context* context, int n, int rank, int batch,
 int rcmps_warmstart_adam(rcmps_context* context, long long count, float* param, const float* grad, float* m, float* v,
                          float lr, float beta1, float beta2, float eps, int step, void* stream);
 
+/* The tile choice of the FP64 trajectory kernel's autotuner for (system: 0 quartic, 1 all-ODE,
+ * 2 <phi>; padded dimension dp): the depth of the operand ring (2, 3 or 4 staged chunks; 0 while
+ * not yet tuned), chosen on the first launch of that pair in this context by timing a few attempts
+ * of the launch's own states at each depth, and the three calibration times in ms (ms may be
+ * NULL). The depth changes the schedule only; results are identical. No counterpart in the
+ * reference (its tiles follow a fixed rule, runtime/generic_layout.py:21-52). */
+int rcmps_trajectory_tuning(const rcmps_context* context, int system, int dp, int* ring, float* ms);
+
 /* Number of kernel launches this library has issued in the process (all contexts). No
  * counterpart in the reference. */
 long long rcmps_launch_count(void);

@@ -856,6 +856,18 @@ long long rcmps_workspace_bytes(const rcmps_context* ctx, int n, const int* dims
 
 long long rcmps_launch_count(void) { return g_launches.load(); }
 
+int rcmps_trajectory_tuning(const rcmps_context* ctx, int system, int dp, int* ring, float* ms) {
+  if (!ctx || !ring || system < 0 || system > 2) return RCMPS_INVALID_ARGUMENT;
+  int i = -1;
+  const int dps[6] = {16, 32, 48, 64, 96, 128};
+  for (int k = 0; k < 6; ++k)
+    if (dps[k] == dp) i = k;
+  if (i < 0) return RCMPS_INVALID_ARGUMENT;
+  *ring = ctx->traj_ring[system][i];
+  for (int r = 0; ms && r < 3; ++r) ms[r] = ctx->traj_ring_ms[system][i][r];
+  return RCMPS_OK;
+}
+
 double rcmps_fp64_peak_tflops(rcmps_context* ctx) {
   if (!ctx) return 0.0;
   cudaSetDevice(ctx->device);

@@ -117,6 +117,55 @@ void full_pull_specs(FullPullSpec* sp) {
 
 }  // namespace
 
+int dp_index(int dp) {
+  switch (dp) {
+    case 16: return 0;
+    case 32: return 1;
+    case 48: return 2;
+    case 64: return 3;
+    case 96: return 4;
+    default: return 5;
+  }
+}
+
+// Tile autotuning of the FP64 trajectory kernel: the depth of its operand ring (2, 3 or 4 staged
+// B chunks). On the first launch of a (system, padded dimension) in a context, each depth runs the
+// launch's own states for a few attempts (kCalibrationAttempts, results discarded: the real launch
+// starts every trajectory afresh) and the fastest by CUDA events is kept. The depth changes the
+// schedule, not the arithmetic: results are identical for every depth.
+constexpr long long kCalibrationAttempts = 6;
+static cudaError_t tune_ring(rcmps_context* ctx, int system, int dp, const TrajState* d_states, int n,
+                             const double* d_points, int npoints, TrajControls tc, cudaStream_t stream) {
+  int& ring = ctx->traj_ring[system][dp_index(dp)];
+  if (ring) return cudaSuccess;
+  cudaEvent_t a = nullptr, b = nullptr;
+  cudaError_t e = cudaEventCreate(&a);
+  if (!e) e = cudaEventCreate(&b);
+  float best = 1e30f;
+  int choice = 4;
+  tc.max_attempts = kCalibrationAttempts;
+  for (int r = 2; r <= 4 && !e; ++r) {
+    tc.ring = r;
+    float ms = 0.f;
+    for (int rep = 0; rep < 2 && !e; ++rep) {   // the first repetition warms up
+      e = cudaEventRecord(a, stream);
+      if (!e) e = trajectory_launch(system, dp, d_states, n, d_points, npoints, tc, stream, 0);
+      if (!e) e = cudaEventRecord(b, stream);
+      if (!e) e = cudaEventSynchronize(b);
+      if (!e) e = cudaEventElapsedTime(&ms, a, b);
+    }
+    ctx->traj_ring_ms[system][dp_index(dp)][r - 2] = ms;
+    if (!e && ms < best) {
+      best = ms;
+      choice = r;
+    }
+  }
+  if (a) cudaEventDestroy(a);
+  if (b) cudaEventDestroy(b);
+  if (!e) ring = choice;
+  return e;
+}
+
 int quartic_run(rcmps_context* ctx, QuarticJob& job, cudaStream_t stream) {
   const rcmps_settings& S = job.settings;
   std::vector<double> points, weights;
@@ -314,6 +363,9 @@ int quartic_run(rcmps_context* ctx, QuarticJob& job, cudaStream_t stream) {
       tc.endpoint = points.back();
       tc.initial_h = S.initial_step;
       tc.max_ns = (unsigned long long)(S.max_device_seconds * 1e9);
+      if (e == cudaSuccess && !split)
+        e = tune_ring(ctx, system, dp, (TrajState*)P(o_states), n, (double*)P(o_points), npoints, tc, stream);
+      if (!split) tc.ring = ctx->traj_ring[system][dp_index(dp)];
       if (e == cudaSuccess) e = cudaEventRecord(e0, stream);
       if (e == cudaSuccess)
         e = trajectory_launch(system, dp, (TrajState*)P(o_states), n, (double*)P(o_points), npoints, tc, stream,

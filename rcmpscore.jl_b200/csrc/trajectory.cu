@@ -221,6 +221,7 @@ struct Rhs {
   long long* gq;   // running chunk counter (uniform across the CTA)
   int nchunk;      // chunks of one right-hand side (uniform)
   int ce, cc;      // producer cursor (thread 0): entry (G1 products, then G2 passes), chunk in it
+  int nst;         // ring stages in use (2 .. GE::NST; the launch's tuned ring depth)
   // Packed Z2 state with d = DP and d/2 a multiple of 16 (zs): each CTA's 16 rows lie in one
   // parity half hh of the two halves of hz rows; the structurally zero output tiles and K
   // halves of every product are skipped.
@@ -256,7 +257,7 @@ struct Rhs {
   }
 
   __device__ void issue(long long gidx, const double2* zb) {
-    const int slot = (int)(gidx % GE::NST);
+    const int slot = (int)(gidx % nst);
     mbar_expect_tx(&sm.full[slot], GE::KC * DP * 16);
     const double2* src = cursor_src(zb);
     double2* dst = sm.ring + slot * GE::KC * GE::LDB;
@@ -270,8 +271,8 @@ struct Rhs {
 
   // Wait for chunk (global index gidx); bounded.
   __device__ const double2* await(long long gidx) {
-    const int slot = (int)(gidx % GE::NST);
-    const uint32_t parity = (uint32_t)((gidx / GE::NST) & 1);
+    const int slot = (int)(gidx % nst);
+    const uint32_t parity = (uint32_t)((gidx / nst) & 1);
     if (!mbar_wait(&sm.full[slot], parity, &sm.ctl->wait_flag)) {}
     return sm.ring + slot * GE::KC * GE::LDB;
   }
@@ -330,9 +331,9 @@ struct Rhs {
       if (lane == 0)
         for (int ch = 0; ch < nch; ++ch) {
           const long long g = g0 + q + ch;
-          if (q + ch + GE::NST < nchunk) {
-            mbar_wait(&sm.empty[(int)(g % GE::NST)], (uint32_t)((g / GE::NST) & 1), &sm.ctl->wait_flag);
-            issue(g + GE::NST, zb);
+          if (q + ch + nst < nchunk) {
+            mbar_wait(&sm.empty[(int)(g % nst)], (uint32_t)((g / nst) & 1), &sm.ctl->wait_flag);
+            issue(g + nst, zb);
           }
         }
       __syncwarp();
@@ -361,7 +362,7 @@ struct Rhs {
         }
       }
       __syncwarp();
-      if (lane == 0) mbar_arrive(&sm.empty[(int)((g0 + q) % GE::NST)]);
+      if (lane == 0) mbar_arrive(&sm.empty[(int)((g0 + q) % nst)]);
     }
     split_reduce<TPW, SK>(acc, tile0, slice);
   }
@@ -495,7 +496,7 @@ struct Rhs {
       fence_proxy_async_global();
       ce = 0;
       cc = 0;
-      for (int q = 0; q < GE::NST && q < nchunk; ++q) issue(g0 + q, zb);
+      for (int q = 0; q < nst && q < nchunk; ++q) issue(g0 + q, zb);
     }
     int q = 0;
     // ------------------------------------------------------------------ G1 products
@@ -644,7 +645,8 @@ trajectory_kernel(const TrajState* __restrict__ states, const double* __restrict
   using RhsT = std::conditional_t<ENG == 0, Rhs<DP, SYS>, RhsSplit<DP>>;
   RhsT rhs;
   if constexpr (ENG == 0) {
-    rhs = Rhs<DP, SYS>{st, sm, row0, tid, lane, warp, &gq, Rhs<DP, SYS>::total_chunks(), 0, 0};
+    rhs = Rhs<DP, SYS>{st, sm, row0, tid, lane, warp, &gq, Rhs<DP, SYS>::total_chunks(), 0, 0,
+                       ctl_in.ring >= 2 && ctl_in.ring <= GE::NST ? ctl_in.ring : GE::NST};
   } else {
     rhs.st = st;
     rhs.ss = ssm;
@@ -716,7 +718,7 @@ trajectory_kernel(const TrajState* __restrict__ states, const double* __restrict
   const double N = packed ? 10.0 * half * half + 1.0
                           : (double)GE::NCH * st->d * st->d + (GE::SCALAR ? 1.0 : 0.0);
   const double atol = st->atol, rtol = st->rtol;
-  const long long max_steps = st->max_steps;
+  const long long max_steps = ctl_in.max_attempts > 0 ? min(st->max_steps, ctl_in.max_attempts) : st->max_steps;
   const unsigned long long t_start = global_ns();
 
   while (true) {
@@ -968,8 +970,8 @@ trajectory_kernel(const TrajState* __restrict__ states, const double* __restrict
   if constexpr (ENG == 0) {
     if (tid == 0 && C.wait_flag) {
       // a copy whose wait gave up may still be in flight: wait for each slot's last use, bounded
-      for (long long g = gq - 1; g >= 0 && g >= gq - GE::NST; --g) {
-        mbar_wait(&sm.full[g % GE::NST], (uint32_t)((g / GE::NST) & 1), nullptr);
+      for (long long g = gq - 1; g >= 0 && g >= gq - rhs.nst; --g) {
+        mbar_wait(&sm.full[g % rhs.nst], (uint32_t)((g / rhs.nst) & 1), nullptr);
       }
     }
   } else {

@@ -43,6 +43,8 @@ struct TrajControls {
   double endpoint;          // sqrt(half_window)
   double initial_h;
   unsigned long long max_ns;  // device-clock watchdog in ns (0: none)
+  int ring = 0;               // stages of the FP64 engine's operand ring (2 .. 4; 0: the default 4)
+  long long max_attempts = 0; // stop every trajectory after this many attempts (0: none; calibration)
 };
 
 cudaError_t trajectory_set_tables();

@@ -101,3 +101,18 @@ def test_controls_are_checked(gpu_context):
         objective.fg_phi4_batch([rec["R"]], [rec["K"]], [rec["rho"]], [1.0],
                                 objective.settings_from_args(None, n_quad=32, kinetic_nodes=64),
                                 tolerances=[(1e-12, 1e-17)])
+
+
+def test_trajectory_tile_autotuner_records_its_choice(gpu_context):
+    """After a D = 64 evaluation the context holds the autotuned ring depth of the quartic
+    trajectory kernel (2, 3 or 4 staged chunks) and the three calibration times."""
+    import ctypes as C
+    from rcmps_b200 import objective
+    rec = load_records("bench.npz")[0]
+    objective.fg_phi4_batch([rec["R"]], [rec["K"]], [rec["rho"]], [rec["g"]],
+                            objective.settings_from_args(None, half_window=2.0, n_quad=16, kinetic_nodes=32))
+    ctx = gpu_context
+    ring, ms = C.c_int(0), (C.c_float * 3)()
+    assert ctx.lib.rcmps_trajectory_tuning(ctx.handle, 0, 64, C.byref(ring), ms) == 0
+    assert ring.value in (2, 3, 4)
+    assert all(x > 0 for x in ms) and ms[ring.value - 2] == min(ms)
