@@ -282,6 +282,26 @@ int rcmps_warmstart_backward(rcmps_context* context, int n, int rank, int batch,
 int rcmps_warmstart_adam(rcmps_context* context, long long count, float* param, const float* grad, float* m, float* v,
                          float lr, float beta1, float beta2, float eps, int step, void* stream);
 
+/* The L-BFGS search direction of the optimizer on the device (one CTA; d <= 128), the algebra of
+ * runtime/optimizer.py:73-107 with the metric <X, Y> = 2 Re tr(X^dag Y (rho + metric_reg I)) and
+ * the preconditioner P(X) = ((rho + precond_reg I)^-1 (X (rho + metric_reg I))^dag)^dag:
+ *   m > 0: the two-loop recursion over the pairs S[j], Y[j] (d x d each, oldest first) with
+ *          inv_sy[j] = 1 / <S[j], Y[j]>, the middle preconditioner scaled by
+ *          gamma = <s, y> / <y, P(y)> of the newest pair; direction = -H g;
+ *   m = 0: the first direction -first_norm P(g) / |P(g)|.
+ * scalars (device, 3 doubles): gamma (NaN for m = 0 or when gamma is not positive: then no
+ * direction is written), the slope <g, direction>, and a status (1: rho + precond_reg I is not
+ * positive definite). work: device scratch of 8 d^2 + m doubles. All device memory, row-major
+ * complex128. No counterpart as an entry in the reference (its controller is host NumPy). */
+int rcmps_lbfgs_direction(rcmps_context* context, int d, int m, const double* rho, const double* gradient,
+                          const double* S, const double* Y, const double* inv_sy, double metric_reg,
+                          double precond_reg, double first_norm, double* direction, double* work, double* scalars,
+                          void* stream);
+/* The canonical retraction on the device: R' = R + alpha X, K' = Herm(K + i alpha/2 (X^dag R - R^dag X))
+ * (runtime/numerics.py:133-136). */
+int rcmps_retract(rcmps_context* context, int d, const double* R, const double* K, const double* direction,
+                  double alpha, double* R_out, double* K_out, void* stream);
+
 /* The tile choice of the FP64 trajectory kernel's autotuner for (system: 0 quartic, 1 all-ODE,
  * 2 <phi>; padded dimension dp): the depth of the operand ring (2, 3 or 4 staged chunks; 0 while
  * not yet tuned), chosen on the first launch of that pair in this context by timing a few attempts

@@ -101,6 +101,8 @@ SIGNATURES = {
     "rcmps_warmstart_backward": (_I, [_P, _I, _I, _I, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
     "rcmps_warmstart_adam": (_I, [_P, C.c_longlong, _P, _P, _P, _P, C.c_float, C.c_float, C.c_float, C.c_float, _I,
                                   _P]),
+    "rcmps_lbfgs_direction": (_I, [_P, _I, _I, _P, _P, _P, _P, _P, _D, _D, _D, _P, _P, _P, _P]),
+    "rcmps_retract": (_I, [_P, _I, _P, _P, _P, _D, _P, _P, _P]),
     "rcmps_trajectory_tuning": (_I, [_P, _I, _I, C.POINTER(_I), C.POINTER(C.c_float)]),
     "rcmps_fp64_peak_tflops": (_D, [_P]),
     "rcmps_launch_count": (C.c_longlong, []),

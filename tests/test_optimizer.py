@@ -94,3 +94,48 @@ def test_warm_stationary_correction_matches_cold_solve(gpu_context):
     assert np.linalg.norm(O.lindblad(qq, rr, warm)) < 1e-11
     with pytest.raises(ValueError):
         objective.stationary_state_correction(qq, rr, 2.0 * rho_prev, tolerance=1e-13)
+
+
+@pytest.mark.gpu
+def test_device_algebra_matches_host(gpu_context):
+    """rcmps_lbfgs_direction and rcmps_retract against the host algebra on random histories."""
+    from rcmps_b200 import optimizer
+    rng = np.random.default_rng(11)
+    for d, m in ((6, 0), (8, 5), (16, 12)):
+        R, K = O.phi4_state(d, 100 + d)
+        rho = O.stationary_state(O.left_canonical_q(R, K), R)
+        tangent = optimizer._Tangent(rho, 1e-3)
+        cplx = lambda: rng.standard_normal((d, d)) + 1j * rng.standard_normal((d, d))
+        g = cplx()
+        hist = optimizer._History(100)
+        for _ in range(m):
+            s, y = cplx(), cplx()
+            s = s / np.sqrt(tangent.inner(s, s))
+            y = y + 3.0 * s
+            hist.push(s, y, 1.0 / tangent.inner(s, y))
+        dev = optimizer._DeviceAlgebra(d)
+        got, gamma, slope = dev.direction(rho, g, list(hist.pairs), 1e-3, 1e-4, 0.01)
+        if m:
+            ref, ref_gamma = hist.direction(tangent, g, 1e-4)
+            assert abs(gamma - ref_gamma) <= 1e-12 * abs(ref_gamma)
+        else:
+            ref = optimizer._first_direction(tangent, g, 1e-4, 0.01)
+        assert np.abs(got - ref).max() <= 1e-11 * np.abs(ref).max()
+        assert abs(slope - tangent.inner(g, ref)) <= 1e-11 * abs(slope)
+        X = cplx()
+        r1, k1 = dev.retract(R, K, X, 0.3)
+        r2, k2 = optimizer.retract(R, K, X, 0.3)
+        assert np.abs(r1 - r2).max() <= 1e-14 and np.abs(k1 - k2).max() <= 1e-13
+
+
+@pytest.mark.gpu
+def test_controller_with_device_algebra_matches_reference(gpu_context):
+    """The eight reference iterations with the directions and retractions formed on the GPU."""
+    from rcmps_b200 import objective, optimizer
+    rec = load_records("optim.npz")[0]
+    args = objective.default_args(window=rec["window"], quadrature=int(rec["n_quad"]), nodes=int(rec["nodes"]))
+    call = lambda r, k, rho: objective.objective(r, k, rho, rec["g"], args)
+    events = list(optimizer.optimize(rec["R"], rec["K"], rec["rho"], rec["energy0"], rec["gradient0"], call,
+                                     dict(max_iterations=int(rec["iterations"]), gradient_tol=1e-9),
+                                     device_algebra=True))
+    _check(rec, _accepted(events), 1e-9)
