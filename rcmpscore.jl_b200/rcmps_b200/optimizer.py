@@ -27,7 +27,8 @@ it implements, stated here in full:
 Every trial's stationary density comes from the library: rcmps_stationary_state_batch, or with
 warm_stationary=True the correction started from the last accepted density
 (rcmps_stationary_correction_batch). objective_callable is normally
-rcmps_b200.objective.objective.
+rcmps_b200.objective.objective. With device_algebra=True the directions and retractions are
+formed on the GPU too (rcmps_lbfgs_direction, rcmps_retract).
 """
 from __future__ import annotations
 
@@ -189,6 +190,65 @@ class _History:
         return -z, float(gamma)
 
 
+class _DeviceAlgebra:
+    """The L-BFGS algebra of one state on the GPU (rcmps_lbfgs_direction, rcmps_retract). The
+    matrices and history pairs go up per call (a few D x D matrices, small next to one objective
+    evaluation); only the direction and its scalars come back."""
+
+    def __init__(self, d):
+        from .objective import context
+        self.ctx = context()
+        self.d = d
+
+    @staticmethod
+    def _dev(arrays):
+        import torch
+        if not arrays:
+            return torch.zeros(1, dtype=torch.complex128, device="cuda")
+        flat = np.concatenate([np.ascontiguousarray(a, dtype=np.complex128).ravel() for a in arrays])
+        return torch.from_numpy(flat).cuda()
+
+    def direction(self, rho, gradient, pairs, metric_reg, precond_reg, first_norm):
+        """(direction, gamma, slope): with pairs, the two-loop direction and its gamma (direction
+        None when gamma is not positive); without, the first direction and gamma None."""
+        import torch
+        from .objective import _stream
+        d, m = self.d, len(pairs)
+        drho, dg = self._dev([rho]), self._dev([gradient])
+        dS, dY = self._dev([p[0] for p in pairs]), self._dev([p[1] for p in pairs])
+        dinv = torch.tensor([float(p[2]) for p in pairs] or [0.0], dtype=torch.float64, device="cuda")
+        out = torch.zeros(d * d, dtype=torch.complex128, device="cuda")
+        work = torch.zeros(8 * d * d + max(m, 1), dtype=torch.float64, device="cuda")
+        scal = torch.zeros(3, dtype=torch.float64, device="cuda")
+        ctx = self.ctx
+        rc = ctx.lib.rcmps_lbfgs_direction(ctx.handle, d, m, drho.data_ptr(), dg.data_ptr(), dS.data_ptr(),
+                                           dY.data_ptr(), dinv.data_ptr(), float(metric_reg), float(precond_reg),
+                                           float(first_norm), out.data_ptr(), work.data_ptr(), scal.data_ptr(),
+                                           _stream())
+        if rc:
+            raise SolverFailure(f"L-BFGS direction on the device: {ctx.error()}")
+        gamma, slope, status = scal.cpu().numpy()
+        if status:
+            raise SolverFailure("rho + precond_reg I is not positive definite")
+        if m == 0:
+            return out.cpu().numpy().reshape(d, d), None, float(slope)
+        if not (np.isfinite(gamma) and gamma > 0):
+            return None, float(gamma), float("nan")
+        return out.cpu().numpy().reshape(d, d), float(gamma), float(slope)
+
+    def retract(self, r, k, x, alpha):
+        import torch
+        from .objective import _stream
+        d, ctx = self.d, self.ctx
+        dR, dK, dX = self._dev([r]), self._dev([k]), self._dev([x])
+        Rn, Kn = torch.empty_like(dR), torch.empty_like(dK)
+        rc = ctx.lib.rcmps_retract(ctx.handle, d, dR.data_ptr(), dK.data_ptr(), dX.data_ptr(), float(alpha),
+                                   Rn.data_ptr(), Kn.data_ptr(), _stream())
+        if rc:
+            raise SolverFailure(f"retraction on the device: {ctx.error()}")
+        return Rn.cpu().numpy().reshape(d, d), Kn.cpu().numpy().reshape(d, d)
+
+
 def _first_direction(tangent, gradient, precond_reg, length):
     pg = tangent.precondition(gradient, precond_reg)
     n = tangent.norm(pg)
@@ -200,7 +260,8 @@ def _first_direction(tangent, gradient, precond_reg, length):
 class _Run:
     """One invocation of the optimizer: the accepted state, its history and counters."""
 
-    def __init__(self, r, k, rho, energy, gradient, objective_callable, controls, resume_state, warm):
+    def __init__(self, r, k, rho, energy, gradient, objective_callable, controls, resume_state, warm,
+                 device_algebra=False):
         self.c = _controls(controls)
         self.objective = objective_callable
         self.warm = bool(warm)
@@ -231,6 +292,7 @@ class _Run:
                 or not (np.isfinite(self.elapsed_before) and self.elapsed_before >= 0)):
             raise ValueError("the resumed optimizer counters or controls are invalid")
         self.last_stats = res.get("stats")
+        self.device = _DeviceAlgebra(shape[0]) if device_algebra else None
         self.start = perf_counter()
 
     # ---------------------------------------------------------------- state and events
@@ -254,6 +316,8 @@ class _Run:
     def search_direction(self, tangent, gnorm):
         if self.c.refresh_curvatures:
             self.history.refresh(tangent, gnorm)
+        if self.device is not None:
+            return self.device_direction()
         gamma = None
         direction = None
         if len(self.history):
@@ -265,6 +329,19 @@ class _Run:
             self.history.clear()
             direction = _first_direction(tangent, self.g, self.precond_reg, self.c.initial_direction_norm)
             slope = tangent.inner(self.g, direction)
+            if not (np.isfinite(slope) and slope < 0):
+                raise SolverFailure("the preconditioned direction does not descend")
+        return direction, slope, gamma
+
+    def device_direction(self):
+        """search_direction's decisions with the algebra on the GPU."""
+        c, dev = self.c, self.device
+        direction, gamma, slope = dev.direction(self.rho, self.g, list(self.history.pairs), c.metric_reg,
+                                                self.precond_reg, c.initial_direction_norm)
+        if direction is None or not (np.isfinite(slope) and slope < 0):
+            self.history.clear()
+            direction, _, slope = dev.direction(self.rho, self.g, [], c.metric_reg, self.precond_reg,
+                                                c.initial_direction_norm)
             if not (np.isfinite(slope) and slope < 0):
                 raise SolverFailure("the preconditioned direction does not descend")
         return direction, slope, gamma
@@ -324,7 +401,8 @@ class _Run:
                     yield self.stopped("optimization time budget reached during line search",
                                        numerical_failures=failures)
                     return
-                r_t, k_t = retract(self.r, self.k, direction, alpha)
+                r_t, k_t = (self.device.retract(self.r, self.k, direction, alpha) if self.device is not None
+                            else retract(self.r, self.k, direction, alpha))
                 try:
                     rho_t, e_t, g_t, stats_t, stationary_t = self.evaluate(r_t, k_t)
                 except (SolverFailure, RuntimeError) as err:
@@ -353,7 +431,8 @@ class _Run:
                        cautious_update=cautious, history_size=len(self.history), evaluations=self.evaluations)
 
 
-def optimize(r, k, rho, energy, gradient, objective_callable, controls, resume_state=None, *, warm_stationary=False):
+def optimize(r, k, rho, energy, gradient, objective_callable, controls, resume_state=None, *, warm_stationary=False,
+             device_algebra=False):
     """Yield the optimizer's events from an accepted, already evaluated state (r, k, rho,
     energy, gradient). objective_callable(r, k, rho) -> (energy, gradient, stats).
 
@@ -363,5 +442,8 @@ def optimize(r, k, rho, energy, gradient, objective_callable, controls, resume_s
     stream with its reason. resume_state continues a run from such a state without a new
     initial evaluation; max_iterations counts accepted iterations across resumes, max_seconds
     this invocation only. warm_stationary=True starts each trial's stationary solve from the
-    last accepted density."""
-    return _Run(r, k, rho, energy, gradient, objective_callable, controls, resume_state, warm_stationary).events()
+    last accepted density. device_algebra=True forms every search direction (two-loop recursion,
+    preconditioner, scaling) and every retraction on the GPU (rcmps_lbfgs_direction,
+    rcmps_retract); the host keeps the line-search decisions."""
+    return _Run(r, k, rho, energy, gradient, objective_callable, controls, resume_state, warm_stationary,
+                device_algebra).events()

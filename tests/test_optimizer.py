@@ -109,9 +109,9 @@ def test_device_algebra_matches_host(gpu_context):
         g = cplx()
         hist = optimizer._History(100)
         for _ in range(m):
-            s, y = cplx(), cplx()
-            s = s / np.sqrt(tangent.inner(s, s))
-            y = y + 3.0 * s
+            s, noise = cplx(), cplx()
+            s = s / tangent.norm(s)
+            y = 3.0 * s + 0.3 * noise / tangent.norm(noise)   # <s, y> >= 2.7: gamma > 0
             hist.push(s, y, 1.0 / tangent.inner(s, y))
         dev = optimizer._DeviceAlgebra(d)
         got, gamma, slope = dev.direction(rho, g, list(hist.pairs), 1e-3, 1e-4, 0.01)
