@@ -118,10 +118,43 @@ def _cpu_eval(args):
 
 
 def cpu_eval_plan(workload):
-    """(d, seed, z2, g) of every state of d64_mixed (the seeds of rcmps_b200.batch)."""
+    """(d, seed, z2, g) of every state of d64_mixed or d64_single (the seeds of rcmps_b200.batch)."""
+    if workload == "d64_single":
+        return [(64, 0, False, 2.0)]
     if workload != "d64_mixed":
         return None
     return [(64, i, False, 2.0) for i in range(16)] + [(64, 100 + i, True, 2.0) for i in range(16)]
+
+
+def single_state_latency(steps):
+    """Latency of one evaluation of the first random D = 64 state of the workload through the
+    public single-state call (rcmps_b200.objective.objective, host arrays in and out), the call an
+    L-BFGS trial makes: wall time per call after one untimed call, the device phases of the last
+    call, and the trajectory's layout (CTAs per state)."""
+    import ctypes as C
+    from rcmps_b200 import objective
+    from rcmps_b200.batch import random_state
+    R, K = random_state(64, 0)
+    Q = -1j * K - R.conj().T @ R / 2
+    rho, _ = objective.stationary_state(Q, R, tolerance=1e-13)
+    args = objective.default_args()
+    e, _, st = objective.objective(R, K, rho, 2.0, args)
+    walls = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        e, _, st = objective.objective(R, K, rho, 2.0, args)
+        walls.append(time.perf_counter() - t0)
+    ctx = objective.context()
+    t = ctx.timings()
+    groups = C.c_int(0)
+    ctx.lib.rcmps_trajectory_groups(ctx.handle, 0, 64, C.byref(groups))
+    return {"workload": "1 random state D=64 (seed 0, scaling 0.2), g=2, the benchmark's settings",
+            "api": "rcmps_b200.objective.objective (host arrays in and out)", "steps": steps,
+            "ms_per_eval": 1000 * statistics.mean(walls), "ms_min": 1000 * min(walls),
+            "phases_ms_last_call": {"trajectory": t[0], "pullback": t[1], "kinetic": t[2], "boundary_finish": t[3],
+                                    "whole_call": t[4]},
+            "trajectory_ctas_per_state": 4 * groups.value, "channel_groups": groups.value,
+            "rhs_calls": st["rhs_calls"], "accepted": st["accepted"], "rejected": st["rejected"], "energy": e}
 
 
 # ----------------------------------------------------------------------------- reference arm
@@ -396,6 +429,11 @@ def run_b200(args, rank, world, local_rank):
                      "ratio_to_fp64": v_split / value, "trajectory_ms": statistics.mean(t_ms),
                      "roofline": split_roofline_of(statistics.mean(t_ms), rhs_s), "split_error": split_error_of()}
 
+    # the latency of one lone state through the single-state call (the L-BFGS caller's view)
+    single = None
+    if not quartic_only and world == 1 and args.workload == "d64_mixed" and args.single_steps > 0:
+        single = single_state_latency(args.single_steps)
+
     # the learned GMRES preconditioner of the boundary solve: trained on the plain solver's triples
     # along a seeded optimizer-like path, measured on a held-out state of it against the fallback
     learned = None
@@ -466,6 +504,8 @@ def run_b200(args, rank, world, local_rank):
             line["split_precision_arm"] = split_arm
         if learned is not None:
             line["learned_gmres"] = learned
+        if single is not None:
+            line["single_state"] = single
         if split:
             line["dtype"] = "f64 (split bf16 trajectory products)"
             line["roofline_fp64_form"] = line["roofline"]
@@ -497,6 +537,8 @@ def main():
     p.add_argument("--learned-epochs", type=int, default=100, help="training epochs of that measurement")
     p.add_argument("--split-arm-steps", type=int, default=3,
                    help="steps of the split-precision arm timed after the FP64 one (0: none)")
+    p.add_argument("--single-steps", type=int, default=3,
+                   help="timed calls of the single-state latency measurement (0: none)")
     p.add_argument("--component", choices=("fg", "quartic"), default="fg",
                    help="time the whole evaluation (default) or the quartic term alone")
     args = p.parse_args()

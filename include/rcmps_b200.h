@@ -61,11 +61,17 @@ typedef struct rcmps_settings {
                                   with that structure, unpacked for the others */
   int precision;               /* quartic trajectory products: 0 FP64 tensor cores (DMMA); 1 split
                                   precision on the 5th-generation tensor cores (each FP64 operand cut
-                                  into six 7-bit BF16 slices, slice products accumulated in FP32 in
-                                  tensor memory, recombined in FP64; error about 2^-43 of the row and
+                                  into seven 7-bit BF16 slices, slice products accumulated in FP32 in
+                                  tensor memory, recombined in FP64; error about 2^-48 of the row and
                                   column scales per term) for the states of padded dimension 64, FP64
                                   for the others. The DOP853 error estimate and step control, the
                                   stage sums and every solve stay FP64. */
+  int trajectory_groups;       /* FP64 quartic trajectory: CTAs per 16-row block of a state, each for
+                                  a group of channels (1, 2 or 4; a state's cluster has dp/16 times
+                                  as many CTAs, at most 16). 0 (default): the most that keeps every
+                                  state of the launch resident at once, so a lone state spreads over
+                                  up to 16 SMs and a full batch keeps one CTA per row block. Results
+                                  agree to rounding (the reductions' summation order changes). */
 } rcmps_settings;
 
 /* Per-state diagnostics. */
@@ -303,12 +309,18 @@ int rcmps_retract(rcmps_context* context, int d, const double* R, const double* 
                   double alpha, double* R_out, double* K_out, void* stream);
 
 /* The tile choice of the FP64 trajectory kernel's autotuner for (system: 0 quartic, 1 all-ODE,
- * 2 <phi>; padded dimension dp): the depth of the operand ring (2, 3 or 4 staged chunks; 0 while
- * not yet tuned), chosen on the first launch of that pair in this context by timing a few attempts
- * of the launch's own states at each depth, and the three calibration times in ms (ms may be
- * NULL). The depth changes the schedule only; results are identical. No counterpart in the
- * reference (its tiles follow a fixed rule, runtime/generic_layout.py:21-52). */
+ * 2 <phi>; padded dimension dp) at the channel-group count of the last launch of that pair: the
+ * depth of the operand ring (2, 3 or 4 staged chunks; 0 while not yet tuned), chosen on the first
+ * launch of that pair and group count in this context by timing a few attempts of the launch's
+ * own states at each depth, and the three calibration times in ms (ms may be NULL). The depth
+ * changes the schedule only; results are identical. No counterpart in the reference (its tiles
+ * follow a fixed rule, runtime/generic_layout.py:21-52). */
 int rcmps_trajectory_tuning(const rcmps_context* context, int system, int dp, int* ring, float* ms);
+/* The channel groups of the last trajectory launch of (system, dp) in this context (1, 2 or 4
+ * CTAs per 16-row block of a state, rcmps_settings.trajectory_groups; 0: no launch yet). No
+ * counterpart in the reference (its cooperative grid takes a fixed CTA count per state,
+ * persistent_trajectory_backend.py:207-283). */
+int rcmps_trajectory_groups(const rcmps_context* context, int system, int dp, int* groups);
 
 /* Number of kernel launches this library has issued in the process (all contexts). No
  * counterpart in the reference. */

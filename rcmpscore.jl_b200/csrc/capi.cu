@@ -202,6 +202,8 @@ int check_settings(rcmps_context* ctx, const rcmps_settings* s) {
     return fail(ctx, RCMPS_INVALID_ARGUMENT, "symmetry must be 0 (unpacked), 1 (packed Z2) or 2 (packed where Z2)");
   if (s->precision < 0 || s->precision > 1)
     return fail(ctx, RCMPS_INVALID_ARGUMENT, "precision must be 0 (FP64 tensor cores) or 1 (split BF16 slices)");
+  if (s->trajectory_groups != 0 && s->trajectory_groups != 1 && s->trajectory_groups != 2 && s->trajectory_groups != 4)
+    return fail(ctx, RCMPS_INVALID_ARGUMENT, "trajectory_groups must be 0 (automatic), 1, 2 or 4");
   return RCMPS_OK;
 }
 
@@ -289,6 +291,7 @@ void rcmps_default_settings(rcmps_settings* s) {
   s->boundary_tolerance = 1e-13;
   s->symmetry = 0;
   s->precision = 0;
+  s->trajectory_groups = 0;
 }
 
 int rcmps_context_create(int device, rcmps_context** out) {
@@ -863,9 +866,21 @@ int rcmps_trajectory_tuning(const rcmps_context* ctx, int system, int dp, int* r
   for (int k = 0; k < 6; ++k)
     if (dps[k] == dp) i = k;
   if (i < 0) return RCMPS_INVALID_ARGUMENT;
-  *ring = ctx->traj_ring[system][i];
-  for (int r = 0; ms && r < 3; ++r) ms[r] = ctx->traj_ring_ms[system][i][r];
+  const int g = ctx->traj_groups[system][i], level = g == 4 ? 2 : g == 2 ? 1 : 0;
+  *ring = ctx->traj_ring[system][i][level];
+  for (int r = 0; ms && r < 3; ++r) ms[r] = ctx->traj_ring_ms[system][i][level][r];
   return RCMPS_OK;
+}
+
+int rcmps_trajectory_groups(const rcmps_context* ctx, int system, int dp, int* groups) {
+  if (!ctx || !groups || system < 0 || system > 2) return RCMPS_INVALID_ARGUMENT;
+  const int dps[6] = {16, 32, 48, 64, 96, 128};
+  for (int k = 0; k < 6; ++k)
+    if (dps[k] == dp) {
+      *groups = ctx->traj_groups[system][k];
+      return RCMPS_OK;
+    }
+  return RCMPS_INVALID_ARGUMENT;
 }
 
 double rcmps_fp64_peak_tflops(rcmps_context* ctx) {

@@ -196,10 +196,23 @@ RCMPS_DEVICE_INLINE uint32_t cluster_id_x() {
   asm volatile("mov.u32 %0, %%clusterid.x;" : "=r"(r));
   return r;
 }
+RCMPS_DEVICE_INLINE uint32_t cluster_size() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%cluster_nctarank;" : "=r"(r));
+  return r;
+}
 // Full cluster barrier with release/acquire semantics at cluster scope (orders global and
 // shared::cluster accesses of every thread of the cluster).
 RCMPS_DEVICE_INLINE void cluster_sync() {
   asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+// The two halves of cluster_sync, for work placed between them: every thread of every CTA of the
+// cluster executes one arrive and then one wait.
+RCMPS_DEVICE_INLINE void cluster_arrive_release() {
+  asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory");
+}
+RCMPS_DEVICE_INLINE void cluster_wait_acquire() {
+  asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory");
 }
 // Read a double from the shared memory of CTA `rank` of this cluster at the address that `p`
 // has in this CTA.

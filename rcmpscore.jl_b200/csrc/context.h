@@ -45,10 +45,12 @@ struct rcmps_context {
   std::mutex mu;                          // guards `error` (the composite entry runs two host threads)
   bool tables = false;
   float last_ms[8] = {0};                 // device times of the last call's phases
-  // trajectory tile autotuning: the operand-ring depth chosen per (system, padded dimension) on
-  // first use, and the calibration times of the depths 2, 3, 4 (ms)
-  int traj_ring[3][6] = {};
-  float traj_ring_ms[3][6][3] = {};
+  // trajectory tile autotuning: the operand-ring depth chosen per (system, padded dimension,
+  // channel-group level 1/2/4) on first use, and the calibration times of the depths 2, 3, 4 (ms);
+  // the channel groups of the last launch per (system, padded dimension)
+  int traj_ring[3][6][3] = {};
+  float traj_ring_ms[3][6][3][3] = {};
+  int traj_groups[3][6] = {};
 };
 
 namespace rcmps {

@@ -134,9 +134,12 @@ int dp_index(int dp) {
 // starts every trajectory afresh) and the fastest by CUDA events is kept. The depth changes the
 // schedule, not the arithmetic: results are identical for every depth.
 constexpr long long kCalibrationAttempts = 6;
+static int group_level(int groups) { return groups == 4 ? 2 : groups == 2 ? 1 : 0; }
+
 static cudaError_t tune_ring(rcmps_context* ctx, int system, int dp, const TrajState* d_states, int n,
                              const double* d_points, int npoints, TrajControls tc, cudaStream_t stream) {
-  int& ring = ctx->traj_ring[system][dp_index(dp)];
+  const int level = group_level(tc.groups);
+  int& ring = ctx->traj_ring[system][dp_index(dp)][level];
   if (ring) return cudaSuccess;
   cudaEvent_t a = nullptr, b = nullptr;
   cudaError_t e = cudaEventCreate(&a);
@@ -154,7 +157,7 @@ static cudaError_t tune_ring(rcmps_context* ctx, int system, int dp, const TrajS
       if (!e) e = cudaEventSynchronize(b);
       if (!e) e = cudaEventElapsedTime(&ms, a, b);
     }
-    ctx->traj_ring_ms[system][dp_index(dp)][r - 2] = ms;
+    ctx->traj_ring_ms[system][dp_index(dp)][level][r - 2] = ms;
     if (!e && ms < best) {
       best = ms;
       choice = r;
@@ -363,9 +366,11 @@ int quartic_run(rcmps_context* ctx, QuarticJob& job, cudaStream_t stream) {
       tc.endpoint = points.back();
       tc.initial_h = S.initial_step;
       tc.max_ns = (unsigned long long)(S.max_device_seconds * 1e9);
+      tc.groups = trajectory_groups(system, dp, n, S.trajectory_groups, split ? 1 : 0);
+      ctx->traj_groups[system][dp_index(dp)] = tc.groups;
       if (e == cudaSuccess && !split)
         e = tune_ring(ctx, system, dp, (TrajState*)P(o_states), n, (double*)P(o_points), npoints, tc, stream);
-      if (!split) tc.ring = ctx->traj_ring[system][dp_index(dp)];
+      if (!split) tc.ring = ctx->traj_ring[system][dp_index(dp)][group_level(tc.groups)];
       if (e == cudaSuccess) e = cudaEventRecord(e0, stream);
       if (e == cudaSuccess)
         e = trajectory_launch(system, dp, (TrajState*)P(o_states), n, (double*)P(o_points), npoints, tc, stream,

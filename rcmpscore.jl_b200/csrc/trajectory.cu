@@ -79,9 +79,14 @@ __device__ __forceinline__ double next_up(double t) {
 //       the pass has the third K block (commutator spec);
 //   lsrc/lcoef/lkind: the left insertion c_l ol_a X_a (P_a for ol = R, L_a for the commutator);
 //   rsrc/rcoef: the right insertion c_r X_b ol_b^dag; fixed: 1 fixed0, 2 fixed6;
-//   init: initial value 0, rho (1) or the identity on the physical block (2).
+//   init: initial value 0, rho (1) or the identity on the physical block (2);
+//   grp_*[k]: the channel groups when a state's rows are also split by channel over 2^k CTAs
+//       (contiguous channel ranges; a G2 pass never straddles two groups), grp_remote[k] when a
+//       left insertion reads P_a of a channel in another group (the CTAs then meet at a cluster
+//       barrier between the G1 products and the G2 epilogues).
 constexpr int kSysQuartic = 0, kSysFull = 1, kSysPhi1 = 2;
 constexpr int kMaxChannels = 26;
+constexpr int kGroupLevels = 3;   // 1, 2 or 4 channel groups
 struct SysTab {
   int nch, ng1;
   int g1_ch[32], g1_kind[32];
@@ -90,6 +95,8 @@ struct SysTab {
   int dir[kMaxChannels], lsrc[kMaxChannels], lkind[kMaxChannels], rsrc[kMaxChannels];
   int fixed[kMaxChannels], init[kMaxChannels];
   double lcoef[kMaxChannels], rcoef[kMaxChannels];
+  int grp_levels;                               // group levels available (1: whole-state CTAs only)
+  int grp_first[kGroupLevels][4], grp_count[kGroupLevels][4], grp_remote[kGroupLevels];
 };
 __constant__ SysTab c_sys[3];
 
@@ -226,6 +233,9 @@ struct Rhs {
   // parity half hh of the two halves of hz rows; the structurally zero output tiles and K
   // halves of every product are skipped.
   int zs, hz, hh;
+  // The CTA's channels [c0, c1) (all of them unless the state's rows are split by channel too)
+  // and whether a left insertion reads P of a channel another CTA computes (remote).
+  int c0, c1, remote;
 
   __device__ static const SysTab& T() { return c_sys[SYS]; }
   __device__ static int gsi() { return GE::GS == 2 ? 1 : 0; }
@@ -236,10 +246,21 @@ struct Rhs {
     if (e < t.ng1) return GE::CH1;
     return (t.p_k3[gsi()][e - t.ng1] ? 3 : 2) * GE::CH1;
   }
-  __device__ static int total_chunks() {
+  __device__ static int entries() { return T().ng1 + T().np[gsi()]; }
+  // Entry e (a G1 product or a G2 pass) belongs to this CTA's channels.
+  __device__ bool mine(int e) const {
     const SysTab& t = T();
+    const int c = e < t.ng1 ? t.g1_ch[e] : t.p_first[gsi()][e - t.ng1];
+    return c >= c0 && c < c1;
+  }
+  __device__ int next_mine(int e) const {
+    while (e < entries() && !mine(e)) ++e;
+    return e;
+  }
+  __device__ int total_chunks() const {
     int n = 0;
-    for (int e = 0; e < t.ng1 + t.np[gsi()]; ++e) n += entry_chunks(e);
+    for (int e = 0; e < entries(); ++e)
+      if (mine(e)) n += entry_chunks(e);
     return n;
   }
 
@@ -265,7 +286,7 @@ struct Rhs {
     for (int r = 0; r < GE::KC; ++r) bulk_g2s(dst + r * GE::LDB, src + r * DP, DP * 16, &sm.full[slot]);
     if (++cc == entry_chunks(ce)) {
       cc = 0;
-      ++ce;
+      ce = next_mine(ce + 1);
     }
   }
 
@@ -410,9 +431,11 @@ struct Rhs {
 
   // G2 pass over the channels first..first+NC-1 (same direction and spec). K3: the pass has the
   // third K block of the commutator spec.
+  // wait: meet the other CTAs' G1 results here (the cluster barrier's wait half, after this
+  // pass's products and before its epilogue reads P of another CTA's channel).
   template <int NC, bool K3>
   __device__ void g2_pass(int first, const double2* zb, double2* kout, double jac, double src, int& q,
-                          long long g0) {
+                          long long g0, bool wait) {
     using TL = PassTiling<DP, 16 * NC, GE::NW>;
     constexpr int TPW = TL::TPW, SK = TL::SK;
     const SysTab& t = T();
@@ -461,6 +484,7 @@ struct Rhs {
       kn1 = (1 - hh) ^ p;
     }
     stream_product<TL>(acc, sm.aprime, GE::LDA2, (K3 ? 3 : 2) * GE::CH1, q, g0, zb, zt, kn0, kn1);
+    if (wait) cluster_wait_acquire();
     if (slice == 0 && warp < GE::NW) {
 #pragma unroll
       for (int j = 0; j < TPW; ++j) {
@@ -494,7 +518,7 @@ struct Rhs {
     const long long g0 = *gq;
     if (tid == GE::NW * 32) {
       fence_proxy_async_global();
-      ce = 0;
+      ce = next_mine(0);
       cc = 0;
       for (int q = 0; q < nst && q < nchunk; ++q) issue(g0 + q, zb);
     }
@@ -503,6 +527,7 @@ struct Rhs {
     int kind_prev = -1;
     for (int e = 0; e < t.ng1; ++e) {
       const int c = t.g1_ch[e], kind = t.g1_kind[e];
+      if (c < c0 || c >= c1) continue;
       if (kind != kind_prev) {
         __syncthreads();
         load_panel(kind, sm.panel);
@@ -513,29 +538,36 @@ struct Rhs {
       else if constexpr (GE::KM == 3) g1_product<16>(c, zb, kout, jac, q, g0);
     }
     __syncthreads();
+    // the G1 results (P) of every CTA are published here and awaited in the first G2 pass
+    if (remote) cluster_arrive_release();
+    bool wait = remote != 0;
     // ------------------------------------------------------------------ G2 passes
     const int gs = gsi();
     for (int p = 0; p < t.np[gs]; ++p) {
       const int first = t.p_first[gs][p];
+      if (first < c0 || first >= c1) continue;
       const bool two = GE::GS == 2 && t.p_count[gs][p] == 2;
       if constexpr (GE::KM == 3) {
         if (t.p_k3[gs][p]) {
           if constexpr (GE::GS == 2) {
-            if (two) g2_pass<2, true>(first, zb, kout, jac, src, q, g0);
-            else g2_pass<1, true>(first, zb, kout, jac, src, q, g0);
+            if (two) g2_pass<2, true>(first, zb, kout, jac, src, q, g0, wait);
+            else g2_pass<1, true>(first, zb, kout, jac, src, q, g0, wait);
           } else {
-            g2_pass<1, true>(first, zb, kout, jac, src, q, g0);
+            g2_pass<1, true>(first, zb, kout, jac, src, q, g0, wait);
           }
+          wait = false;
           continue;
         }
       }
       if constexpr (GE::GS == 2) {
-        if (two) g2_pass<2, false>(first, zb, kout, jac, src, q, g0);
-        else g2_pass<1, false>(first, zb, kout, jac, src, q, g0);
+        if (two) g2_pass<2, false>(first, zb, kout, jac, src, q, g0, wait);
+        else g2_pass<1, false>(first, zb, kout, jac, src, q, g0, wait);
       } else {
-        g2_pass<1, false>(first, zb, kout, jac, src, q, g0);
+        g2_pass<1, false>(first, zb, kout, jac, src, q, g0, wait);
       }
+      wait = false;
     }
+    if (wait) cluster_wait_acquire();   // (every group has a G2 pass; kept for a uniform barrier count)
     *gq = g0 + nchunk;
     __syncthreads();
   }
@@ -590,7 +622,14 @@ trajectory_kernel(const TrajState* __restrict__ states, const double* __restrict
   const uint32_t rank = cluster_rank();
   const int sidx = (int)cluster_id_x();
   const TrajState* st = states + sidx;
-  const int row0 = (int)rank * 16;
+  // cluster of G x CG CTAs: rows 16 (rank % G) .. + 15 of the channel group rank / G
+  const uint32_t nrank = cluster_size();
+  const int ngroups = (int)nrank / GE::G;
+  const int glevel = ngroups == 4 ? 2 : ngroups == 2 ? 1 : 0;
+  const int row0 = (int)(rank % GE::G) * 16;
+  const int grp = (int)rank / GE::G;
+  const int c0 = c_sys[SYS].grp_first[glevel][grp], c1 = c0 + c_sys[SYS].grp_count[glevel][grp];
+  const int e0 = c0 * 16 * DP, e1 = c1 * 16 * DP;   // the CTA's elements (own_offset numbering)
   Ctl& C = *sm.ctl;
   long long gq = 0;
   if (SYS == kSysQuartic && st->z2 < 0) {
@@ -645,8 +684,12 @@ trajectory_kernel(const TrajState* __restrict__ states, const double* __restrict
   using RhsT = std::conditional_t<ENG == 0, Rhs<DP, SYS>, RhsSplit<DP>>;
   RhsT rhs;
   if constexpr (ENG == 0) {
-    rhs = Rhs<DP, SYS>{st, sm, row0, tid, lane, warp, &gq, Rhs<DP, SYS>::total_chunks(), 0, 0,
+    rhs = Rhs<DP, SYS>{st, sm, row0, tid, lane, warp, &gq, 0, 0, 0,
                        ctl_in.ring >= 2 && ctl_in.ring <= GE::NST ? ctl_in.ring : GE::NST};
+    rhs.c0 = c0;
+    rhs.c1 = c1;
+    rhs.remote = c_sys[SYS].grp_remote[glevel];
+    rhs.nchunk = rhs.total_chunks();
   } else {
     rhs.st = st;
     rhs.ss = ssm;
@@ -676,7 +719,7 @@ trajectory_kernel(const TrajState* __restrict__ states, const double* __restrict
   }
   if (zskip) {
     // every work vector's own rows start at zero: the skipped parts are never written again
-    for (int e = tid; e < GE::OWN; e += GE::NT) {
+    for (int e = e0 + tid; e < e1; e += GE::NT) {
       const size_t off = own_offset<DP>(e, row0);
       const double2 z0 = make_double2(0.0, 0.0);
       st->y[off] = z0;
@@ -700,7 +743,7 @@ trajectory_kernel(const TrajState* __restrict__ states, const double* __restrict
   // initial y on own rows (zero, rho or the identity of the physical block), and f = RHS(-a, y)
   {
     const SysTab& tab = c_sys[SYS];
-    for (int e = tid; e < GE::OWN; e += GE::NT) {
+    for (int e = e0 + tid; e < e1; e += GE::NT) {
       const size_t off = own_offset<DP>(e, row0);
       const int c = e / (16 * DP), row = row0 + (e % (16 * DP)) / DP, col = e % DP;
       double2 v = make_double2(0.0, 0.0);
@@ -758,7 +801,7 @@ trajectory_kernel(const TrajState* __restrict__ states, const double* __restrict
         kp[j] = kb(j);
         ha[j] = j < terms ? h * w[j] : 0.0;
       }
-      for (int e = tid; e < GE::OWN; e += GE::NT) {
+      for (int e = e0 + tid; e < e1; e += GE::NT) {
         if (zskip && z2_zero_element<DP>(e, row0, half)) continue;
         const size_t off = own_offset<DP>(e, row0);
         double2 kv[12];
@@ -787,7 +830,7 @@ trajectory_kernel(const TrajState* __restrict__ states, const double* __restrict
     // ---------------------------------------------------------------- error norms
     {
       double s5 = 0.0, s3 = 0.0;
-      for (int e = tid; e < GE::OWN; e += GE::NT) {
+      for (int e = e0 + tid; e < e1; e += GE::NT) {
         const size_t off = own_offset<DP>(e, row0);
         if (packed) {
           const int c = e / (16 * DP), row = row0 + (e % (16 * DP)) / DP, col = e % DP;
@@ -823,7 +866,7 @@ trajectory_kernel(const TrajState* __restrict__ states, const double* __restrict
         double ks[13];
         for (int s = 1; s < 13; ++s) ks[s] = 0.0;
         int flag = 0;
-        for (uint32_t g = 0; g < (uint32_t)GE::G; ++g) {
+        for (uint32_t g = 0; g < nrank; ++g) {
           t5 += dsmem_load(&sm.xch->s5, g);
           t3 += dsmem_load(&sm.xch->s3, g);
           for (int s = 1; s < 13; ++s) ks[s] += dsmem_load(&sm.xch->kscp[s], g);
@@ -889,7 +932,7 @@ trajectory_kernel(const TrajState* __restrict__ states, const double* __restrict
             kp[j] = kb(j);
             ha[j] = j < s ? h * c_dop_a[16 * s + j] : 0.0;
           }
-          for (int e = tid; e < GE::OWN; e += GE::NT) {
+          for (int e = e0 + tid; e < e1; e += GE::NT) {
             const size_t off = own_offset<DP>(e, row0);
             double2 kv[15];
 #pragma unroll
@@ -908,7 +951,7 @@ trajectory_kernel(const TrajState* __restrict__ states, const double* __restrict
         // order-7 interpolation at the nodes in (t, t_new]
         const double t = C.t, tn = C.t_new;
         const long long first = C.first, last = C.last;
-        for (int e = tid; e < GE::OWN; e += GE::NT) {
+        for (int e = e0 + tid; e < e1; e += GE::NT) {
           const size_t off = own_offset<DP>(e, row0);
           const double2 yo = ybuf[off], yn = pbuf[off], f0 = kb(0)[off], f12 = kb(12)[off];
           double2 cf[7];
@@ -1011,29 +1054,82 @@ trajectory_kernel(const TrajState* __restrict__ states, const double* __restrict
   cluster_sync();
 }
 
-template <int DP, int SYS, int ENG = 0>
-static cudaError_t launch_dp(const TrajState* d_states, int nstates, const double* d_points, int npoints,
-                             const TrajControls& ctl, cudaStream_t stream) {
+int trajectory_group_levels(int system);   // channel-group levels of a system's table (below)
+
+// Launch configuration of `nstates` clusters of cluster_ctas CTAs each.
+template <int DP, int SYS, int ENG>
+static cudaLaunchConfig_t launch_config(int nstates, int cluster_ctas, cudaStream_t stream, cudaLaunchAttribute* attr) {
   using GE = Geo<DP, SYS>;
-  constexpr size_t smem = kernel_smem<DP, SYS, ENG>();
-  static_assert(smem <= 232448, "shared memory per CTA");
-  auto kern = trajectory_kernel<DP, SYS, ENG>;
-  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e != cudaSuccess) return e;
   cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3(nstates * GE::G, 1, 1);
+  cfg.gridDim = dim3(nstates * cluster_ctas, 1, 1);
   cfg.blockDim = dim3(GE::NT, 1, 1);
-  cfg.dynamicSmemBytes = smem;
+  cfg.dynamicSmemBytes = kernel_smem<DP, SYS, ENG>();
   cfg.stream = stream;
-  cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeClusterDimension;
-  attr[0].val.clusterDim.x = GE::G;
+  attr[0].val.clusterDim.x = cluster_ctas;
   attr[0].val.clusterDim.y = 1;
   attr[0].val.clusterDim.z = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
+  return cfg;
+}
+
+template <int DP, int SYS, int ENG>
+static cudaError_t prepare_kernel() {
+  constexpr size_t smem = kernel_smem<DP, SYS, ENG>();
+  static_assert(smem <= 232448, "shared memory per CTA");
+  auto kern = trajectory_kernel<DP, SYS, ENG>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+  return e;
+}
+
+// Channel groups for nstates states (see trajectory_groups).
+template <int DP, int SYS, int ENG>
+static int choose_groups(int nstates, int requested) {
+  using GE = Geo<DP, SYS>;
+  static int levels = -1;
+  if (levels < 0) levels = ENG == 0 ? trajectory_group_levels(SYS) : 1;
+  auto allowed = [&](int cg) {
+    const int level = cg == 4 ? 2 : cg == 2 ? 1 : 0;
+    return (cg == 1 || cg == 2 || cg == 4) && level < levels && GE::G * cg <= 16;
+  };
+  // clusters of G x cg CTAs the device holds at once (0 when it cannot place one)
+  auto resident = [&](int cg) {
+    if (prepare_kernel<DP, SYS, ENG>() != cudaSuccess) return 0;
+    cudaLaunchAttribute attr[1];
+    cudaLaunchConfig_t cfg = launch_config<DP, SYS, ENG>(nstates, GE::G * cg, nullptr, attr);
+    int clusters = 0;
+    if (cudaOccupancyMaxActiveClusters(&clusters, trajectory_kernel<DP, SYS, ENG>, &cfg) != cudaSuccess) {
+      cudaGetLastError();
+      return 0;
+    }
+    return clusters;
+  };
+  if (requested > 0) {   // the largest supported count up to the request
+    for (int cg = requested; cg > 1; cg /= 2)
+      if (allowed(cg) && resident(cg) >= 1) return cg;
+    return 1;
+  }
+  int dev = 0, sms = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) return 1;
+  for (int cg = 4; cg > 1; cg /= 2)
+    if (allowed(cg) && (long long)nstates * GE::G * cg <= sms && resident(cg) >= nstates) return cg;
+  return 1;
+}
+
+template <int DP, int SYS, int ENG = 0>
+static cudaError_t launch_dp(const TrajState* d_states, int nstates, const double* d_points, int npoints,
+                             const TrajControls& ctl, cudaStream_t stream) {
+  using GE = Geo<DP, SYS>;
+  cudaError_t e = prepare_kernel<DP, SYS, ENG>();
+  if (e != cudaSuccess) return e;
+  const int cg = choose_groups<DP, SYS, ENG>(nstates, ctl.groups);
+  if (cg == 0) return cudaErrorInvalidValue;
+  cudaLaunchAttribute attr[1];
+  cudaLaunchConfig_t cfg = launch_config<DP, SYS, ENG>(nstates, GE::G * cg, stream, attr);
   note_launch();
-  return cudaLaunchKernelEx(&cfg, kern, d_states, d_points, npoints, ctl);
+  return cudaLaunchKernelEx(&cfg, trajectory_kernel<DP, SYS, ENG>, d_states, d_points, npoints, ctl);
 }
 
 // Node weights of the pullback: wj[2i] = weight_i 2|t_i|, wj[2i+1] = weight_i source(t_i).
@@ -1168,6 +1264,60 @@ static void phi1_table(SysTab& t) {
   spec_table(t, &spec, 1);
 }
 
+// Channel groups of level k (2^k groups of contiguous channels: first[i], count[i]). The level is
+// kept only when every G2 pass of both tilings lies inside one group; grp_remote[k] records a left
+// insertion whose source channel lies in another group.
+static bool set_groups(SysTab& t, int k, const int* first, const int* count) {
+  const int ng = 1 << k;
+  int owner[kMaxChannels];
+  for (int c = 0; c < t.nch; ++c) owner[c] = -1;
+  for (int g = 0, c = 0; g < ng; ++g) {
+    if (first[g] != c || count[g] < 1) return false;
+    for (int i = 0; i < count[g]; ++i) owner[c++] = g;
+    if (g == ng - 1 && c != t.nch) return false;
+  }
+  for (int gs = 0; gs < 2; ++gs)
+    for (int p = 0; p < t.np[gs]; ++p)
+      if (owner[t.p_first[gs][p]] != owner[t.p_first[gs][p] + t.p_count[gs][p] - 1]) return false;
+  int remote = 0;
+  for (int c = 0; c < t.nch; ++c)
+    if (t.lsrc[c] >= 0 && owner[t.lsrc[c]] != owner[c]) remote = 1;
+  for (int g = 0; g < 4; ++g) {
+    t.grp_first[k][g] = g < ng ? first[g] : 0;
+    t.grp_count[k][g] = g < ng ? count[g] : 0;
+  }
+  t.grp_remote[k] = remote;
+  return true;
+}
+
+static void whole_state_groups(SysTab& t) {
+  const int first[1] = {0}, count[1] = {t.nch};
+  set_groups(t, 0, first, count);
+  t.grp_levels = 1;
+}
+
+// The quartic system by direction ({0,1,2} forward, {3..6} adjoint: no insertion crosses) and in
+// four groups along the G2 pairs ({0,1}, {2}, {3,4}, {5,6}: the insertions 2 <- 1 and 4 <- 5 cross).
+static void quartic_groups(SysTab& t) {
+  whole_state_groups(t);
+  const int f2[2] = {0, 3}, n2[2] = {3, 4};
+  const int f4[4] = {0, 2, 3, 5}, n4[4] = {2, 1, 2, 2};
+  if (set_groups(t, 1, f2, n2)) {
+    t.grp_levels = 2;
+    if (set_groups(t, 2, f4, n4)) t.grp_levels = 3;
+  }
+}
+
+int trajectory_group_levels(int system) {
+  SysTab t;
+  if (system == kSysQuartic) {
+    quartic_table(t);
+    quartic_groups(t);
+    return t.grp_levels;
+  }
+  return 1;
+}
+
 cudaError_t trajectory_set_tables() {
   cudaError_t e;
   if ((e = cudaMemcpyToSymbol(c_dop_a, rcmps_dop_a, sizeof(rcmps_dop_a))) != cudaSuccess) return e;
@@ -1180,6 +1330,9 @@ cudaError_t trajectory_set_tables() {
   quartic_table(tabs[0]);
   full_table(tabs[1]);
   phi1_table(tabs[2]);
+  quartic_groups(tabs[0]);
+  whole_state_groups(tabs[1]);
+  whole_state_groups(tabs[2]);
   if ((e = cudaMemcpyToSymbol(c_sys, tabs, sizeof(tabs))) != cudaSuccess) return e;
   return cudaMemcpyToSymbol(c_source, rcmps_source_table, sizeof(rcmps_source_table));
 }
@@ -1227,5 +1380,26 @@ cudaError_t trajectory_launch(int system, int dp, const TrajState* d_states, int
 }
 
 int trajectory_channels(int system) { return system == kSysFull ? 26 : system == kSysPhi1 ? 4 : 7; }
+
+template <int SYS>
+static int groups_sys(int dp, int nstates, int requested) {
+  switch (dp) {
+    case 16: return choose_groups<16, SYS, 0>(nstates, requested);
+    case 32: return choose_groups<32, SYS, 0>(nstates, requested);
+    case 48: return choose_groups<48, SYS, 0>(nstates, requested);
+    case 64: return choose_groups<64, SYS, 0>(nstates, requested);
+    case 96: return choose_groups<96, SYS, 0>(nstates, requested);
+    case 128: return choose_groups<128, SYS, 0>(nstates, requested);
+    default: return 0;
+  }
+}
+
+int trajectory_groups(int system, int dp, int nstates, int requested, int engine) {
+  if (engine == 1) return 1;
+  if (system == kSysQuartic) return groups_sys<kSysQuartic>(dp, nstates, requested);
+  if (system == kSysFull) return groups_sys<kSysFull>(dp, nstates, requested);
+  if (system == kSysPhi1) return groups_sys<kSysPhi1>(dp, nstates, requested);
+  return 0;
+}
 
 }  // namespace rcmps

@@ -45,6 +45,8 @@ struct TrajControls {
   unsigned long long max_ns;  // device-clock watchdog in ns (0: none)
   int ring = 0;               // stages of the FP64 engine's operand ring (2 .. 4; 0: the default 4)
   long long max_attempts = 0; // stop every trajectory after this many attempts (0: none; calibration)
+  int groups = 0;             // CTAs per row block of a state, each for a group of channels: 1, 2 or 4
+                              // (0: chosen by the launch, see trajectory_groups)
 };
 
 cudaError_t trajectory_set_tables();
@@ -58,6 +60,11 @@ size_t split_state_bytes();
 void split_state_pointers(unsigned char* block, TrajState& t);   // t.split_* inside `block`
 cudaError_t split_prep_launch(const TrajState* d_states, int nstates, cudaStream_t stream);
 int trajectory_channels(int system);
+// The channel groups a launch of nstates states takes (requested 0: the most, up to 4, that keeps
+// every state's cluster resident at once; 1, 2, 4: the largest supported count up to that one).
+// A state's cluster has dp/16 x groups CTAs (at most 16). Only the FP64 engine on the quartic
+// system groups; everything else takes 1.
+int trajectory_groups(int system, int dp, int nstates, int requested, int engine = 0);
 cudaError_t node_weights_launch(const double* d_points, const double* d_weights, int n, double* d_wj,
                                 cudaStream_t stream);
 

@@ -27,7 +27,7 @@ class Settings(C.Structure):
         ("initial_step", C.c_double), ("max_steps", C.c_longlong), ("max_device_seconds", C.c_double),
         ("kinetic_nodes", C.c_int), ("krylov_tolerance", C.c_double), ("krylov_initialdim", C.c_int),
         ("krylov_maxdim", C.c_int), ("metric_reg", C.c_double), ("boundary_tolerance", C.c_double),
-        ("symmetry", C.c_int), ("precision", C.c_int),
+        ("symmetry", C.c_int), ("precision", C.c_int), ("trajectory_groups", C.c_int),
     ]
 
 
@@ -104,6 +104,7 @@ SIGNATURES = {
     "rcmps_lbfgs_direction": (_I, [_P, _I, _I, _P, _P, _P, _P, _P, _D, _D, _D, _P, _P, _P, _P]),
     "rcmps_retract": (_I, [_P, _I, _P, _P, _P, _D, _P, _P, _P]),
     "rcmps_trajectory_tuning": (_I, [_P, _I, _I, C.POINTER(_I), C.POINTER(C.c_float)]),
+    "rcmps_trajectory_groups": (_I, [_P, _I, _I, C.POINTER(_I)]),
     "rcmps_fp64_peak_tflops": (_D, [_P]),
     "rcmps_launch_count": (C.c_longlong, []),
 }

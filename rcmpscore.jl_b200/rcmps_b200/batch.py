@@ -45,6 +45,8 @@ def config_states(name):
     d64_mixed: 16 random (seeds 0..15) + 16 Z2 (seeds 100..115) states at D = 64, g = 2;
     d32_batch: 64 random D = 32 states (seeds 0..63), g ~ U[0.5, 3] (seed 12345);
     d64_pair: the first random and the first Z2 state of d64_mixed (a small profiling case);
+    d64_single: the first random state of d64_mixed alone (the latency of one evaluation, the call
+    an L-BFGS trial makes);
     uneven200: 200 random states with D drawn from {16, 32, 48, 64, 96, 128}, g ~ U[0.5, 3] and
     atol, rtol each drawn from {1e-10, 1e-12} (use uneven_states for the tolerances)."""
     if name == "uneven200":
@@ -64,6 +66,9 @@ def config_states(name):
     if name == "d64_pair":
         (r0, k0), (r1, k1) = random_state(64, 0), z2_state(64, 100)
         return [r0, r1], [k0, k1], [2.0, 2.0], "2 states D=64: 1 random + 1 Z2 (scaling 0.2), g=2"
+    if name == "d64_single":
+        r0, k0 = random_state(64, 0)
+        return [r0], [k0], [2.0], "1 random state D=64 (seed 0, scaling 0.2), g=2"
     if name == "d32_batch":
         R, K = zip(*(random_state(32, s) for s in range(64)))
         g = np.random.default_rng(12345).uniform(0.5, 3.0, 64)
