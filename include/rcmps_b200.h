@@ -72,6 +72,13 @@ typedef struct rcmps_settings {
                                   state of the launch resident at once, so a lone state spreads over
                                   up to 16 SMs and a full batch keeps one CTA per row block. Results
                                   agree to rounding (the reductions' summation order changes). */
+  int boundary_preconditioner; /* boundary Poisson GMRES: 1 (default) right-preconditioned by the
+                                  no-jump inverse with the Sherman-Morrison correction, as the
+                                  reference solves it (numerics.py:37-71, 103-117), restart
+                                  min(40, d^2); the inverse is applied in the eigenbasis of Q
+                                  (found once per state and call on the device); a state whose
+                                  eigenbasis is ill-conditioned runs unpreconditioned. 0:
+                                  unpreconditioned GMRES(64). */
 } rcmps_settings;
 
 /* Per-state diagnostics. */
@@ -87,6 +94,9 @@ typedef struct rcmps_state_stats {
   int gmres_iterations;        /* boundary Poisson solve */
   double boundary_residual;
   int packed_z2;               /* 1: the quartic term took the packed Z2 route */
+  int gmres_matvecs;           /* boundary Poisson solve: operator applications as the reference's
+                                  GMRES counts them (Arnoldi steps plus one true residual per
+                                  restart cycle) */
 } rcmps_state_stats;
 
 void rcmps_default_settings(rcmps_settings* settings);

@@ -204,6 +204,8 @@ int check_settings(rcmps_context* ctx, const rcmps_settings* s) {
     return fail(ctx, RCMPS_INVALID_ARGUMENT, "precision must be 0 (FP64 tensor cores) or 1 (split BF16 slices)");
   if (s->trajectory_groups != 0 && s->trajectory_groups != 1 && s->trajectory_groups != 2 && s->trajectory_groups != 4)
     return fail(ctx, RCMPS_INVALID_ARGUMENT, "trajectory_groups must be 0 (automatic), 1, 2 or 4");
+  if (s->boundary_preconditioner != 0 && s->boundary_preconditioner != 1)
+    return fail(ctx, RCMPS_INVALID_ARGUMENT, "boundary_preconditioner must be 0 (none) or 1 (no-jump inverse)");
   return RCMPS_OK;
 }
 
@@ -292,6 +294,7 @@ void rcmps_default_settings(rcmps_settings* s) {
   s->symmetry = 0;
   s->precision = 0;
   s->trajectory_groups = 0;
+  s->boundary_preconditioner = 1;
 }
 
 int rcmps_context_create(int device, rcmps_context** out) {

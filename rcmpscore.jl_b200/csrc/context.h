@@ -26,6 +26,7 @@ struct rcmps_gmres_graph {
   const void* net2 = nullptr;           // rank and identity weight (all baked into the kernels)
   int net_rank = 0;
   float net_identity = 0.f;
+  const void* pre = nullptr;            // the no-jump preconditioner's sets, if any
   long long kernels = 0;                // kernels the graph replays
   cudaGraphExec_t exec = nullptr;
 };

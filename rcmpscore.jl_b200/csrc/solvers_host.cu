@@ -11,6 +11,7 @@
 #include "../../include/rcmps_b200.h"
 #include "context.h"
 #include "kinetic.h"
+#include "nojump.h"
 #include "prep.h"
 #include "quartic.h"
 #include "solvers.h"
@@ -40,15 +41,24 @@ struct GmresNet {
   float *X32 = nullptr, *H32 = nullptr, *Y32 = nullptr;   // n x NP, rank x NP, n x NP
 };
 
+// The no-jump preconditioner of a GMRES: every problem's set and the apply kernel's scratch.
+struct GmresNoJump {
+  const NoJumpSet* sets = nullptr;   // device [NP]
+  double2* W = nullptr;              // device [NP][dp^2]
+};
+
 // The m Arnoldi steps of one restart cycle: launches that depend on nothing the host learns
 // between them (converged problems are skipped inside the kernels). With a learned
-// preconditioner every step first forms Z_j = M V_j (pack, two GEMMs, unpack).
+// preconditioner every step first forms Z_j = M V_j (pack, two GEMMs, unpack); with the no-jump
+// preconditioner Z_j = P(V_j) (one clustered launch).
 static cudaError_t gmres_cycle_launches(ArnoldiProblem* d_probs, int NP, int dp, int m, LindbladTask* d_tasks,
-                                        cudaStream_t stream, const GmresNet* net = nullptr) {
+                                        cudaStream_t stream, const GmresNet* net = nullptr,
+                                        const GmresNoJump* nj = nullptr) {
   const int nvec = dp * dp;
   cudaError_t e = cudaSuccess;
   for (int j = 0; j < m && !e; ++j) {
-    if (net) {
+    if (nj) e = nojump_apply_launch(d_probs, NP, j, nj->sets, nj->W, dp, stream);
+    if (!e && net) {
       e = net_pack_launch(d_probs, NP, j, net->d, dp, net->X32, stream);
       if (!e) e = warmstart_gemm(false, false, net->rank, NP, net->n, 1.f, net->W1, net->n, net->X32, NP, 0.f, net->H32,
                                  NP, stream);
@@ -69,14 +79,16 @@ static cudaError_t gmres_cycle_launches(ArnoldiProblem* d_probs, int NP, int dp,
 // addresses and sizes and kept by the context (the cycle's several hundred launches then cost
 // one). If capture is not possible the cycle is launched directly.
 static cudaError_t gmres_cycle(rcmps_context* ctx, ArnoldiProblem* d_probs, int NP, int dp, int m,
-                               LindbladTask* d_tasks, cudaStream_t stream, const GmresNet* net = nullptr) {
+                               LindbladTask* d_tasks, cudaStream_t stream, const GmresNet* net = nullptr,
+                               const GmresNoJump* nj = nullptr) {
   const void* key = net ? static_cast<const void*>(net->W1) : nullptr;
+  const void* kpre = nj ? static_cast<const void*>(nj->sets) : nullptr;
   const void* key2 = net ? static_cast<const void*>(net->W2) : nullptr;
   const int krank = net ? net->rank : 0;
   const float kid = net ? net->identity : 0.f;
   for (auto& g : ctx->gmres_graphs)
     if (g.exec && g.probs == d_probs && g.tasks == d_tasks && g.np == NP && g.dp == dp && g.m == m &&
-        g.net == key && g.net2 == key2 && g.net_rank == krank && g.net_identity == kid) {
+        g.net == key && g.net2 == key2 && g.net_rank == krank && g.net_identity == kid && g.pre == kpre) {
       note_launches(g.kernels);
       return cudaGraphLaunch(g.exec, stream);
     }
@@ -84,9 +96,9 @@ static cudaError_t gmres_cycle(rcmps_context* ctx, ArnoldiProblem* d_probs, int 
   cudaGraph_t graph = nullptr;
   if (cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
     cudaGetLastError();
-    return gmres_cycle_launches(d_probs, NP, dp, m, d_tasks, stream, net);
+    return gmres_cycle_launches(d_probs, NP, dp, m, d_tasks, stream, net, nj);
   }
-  cudaError_t e = gmres_cycle_launches(d_probs, NP, dp, m, d_tasks, stream, net);
+  cudaError_t e = gmres_cycle_launches(d_probs, NP, dp, m, d_tasks, stream, net, nj);
   const cudaError_t ec = cudaStreamEndCapture(stream, &graph);
   cudaGraphExec_t exec = nullptr;
   if (!e && !ec && graph && cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess) {
@@ -103,6 +115,7 @@ static cudaError_t gmres_cycle(rcmps_context* ctx, ArnoldiProblem* d_probs, int 
     g.net2 = key2;
     g.net_rank = krank;
     g.net_identity = kid;
+    g.pre = kpre;
     g.kernels = thread_launch_count() - before;
     g.exec = exec;
     return cudaGraphLaunch(exec, stream);
@@ -110,14 +123,15 @@ static cudaError_t gmres_cycle(rcmps_context* ctx, ArnoldiProblem* d_probs, int 
   // capture or instantiation failed: nothing was launched by the capture; launch directly
   if (graph) cudaGraphDestroy(graph);
   cudaGetLastError();
-  return gmres_cycle_launches(d_probs, NP, dp, m, d_tasks, stream, net);
+  return gmres_cycle_launches(d_probs, NP, dp, m, d_tasks, stream, net, nj);
 }
 
 // Restarted GMRES(m) over NP problems that share dp; hp/d_probs hold set-up problems with x = 0.
 // Returns 0, or a CUDA error code. Convergence per problem is in hp[p].converged / residual.
 static cudaError_t gmres_run(rcmps_context* ctx, ArnoldiProblem* hp, ArnoldiProblem* d_probs, int NP, int dp,
                              int m, int maxrestart, LindbladTask* d_tasks, cudaStream_t stream,
-                             bool bnorm_from_b = false, const GmresNet* net = nullptr) {
+                             bool bnorm_from_b = false, const GmresNet* net = nullptr,
+                             const GmresNoJump* nj = nullptr) {
   const int nvec = dp * dp;
   cudaError_t e = cudaMemcpyAsync(d_probs, hp, NP * sizeof(ArnoldiProblem), cudaMemcpyHostToDevice, stream);
   // a warm start: the first residual is not |b|, so |b| is measured for the stopping target
@@ -132,7 +146,7 @@ static cudaError_t gmres_run(rcmps_context* ctx, ArnoldiProblem* hp, ArnoldiProb
     bool all = true;
     for (int p = 0; p < NP; ++p) all &= hp[p].converged != 0;
     if (all || it == maxrestart) break;
-    e = gmres_cycle(ctx, d_probs, NP, dp, m, d_tasks, stream, net);
+    e = gmres_cycle(ctx, d_probs, NP, dp, m, d_tasks, stream, net, nj);
     if (!e) e = gmres_update_launch(d_probs, NP, nvec, m, stream);
   }
   return e;
@@ -197,6 +211,7 @@ struct FinishPlan::Group {
   std::vector<int> idx;
   size_t o_dims = 0, o_off = 0, o_in = 0, o_ops = 0, o_b = 0, o_tmp = 0, o_status = 0;
   size_t o_z = 0, o_x32 = 0, o_h32 = 0, o_y32 = 0;   // learned preconditioner (flexible GMRES)
+  size_t o_nj = 0, o_njv = 0, o_njs = 0, o_njw = 0, h_njs = 0;   // no-jump preconditioner
   GmresBuffers gb{};
   size_t h_dims = 0, h_off = 0, h_probs = 0, h_status = 0;
 };
@@ -225,7 +240,10 @@ FinishPlan::~FinishPlan() = default;
 
 int finish_solve(rcmps_context* ctx, FinishJob& job, cudaStream_t stream, FinishPlan& plan) {
   const rcmps_settings& S = job.settings;
-  const int m = 64, maxrestart = job.max_restarts;
+  // the no-jump preconditioner takes the reference's restart length min(40, d^2)
+  // (numerics.py:55-71); the unpreconditioned and learned solves GMRES(64)
+  const bool nojump = !job.net && S.boundary_preconditioner == 1;
+  const int m = nojump ? 40 : 64, maxrestart = job.max_restarts;
   const double tol = S.boundary_tolerance;
   if (!(tol > 0.0) || !(S.metric_reg >= 0.0)) return fail(ctx, RCMPS_INVALID_ARGUMENT, "invalid boundary controls");
   plan.off.assign(job.n + 1, 0);
@@ -250,6 +268,14 @@ int finish_solve(rcmps_context* ctx, FinishJob& job, cudaStream_t stream, Finish
     g.o_tmp = L.add(n * 4 * mat * 16);
     g.o_status = L.add(n * 4);
     g.gb = gmres_layout(L, n, g.dp, m);
+    if (nojump) {   // flexible GMRES through the no-jump sets
+      g.o_z = L.add((size_t)n * m * mat * 16);
+      g.o_nj = L.add((size_t)n * kNoJumpMats * mat * 16);
+      g.o_njv = L.add((size_t)n * (g.dp + 2) * 16 + (size_t)n * 8 + (size_t)n * 4);
+      g.o_njs = L.add((size_t)n * sizeof(NoJumpSet));
+      g.o_njw = L.add((size_t)n * mat * 16);
+      g.h_njs = H.add((size_t)n * sizeof(NoJumpSet));
+    }
     if (job.net) {   // flexible GMRES: the preconditioned basis and the network's buffers
       g.o_z = L.add((size_t)n * m * mat * 16);
       g.o_x32 = L.add((size_t)job.net->n * n * 4);
@@ -295,6 +321,34 @@ int finish_solve(rcmps_context* ctx, FinishJob& job, cudaStream_t stream, Finish
     if (!e) e = launch_pad(job.rho, (long long*)P(g.o_off), (int*)P(g.o_dims), dP, dp, mat, n, stream);
     if (!e) e = launch_pad(job.environment, (long long*)P(g.o_off), (int*)P(g.o_dims), dE, dp, mat, n, stream);
     if (!e) e = launch_prepare(dR, dK, dP, (double*)P(g.o_ops), dp, mat, 8 * mat, n, stream);
+    GmresNoJump nj;
+    if (!e && nojump) {
+      NoJumpSet* hs = (NoJumpSet*)(h + g.h_njs);
+      double2* mats = (double2*)P(g.o_nj);
+      double2* vecs = (double2*)P(g.o_njv);
+      double* shifts = (double*)(vecs + (size_t)n * (dp + 2));
+      int* status = (int*)(shifts + n);
+      for (int i = 0; i < n; ++i) {
+        NoJumpSet& t = hs[i];
+        const double2* ops = (double2*)P(g.o_ops) + (size_t)i * 8 * mat;
+        double2* b = mats + (size_t)i * kNoJumpMats * mat;
+        t.Q = ops + kQ * mat;
+        t.R = ops + kR * mat;
+        t.rho = ops + kRho * mat;
+        double2** outs[kNoJumpMats] = {&t.V, &t.Vh, &t.Vinv, &t.Vinvh, &t.nS, &t.z, &t.H, &t.U, &t.W, &t.M, &t.T};
+        for (int q = 0; q < kNoJumpMats; ++q) *outs[q] = b + (size_t)q * mat;
+        t.lambda = vecs + (size_t)i * (dp + 2);
+        t.den = t.lambda + dp;
+        t.shift = shifts + i;
+        t.status = status + i;
+        t.d = hd[i];
+        t.dp = dp;
+      }
+      e = cudaMemcpyAsync(P(g.o_njs), hs, (size_t)n * sizeof(NoJumpSet), cudaMemcpyHostToDevice, stream);
+      if (!e) e = nojump_setup_launch((const NoJumpSet*)P(g.o_njs), n, dp, stream);
+      nj.sets = (const NoJumpSet*)P(g.o_njs);
+      nj.W = (double2*)P(g.o_njw);
+    }
     FinishArgs fa = finish_args(plan, g, base, S.metric_reg);
     if (!e) e = boundary_rhs_launch(fa, n, stream);
     if (e) return fail(ctx, RCMPS_CUDA_ERROR, std::string("boundary set-up: ") + cudaGetErrorString(e));
@@ -308,7 +362,7 @@ int finish_solve(rcmps_context* ctx, FinishJob& job, cudaStream_t stream, Finish
       A.A2h = ops + 2 * mat;
       A.trw = ops + 7 * mat;  // + tr(rho X) I
       A.b = fa.b + (size_t)i * mat;
-      if (job.net) A.Z = (double2*)P(g.o_z) + (size_t)i * m * mat;
+      if (job.net || nojump) A.Z = (double2*)P(g.o_z) + (size_t)i * m * mat;
     }
     GmresNet net;
     if (job.net) {
@@ -323,7 +377,7 @@ int finish_solve(rcmps_context* ctx, FinishJob& job, cudaStream_t stream, Finish
       net.Y32 = (float*)P(g.o_y32);
     }
     e = gmres_run(ctx, hp, (ArnoldiProblem*)P(g.gb.o_probs), n, dp, m, maxrestart, (LindbladTask*)P(g.gb.o_tasks),
-                  stream, job.x0 != nullptr, job.net ? &net : nullptr);
+                  stream, job.x0 != nullptr, job.net ? &net : nullptr, nojump ? &nj : nullptr);
     if (e) return fail(ctx, RCMPS_CUDA_ERROR, std::string("boundary GMRES: ") + cudaGetErrorString(e));
   }
   return RCMPS_OK;
@@ -353,6 +407,7 @@ int boundary_run(rcmps_context* ctx, FinishJob& job, double* H, cudaStream_t str
       rcmps_state_stats& st = job.stats[g.idx[i]];
       const ArnoldiProblem& A = hp[i];
       st.gmres_iterations = A.iters;
+      st.gmres_matvecs = A.iters + A.restarts;
       st.boundary_residual = A.residual;
       const bool ok = A.converged || A.residual <= 20.0 * tol * std::max(1.0, A.bnorm);
       if (!st.status && (A.nonfinite || !std::isfinite(A.residual) || !ok)) {
@@ -392,6 +447,7 @@ int finish_complete(rcmps_context* ctx, FinishJob& job, cudaStream_t stream, Fin
       rcmps_state_stats& st = job.stats[g.idx[i]];
       const ArnoldiProblem& A = hp[i];
       st.gmres_iterations = A.iters;
+      st.gmres_matvecs = A.iters + A.restarts;
       st.boundary_residual = A.residual;
       const bool ok = A.converged || A.residual <= 20.0 * tol * std::max(1.0, A.bnorm);
       if (st.status) continue;

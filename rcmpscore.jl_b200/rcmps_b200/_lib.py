@@ -28,6 +28,7 @@ class Settings(C.Structure):
         ("kinetic_nodes", C.c_int), ("krylov_tolerance", C.c_double), ("krylov_initialdim", C.c_int),
         ("krylov_maxdim", C.c_int), ("metric_reg", C.c_double), ("boundary_tolerance", C.c_double),
         ("symmetry", C.c_int), ("precision", C.c_int), ("trajectory_groups", C.c_int),
+        ("boundary_preconditioner", C.c_int),
     ]
 
 
@@ -50,6 +51,7 @@ class StateStats(C.Structure):
         ("quartic_value", C.c_double), ("kinetic_value", C.c_double),
         ("krylov_basis", C.c_int * 4), ("krylov_residual", C.c_double),
         ("gmres_iterations", C.c_int), ("boundary_residual", C.c_double), ("packed_z2", C.c_int),
+        ("gmres_matvecs", C.c_int),
     ]
 
     def as_dict(self):

@@ -435,21 +435,28 @@ def finish_gradient(q, r, rho, covector, environment, *, metric_reg=1e-3, tolera
     return _unpack(grad, [d])[0], {"matvecs": stats[0].gmres_iterations, "residual": stats[0].boundary_residual}
 
 
-def boundary_environment_batch(R, K, rho, environments, *, tolerance=1e-13, x0=None, network=None, device=None):
+def boundary_environment_batch(R, K, rho, environments, *, tolerance=1e-13, x0=None, network=None, device=None,
+                               preconditioner="nojump"):
     """The boundary Poisson solutions H_i, (-L*(H) + tr(rho H) I) = E - tr(rho E) I, of one
     environment E_i per entry (lists of D_i x D_i matrices; an entry may repeat a state with
     different environments), by restarted GMRES on the GPU (rcmps_boundary_environment_batch).
-    x0: optional initial guesses (a warm start); network: an optional learned right preconditioner
-    (rcmps_b200.warmstart.WarmStartNet, every state of its d), applied in flexible GMRES. Returns
-    (H list, stats list) with stats[i] = dict(matvecs, residual) as the reference's
-    boundary_environment (numerics.py:103-117)."""
+    preconditioner: "nojump" (the reference's right preconditioner, numerics.py:37-71, restart
+    min(40, d^2)) or None (GMRES(64) unpreconditioned); x0: optional initial guesses (a warm
+    start); network: a learned right preconditioner (rcmps_b200.warmstart.WarmStartNet, every
+    state of its d) applied in flexible GMRES instead. Returns (H list, stats list) with
+    stats[i] = dict(matvecs, iterations, residual): matvecs counted as the reference's GMRES
+    counts them (Arnoldi steps plus one residual per restart cycle), as in boundary_environment
+    (numerics.py:103-117)."""
+    if preconditioner not in ("nojump", None):
+        raise ValueError("preconditioner is 'nojump' or None")
     import torch
     n = len(R)
     if not (len(K) == len(rho) == len(environments) == n) or (x0 is not None and len(x0) != n):
         raise ValueError("R, K, rho, environments (and x0) must have the same length")
     dims = [_check_matrices(R[i], K[i], rho[i], environments[i]) for i in range(n)]
     ctx = context(device)
-    s = _lib.default_settings(boundary_tolerance=float(tolerance))
+    s = _lib.default_settings(boundary_tolerance=float(tolerance),
+                              boundary_preconditioner=1 if preconditioner == "nojump" else 0)
     dR, dK, dP, dE = _device(R), _device(K), _device(rho), _device(environments)
     dX = _device(x0) if x0 is not None else None
     H = torch.zeros(sum(d * d for d in dims), dtype=torch.complex128, device="cuda")
@@ -461,14 +468,14 @@ def boundary_environment_batch(R, K, rho, environments, *, tolerance=1e-13, x0=N
                                                   C.byref(s), H.data_ptr(), stats, _stream())
     if rc:
         raise SolverFailure(f"Poisson GMRES failed: {_lib.STATUS_NAMES.get(rc, rc)} ({ctx.error()})")
-    return _unpack(H, dims), [{"matvecs": stats[i].gmres_iterations, "residual": stats[i].boundary_residual}
-                              for i in range(n)]
+    return _unpack(H, dims), [{"matvecs": stats[i].gmres_matvecs, "iterations": stats[i].gmres_iterations,
+                               "residual": stats[i].boundary_residual} for i in range(n)]
 
 
-def boundary_environment(q, r, rho, environment, *, tolerance=1e-13, x0=None):
+def boundary_environment(q, r, rho, environment, *, tolerance=1e-13, x0=None, preconditioner="nojump"):
     """(H, stats) of one state: the reference's boundary_environment (numerics.py:103-117)."""
     H, st = boundary_environment_batch([r], [_k_from_q(q, r)], [rho], [environment], tolerance=tolerance,
-                                       x0=None if x0 is None else [x0])
+                                       x0=None if x0 is None else [x0], preconditioner=preconditioner)
     return H[0], st[0]
 
 

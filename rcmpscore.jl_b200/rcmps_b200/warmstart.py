@@ -43,7 +43,8 @@ def random_environments(rho, count, rng):
 
 
 def solve_triples(R, K, rho, environments, *, tolerance=1e-13):
-    """(b, H) pairs of one state by the plain solver (GMRES from zero): the training data."""
+    """(b, H) pairs of one state by the library's solver (GMRES from zero, no-jump preconditioned):
+    the training data."""
     H, stats = boundary_environment_batch([R] * len(environments), [K] * len(environments),
                                           [rho] * len(environments), environments, tolerance=tolerance)
     eye = np.eye(len(rho))
@@ -163,9 +164,10 @@ def gmres_gain(net, R, K, rho, environments, *, tolerance=1e-13):
     dict(cold, warm, preconditioned, *_residual, target, *_difference)."""
     rhs = [e - np.trace(rho @ e) * np.eye(len(rho)) for e in environments]
     n = len(environments)
-    H0, st0 = boundary_environment_batch([R] * n, [K] * n, [rho] * n, environments, tolerance=tolerance)
+    H0, st0 = boundary_environment_batch([R] * n, [K] * n, [rho] * n, environments, tolerance=tolerance,
+                                         preconditioner=None)
     H1, st1 = boundary_environment_batch([R] * n, [K] * n, [rho] * n, environments, tolerance=tolerance,
-                                         x0=net.predict(rhs))
+                                         x0=net.predict(rhs), preconditioner=None)
     H2, st2 = boundary_environment_batch([R] * n, [K] * n, [rho] * n, environments, tolerance=tolerance,
                                          network=net)
     diff = lambda A, B: max(np.abs(a - b).max() / max(1.0, np.abs(a).max()) for a, b in zip(A, B))
@@ -231,19 +233,22 @@ def path_experiment(d, *, train_states=8, rhs_per_state=512, test_rhs=64, rank=N
         torch.cuda.synchronize()
         return Hs, st, ev0.elapsed_time(ev1)
 
-    timed()                                        # warm-up (graph capture of the cycles)
-    H0, st0, ms0 = timed()
+    timed(preconditioner=None)                     # warm-up (graph capture of the cycles)
+    H0, st0, ms0 = timed(preconditioner=None)
     timed(network=net)
     H2, st2, ms2 = timed(network=net)
     rhs = [e - np.trace(rho @ e) * np.eye(d) for e in envs]
-    H1, st1, ms1 = timed(x0=net.predict(rhs))
+    H1, st1, ms1 = timed(x0=net.predict(rhs), preconditioner=None)
+    timed()
+    H3, st3, ms3 = timed()                         # the no-jump preconditioner (the default solve)
     diff = lambda A, Bm: max(np.abs(a - b).max() / max(1.0, np.abs(a).max()) for a, b in zip(A, Bm))
     return {"d": d, "train_triples": len(B), "rank": net.rank, "epochs": epochs, "loss_first": losses[0],
             "loss_last": losses[-1], "data_seconds": t_data, "train_seconds": t_train,
             "matvecs_cold": float(np.mean([s["matvecs"] for s in st0])),
             "matvecs_warm": float(np.mean([s["matvecs"] for s in st1])),
             "matvecs_preconditioned": float(np.mean([s["matvecs"] for s in st2])),
-            "ms_cold": ms0, "ms_warm": ms1, "ms_preconditioned": ms2,
+            "matvecs_nojump": float(np.mean([s["matvecs"] for s in st3])),
+            "ms_cold": ms0, "ms_warm": ms1, "ms_preconditioned": ms2, "ms_nojump": ms3,
             "max_residual_over_target": max(s["residual"] / (tolerance * max(1.0, float(np.linalg.norm(b))))
-                                            for st in (st0, st1, st2) for s, b in zip(st, rhs)),
-            "solution_difference": max(diff(H0, H1), diff(H0, H2))}
+                                            for st in (st0, st1, st2, st3) for s, b in zip(st, rhs)),
+            "solution_difference": max(diff(H0, H1), diff(H0, H2), diff(H0, H3))}
