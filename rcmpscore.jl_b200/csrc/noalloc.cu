@@ -204,6 +204,7 @@ extern "C" int rcmps_finish_gradient_noalloc(rcmps_context* ctx, int d, const do
   if (!e) e = cudaStreamSynchronize(s);
   if (e) return fail(ctx, RCMPS_CUDA_ERROR, std::string("no-alloc finish: ") + cudaGetErrorString(e));
   stats->gmres_iterations = A.iters;
+  stats->gmres_matvecs = A.iters + A.restarts;
   stats->boundary_residual = A.residual;
   const bool ok = A.converged || A.residual <= 20.0 * tol * (A.bnorm > 1.0 ? A.bnorm : 1.0);
   if (A.nonfinite || !std::isfinite(A.residual) || !ok) {
