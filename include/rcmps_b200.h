@@ -253,7 +253,9 @@ int rcmps_boundary_environment_batch(rcmps_context* context, int n_states, const
  * calls that overlap on the GPU (different streams or host threads) race on it, and the
  * caller must order them. Each call clears what must start at zero (the Poisson solution and
  * the status words). Arguments are those of rcmps_finish_gradient_batch with n_states = 1:
- * R, K, rho, covector, environment and gradient are d x d device matrices. */
+ * R, K, rho, covector, environment and gradient are d x d device matrices. Its boundary solve
+ * is unpreconditioned GMRES(64) whatever settings->boundary_preconditioner says (the no-jump
+ * sets would not fit the fixed array); the result meets the same residual bound. */
 int rcmps_finish_gradient_noalloc(rcmps_context* context, int d, const double* R, const double* K,
                                   const double* rho, const double* covector, const double* environment,
                                   const rcmps_settings* settings, double* gradient, rcmps_state_stats* stats,
