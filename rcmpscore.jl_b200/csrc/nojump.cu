@@ -129,21 +129,40 @@ __device__ double spectral_norm(const double2* A, int n, int dp, double2* tmp, d
   return sqrt(nrm);
 }
 
+// Shared-memory plan of the set-up: H (and U when it fits) with leading dimension dp + 1, so that
+// both a row and a column of threads read conflict-free.
+__host__ __device__ constexpr int setup_ld(int dp) { return dp + 1; }
+__host__ __device__ constexpr bool setup_h_shared(int dp) { return dp <= 96; }
+__host__ __device__ constexpr bool setup_u_shared(int dp) { return dp <= 64; }
+__host__ __device__ constexpr size_t setup_smem(int dp) {
+  return ((setup_h_shared(dp) ? 1 : 0) + (setup_u_shared(dp) ? 1 : 0)) * (size_t)dp * setup_ld(dp) * 16;
+}
+
+struct Rotation {   // G = [c s; -conj(s) c] on rows/columns k, k+1
+  double2 s;
+  double c;
+  int k;
+};
+
 __global__ void __launch_bounds__(kSetupThreads) nojump_setup_kernel(const NoJumpSet* __restrict__ sets) {
   const NoJumpSet S = sets[blockIdx.x];
   const int n = S.d, dp = S.dp, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  double2* H = S.H;
-  double2* U = S.U;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int lds = setup_ld(dp);
+  double2* H = setup_h_shared(dp) ? reinterpret_cast<double2*>(smem_raw) : S.H;
+  const int ldh = setup_h_shared(dp) ? lds : dp;
+  double2* U = setup_u_shared(dp) ? reinterpret_cast<double2*>(smem_raw) + (size_t)dp * lds : S.U;
+  const int ldu = setup_u_shared(dp) ? lds : dp;
   __shared__ double red[kSetupThreads / 32];
   __shared__ double2 v[kMaxDp];
   __shared__ double2 vtmp[2 * kMaxDp];
-  __shared__ int fail_sh;
+  __shared__ Rotation rot[kMaxDp];
+  __shared__ int sh_l, sh_ihi, sh_nrot, sh_state;   // state: 0 sweep to apply, 1 done, 2 failed
   const double ulp = DBL_EPSILON, smlnum = DBL_MIN * ((double)n / ulp);
-  if (tid == 0) fail_sh = 0;
-  for (int e = tid; e < dp * dp; e += blockDim.x) {
-    const int i = e / dp, j = e % dp;
-    H[e] = (i < n && j < n) ? S.Q[e] : make_double2(0.0, 0.0);
-    U[e] = make_double2(i == j ? 1.0 : 0.0, 0.0);
+  for (int e = tid; e < n * n; e += blockDim.x) {
+    const int i = e / n, j = e % n;
+    H[i * ldh + j] = S.Q[i * dp + j];
+    U[i * ldu + j] = make_double2(i == j ? 1.0 : 0.0, 0.0);
   }
   __syncthreads();
 
@@ -151,29 +170,29 @@ __global__ void __launch_bounds__(kSetupThreads) nojump_setup_kernel(const NoJum
   for (int k = 0; k + 2 < n; ++k) {
     const int m = n - k - 1;
     double part = 0.0;
-    for (int i = 1 + tid; i < m; i += blockDim.x) part += zabs2(H[(k + 1 + i) * dp + k]);
+    for (int i = 1 + tid; i < m; i += blockDim.x) part += zabs2(H[(k + 1 + i) * ldh + k]);
     const double tail = block_sum(part, red);
     if (tail == 0.0) continue;   // column k is already reduced (the sum is uniform)
-    const double2 x0 = H[(k + 1) * dp + k];
+    const double2 x0 = H[(k + 1) * ldh + k];
     const double ax0 = hypot(x0.x, x0.y);
     const double alpha = sqrt(ax0 * ax0 + tail);
     const double2 ph = ax0 > 0.0 ? zscale(1.0 / ax0, x0) : make_double2(1.0, 0.0);
     const double2 beta = zscale(-alpha, ph);
     const double tau = 2.0 / ((ax0 + alpha) * (ax0 + alpha) + tail);
-    for (int i = tid; i < m; i += blockDim.x) v[i] = i == 0 ? zscale(ax0 + alpha, ph) : H[(k + 1 + i) * dp + k];
+    for (int i = tid; i < m; i += blockDim.x) v[i] = i == 0 ? zscale(ax0 + alpha, ph) : H[(k + 1 + i) * ldh + k];
     __syncthreads();
     // left: rows k+1.., columns k+1.. (column k becomes beta e1)
     for (int j = k + 1 + tid; j < n; j += blockDim.x) {
       double2 w = make_double2(0.0, 0.0);
-      for (int i = 0; i < m; ++i) w = zadd(w, zmul(zconj(v[i]), H[(k + 1 + i) * dp + j]));
+      for (int i = 0; i < m; ++i) w = zadd(w, zmul(zconj(v[i]), H[(k + 1 + i) * ldh + j]));
       w = zscale(tau, w);
-      for (int i = 0; i < m; ++i) H[(k + 1 + i) * dp + j] = zsub(H[(k + 1 + i) * dp + j], zmul(v[i], w));
+      for (int i = 0; i < m; ++i) H[(k + 1 + i) * ldh + j] = zsub(H[(k + 1 + i) * ldh + j], zmul(v[i], w));
     }
-    for (int i = tid; i < m; i += blockDim.x) H[(k + 1 + i) * dp + k] = i == 0 ? beta : make_double2(0.0, 0.0);
+    for (int i = tid; i < m; i += blockDim.x) H[(k + 1 + i) * ldh + k] = i == 0 ? beta : make_double2(0.0, 0.0);
     __syncthreads();
     // right: every row, columns k+1.. of H, and U <- U P
     for (int r = tid; r < 2 * n; r += blockDim.x) {
-      double2* row = (r < n ? H : U) + (size_t)(r % n) * dp + k + 1;
+      double2* row = r < n ? H + (size_t)r * ldh + k + 1 : U + (size_t)(r - n) * ldu + k + 1;
       double2 w = make_double2(0.0, 0.0);
       for (int q = 0; q < m; ++q) w = zadd(w, zmul(row[q], v[q]));
       w = zscale(tau, w);
@@ -182,23 +201,34 @@ __global__ void __launch_bounds__(kSetupThreads) nojump_setup_kernel(const NoJum
     __syncthreads();
   }
 
-  // 2. complex QR iteration to the Schur form (warp 0)
-  if (warp == 0) {
-    int ihi = n - 1, fail = 0;
-    while (ihi > 0 && !fail) {
-      int its = 0, l = 0;
+  // 2. complex QR iteration to the Schur form. Warp 0 sweeps the active block l..ihi and records
+  // its rotations; then every thread applies them to one line outside the block: a row of U, a
+  // row of H above the block or a column of H right of it.
+  if (tid == 0) {
+    sh_ihi = n - 1;
+    sh_state = n > 1 ? 0 : 1;
+  }
+  __syncthreads();
+  int its = 0;   // warp 0: iterations on the current eigenvalue
+  for (;;) {
+    // every thread reads the state before warp 0 may change it
+    const int state_now = sh_state;
+    __syncthreads();
+    if (state_now != 0) break;
+    if (warp == 0) {
+      int ihi = sh_ihi, l = 0, state = 0, nrot = 0;
       for (;;) {
         for (l = ihi; l > 0; --l) {
-          const double h = cabs1(H[l * dp + l - 1]);
+          const double h = cabs1(H[l * ldh + l - 1]);
           if (h <= smlnum) break;
-          const double2 hll = H[l * dp + l], hpp = H[(l - 1) * dp + l - 1];
+          const double2 hll = H[l * ldh + l], hpp = H[(l - 1) * ldh + l - 1];
           double tst = cabs1(hpp) + cabs1(hll);
           if (tst == 0.0) {
-            if (l - 2 >= 0) tst += cabs1(H[(l - 1) * dp + l - 2]);
-            if (l + 1 <= ihi) tst += cabs1(H[(l + 1) * dp + l]);
+            if (l - 2 >= 0) tst += cabs1(H[(l - 1) * ldh + l - 2]);
+            if (l + 1 <= ihi) tst += cabs1(H[(l + 1) * ldh + l]);
           }
           if (h <= ulp * tst) {
-            const double hup = cabs1(H[(l - 1) * dp + l]);
+            const double hup = cabs1(H[(l - 1) * ldh + l]);
             const double ab = fmax(h, hup), ba = fmin(h, hup);
             const double dd = cabs1(zsub(hpp, hll));
             const double aa = fmax(cabs1(hll), dd), bb = fmin(cabs1(hll), dd);
@@ -207,28 +237,34 @@ __global__ void __launch_bounds__(kSetupThreads) nojump_setup_kernel(const NoJum
           }
         }
         if (l > 0) {
-          if (lane == 0) H[l * dp + l - 1] = make_double2(0.0, 0.0);
+          if (lane == 0) H[l * ldh + l - 1] = make_double2(0.0, 0.0);
           __syncwarp();
         }
-        if (l >= ihi) break;
-        if (its >= kQrIterations) {
-          fail = 1;
+        if (l < ihi) break;
+        // the trailing 1 x 1 block converged
+        ihi = l - 1;
+        its = 0;
+        if (ihi <= 0) {
+          state = 1;
           break;
         }
+      }
+      if (state == 0 && its >= kQrIterations) state = 2;
+      if (state == 0) {
         // shift
         double2 t;
         if (its == 10) {
-          t = H[l * dp + l];
-          t.x += 0.75 * cabs1(H[(l + 1) * dp + l]);
+          t = H[l * ldh + l];
+          t.x += 0.75 * cabs1(H[(l + 1) * ldh + l]);
         } else if (its == 20) {
-          t = H[ihi * dp + ihi];
-          t.x += 0.75 * cabs1(H[ihi * dp + ihi - 1]);
+          t = H[ihi * ldh + ihi];
+          t.x += 0.75 * cabs1(H[ihi * ldh + ihi - 1]);
         } else {
-          t = H[ihi * dp + ihi];
-          const double2 u = zmul(zsqrt(H[(ihi - 1) * dp + ihi]), zsqrt(H[ihi * dp + ihi - 1]));
+          t = H[ihi * ldh + ihi];
+          const double2 u = zmul(zsqrt(H[(ihi - 1) * ldh + ihi]), zsqrt(H[ihi * ldh + ihi - 1]));
           const double su = cabs1(u);
           if (su != 0.0) {
-            const double2 x = zscale(0.5, zsub(H[(ihi - 1) * dp + ihi - 1], t));
+            const double2 x = zscale(0.5, zsub(H[(ihi - 1) * ldh + ihi - 1], t));
             const double sx = cabs1(x);
             const double sm = fmax(su, sx);
             const double2 xs = zscale(1.0 / sm, x), us = zscale(1.0 / sm, u);
@@ -237,10 +273,10 @@ __global__ void __launch_bounds__(kSetupThreads) nojump_setup_kernel(const NoJum
             t = zsub(t, zmul(u, zdiv(u, zadd(x, y))));
           }
         }
-        // one implicit single-shift sweep over the active block l..ihi
+        // one implicit single-shift sweep inside the active block
         for (int k = l; k < ihi; ++k) {
-          const double2 a = k == l ? zsub(H[l * dp + l], t) : H[k * dp + k - 1];
-          const double2 b = k == l ? H[(l + 1) * dp + l] : H[(k + 1) * dp + k - 1];
+          const double2 a = k == l ? zsub(H[l * ldh + l], t) : H[k * ldh + k - 1];
+          const double2 b = k == l ? H[(l + 1) * ldh + l] : H[(k + 1) * ldh + k - 1];
           const double na = hypot(a.x, a.y), nb = hypot(b.x, b.y);
           double c;
           double2 s;
@@ -255,36 +291,76 @@ __global__ void __launch_bounds__(kSetupThreads) nojump_setup_kernel(const NoJum
             c = na / nrm;
             s = zscale(1.0 / (na * nrm), zmul(a, zconj(b)));
           }
+          if (lane == 0) rot[nrot] = Rotation{s, c, k};
+          ++nrot;
           __syncwarp();
-          // rows k, k+1 <- G rows (G = [c s; -conj(s) c])
-          for (int j = (k == l ? l : k - 1) + lane; j < n; j += 32) {
-            const double2 x = H[k * dp + j], y = H[(k + 1) * dp + j];
-            H[k * dp + j] = zadd(zscale(c, x), zmul(s, y));
-            H[(k + 1) * dp + j] = zsub(zscale(c, y), zmul(zconj(s), x));
+          // rows k, k+1 <- G rows, columns of the block
+          for (int j = (k == l ? l : k - 1) + lane; j <= ihi; j += 32) {
+            const double2 x = H[k * ldh + j], y = H[(k + 1) * ldh + j];
+            H[k * ldh + j] = zadd(zscale(c, x), zmul(s, y));
+            H[(k + 1) * ldh + j] = zsub(zscale(c, y), zmul(zconj(s), x));
           }
           __syncwarp();
-          if (k > l && lane == 0) H[(k + 1) * dp + k - 1] = make_double2(0.0, 0.0);
-          // columns k, k+1 <- columns G^dag, in H (rows 0..min(k+2, ihi)) and U (every row)
-          const int r1 = min(k + 2, ihi);
-          for (int r = lane; r <= r1 + n; r += 32) {
-            double2* row = r <= r1 ? H + (size_t)r * dp : U + (size_t)(r - r1 - 1) * dp;
-            const double2 x = row[k], y = row[k + 1];
-            row[k] = zadd(zscale(c, x), zmul(y, zconj(s)));
-            row[k + 1] = zsub(zscale(c, y), zmul(x, s));
+          if (k > l && lane == 0) H[(k + 1) * ldh + k - 1] = make_double2(0.0, 0.0);
+          // columns k, k+1 <- columns G^dag, rows of the block
+          for (int r = l + lane; r <= min(k + 2, ihi); r += 32) {
+            const double2 x = H[r * ldh + k], y = H[r * ldh + k + 1];
+            H[r * ldh + k] = zadd(zscale(c, x), zmul(y, zconj(s)));
+            H[r * ldh + k + 1] = zsub(zscale(c, y), zmul(x, s));
           }
           __syncwarp();
         }
         ++its;
       }
-      if (!fail) ihi = l - 1;
+      if (lane == 0) {
+        sh_l = l;
+        sh_ihi = ihi;
+        sh_nrot = nrot;
+        sh_state = state;
+      }
     }
-    if (lane == 0 && fail) fail_sh = 1;
+    __syncthreads();
+    // the sweep's rotations outside the block (state 0: a sweep ran on l..ihi)
+    if (sh_state == 0) {
+      const int l = sh_l, ihi = sh_ihi, nrot = sh_nrot;
+      const int ncol = n - 1 - ihi;   // columns right of the block
+      for (int line = tid; line < n + l + ncol; line += blockDim.x) {
+        if (line < n + l) {   // a row of U, or a row of H above the block: column rotations
+          double2* row = line < n ? U + (size_t)line * ldu : H + (size_t)(line - n) * ldh;
+          for (int q = 0; q < nrot; ++q) {
+            const Rotation g = rot[q];
+            const double2 x = row[g.k], y = row[g.k + 1];
+            row[g.k] = zadd(zscale(g.c, x), zmul(y, zconj(g.s)));
+            row[g.k + 1] = zsub(zscale(g.c, y), zmul(x, g.s));
+          }
+        } else {              // a column of H right of the block: row rotations
+          const int j = ihi + 1 + (line - n - l);
+          for (int q = 0; q < nrot; ++q) {
+            const Rotation g = rot[q];
+            const double2 x = H[g.k * ldh + j], y = H[(g.k + 1) * ldh + j];
+            H[g.k * ldh + j] = zadd(zscale(g.c, x), zmul(g.s, y));
+            H[(g.k + 1) * ldh + j] = zsub(zscale(g.c, y), zmul(zconj(g.s), x));
+          }
+        }
+      }
+    }
+    __syncthreads();
   }
-  __syncthreads();
-  if (fail_sh) {
+  if (sh_state == 2) {
     if (tid == 0) *S.status = 1;
     return;
   }
+  // T and U to their global homes (leading dimension dp) for the rest of the set-up
+  if (H != S.H || U != S.U) {
+    for (int e = tid; e < n * n; e += blockDim.x) {
+      const int i = e / n, j = e % n;
+      if (H != S.H) S.H[i * dp + j] = H[i * ldh + j];
+      if (U != S.U) S.U[i * dp + j] = U[i * ldu + j];
+    }
+    __syncthreads();
+  }
+  H = S.H;
+  U = S.U;
 
   // 3. eigenvectors W of T = H (upper triangular) and W^-1
   double2* W = S.W;
@@ -580,8 +656,11 @@ cudaError_t launch_apply(const ArnoldiProblem* probs, int NP, int j, const NoJum
 cudaError_t nojump_setup_launch(const NoJumpSet* d_sets, int n, int dp, cudaStream_t stream) {
   if (n == 0) return cudaSuccess;
   if (dp > kMaxDp) return cudaErrorInvalidValue;
+  const size_t smem = setup_smem(dp);
+  cudaError_t e = cudaFuncSetAttribute(nojump_setup_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
   note_launch();
-  nojump_setup_kernel<<<n, kSetupThreads, 0, stream>>>(d_sets);
+  nojump_setup_kernel<<<n, kSetupThreads, smem, stream>>>(d_sets);
   return cudaGetLastError();
 }
 
