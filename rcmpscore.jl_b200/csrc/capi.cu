@@ -744,8 +744,6 @@ int rcmps_fg_phi4_batch_controls(rcmps_context* ctx, int n, const int* dims, con
     qrc = quartic_run(ctx, qj, ctx->slot[0].stream);
     if (!env_signalled) env_promise.set_value(false);
   });
-  kworker.join();
-  const bool env_ok = env_future.get();
   cudaStream_t s2 = ctx->slot[2].stream;
   const int nsum = (int)std::min<long long>(4096, (total + 255) / 256 + 1);
   std::vector<rcmps_state_stats> fst(n);
@@ -763,8 +761,14 @@ int rcmps_fg_phi4_batch_controls(rcmps_context* ctx, int n, const int* dims, con
   fj.stats = fst.data();
   fj.slot = 2;
   FinishPlan plan;
-  int frc = RCMPS_OK;
-  const bool solve = env_ok && krc == RCMPS_OK;
+  // the solve's operators and the no-jump preconditioner's eigenbasis need only R, K and rho:
+  // they are prepared on the solve stream while the two terms run
+  cudaEventRecord(ctx->slot[2].ev[4], s2);
+  int frc = finish_prepare(ctx, fj, s2, plan);
+  cudaEventRecord(ctx->slot[2].ev[5], s2);
+  kworker.join();
+  const bool env_ok = env_future.get();
+  const bool solve = env_ok && krc == RCMPS_OK && frc == RCMPS_OK;
   if (solve) {
     cudaStreamWaitEvent(s2, qj.env_ready, 0);
     cudaEventRecord(ctx->slot[2].ev[1], s2);
@@ -784,6 +788,7 @@ int rcmps_fg_phi4_batch_controls(rcmps_context* ctx, int n, const int* dims, con
     }
   }
   if (qrc || krc) return qrc ? qrc : krc;
+  if (frc) return frc;
   if (!solve) return fail(ctx, RCMPS_CUDA_ERROR, "fg_phi4: the quartic environment was not produced");
   if (frc == RCMPS_OK) {
     note_launch();
@@ -796,8 +801,10 @@ int rcmps_fg_phi4_batch_controls(rcmps_context* ctx, int n, const int* dims, con
   cudaEventSynchronize(ctx->slot[2].ev[2]);
   cudaEventElapsedTime(&ctx->last_ms[3], ctx->slot[2].ev[1], ctx->slot[2].ev[2]);
   cudaEventElapsedTime(&ctx->last_ms[4], ctx->slot[2].ev[0], ctx->slot[2].ev[2]);
+  cudaEventElapsedTime(&ctx->last_ms[5], ctx->slot[2].ev[4], ctx->slot[2].ev[5]);
   for (int i = 0; i < n; ++i) {
     stats[i].gmres_iterations = fst[i].gmres_iterations;
+    stats[i].gmres_matvecs = fst[i].gmres_matvecs;
     stats[i].boundary_residual = fst[i].boundary_residual;
     if (!stats[i].status && fst[i].status) {
       stats[i].status = fst[i].status;

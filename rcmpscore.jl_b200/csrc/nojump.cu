@@ -147,7 +147,7 @@ struct Rotation {   // G = [c s; -conj(s) c] on rows/columns k, k+1
 __global__ void __launch_bounds__(kSetupThreads) nojump_setup_kernel(const NoJumpSet* __restrict__ sets) {
   const NoJumpSet S = sets[blockIdx.x];
   const int n = S.d, dp = S.dp, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   const int lds = setup_ld(dp);
   double2* H = setup_h_shared(dp) ? reinterpret_cast<double2*>(smem_raw) : S.H;
   const int ldh = setup_h_shared(dp) ? lds : dp;

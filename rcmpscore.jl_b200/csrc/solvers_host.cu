@@ -212,6 +212,8 @@ struct FinishPlan::Group {
   size_t o_dims = 0, o_off = 0, o_in = 0, o_ops = 0, o_b = 0, o_tmp = 0, o_status = 0;
   size_t o_z = 0, o_x32 = 0, o_h32 = 0, o_y32 = 0;   // learned preconditioner (flexible GMRES)
   size_t o_nj = 0, o_njv = 0, o_njs = 0, o_njw = 0, h_njs = 0;   // no-jump preconditioner
+  const NoJumpSet* nj_sets = nullptr;
+  double2* nj_W = nullptr;
   GmresBuffers gb{};
   size_t h_dims = 0, h_off = 0, h_probs = 0, h_status = 0;
 };
@@ -238,12 +240,14 @@ static FinishArgs finish_args(const FinishPlan& plan, const FinishPlan::Group& g
 FinishPlan::FinishPlan() = default;
 FinishPlan::~FinishPlan() = default;
 
-int finish_solve(rcmps_context* ctx, FinishJob& job, cudaStream_t stream, FinishPlan& plan) {
+int finish_prepare(rcmps_context* ctx, FinishJob& job, cudaStream_t stream, FinishPlan& plan) {
   const rcmps_settings& S = job.settings;
   // the no-jump preconditioner takes the reference's restart length min(40, d^2)
   // (numerics.py:55-71); the unpreconditioned and learned solves GMRES(64)
   const bool nojump = !job.net && S.boundary_preconditioner == 1;
-  const int m = nojump ? 40 : 64, maxrestart = job.max_restarts;
+  const int m = nojump ? 40 : 64;
+  plan.nojump = nojump;
+  plan.m = m;
   const double tol = S.boundary_tolerance;
   if (!(tol > 0.0) || !(S.metric_reg >= 0.0)) return fail(ctx, RCMPS_INVALID_ARGUMENT, "invalid boundary controls");
   plan.off.assign(job.n + 1, 0);
@@ -300,7 +304,6 @@ int finish_solve(rcmps_context* ctx, FinishJob& job, cudaStream_t stream, Finish
     const size_t mat = (size_t)dp * dp;
     int* hd = (int*)(h + g.h_dims);
     long long* ho = (long long*)(h + g.h_off);
-    ArnoldiProblem* hp = (ArnoldiProblem*)(h + g.h_probs);
     for (int i = 0; i < n; ++i) {
       hd[i] = job.dims[g.idx[i]];
       ho[i] = plan.off[g.idx[i]];
@@ -309,19 +312,13 @@ int finish_solve(rcmps_context* ctx, FinishJob& job, cudaStream_t stream, Finish
     double* dR = (double*)d_in;
     double* dK = (double*)(d_in + n * mat);
     double* dP = (double*)(d_in + 2 * n * mat);
-    double* dE = (double*)(d_in + 4 * n * mat);
     e = cudaMemcpyAsync(P(g.o_dims), hd, n * 4, cudaMemcpyHostToDevice, stream);
     if (!e) e = cudaMemcpyAsync(P(g.o_off), ho, n * 8, cudaMemcpyHostToDevice, stream);
     if (!e) e = cudaMemsetAsync(P(g.o_status), 0, n * 4, stream);
-    if (!e) e = cudaMemsetAsync(P(g.gb.o_x), 0, (size_t)n * mat * 16, stream);
-    if (!e && job.x0)
-      e = launch_pad(job.x0, (long long*)P(g.o_off), (int*)P(g.o_dims), (double*)P(g.gb.o_x), dp, mat, n, stream);
     if (!e) e = launch_pad(job.R, (long long*)P(g.o_off), (int*)P(g.o_dims), dR, dp, mat, n, stream);
     if (!e) e = launch_pad(job.K, (long long*)P(g.o_off), (int*)P(g.o_dims), dK, dp, mat, n, stream);
     if (!e) e = launch_pad(job.rho, (long long*)P(g.o_off), (int*)P(g.o_dims), dP, dp, mat, n, stream);
-    if (!e) e = launch_pad(job.environment, (long long*)P(g.o_off), (int*)P(g.o_dims), dE, dp, mat, n, stream);
     if (!e) e = launch_prepare(dR, dK, dP, (double*)P(g.o_ops), dp, mat, 8 * mat, n, stream);
-    GmresNoJump nj;
     if (!e && nojump) {
       NoJumpSet* hs = (NoJumpSet*)(h + g.h_njs);
       double2* mats = (double2*)P(g.o_nj);
@@ -346,9 +343,44 @@ int finish_solve(rcmps_context* ctx, FinishJob& job, cudaStream_t stream, Finish
       }
       e = cudaMemcpyAsync(P(g.o_njs), hs, (size_t)n * sizeof(NoJumpSet), cudaMemcpyHostToDevice, stream);
       if (!e) e = nojump_setup_launch((const NoJumpSet*)P(g.o_njs), n, dp, stream);
-      nj.sets = (const NoJumpSet*)P(g.o_njs);
-      nj.W = (double2*)P(g.o_njw);
+      g.nj_sets = (const NoJumpSet*)P(g.o_njs);
+      g.nj_W = (double2*)P(g.o_njw);
     }
+    if (e) return fail(ctx, RCMPS_CUDA_ERROR, std::string("boundary set-up: ") + cudaGetErrorString(e));
+  }
+  plan.prepared = true;
+  return RCMPS_OK;
+}
+
+// The Poisson GMRES of every state (after finish_prepare, which it runs first if the caller has
+// not): the environment and the right-hand side, then the batched solve per padded dimension.
+int finish_solve(rcmps_context* ctx, FinishJob& job, cudaStream_t stream, FinishPlan& plan) {
+  if (!plan.prepared) {
+    const int rc = finish_prepare(ctx, job, stream, plan);
+    if (rc) return rc;
+  }
+  const rcmps_settings& S = job.settings;
+  const double tol = S.boundary_tolerance;
+  const int m = plan.m, maxrestart = job.max_restarts;
+  const bool nojump = plan.nojump;
+  rcmps_slot& SL = ctx->slot[job.slot];
+  char* base = static_cast<char*>(SL.arena);
+  char* h = static_cast<char*>(SL.pinned);
+  auto P = [&](size_t o) { return static_cast<void*>(base + o); };
+  cudaError_t e = cudaSuccess;
+  for (auto& g : plan.groups) {
+    const int dp = g.dp, n = g.n;
+    const size_t mat = (size_t)dp * dp;
+    int* hd = (int*)(h + g.h_dims);
+    ArnoldiProblem* hp = (ArnoldiProblem*)(h + g.h_probs);
+    double* dE = (double*)((double2*)P(g.o_in) + 4 * n * mat);
+    e = cudaMemsetAsync(P(g.gb.o_x), 0, (size_t)n * mat * 16, stream);
+    if (!e && job.x0)
+      e = launch_pad(job.x0, (long long*)P(g.o_off), (int*)P(g.o_dims), (double*)P(g.gb.o_x), dp, mat, n, stream);
+    if (!e) e = launch_pad(job.environment, (long long*)P(g.o_off), (int*)P(g.o_dims), dE, dp, mat, n, stream);
+    GmresNoJump nj;
+    nj.sets = g.nj_sets;
+    nj.W = g.nj_W;
     FinishArgs fa = finish_args(plan, g, base, S.metric_reg);
     if (!e) e = boundary_rhs_launch(fa, n, stream);
     if (e) return fail(ctx, RCMPS_CUDA_ERROR, std::string("boundary set-up: ") + cudaGetErrorString(e));

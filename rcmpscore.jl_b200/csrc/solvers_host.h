@@ -48,9 +48,17 @@ struct FinishPlan {
   struct Group;
   std::vector<Group> groups;
   std::vector<long long> off;
+  bool prepared = false;   // finish_prepare ran
+  bool nojump = false;     // the boundary GMRES takes the no-jump preconditioner
+  int m = 64;              // its restart length
   FinishPlan();
   ~FinishPlan();
 };
+// finish_prepare needs only R, K and rho: the workspace, the per-state operators and the no-jump
+// preconditioner's eigenbasis. A caller may run it before the environment exists (the composite
+// entry does, on the solve stream, while the trajectory integrates); finish_solve runs it itself
+// otherwise.
+int finish_prepare(rcmps_context* ctx, FinishJob& job, cudaStream_t stream, FinishPlan& plan);
 int finish_solve(rcmps_context* ctx, FinishJob& job, cudaStream_t stream, FinishPlan& plan);
 int finish_complete(rcmps_context* ctx, FinishJob& job, cudaStream_t stream, FinishPlan& plan);
 int stationary_run(rcmps_context* ctx, StationaryJob& job, cudaStream_t stream);
