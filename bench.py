@@ -152,7 +152,8 @@ def single_state_latency(steps):
             "api": "rcmps_b200.objective.objective (host arrays in and out)", "steps": steps,
             "ms_per_eval": 1000 * statistics.mean(walls), "ms_min": 1000 * min(walls),
             "phases_ms_last_call": {"trajectory": t[0], "pullback": t[1], "kinetic": t[2], "boundary_finish": t[3],
-                                    "whole_call": t[4], "boundary_prepare_beside_trajectory": t[5]},
+                                    "whole_call": t[4], "boundary_prepare_beside_trajectory": t[5],
+                                    "boundary_gmres": t[6]},
             "trajectory_ctas_per_state": 4 * groups.value, "channel_groups": groups.value,
             "rhs_calls": st["rhs_calls"], "accepted": st["accepted"], "rejected": st["rejected"], "energy": e}
 
@@ -264,7 +265,7 @@ def run_b200(args, rank, world, local_rank):
 
     for _ in range(args.warmup):
         step()
-    traj_ms, pull_ms, kin_ms, fin_ms, call_ms, prep_ms = [], [], [], [], [], []
+    traj_ms, pull_ms, kin_ms, fin_ms, call_ms, prep_ms, gmres_ms = [], [], [], [], [], [], []
     barrier()
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     launches0 = lib.rcmps_launch_count()   # library launches before the timed region
@@ -278,6 +279,7 @@ def run_b200(args, rank, world, local_rank):
             kin_ms.append(t[2])
             fin_ms.append(t[3])
             prep_ms.append(t[5])
+            gmres_ms.append(t[6])
             call_ms.append(t[4])
         end.record(stream)
         barrier()
@@ -480,7 +482,8 @@ def run_b200(args, rank, world, local_rank):
                 "phases_ms": {"trajectory": traj, "pullback": statistics.mean(pull_ms),
                               "kinetic": statistics.mean(kin_ms), "boundary_finish": statistics.mean(fin_ms),
                               "whole_call": statistics.mean(call_ms),
-                              "boundary_prepare_beside_trajectory": statistics.mean(prep_ms)},
+                              "boundary_prepare_beside_trajectory": statistics.mean(prep_ms),
+                              "boundary_gmres": statistics.mean(gmres_ms)},
                 "steps_per_state": {"rhs_calls_mean": statistics.mean(rhs_calls), "accepted_mean":
                                     statistics.mean(stats[i].accepted for i in range(n)),
                                     "gmres_iterations_mean": statistics.mean(stats[i].gmres_iterations for i in range(n)),

@@ -114,7 +114,8 @@ const char* rcmps_status_name(int status);
 /* Device milliseconds of the phases of the last batched call: 0 trajectory, 1 pullback,
  * 2 kinetic, 3 boundary/finish (from the environment to the gradient), 4 whole call, 5 the
  * boundary solve's preparation (operators and the no-jump preconditioner's eigenbasis; it runs
- * on the solve stream beside the trajectory). */
+ * on the solve stream beside the trajectory), 6 the boundary GMRES alone (from the environment
+ * to the solution; phase 3 also waits for the pullback's covector). */
 int rcmps_last_timings(const rcmps_context* context, float* milliseconds, int n);
 /* Bytes of device workspace that rcmps_fg_phi4_batch needs for these dimensions. */
 long long rcmps_workspace_bytes(const rcmps_context* context, int n_states, const int* dims,

@@ -776,6 +776,7 @@ int rcmps_fg_phi4_batch_controls(rcmps_context* ctx, int n, const int* dims, con
     sum_parts_kernel<<<nsum, 256, 0, s2>>>(n, total, vq, vk, (double2*)cq, (double2*)ck, (double2*)eq, (double2*)ek,
                                            nullptr, nullptr, (double2*)esum);
     frc = finish_solve(ctx, fj, s2, plan);
+    cudaEventRecord(ctx->slot[2].ev[6], s2);
   }
   qworker.join();
   for (int i = 0; i < n; ++i) {
@@ -802,6 +803,7 @@ int rcmps_fg_phi4_batch_controls(rcmps_context* ctx, int n, const int* dims, con
   cudaEventElapsedTime(&ctx->last_ms[3], ctx->slot[2].ev[1], ctx->slot[2].ev[2]);
   cudaEventElapsedTime(&ctx->last_ms[4], ctx->slot[2].ev[0], ctx->slot[2].ev[2]);
   cudaEventElapsedTime(&ctx->last_ms[5], ctx->slot[2].ev[4], ctx->slot[2].ev[5]);
+  cudaEventElapsedTime(&ctx->last_ms[6], ctx->slot[2].ev[1], ctx->slot[2].ev[6]);
   for (int i = 0; i < n; ++i) {
     stats[i].gmres_iterations = fst[i].gmres_iterations;
     stats[i].gmres_matvecs = fst[i].gmres_matvecs;

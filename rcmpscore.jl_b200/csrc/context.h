@@ -13,7 +13,7 @@ struct rcmps_slot {
   size_t arena_bytes = 0;
   void* pinned = nullptr;
   size_t pinned_bytes = 0;
-  cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+  cudaEvent_t ev[8] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
 };
 
 // One restart cycle of the batched GMRES captured as a CUDA graph, for the problems and tasks at
