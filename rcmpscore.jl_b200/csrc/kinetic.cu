@@ -42,9 +42,30 @@ struct LGeo<96> {
   static constexpr int MINB = 1;
 };
 
+// The Arnoldi matvec task of step j of problem P: W = L(V_j), or L(Z_j) for a flexible GMRES
+// problem whose preconditioned basis Z_j = M V_j was formed before; X = NULL skips the problem.
+__device__ __forceinline__ LindbladTask arnoldi_task(const ArnoldiProblem& P, int j) {
+  LindbladTask t;
+  t.X = (P.active && !P.exhausted && j < P.target) ? (P.Z ? P.Z : P.V) + (size_t)j * P.ldv : nullptr;
+  t.out = P.W;
+  t.A1 = P.A1;
+  t.A1h = P.A1h;
+  t.A2 = P.A2;
+  t.A2h = P.A2h;
+  t.rhs = nullptr;
+  t.res = nullptr;
+  t.shift = 0.0;
+  t.flag = P.flag;
+  t.trw = P.trw;
+  t.d = P.d;
+  return t;
+}
+
+// tasks: one task per slot; or (tasks NULL) the Arnoldi step j of problems probs[0..ntasks).
 template <int DP>
 __global__ void __launch_bounds__(LGeo<DP>::NT, LGeo<DP>::MINB)
-lindblad_kernel(const LindbladTask* __restrict__ tasks, int ntasks, int mode) {
+lindblad_kernel(const LindbladTask* __restrict__ tasks, const ArnoldiProblem* __restrict__ probs, int j, int ntasks,
+                int mode) {
   using LG = LGeo<DP>;
   using GR = RowGemmRing<DP, LG::NW, LG::KC, LG::NST>;
   constexpr int MAT = DP * DP;   // used by the trace term
@@ -59,7 +80,7 @@ lindblad_kernel(const LindbladTask* __restrict__ tasks, int ntasks, int mode) {
   const int rb = blockIdx.x % (DP / 16);
   const int task = blockIdx.x / (DP / 16);
   if (task >= ntasks) return;
-  const LindbladTask T = tasks[task];
+  const LindbladTask T = tasks ? tasks[task] : arnoldi_task(probs[task], j);
   if (!T.X) return;   // inactive slot
   const int row0 = rb * 16;
   // tr(trw X) for the GMRES operators, computed redundantly by every row block
@@ -346,26 +367,169 @@ __global__ void cgs_finish(ArnoldiProblem* __restrict__ probs, int nprob, int j,
   }
 }
 
+// One whole Gram-Schmidt step (both passes of cgs_partial/cgs_subtract and cgs_finish) in one
+// launch: a cluster of G CTAs per problem, each holding its rows of w in shared memory; the
+// projections h_i and the norms are summed across the cluster through distributed shared memory
+// (in chunk order, as the three-launch form sums its partials). The basis is still streamed twice
+// per pass; what goes is four launches and the global round trips between them.
+constexpr int kCgsMaxCluster = 8;
+constexpr int kCgsThreads = 256;
+
+__host__ __device__ inline int cgs_cluster(int n) {
+  const int g = (n + CH - 1) / CH;
+  return g < kCgsMaxCluster ? g : kCgsMaxCluster;
+}
+__host__ __device__ inline int cgs_rows(int n) {   // rows per CTA, a multiple of 128
+  const int g = cgs_cluster(n);
+  return ((n + g - 1) / g + 127) / 128 * 128;
+}
+
+__global__ void __launch_bounds__(kCgsThreads) cgs_fused(ArnoldiProblem* __restrict__ probs, int nprob, int j) {
+  const int p = blockIdx.y;
+  ArnoldiProblem& P = probs[p];
+  // uniform over the cluster (one problem per cluster)
+  if (!P.active || P.exhausted || j >= P.target) return;
+  extern __shared__ __align__(16) double2 dyn[];
+  const int n = P.n, rows = cgs_rows(n), G = (int)cluster_size(), ch = (int)cluster_rank();
+  double2* w = dyn;                        // [rows]
+  double2* part = dyn + rows;              // [j + 1]: this CTA's projections
+  double2* h = part + (j + 1);             // [j + 1]: the summed projections
+  __shared__ double red[kCgsThreads / 32];
+  __shared__ double xch[2];                // this CTA's |w|^2 before / after the current pass
+  const int r0 = ch * rows, r1 = min(n, r0 + rows);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = kCgsThreads / 32;
+  auto block_sum = [&](double v) {
+    v = warp_sum(v);
+    __syncthreads();
+    if (lane == 0) red[warp] = v;
+    __syncthreads();
+    double t = 0.0;
+    for (int i = 0; i < nw; ++i) t += red[i];
+    return t;
+  };
+  auto cluster_total = [&](int slot) {   // sum of xch[slot] over the cluster, in rank order
+    double t = 0.0;
+    for (int g = 0; g < G; ++g) t += dsmem_load(&xch[slot], (uint32_t)g);
+    return t;
+  };
+  double s0 = 0.0;
+  for (int r = threadIdx.x; r < rows; r += kCgsThreads) {
+    const double2 v = r0 + r < r1 ? P.W[r0 + r] : make_double2(0, 0);
+    w[r] = v;
+    s0 += zabs2(v);
+    // before the first projection w = L(V_j): kept for the true residuals of the shifted solves
+    if (P.LV && r0 + r < r1) P.LV[(size_t)j * P.ldv + r0 + r] = v;
+  }
+  s0 = block_sum(s0);
+  if (threadIdx.x == 0) xch[0] = s0;
+  double before = 0.0, after = 0.0;
+  for (int pass = 0; pass < 2; ++pass) {
+    // projections of this CTA's rows: a warp takes two basis vectors at a time
+    for (int i = warp; i <= j; i += 2 * nw) {
+      const bool two = i + nw <= j;
+      const double2* v0 = P.V + (size_t)i * P.ldv;
+      const double2* v1 = P.V + (size_t)(two ? i + nw : i) * P.ldv;
+      double re0 = 0.0, im0 = 0.0, re1 = 0.0, im1 = 0.0;
+      int r = r0 + lane;
+      for (; r + 96 < r1; r += 128) {
+        double2 a[4], c[4], b[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          a[u] = v0[r + 32 * u];
+          c[u] = v1[r + 32 * u];
+          b[u] = w[r - r0 + 32 * u];
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          re0 += a[u].x * b[u].x + a[u].y * b[u].y;
+          im0 += a[u].x * b[u].y - a[u].y * b[u].x;
+          re1 += c[u].x * b[u].x + c[u].y * b[u].y;
+          im1 += c[u].x * b[u].y - c[u].y * b[u].x;
+        }
+      }
+      for (; r < r1; r += 32) {
+        const double2 a = v0[r], c = v1[r], b = w[r - r0];
+        re0 += a.x * b.x + a.y * b.y;
+        im0 += a.x * b.y - a.y * b.x;
+        re1 += c.x * b.x + c.y * b.y;
+        im1 += c.x * b.y - c.y * b.x;
+      }
+      re0 = warp_sum(re0);
+      im0 = warp_sum(im0);
+      re1 = warp_sum(re1);
+      im1 = warp_sum(im1);
+      if (lane == 0) {
+        part[i] = make_double2(re0, im0);
+        if (two) part[i + nw] = make_double2(re1, im1);
+      }
+    }
+    cluster_sync();
+    if (pass == 0) before = cluster_total(0);
+    for (int i = threadIdx.x; i <= j; i += kCgsThreads) {
+      double2 t = make_double2(0, 0);
+      for (int g = 0; g < G; ++g) {
+        t.x += dsmem_load(&part[i].x, (uint32_t)g);
+        t.y += dsmem_load(&part[i].y, (uint32_t)g);
+      }
+      h[i] = t;
+      if (ch == 0) P.H[(size_t)i * P.kmax + j] = zadd(P.H[(size_t)i * P.kmax + j], t);
+    }
+    cluster_sync();   // every CTA has read the others' projections (and xch[0]) before they change
+    double nrm = 0.0;
+    for (int r = threadIdx.x; r < r1 - r0; r += kCgsThreads) {
+      double2 acc = w[r];
+      const double2* v = P.V + r0 + r;
+      int i = 0;
+      for (; i + 3 <= j; i += 4) {
+        double2 x[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) x[u] = v[(size_t)(i + u) * P.ldv];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const double2 c = h[i + u];
+          acc.x -= x[u].x * c.x - x[u].y * c.y;
+          acc.y -= x[u].x * c.y + x[u].y * c.x;
+        }
+      }
+      for (; i <= j; ++i) {
+        const double2 x = v[(size_t)i * P.ldv], c = h[i];
+        acc.x -= x.x * c.x - x.y * c.y;
+        acc.y -= x.x * c.y + x.y * c.x;
+      }
+      w[r] = acc;
+      nrm += zabs2(acc);
+    }
+    nrm = block_sum(nrm);
+    if (threadIdx.x == 0) xch[1] = nrm;
+    cluster_sync();
+    after = cluster_total(1);
+    cluster_sync();   // xch[1] is rewritten by the second pass
+    // the second pass only when the first lost more than 1 - 1/sqrt(2) of the norm (uniform)
+    if (pass == 0 && after > 0.5 * before) break;
+  }
+  // beta = |w|; H[j+1][j] = beta; breakdown test; V_{j+1} = w / beta (zero after a breakdown)
+  const double old = sqrt(before), beta = sqrt(after);
+  const double eps = DBL_EPSILON;
+  const bool exhausted = beta <= 10.0 * eps * fmax(old, eps) || j + 1 == P.n_phys;
+  double2* next = P.V + (size_t)(j + 1) * P.ldv;
+  const double inv = 1.0 / fmax(beta, DBL_MIN);
+  for (int r = threadIdx.x; r < r1 - r0; r += kCgsThreads)
+    next[r0 + r] = exhausted ? make_double2(0, 0) : zscale(inv, w[r]);
+  if (ch == 0 && threadIdx.x == 0) {
+    P.H[(size_t)(j + 1) * P.kmax + j] = make_double2(beta, 0.0);
+    P.reorth = after > 0.5 * before ? 0 : 1;
+    P.k = j + 1;
+    if (!isfinite(beta)) P.nonfinite = 1;
+    if (exhausted) P.exhausted = 1;
+  }
+}
+
 // Arnoldi matvec tasks of step j: W = L(V_j) for every problem still extending (L(Z_j) for a
 // flexible GMRES problem, whose preconditioned basis Z_j = M V_j was formed before).
 __global__ void arnoldi_tasks(const ArnoldiProblem* __restrict__ probs, int nprob, int j, LindbladTask* tasks) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= nprob) return;
-  const ArnoldiProblem& P = probs[p];
-  LindbladTask t;
-  t.X = (P.active && !P.exhausted && j < P.target) ? (P.Z ? P.Z : P.V) + (size_t)j * P.ldv : nullptr;
-  t.out = P.W;
-  t.A1 = P.A1;
-  t.A1h = P.A1h;
-  t.A2 = P.A2;
-  t.A2h = P.A2h;
-  t.rhs = nullptr;
-  t.res = nullptr;
-  t.shift = 0.0;
-  t.flag = P.flag;
-  t.trw = P.trw;
-  t.d = P.d;
-  tasks[p] = t;
+  tasks[p] = arnoldi_task(probs[p], j);
 }
 
 // start: beta = |rhs|, V_0 = rhs / beta
@@ -935,27 +1099,37 @@ __global__ void residual_reduce(ArnoldiProblem* __restrict__ probs, int nprob, c
 
 // ======================================================================= launchers
 template <int DP>
-static cudaError_t launch_l(const LindbladTask* tasks, int ntasks, int mode, cudaStream_t s) {
+static cudaError_t launch_l(const LindbladTask* tasks, const ArnoldiProblem* probs, int j, int ntasks, int mode,
+                            cudaStream_t s) {
   using LG = LGeo<DP>;
   auto k = lindblad_kernel<DP>;
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)LG::SMEM);
   if (e != cudaSuccess) return e;
   if (ntasks == 0) return cudaSuccess;
   note_launch();
-  k<<<ntasks * (DP / 16), LG::NT, LG::SMEM, s>>>(tasks, ntasks, mode);
+  k<<<ntasks * (DP / 16), LG::NT, LG::SMEM, s>>>(tasks, probs, j, ntasks, mode);
   return cudaGetLastError();
 }
 
-cudaError_t lindblad_launch(int dp, const LindbladTask* d_tasks, int ntasks, int mode, cudaStream_t s) {
+static cudaError_t launch_l_dp(int dp, const LindbladTask* tasks, const ArnoldiProblem* probs, int j, int ntasks,
+                               int mode, cudaStream_t s) {
   switch (dp) {
-    case 16: return launch_l<16>(d_tasks, ntasks, mode, s);
-    case 32: return launch_l<32>(d_tasks, ntasks, mode, s);
-    case 48: return launch_l<48>(d_tasks, ntasks, mode, s);
-    case 64: return launch_l<64>(d_tasks, ntasks, mode, s);
-    case 96: return launch_l<96>(d_tasks, ntasks, mode, s);
-    case 128: return launch_l<128>(d_tasks, ntasks, mode, s);
+    case 16: return launch_l<16>(tasks, probs, j, ntasks, mode, s);
+    case 32: return launch_l<32>(tasks, probs, j, ntasks, mode, s);
+    case 48: return launch_l<48>(tasks, probs, j, ntasks, mode, s);
+    case 64: return launch_l<64>(tasks, probs, j, ntasks, mode, s);
+    case 96: return launch_l<96>(tasks, probs, j, ntasks, mode, s);
+    case 128: return launch_l<128>(tasks, probs, j, ntasks, mode, s);
   }
   return cudaErrorInvalidValue;
+}
+
+cudaError_t lindblad_launch(int dp, const LindbladTask* d_tasks, int ntasks, int mode, cudaStream_t s) {
+  return launch_l_dp(dp, d_tasks, nullptr, 0, ntasks, mode, s);
+}
+
+cudaError_t lindblad_arnoldi_launch(int dp, const ArnoldiProblem* d_probs, int nprob, int j, cudaStream_t s) {
+  return launch_l_dp(dp, nullptr, d_probs, j, nprob, 0, s);
 }
 
 cudaError_t arnoldi_tasks_launch(const ArnoldiProblem* d_probs, int nprob, int j, LindbladTask* d_tasks,
@@ -984,6 +1158,28 @@ cudaError_t cgs_step_launch(ArnoldiProblem* d_probs, int nprob, int j, int n, cu
   note_launch();
   cgs_finish<<<grid, 256, 0, s>>>(d_probs, nprob, j, nchunk);
   return cudaGetLastError();
+}
+
+cudaError_t cgs_fused_launch(ArnoldiProblem* d_probs, int nprob, int j, int n, cudaStream_t s) {
+  if (nprob == 0) return cudaSuccess;
+  const int g = cgs_cluster(n), rows = cgs_rows(n);
+  const size_t smem = ((size_t)rows + 2 * (size_t)(j + 1)) * sizeof(double2);
+  cudaError_t e = cudaFuncSetAttribute(cgs_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(g, nprob, 1);
+  cfg.blockDim = dim3(kCgsThreads, 1, 1);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = g;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  note_launch();
+  return cudaLaunchKernelEx(&cfg, cgs_fused, d_probs, nprob, j);
 }
 
 cudaError_t hessenberg_launch(ArnoldiProblem* d_probs, int nprob, const double* d_shifts, int nshift,

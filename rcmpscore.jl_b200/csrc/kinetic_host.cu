@@ -231,9 +231,8 @@ int kinetic_run(rcmps_context* ctx, KineticJob& job, cudaStream_t stream) {
         }
         e = cudaMemcpyAsync(d_probs, hp, NP * sizeof(ArnoldiProblem), cudaMemcpyHostToDevice, stream);
         for (int j = jlo; j < jhi && !e; ++j) {
-          e = arnoldi_tasks_launch(d_probs, NP, j, (LindbladTask*)P(o_mtasks), stream);
-          if (!e) e = lindblad_launch(dp, (LindbladTask*)P(o_mtasks), NP, 0, stream);
-          if (!e) e = cgs_step_launch(d_probs, NP, j, nvec, stream);
+          e = lindblad_arnoldi_launch(dp, d_probs, NP, j, stream);
+          if (!e) e = cgs_fused_launch(d_probs, NP, j, nvec, stream);
         }
         // ---- projected solves of every open problem
         int kcur = 1;

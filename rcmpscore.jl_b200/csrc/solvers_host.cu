@@ -67,9 +67,8 @@ static cudaError_t gmres_cycle_launches(ArnoldiProblem* d_probs, int NP, int dp,
       if (!e) e = net_unpack_launch(d_probs, NP, j, net->d, dp, net->Y32, net->identity, stream);
       if (e) break;
     }
-    e = arnoldi_tasks_launch(d_probs, NP, j, d_tasks, stream);
-    if (!e) e = lindblad_launch(dp, d_tasks, NP, 0, stream);
-    if (!e) e = cgs_step_launch(d_probs, NP, j, nvec, stream);
+    e = lindblad_arnoldi_launch(dp, d_probs, NP, j, stream);
+    if (!e) e = cgs_fused_launch(d_probs, NP, j, nvec, stream);
     if (!e) e = gmres_givens_launch(d_probs, NP, j, stream);
   }
   return e;
