@@ -1182,6 +1182,14 @@ cudaError_t cgs_fused_launch(ArnoldiProblem* d_probs, int nprob, int j, int n, c
   return cudaLaunchKernelEx(&cfg, cgs_fused, d_probs, nprob, j);
 }
 
+cudaError_t gram_schmidt_launch(ArnoldiProblem* d_probs, int nprob, int j, int n, int sms, cudaStream_t s) {
+  // few problems: the step is latency-bound and one clustered launch wins; a large batch streams
+  // the basis from HBM on whatever SMs the concurrent trajectory leaves, where the independent
+  // CTAs of the three-kernel form keep those SMs busier than clusters waiting at their barriers
+  if ((long long)nprob * cgs_cluster(n) <= 2ll * sms) return cgs_fused_launch(d_probs, nprob, j, n, s);
+  return cgs_step_launch(d_probs, nprob, j, n, s);
+}
+
 cudaError_t hessenberg_launch(ArnoldiProblem* d_probs, int nprob, const double* d_shifts, int nshift,
                               double2* scratch, long long slot_elems, int nslots, int kmax, cudaStream_t s) {
   const int blocks = (nslots * 32 + 255) / 256;

@@ -82,6 +82,8 @@ cudaError_t arnoldi_start_launch(ArnoldiProblem* d_probs, int nprob, cudaStream_
 cudaError_t cgs_step_launch(ArnoldiProblem* d_probs, int nprob, int j, int n, cudaStream_t s);
 // The same Gram-Schmidt step in one launch (a cluster per problem; no partial or norm arrays).
 cudaError_t cgs_fused_launch(ArnoldiProblem* d_probs, int nprob, int j, int n, cudaStream_t s);
+// The Gram-Schmidt step by whichever of the two forms suits the batch (sms: the device's SMs).
+cudaError_t gram_schmidt_launch(ArnoldiProblem* d_probs, int nprob, int j, int n, int sms, cudaStream_t s);
 // W = L(V_j) (or L(Z_j)) of step j of every problem still extending, the task built in the kernel.
 cudaError_t lindblad_arnoldi_launch(int dp, const ArnoldiProblem* d_probs, int nprob, int j, cudaStream_t s);
 cudaError_t hessenberg_launch(ArnoldiProblem* d_probs, int nprob, const double* d_shifts, int nshift,

@@ -232,7 +232,7 @@ int kinetic_run(rcmps_context* ctx, KineticJob& job, cudaStream_t stream) {
         e = cudaMemcpyAsync(d_probs, hp, NP * sizeof(ArnoldiProblem), cudaMemcpyHostToDevice, stream);
         for (int j = jlo; j < jhi && !e; ++j) {
           e = lindblad_arnoldi_launch(dp, d_probs, NP, j, stream);
-          if (!e) e = cgs_fused_launch(d_probs, NP, j, nvec, stream);
+          if (!e) e = gram_schmidt_launch(d_probs, NP, j, nvec, ctx->sms, stream);
         }
         // ---- projected solves of every open problem
         int kcur = 1;

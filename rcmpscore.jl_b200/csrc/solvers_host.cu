@@ -51,9 +51,8 @@ struct GmresNoJump {
 // between them (converged problems are skipped inside the kernels). With a learned
 // preconditioner every step first forms Z_j = M V_j (pack, two GEMMs, unpack); with the no-jump
 // preconditioner Z_j = P(V_j) (one clustered launch).
-static cudaError_t gmres_cycle_launches(ArnoldiProblem* d_probs, int NP, int dp, int m, LindbladTask* d_tasks,
-                                        cudaStream_t stream, const GmresNet* net = nullptr,
-                                        const GmresNoJump* nj = nullptr) {
+static cudaError_t gmres_cycle_launches(ArnoldiProblem* d_probs, int NP, int dp, int m, int sms, cudaStream_t stream,
+                                        const GmresNet* net = nullptr, const GmresNoJump* nj = nullptr) {
   const int nvec = dp * dp;
   cudaError_t e = cudaSuccess;
   for (int j = 0; j < m && !e; ++j) {
@@ -68,7 +67,7 @@ static cudaError_t gmres_cycle_launches(ArnoldiProblem* d_probs, int NP, int dp,
       if (e) break;
     }
     e = lindblad_arnoldi_launch(dp, d_probs, NP, j, stream);
-    if (!e) e = cgs_fused_launch(d_probs, NP, j, nvec, stream);
+    if (!e) e = gram_schmidt_launch(d_probs, NP, j, nvec, sms, stream);
     if (!e) e = gmres_givens_launch(d_probs, NP, j, stream);
   }
   return e;
@@ -95,9 +94,9 @@ static cudaError_t gmres_cycle(rcmps_context* ctx, ArnoldiProblem* d_probs, int 
   cudaGraph_t graph = nullptr;
   if (cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
     cudaGetLastError();
-    return gmres_cycle_launches(d_probs, NP, dp, m, d_tasks, stream, net, nj);
+    return gmres_cycle_launches(d_probs, NP, dp, m, ctx->sms, stream, net, nj);
   }
-  cudaError_t e = gmres_cycle_launches(d_probs, NP, dp, m, d_tasks, stream, net, nj);
+  cudaError_t e = gmres_cycle_launches(d_probs, NP, dp, m, ctx->sms, stream, net, nj);
   const cudaError_t ec = cudaStreamEndCapture(stream, &graph);
   cudaGraphExec_t exec = nullptr;
   if (!e && !ec && graph && cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess) {
@@ -122,7 +121,7 @@ static cudaError_t gmres_cycle(rcmps_context* ctx, ArnoldiProblem* d_probs, int 
   // capture or instantiation failed: nothing was launched by the capture; launch directly
   if (graph) cudaGraphDestroy(graph);
   cudaGetLastError();
-  return gmres_cycle_launches(d_probs, NP, dp, m, d_tasks, stream, net, nj);
+  return gmres_cycle_launches(d_probs, NP, dp, m, ctx->sms, stream, net, nj);
 }
 
 // Restarted GMRES(m) over NP problems that share dp; hp/d_probs hold set-up problems with x = 0.
