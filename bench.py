@@ -225,7 +225,8 @@ def run_b200(args, rank, world, local_rank):
     # the unpacked channels for the others
     split = args.precision == "split"
     s = _lib.default_settings(symmetry=2 if args.quartic_route == "auto" else 0, precision=1 if split else 0,
-                              half_window=args.half_window, n_quad=args.n_quad)
+                              half_window=args.half_window, n_quad=args.n_quad,
+                              trajectory_groups=args.trajectory_groups)
     cdims = (C.c_int * n)(*dims)
     cg = (C.c_double * n)(*g)
     pack = lambda L: torch.from_numpy(np.concatenate([np.ascontiguousarray(x).ravel() for x in L])).cuda()
@@ -542,6 +543,8 @@ def main():
     p.add_argument("--learned-epochs", type=int, default=100, help="training epochs of that measurement")
     p.add_argument("--split-arm-steps", type=int, default=3,
                    help="steps of the split-precision arm timed after the FP64 one (0: none)")
+    p.add_argument("--trajectory-groups", type=int, choices=(0, 1, 2, 4), default=0,
+                   help="CTAs per 16-row block of a state's trajectory cluster (0: chosen per launch)")
     p.add_argument("--single-steps", type=int, default=3,
                    help="timed calls of the single-state latency measurement (0: none)")
     p.add_argument("--component", choices=("fg", "quartic"), default="fg",
