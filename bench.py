@@ -501,7 +501,8 @@ def run_b200(args, rank, world, local_rank):
         for dp in sorted(set(((d + 15) // 16) * 16 if d <= 64 else (96 if d <= 96 else 128) for d in dims)):
             ring, ms = C.c_int(0), (C.c_float * 3)()
             if lib.rcmps_trajectory_tuning(ctx.handle, 0, dp, C.byref(ring), ms) == 0 and ring.value:
-                tuning[str(dp)] = {"ring_stages": ring.value, "calibration_ms": [round(x, 3) for x in ms]}
+                tuning[str(dp)] = {"ring_stages": ring.value,
+                                   "ms_per_1000_rhs_at_depth_2_3_4": [round(x, 3) for x in ms]}
         line["config"]["autotuned_tiles"] = tuning
         line["config"]["precision"] = ("split: trajectory products of the D=64 states on tcgen05 BF16 slices "
                                        "(7 x 7 bits), FP64 step control, sums and solves" if split else

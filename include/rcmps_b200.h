@@ -325,11 +325,13 @@ int rcmps_retract(rcmps_context* context, int d, const double* R, const double* 
 
 /* The tile choice of the FP64 trajectory kernel's autotuner for (system: 0 quartic, 1 all-ODE,
  * 2 <phi>; padded dimension dp) at the channel-group count of the last launch of that pair: the
- * depth of the operand ring (2, 3 or 4 staged chunks; 0 while not yet tuned), chosen on the first
- * launch of that pair and group count in this context by timing a few attempts of the launch's
- * own states at each depth, and the three calibration times in ms (ms may be NULL). The depth
- * changes the schedule only; results are identical. No counterpart in the reference (its tiles
- * follow a fixed rule, runtime/generic_layout.py:21-52). */
+ * depth of the operand ring (2, 3 or 4 staged chunks; 0 while not yet decided). The quartic
+ * system tunes on the caller's own launches: the first three of a pair and group count take the
+ * depths 4, 2, 3 and each records its device ms per 1000 right-hand sides of the launch's longest
+ * trajectory (ms[0..2] for the depths 2, 3, 4; ms may be NULL); the fastest is then kept, the
+ * default 4 unless another is faster by more than 2%. The other systems use 4 (3 for the all-ODE
+ * route at dp 128). The depth changes the schedule only; results are identical. No counterpart
+ * in the reference (its tiles follow a fixed rule, runtime/generic_layout.py:21-52). */
 int rcmps_trajectory_tuning(const rcmps_context* context, int system, int dp, int* ring, float* ms);
 /* The channel groups of the last trajectory launch of (system, dp) in this context (1, 2 or 4
  * CTAs per 16-row block of a state, rcmps_settings.trajectory_groups; 0: no launch yet). No

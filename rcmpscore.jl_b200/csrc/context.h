@@ -47,8 +47,9 @@ struct rcmps_context {
   bool tables = false;
   float last_ms[8] = {0};                 // device times of the last call's phases
   // trajectory tile autotuning: the operand-ring depth chosen per (system, padded dimension,
-  // channel-group level 1/2/4) on first use, and the calibration times of the depths 2, 3, 4 (ms);
-  // the channel groups of the last launch per (system, padded dimension)
+  // channel-group level 1/2/4) after its first three launches, and the device ms per 1000
+  // right-hand sides (of each launch's longest trajectory) those launches took at the depths 2,
+  // 3, 4; the channel groups of the last launch per (system, padded dimension)
   int traj_ring[3][6][3] = {};
   float traj_ring_ms[3][6][3][3] = {};
   int traj_groups[3][6] = {};

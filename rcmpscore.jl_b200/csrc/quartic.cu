@@ -129,44 +129,38 @@ int dp_index(int dp) {
 }
 
 // Tile autotuning of the FP64 trajectory kernel: the depth of its operand ring (2, 3 or 4 staged
-// B chunks). On the first launch of a (system, padded dimension) in a context, each depth runs the
-// launch's own states for a few attempts (kCalibrationAttempts, results discarded: the real launch
-// starts every trajectory afresh) and the fastest by CUDA events is kept. The depth changes the
-// schedule, not the arithmetic: results are identical for every depth.
-constexpr long long kCalibrationAttempts = 6;
+// B chunks, compiled variants of the quartic system). It tunes on the caller's own launches: while
+// a (system, padded dimension, channel-group level) is undecided in a context, its launches take
+// the depths 4, 2 and 3 in turn and each records its device time per 1000 right-hand sides of the
+// launch's longest trajectory (the launch lasts as long as that one); after the third the fastest
+// is kept, the default 4 unless another is faster by more than 2%. The timing thus includes
+// whatever runs beside the trajectory (the kinetic term). The depth changes the schedule, not the
+// arithmetic: results are identical for every depth.
 static int group_level(int groups) { return groups == 4 ? 2 : groups == 2 ? 1 : 0; }
 
-static cudaError_t tune_ring(rcmps_context* ctx, int system, int dp, const TrajState* d_states, int n,
-                             const double* d_points, int npoints, TrajControls tc, cudaStream_t stream) {
-  const int level = group_level(tc.groups);
-  int& ring = ctx->traj_ring[system][dp_index(dp)][level];
-  if (ring) return cudaSuccess;
-  cudaEvent_t a = nullptr, b = nullptr;
-  cudaError_t e = cudaEventCreate(&a);
-  if (!e) e = cudaEventCreate(&b);
-  float best = 1e30f;
+static int ring_for_launch(const rcmps_context* ctx, int system, int dp, int level) {
+  if (system != 0) return 4;
+  const int chosen = ctx->traj_ring[system][dp_index(dp)][level];
+  if (chosen) return chosen;
+  const float* t = ctx->traj_ring_ms[system][dp_index(dp)][level];
+  for (int depth : {4, 2, 3})
+    if (t[depth - 2] <= 0.f) return depth;
+  return 4;
+}
+
+static void ring_record(rcmps_context* ctx, int system, int dp, int level, int depth, float ms, long long rhs) {
+  if (system != 0 || ctx->traj_ring[system][dp_index(dp)][level] || rhs <= 0 || !(ms > 0.f)) return;
+  float* t = ctx->traj_ring_ms[system][dp_index(dp)][level];
+  t[depth - 2] = 1000.f * ms / (float)rhs;
+  if (t[0] <= 0.f || t[1] <= 0.f || t[2] <= 0.f) return;
   int choice = 4;
-  tc.max_attempts = kCalibrationAttempts;
-  for (int r = 2; r <= 4 && !e; ++r) {
-    tc.ring = r;
-    float ms = 0.f;
-    for (int rep = 0; rep < 2 && !e; ++rep) {   // the first repetition warms up
-      e = cudaEventRecord(a, stream);
-      if (!e) e = trajectory_launch(system, dp, d_states, n, d_points, npoints, tc, stream, 0);
-      if (!e) e = cudaEventRecord(b, stream);
-      if (!e) e = cudaEventSynchronize(b);
-      if (!e) e = cudaEventElapsedTime(&ms, a, b);
-    }
-    ctx->traj_ring_ms[system][dp_index(dp)][level][r - 2] = ms;
-    if (!e && ms < best) {
-      best = ms;
+  float best = t[2];
+  for (int r = 2; r <= 3; ++r)
+    if (t[r - 2] < 0.98f * best) {
+      best = t[r - 2];
       choice = r;
     }
-  }
-  if (a) cudaEventDestroy(a);
-  if (b) cudaEventDestroy(b);
-  if (!e) ring = choice;
-  return e;
+  ctx->traj_ring[system][dp_index(dp)][level] = choice;
 }
 
 int quartic_run(rcmps_context* ctx, QuarticJob& job, cudaStream_t stream) {
@@ -368,9 +362,7 @@ int quartic_run(rcmps_context* ctx, QuarticJob& job, cudaStream_t stream) {
       tc.max_ns = (unsigned long long)(S.max_device_seconds * 1e9);
       tc.groups = trajectory_groups(system, dp, n, S.trajectory_groups, split ? 1 : 0);
       ctx->traj_groups[system][dp_index(dp)] = tc.groups;
-      if (e == cudaSuccess && !split)
-        e = tune_ring(ctx, system, dp, (TrajState*)P(o_states), n, (double*)P(o_points), npoints, tc, stream);
-      if (!split) tc.ring = ctx->traj_ring[system][dp_index(dp)][group_level(tc.groups)];
+      if (!split) tc.ring = ring_for_launch(ctx, system, dp, group_level(tc.groups));
       if (e == cudaSuccess) e = cudaEventRecord(e0, stream);
       if (e == cudaSuccess)
         e = trajectory_launch(system, dp, (TrajState*)P(o_states), n, (double*)P(o_points), npoints, tc, stream,
@@ -469,6 +461,12 @@ int quartic_run(rcmps_context* ctx, QuarticJob& job, cudaStream_t stream) {
       float ms = 0.f;
       cudaEventElapsedTime(&ms, e0, e1);
       traj_ms += ms;
+      if (!split) {
+        long long longest = 0;
+        for (int i = 0; i < n; ++i)
+          longest = std::max(longest, 1 + 12 * h_tstats[i].attempts + 3 * h_tstats[i].dense_steps);
+        ring_record(ctx, system, dp, group_level(tc.groups), tc.ring, ms, longest);
+      }
       cudaEventElapsedTime(&ms, e1, e2);
       pull_ms += ms;
       for (int i = 0; i < n; ++i) {

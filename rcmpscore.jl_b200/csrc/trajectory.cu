@@ -219,16 +219,19 @@ __device__ void block_sum2(double& a, double& b, double* red) {
   b = y;
 }
 
-template <int DP, int SYS>
+// NST: stages of the operand ring (a compile-time depth keeps the slot arithmetic of every wait
+// and release a shift and a mask; the tile autotuner picks among the compiled depths).
+template <int DP, int SYS, int NST>
 struct Rhs {
   using GE = Geo<DP, SYS>;
+  static_assert(NST >= 2 && NST <= GE::NST, "ring depth");
   const TrajState* st;
   Smem<DP, SYS> sm;
   int row0, tid, lane, warp;
   long long* gq;   // running chunk counter (uniform across the CTA)
   int nchunk;      // chunks of one right-hand side (uniform)
   int ce, cc;      // producer cursor (thread 0): entry (G1 products, then G2 passes), chunk in it
-  int nst;         // ring stages in use (2 .. GE::NST; the launch's tuned ring depth)
+  static constexpr int nst = NST;   // ring stages in use
   // Packed Z2 state with d = DP and d/2 a multiple of 16 (zs): each CTA's 16 rows lie in one
   // parity half hh of the two halves of hz rows; the structurally zero output tiles and K
   // halves of every product are skipped.
@@ -610,7 +613,7 @@ __device__ __forceinline__ Smem<DP, SYS> carve_engine(unsigned char* base) {
   }
 }
 
-template <int DP, int SYS, int ENG>
+template <int DP, int SYS, int ENG, int NST = Geo<DP, SYS>::NST>
 __global__ void __launch_bounds__(Geo<DP, SYS>::NT, 1)
 trajectory_kernel(const TrajState* __restrict__ states, const double* __restrict__ points, int npoints,
                   TrajControls ctl_in) {
@@ -681,11 +684,10 @@ trajectory_kernel(const TrajState* __restrict__ states, const double* __restrict
     tmem = *ssm.tslot;
   }
   __syncthreads();
-  using RhsT = std::conditional_t<ENG == 0, Rhs<DP, SYS>, RhsSplit<DP>>;
+  using RhsT = std::conditional_t<ENG == 0, Rhs<DP, SYS, NST>, RhsSplit<DP>>;
   RhsT rhs;
   if constexpr (ENG == 0) {
-    rhs = Rhs<DP, SYS>{st, sm, row0, tid, lane, warp, &gq, 0, 0, 0,
-                       ctl_in.ring >= 2 && ctl_in.ring <= GE::NST ? ctl_in.ring : GE::NST};
+    rhs = Rhs<DP, SYS, NST>{st, sm, row0, tid, lane, warp, &gq, 0, 0, 0};
     rhs.c0 = c0;
     rhs.c1 = c1;
     rhs.remote = c_sys[SYS].grp_remote[glevel];
@@ -761,7 +763,7 @@ trajectory_kernel(const TrajState* __restrict__ states, const double* __restrict
   const double N = packed ? 10.0 * half * half + 1.0
                           : (double)GE::NCH * st->d * st->d + (GE::SCALAR ? 1.0 : 0.0);
   const double atol = st->atol, rtol = st->rtol;
-  const long long max_steps = ctl_in.max_attempts > 0 ? min(st->max_steps, ctl_in.max_attempts) : st->max_steps;
+  const long long max_steps = st->max_steps;
   const unsigned long long t_start = global_ns();
 
   while (true) {
@@ -1074,11 +1076,11 @@ static cudaLaunchConfig_t launch_config(int nstates, int cluster_ctas, cudaStrea
   return cfg;
 }
 
-template <int DP, int SYS, int ENG>
+template <int DP, int SYS, int ENG, int NST = Geo<DP, SYS>::NST>
 static cudaError_t prepare_kernel() {
   constexpr size_t smem = kernel_smem<DP, SYS, ENG>();
   static_assert(smem <= 232448, "shared memory per CTA");
-  auto kern = trajectory_kernel<DP, SYS, ENG>;
+  auto kern = trajectory_kernel<DP, SYS, ENG, NST>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e == cudaSuccess) e = cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
   return e;
@@ -1118,18 +1120,30 @@ static int choose_groups(int nstates, int requested) {
   return 1;
 }
 
-template <int DP, int SYS, int ENG = 0>
-static cudaError_t launch_dp(const TrajState* d_states, int nstates, const double* d_points, int npoints,
-                             const TrajControls& ctl, cudaStream_t stream) {
+template <int DP, int SYS, int ENG, int NST>
+static cudaError_t launch_kernel(const TrajState* d_states, int nstates, const double* d_points, int npoints,
+                                 const TrajControls& ctl, cudaStream_t stream) {
   using GE = Geo<DP, SYS>;
-  cudaError_t e = prepare_kernel<DP, SYS, ENG>();
+  cudaError_t e = prepare_kernel<DP, SYS, ENG, NST>();
   if (e != cudaSuccess) return e;
   const int cg = choose_groups<DP, SYS, ENG>(nstates, ctl.groups);
   if (cg == 0) return cudaErrorInvalidValue;
   cudaLaunchAttribute attr[1];
   cudaLaunchConfig_t cfg = launch_config<DP, SYS, ENG>(nstates, GE::G * cg, stream, attr);
   note_launch();
-  return cudaLaunchKernelEx(&cfg, trajectory_kernel<DP, SYS, ENG>, d_states, d_points, npoints, ctl);
+  return cudaLaunchKernelEx(&cfg, trajectory_kernel<DP, SYS, ENG, NST>, d_states, d_points, npoints, ctl);
+}
+
+// The ring depth the launch asked for (ctl.ring 2 or 3; the quartic FP64 system compiles those),
+// else the system's default depth.
+template <int DP, int SYS, int ENG = 0>
+static cudaError_t launch_dp(const TrajState* d_states, int nstates, const double* d_points, int npoints,
+                             const TrajControls& ctl, cudaStream_t stream) {
+  if constexpr (ENG == 0 && SYS == kSysQuartic) {
+    if (ctl.ring == 2) return launch_kernel<DP, SYS, ENG, 2>(d_states, nstates, d_points, npoints, ctl, stream);
+    if (ctl.ring == 3) return launch_kernel<DP, SYS, ENG, 3>(d_states, nstates, d_points, npoints, ctl, stream);
+  }
+  return launch_kernel<DP, SYS, ENG, Geo<DP, SYS>::NST>(d_states, nstates, d_points, npoints, ctl, stream);
 }
 
 // Node weights of the pullback: wj[2i] = weight_i 2|t_i|, wj[2i+1] = weight_i source(t_i).

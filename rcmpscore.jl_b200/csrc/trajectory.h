@@ -43,8 +43,8 @@ struct TrajControls {
   double endpoint;          // sqrt(half_window)
   double initial_h;
   unsigned long long max_ns;  // device-clock watchdog in ns (0: none)
-  int ring = 0;               // stages of the FP64 engine's operand ring (2 .. 4; 0: the default 4)
-  long long max_attempts = 0; // stop every trajectory after this many attempts (0: none; calibration)
+  int ring = 0;               // stages of the FP64 engine's operand ring on the quartic system (2, 3;
+                              // anything else: the default 4)
   int groups = 0;             // CTAs per row block of a state, each for a group of channels: 1, 2 or 4
                               // (0: chosen by the launch, see trajectory_groups)
 };

@@ -104,15 +104,22 @@ def test_controls_are_checked(gpu_context):
 
 
 def test_trajectory_tile_autotuner_records_its_choice(gpu_context):
-    """After a D = 64 evaluation the context holds the autotuned ring depth of the quartic
-    trajectory kernel (2, 3 or 4 staged chunks) and the three calibration times."""
+    """The first three D = 64 evaluations of a layout take the ring depths 4, 2, 3 (results are
+    identical) and record their device time per 1000 right-hand sides; the context then holds the
+    chosen depth: the default 4 unless another was faster by more than 2%."""
     import ctypes as C
     from rcmps_b200 import objective
     rec = load_records("bench.npz")[0]
-    objective.fg_phi4_batch([rec["R"]], [rec["K"]], [rec["rho"]], [rec["g"]],
-                            objective.settings_from_args(None, half_window=2.0, n_quad=16, kinetic_nodes=32))
+    s = objective.settings_from_args(None, half_window=2.0, n_quad=16, kinetic_nodes=32, trajectory_groups=1)
+    results = [objective.fg_phi4_batch([rec["R"]], [rec["K"]], [rec["rho"]], [rec["g"]], s) for _ in range(3)]
+    for E, G, _ in results[1:]:
+        assert E[0] == results[0][0][0] and np.array_equal(G[0], results[0][1][0])
     ctx = gpu_context
     ring, ms = C.c_int(0), (C.c_float * 3)()
     assert ctx.lib.rcmps_trajectory_tuning(ctx.handle, 0, 64, C.byref(ring), ms) == 0
-    assert ring.value in (2, 3, 4)
-    assert all(x > 0 for x in ms) and ms[ring.value - 2] == min(ms)
+    ms = list(ms)
+    assert ring.value in (2, 3, 4) and all(x > 0 for x in ms)
+    if ring.value == 4:
+        assert min(ms[:2]) >= 0.98 * ms[2]
+    else:
+        assert ms[ring.value - 2] == min(ms) and ms[ring.value - 2] < 0.98 * ms[2]
