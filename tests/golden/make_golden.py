@@ -15,6 +15,8 @@ RCMPS_REFERENCE_SRC; there is no default) and writes .npz files:
                 D = 4 random state, objective = quartic (W = 6, n_quad = 24) + kinetic (32 nodes)
                 + finished gradient, stationary densities by numerics.stationary_state: per
                 accepted iteration the energy, step alpha, trials and gradient norm
+  config0.npz   the same controller for 100 iterations from the seed-42 D = 8 random state with
+                g = 2 at the optimizer defaults (W = 30, n_quad = 512, 512 kinetic nodes)
   finish.npz    the reference's preconditioned boundary solve and finished gradient
                 (numerics.finish_gradient) with its GMRES matvec count, on random states D = 8, 16
                 and a Z2 state D = 16 with seeded covectors and environments
@@ -43,7 +45,7 @@ is the reference's test/fixtures/phi4_g2_D16_z2_portable (exported by RcmpsCore 
 States: NumPy PCG64 default_rng(seed); R and A with i.i.d. standard complex Gaussian entries
 times 0.2 (R drawn first), K = (A + A^dag)/2; Z2 states draw blocks in the order k1, k2, R12, R21.
 Run: python tests/golden/make_golden.py --reference PATH/gpu/src [name ...]  (all files by
-default; names: small d16 d64 samples ode packed phi optim finish d32batch bench uneven; the D = 64
+default; names: small d16 d64 samples ode packed phi optim config0 finish d32batch bench uneven; the D = 64
 records dominate, about a minute each on one core)
 """
 from __future__ import annotations
@@ -152,11 +154,12 @@ def evaluate_phi(r, k, window, nq, atol=1e-13, rtol=1e-12):
 
 
 OPTIM = dict(seed=414, d=4, g=1.0, window=6.0, n_quad=24, nodes=32, iterations=8)
+# the config-0 run: D = 8, seed 42, g = 2 at the optimizer defaults, 100 L-BFGS iterations
+CONFIG0 = dict(seed=42, d=8, g=2.0, window=30.0, n_quad=512, nodes=512, iterations=100)
 
 
-def optim_run():
+def optim_run(c=OPTIM):
     from rcmps_gpu.optimizer.runtime import optimizer as opt
-    c = OPTIM
     r, k = random_state(c["d"], c["seed"])
 
     def objective(rr, kk, rho):
@@ -171,14 +174,13 @@ def optim_run():
     q0 = -1j * k - r.conj().T @ r / 2
     rho0, _ = nm.stationary_state(q0, r, tolerance=1e-13)
     e0, g0, _ = objective(r, k, rho0)
-    accepted = [ev for ev in opt.optimize(r, k, rho0, e0, g0, objective,
-                                          dict(max_iterations=c["iterations"], gradient_tol=1e-9))
-                if ev["type"] == "accepted"]
+    events = list(opt.optimize(r, k, rho0, e0, g0, objective, dict(max_iterations=c["iterations"], gradient_tol=1e-9)))
+    accepted = [ev for ev in events if ev["type"] == "accepted"]
     last = accepted[-1]["state"]
     return dict(R=r, K=k, rho=rho0, energy0=e0, gradient0=g0, **{key: value for key, value in c.items()},
                 energies=[ev["energy"] for ev in accepted], alphas=[ev["alpha"] for ev in accepted],
                 trials=[ev["trials"] for ev in accepted], gradient_norms=[ev["gradient_norm"] for ev in accepted],
-                R_final=last["R"], K_final=last["K"])
+                R_final=last["R"], K_final=last["K"], stop_reason=events[-1].get("reason", ""))
 
 
 def finish_record(r, k, seed):
@@ -239,6 +241,8 @@ def main(names):
                             finish_record(*z2_state(16, 826), 3)])
     if "optim" in names:
         save("optim.npz", [optim_run()])
+    if "config0" in names:
+        save("config0.npz", [optim_run(CONFIG0)])
     if "d32batch" in names:
         gs = np.random.default_rng(12345).uniform(0.5, 3.0, 64)
         save("d32batch.npz", [evaluate(*random_state(32, seed), float(gs[seed]), 30.0, 512, 512) for seed in range(8)])
@@ -290,7 +294,8 @@ def uneven_draws(count, seed=2024):
     return out
 
 
-ALL = ["small", "d16", "d64", "ode", "samples", "packed", "phi", "optim", "finish", "d32batch", "bench", "uneven"]
+ALL = ["small", "d16", "d64", "ode", "samples", "packed", "phi", "optim", "config0", "finish", "d32batch", "bench",
+       "uneven"]
 
 if __name__ == "__main__":
     import argparse

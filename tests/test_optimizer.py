@@ -139,3 +139,26 @@ def test_controller_with_device_algebra_matches_reference(gpu_context):
                                      dict(max_iterations=int(rec["iterations"]), gradient_tol=1e-9),
                                      device_algebra=True))
     _check(rec, _accepted(events), 1e-9)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("device_algebra", [False, True])
+def test_config0_hundred_iterations_match_reference(gpu_context, device_algebra):
+    """Config 0: one evaluation and 100 L-BFGS iterations from the seed-42 D = 8 state (g = 2, the
+    optimizer defaults) against the reference's own controller and objective
+    (tests/golden/config0.npz): every iteration's trial count, step length and energy."""
+    from rcmps_b200 import objective, optimizer
+    rec = load_records("config0.npz")[0]
+    args = objective.default_args(window=rec["window"], quadrature=int(rec["n_quad"]), nodes=int(rec["nodes"]))
+    call = lambda r, k, rho: objective.objective(r, k, rho, rec["g"], args)
+    e0, g0, _ = call(rec["R"], rec["K"], rec["rho"])
+    assert abs(e0 - rec["energy0"]) <= 1e-12 * abs(rec["energy0"])
+    events = list(optimizer.optimize(rec["R"], rec["K"], rec["rho"], e0, g0, call,
+                                     dict(max_iterations=int(rec["iterations"]), gradient_tol=1e-9),
+                                     device_algebra=device_algebra))
+    accepted = _accepted(events)
+    assert len(accepted) == 100 and events[-1]["reason"] == str(rec["stop_reason"])
+    assert [ev["trials"] for ev in accepted] == list(rec["trials"])
+    np.testing.assert_allclose([ev["alpha"] for ev in accepted], rec["alphas"], rtol=1e-7)
+    np.testing.assert_allclose([ev["energy"] for ev in accepted], rec["energies"], rtol=1e-10, atol=1e-12)
+    np.testing.assert_allclose(accepted[-1]["state"]["R"], rec["R_final"], atol=1e-7)
