@@ -180,7 +180,10 @@ def optim_run(c=OPTIM):
     return dict(R=r, K=k, rho=rho0, energy0=e0, gradient0=g0, **{key: value for key, value in c.items()},
                 energies=[ev["energy"] for ev in accepted], alphas=[ev["alpha"] for ev in accepted],
                 trials=[ev["trials"] for ev in accepted], gradient_norms=[ev["gradient_norm"] for ev in accepted],
-                R_final=last["R"], K_final=last["K"], stop_reason=events[-1].get("reason", ""))
+                R_final=last["R"], K_final=last["K"], stop_reason=events[-1].get("reason", ""),
+                trial_iteration=[ev["iteration"] for ev in events if ev["type"] == "trial"],
+                trial_energy=[ev.get("energy", np.nan) for ev in events if ev["type"] == "trial"],
+                trial_bound=[ev.get("armijo_bound", np.nan) for ev in events if ev["type"] == "trial"])
 
 
 def finish_record(r, k, seed):
