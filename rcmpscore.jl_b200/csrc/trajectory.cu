@@ -832,6 +832,9 @@ trajectory_kernel(const TrajState* __restrict__ states, const double* __restrict
     // ---------------------------------------------------------------- error norms
     {
       double s5 = 0.0, s3 = 0.0;
+      const double2* ke_p[13];
+#pragma unroll
+      for (int j = 0; j < 13; ++j) ke_p[j] = kb(j);
       for (int e = e0 + tid; e < e1; e += GE::NT) {
         const size_t off = own_offset<DP>(e, row0);
         if (packed) {
@@ -839,12 +842,14 @@ trajectory_kernel(const TrajState* __restrict__ states, const double* __restrict
           const bool lo_r = row < half, lo_c = col < half;
           if ((c % 2 == 0) ? !(lo_r && !lo_c) : (lo_r != lo_c)) continue;
         }
+        double2 kv[13];
+#pragma unroll
+        for (int j = 0; j <= 12; ++j) kv[j] = __ldcg(ke_p[j] + off);
         double2 e5 = make_double2(0.0, 0.0), e3 = make_double2(0.0, 0.0);
 #pragma unroll
-        for (int s = 0; s <= 12; ++s) {
-          const double2 kv = kb(s)[off];
-          e5 = zaxpy(c_dop_e5[s], kv, e5);
-          e3 = zaxpy(c_dop_e3[s], kv, e3);
+        for (int j = 0; j <= 12; ++j) {
+          e5 = zaxpy(c_dop_e5[j], kv[j], e5);
+          e3 = zaxpy(c_dop_e3[j], kv[j], e3);
         }
         const double2 yo = ybuf[off], yn = pbuf[off];
         const double scale = atol + rtol * fmax(hypot(yo.x, yo.y), hypot(yn.x, yn.y));
@@ -950,12 +955,20 @@ trajectory_kernel(const TrajState* __restrict__ states, const double* __restrict
           rhs(z, kb(s), C.jac[s], C.src[s]);
           ++zcount;
         }
-        // order-7 interpolation at the nodes in (t, t_new]
+        // order-7 interpolation at the nodes in (t, t_new]: every stage the dense matrix reads
+        // (rcmps_dop_dense_mask, k0 and k12 among them) is loaded once per element, all at once
         const double t = C.t, tn = C.t_new;
         const long long first = C.first, last = C.last;
+        const double2* kd_p[16];
+#pragma unroll
+        for (int j = 0; j < 16; ++j) kd_p[j] = kb(j);
         for (int e = e0 + tid; e < e1; e += GE::NT) {
           const size_t off = own_offset<DP>(e, row0);
-          const double2 yo = ybuf[off], yn = pbuf[off], f0 = kb(0)[off], f12 = kb(12)[off];
+          double2 kd[16];
+#pragma unroll
+          for (int j = 0; j < 16; ++j)
+            kd[j] = ((rcmps_dop_dense_mask >> j) & 1u) ? __ldcg(kd_p[j] + off) : make_double2(0.0, 0.0);
+          const double2 yo = ybuf[off], yn = pbuf[off], f0 = kd[0], f12 = kd[12];
           double2 cf[7];
           const double2 delta = zsub(yn, yo);
           cf[0] = delta;
@@ -964,10 +977,9 @@ trajectory_kernel(const TrajState* __restrict__ states, const double* __restrict
 #pragma unroll
           for (int row = 0; row < 4; ++row) {
             double2 v = make_double2(0.0, 0.0);
-            for (int s = 0; s < 16; ++s) {
-              const double dcoef = c_dop_d[16 * row + s];
-              if (dcoef != 0.0) v = zaxpy(h * dcoef, kb(s)[off], v);
-            }
+#pragma unroll
+            for (int j = 0; j < 16; ++j)
+              if ((rcmps_dop_dense_mask >> j) & 1u) v = zaxpy(h * c_dop_d[16 * row + j], kd[j], v);
             cf[3 + row] = v;
           }
           for (long long node = first; node < last; ++node) {
