@@ -137,12 +137,20 @@ struct Geo {
   static constexpr int VEC = NCH * MAT;               // elements of one stage vector
   static constexpr int OWN = NCH * 16 * DP;           // elements owned by one CTA
   static constexpr int cmax(int a, int b) { return a > b ? a : b; }
-  // shared memory (double2 units): one direction panel, the A' rows of a pass, the ring, split-K
+  // shared memory (double2 units): the direction panels, the A' rows of a pass, the ring, split-K.
+  // The quartic system keeps both directions' panels ([Q; R] and [Q^dag; R^dag] rows, constant
+  // over the trajectory) resident when they fit; otherwise one panel is reloaded per direction.
+  static constexpr int PANEL = 32 * LDP;
+  static constexpr int SPLIT_MAX = cmax(T1::SPLIT, cmax(T2a::SPLIT, T2b::SPLIT));
+  static constexpr size_t smem_with(int panels) {
+    return ((size_t)panels * PANEL + 16 * GS * LDA2 + NST * KC * LDB + SPLIT_MAX) * 16 + 2048;
+  }
+  static constexpr int NPANEL = (SYS == kSysQuartic && smem_with(2) <= 232448) ? 2 : 1;
   static constexpr int OFF_PANEL = 0;
-  static constexpr int OFF_APRIME = OFF_PANEL + 32 * LDP;
+  static constexpr int OFF_APRIME = OFF_PANEL + NPANEL * PANEL;
   static constexpr int OFF_RING = OFF_APRIME + 16 * GS * LDA2;
   static constexpr int OFF_SPLIT = OFF_RING + NST * KC * LDB;
-  static constexpr int END2 = OFF_SPLIT + cmax(T1::SPLIT, cmax(T2a::SPLIT, T2b::SPLIT));
+  static constexpr int END2 = OFF_SPLIT + SPLIT_MAX;
   static constexpr size_t SMEM = (size_t)END2 * 16 + 2048;   // + barriers and scalars (see carve)
   static_assert(SMEM <= 232448, "shared memory per CTA");
 };
@@ -166,7 +174,7 @@ struct Xch {                             // exchanged through distributed shared
 
 template <int DP, int SYS>
 struct Smem {
-  double2* panel;     // [32][LDP]: the current direction's [Qc; Rc] rows
+  double2* panel;     // [NPANEL][32][LDP]: the direction panels ([Qc; Rc] rows)
   double2* aprime;    // [16 GS][LDA2]
   double2* ring;      // [NST][KC*LDB]
   double2* split;     // split-K partial fragments
@@ -394,7 +402,8 @@ struct Rhs {
   // G1 product of channel c with a panel of 32 rows ([Qc; Rc]: Qc X_c -> kout scaled by jac,
   // P_c = Rc X_c) or 16 rows (L_c = Oc X_c).
   template <int M>
-  __device__ void g1_product(int c, const double2* zb, double2* kout, double jac, int& q, long long g0) {
+  __device__ void g1_product(int c, const double2* panel, const double2* zb, double2* kout, double jac, int& q,
+                             long long g0) {
     using TL = PassTiling<DP, M, GE::NW>;
     constexpr int TPW = TL::TPW, SK = TL::SK;
     const int tile0 = SK > 1 ? warp / SK : warp * TPW;
@@ -414,7 +423,7 @@ struct Rhs {
     ZFrag acc[TPW];
 #pragma unroll
     for (int j = 0; j < TPW; ++j) acc[j].zero();
-    stream_product<TL>(acc, sm.panel, GE::LDP, GE::CH1, q, g0, zb, zt, kn0, -1);
+    stream_product<TL>(acc, panel, GE::LDP, GE::CH1, q, g0, zb, zt, kn0, -1);
     if (slice == 0 && warp < GE::NW) {
 #pragma unroll
       for (int j = 0; j < TPW; ++j) {
@@ -531,14 +540,17 @@ struct Rhs {
     for (int e = 0; e < t.ng1; ++e) {
       const int c = t.g1_ch[e], kind = t.g1_kind[e];
       if (c < c0 || c >= c1) continue;
-      if (kind != kind_prev) {
+      const double2* panel = sm.panel;
+      if constexpr (GE::NPANEL == 2) {
+        panel += kind * GE::PANEL;   // both resident (loaded once per trajectory)
+      } else if (kind != kind_prev) {
         __syncthreads();
         load_panel(kind, sm.panel);
         __syncthreads();
         kind_prev = kind;
       }
-      if (kind < 2) g1_product<32>(c, zb, kout, jac, q, g0);
-      else if constexpr (GE::KM == 3) g1_product<16>(c, zb, kout, jac, q, g0);
+      if (kind < 2) g1_product<32>(c, panel, zb, kout, jac, q, g0);
+      else if constexpr (GE::KM == 3) g1_product<16>(c, panel, zb, kout, jac, q, g0);
     }
     __syncthreads();
     // the G1 results (P) of every CTA are published here and awaited in the first G2 pass
@@ -754,6 +766,10 @@ trajectory_kernel(const TrajState* __restrict__ states, const double* __restrict
       ybuf[off] = v;
       zb(zcount)[off] = v;
     }
+  }
+  if constexpr (ENG == 0 && GE::NPANEL == 2) {   // both direction panels, once per trajectory
+    rhs.load_panel(0, sm.panel);
+    rhs.load_panel(1, sm.panel + GE::PANEL);
   }
   fence_proxy_async_global();
   cluster_sync();
