@@ -114,6 +114,10 @@ struct PassTiling {
   static constexpr int SPLIT = SK > 1 ? T * (SK - 1) * 128 : 0;   // split-K scratch (double2)
 };
 
+// Bytes after the engine's buffers: ring barriers, the controller's scalars, the exchange record,
+// reduction scratch and the gathered exchange records of up to 16 CTAs.
+constexpr size_t kTail = 4096;
+
 template <int DP, int SYS>
 struct Geo {
   static constexpr int NCH = SYS == kSysQuartic ? 7 : SYS == kSysFull ? 26 : 4;   // matrix channels
@@ -143,7 +147,7 @@ struct Geo {
   static constexpr int PANEL = 32 * LDP;
   static constexpr int SPLIT_MAX = cmax(T1::SPLIT, cmax(T2a::SPLIT, T2b::SPLIT));
   static constexpr size_t smem_with(int panels) {
-    return ((size_t)panels * PANEL + 16 * GS * LDA2 + NST * KC * LDB + SPLIT_MAX) * 16 + 2048;
+    return ((size_t)panels * PANEL + 16 * GS * LDA2 + NST * KC * LDB + SPLIT_MAX) * 16 + kTail;
   }
   static constexpr int NPANEL = (SYS == kSysQuartic && smem_with(2) <= 232448) ? 2 : 1;
   static constexpr int OFF_PANEL = 0;
@@ -151,7 +155,7 @@ struct Geo {
   static constexpr int OFF_RING = OFF_APRIME + 16 * GS * LDA2;
   static constexpr int OFF_SPLIT = OFF_RING + NST * KC * LDB;
   static constexpr int END2 = OFF_SPLIT + SPLIT_MAX;
-  static constexpr size_t SMEM = (size_t)END2 * 16 + 2048;   // + barriers and scalars (see carve)
+  static constexpr size_t SMEM = (size_t)END2 * 16 + kTail;   // + barriers and scalars (see carve)
   static_assert(SMEM <= 232448, "shared memory per CTA");
 };
 
@@ -184,6 +188,7 @@ struct Smem {
   Xch* xch;
   double* red;        // [NW * 2] block reduction scratch
   double* kscp;       // [16] this CTA's partial scalar k by stage
+  double* gat;        // [16][16] the exchange records of the cluster's CTAs, gathered
 };
 
 template <int DP, int SYS>
@@ -201,7 +206,8 @@ __device__ __forceinline__ Smem<DP, SYS> carve(unsigned char* base) {
   constexpr size_t o_xch = o_ctl + ((sizeof(Ctl) + 15) / 16) * 16;
   constexpr size_t o_red = o_xch + ((sizeof(Xch) + 15) / 16) * 16;
   constexpr size_t o_ksc = o_red + 32 * sizeof(double) * 2;
-  static_assert(o_ksc + 16 * sizeof(double) <= 2048, "shared tail");
+  constexpr size_t o_gat = o_ksc + 16 * sizeof(double);
+  static_assert(o_gat + 256 * sizeof(double) <= kTail, "shared tail");
   unsigned char* tail = base + (size_t)GE::END2 * 16;
   s.full = reinterpret_cast<uint64_t*>(tail);
   s.empty = reinterpret_cast<uint64_t*>(tail + 64);
@@ -209,6 +215,7 @@ __device__ __forceinline__ Smem<DP, SYS> carve(unsigned char* base) {
   s.xch = reinterpret_cast<Xch*>(tail + o_xch);
   s.red = reinterpret_cast<double*>(tail + o_red);
   s.kscp = reinterpret_cast<double*>(tail + o_ksc);
+  s.gat = reinterpret_cast<double*>(tail + o_gat);
   return s;
 }
 
@@ -606,10 +613,10 @@ __device__ __forceinline__ bool z2_zero_element(int e, int row0, int half) {
 }
 
 // Shared memory of the kernel: the FP64 engine's panels and ring (Geo::SMEM), or the split
-// engine's chunk buffers followed by the controller's tail (2048 bytes).
+// engine's chunk buffers followed by the controller's tail (kTail bytes).
 template <int DP, int SYS, int ENG>
 constexpr size_t kernel_smem() {
-  return ENG == 0 ? Geo<DP, SYS>::SMEM : ((split_engine::kEnd + 127) / 128) * 128 + 2048;
+  return ENG == 0 ? Geo<DP, SYS>::SMEM : ((split_engine::kEnd + 127) / 128) * 128 + kTail;
 }
 
 template <int DP, int SYS, int ENG>
@@ -837,8 +844,11 @@ trajectory_kernel(const TrajState* __restrict__ states, const double* __restrict
           }
         }
       }
-      block_sum2<GE::NWT>(part, dummy, sm.red);
-      if (tid == 0) sm.kscp[s] = 4.0 * C.src[s] * part;
+      // the scalar channel's partial trace (channel 2's rows): only its CTAs reduce it
+      if (GE::SCALAR && c0 <= 2 && 2 < c1) {
+        block_sum2<GE::NWT>(part, dummy, sm.red);
+        if (tid == 0) sm.kscp[s] = 4.0 * C.src[s] * part;
+      }
       fence_proxy_async_global();
       cluster_sync();
       rhs(z, kb(s), C.jac[s], C.src[s]);
@@ -884,16 +894,31 @@ trajectory_kernel(const TrajState* __restrict__ states, const double* __restrict
         sm.xch->flag = f;
       }
       cluster_sync();
+      // every CTA's record, one distributed-shared-memory load per thread (a serial walk over 16
+      // CTAs' records by one thread took tens of microseconds per attempt); summed below in rank
+      // order as before
+      for (int i = tid; i < (int)nrank * 16; i += GE::NT) {
+        const uint32_t g = (uint32_t)(i >> 4);
+        const int v = i & 15;
+        double x = 0.0;
+        if (v == 0) x = dsmem_load(&sm.xch->s5, g);
+        else if (v == 1) x = dsmem_load(&sm.xch->s3, g);
+        else if (v <= 13) x = dsmem_load(&sm.xch->kscp[v - 1], g);
+        else if (v == 14) x = (double)dsmem_load_int(&sm.xch->flag, g);
+        sm.gat[i] = x;
+      }
+      __syncthreads();
       if (tid == 0) {
         double t5 = 0.0, t3 = 0.0;
         double ks[13];
         for (int s = 1; s < 13; ++s) ks[s] = 0.0;
         int flag = 0;
         for (uint32_t g = 0; g < nrank; ++g) {
-          t5 += dsmem_load(&sm.xch->s5, g);
-          t3 += dsmem_load(&sm.xch->s3, g);
-          for (int s = 1; s < 13; ++s) ks[s] += dsmem_load(&sm.xch->kscp[s], g);
-          flag |= dsmem_load_int(&sm.xch->flag, g);
+          const double* r = sm.gat + 16 * g;
+          t5 += r[0];
+          t3 += r[1];
+          for (int s = 1; s < 13; ++s) ks[s] += r[s + 1];
+          flag |= (int)r[14];
         }
         ks[0] = C.ksc[0];
         for (int s = 1; s < 13; ++s) C.ksc[s] = ks[s];
