@@ -508,22 +508,38 @@ struct Rhs {
 #pragma unroll
       for (int j = 0; j < TPW; ++j) {
         const int tile = tile0 + j, mt = tile / TL::NTN, nt = tile % TL::NTN;
+        // a tile's rows lie in one channel: its insertion source and fixed term are uniform
+        const int c = first + mt;
+        const int a = t.lsrc[c], fx = t.fixed[c];
+        if (zt) {   // structurally zero: every term of the sum is an exact zero
+#pragma unroll
+          for (int i = 0; i < 4; ++i) {
+            const int r = mt * 16 + frag_row(lane, i), col = nt * 8 + frag_col(lane, i);
+            kout[(size_t)c * GE::MAT + (size_t)(row0 + (r & 15)) * DP + col] = make_double2(0.0, 0.0);
+          }
+          continue;
+        }
+        // every operand of the tile's four elements is loaded before the first store, so their
+        // L2 round trips overlap (a store to kout between them would order each element's loads
+        // after the previous element's store)
+        const double2* ins = (t.lkind[c] ? st->L : st->P) + (size_t)(a >= 0 ? a : 0) * GE::MAT;
+        const double2* fxp = fx == 2 ? st->fixed6 : st->fixed0;
+        size_t loc[4];
+        double2 kv[4], iv[4], fv[4];
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
           const int r = mt * 16 + frag_row(lane, i), col = nt * 8 + frag_col(lane, i);
-          const int c = first + r / 16;
-          const int a = t.lsrc[c];
-          const size_t loc = (size_t)(row0 + (r & 15)) * DP + col;
-          const size_t off = (size_t)c * GE::MAT + loc;
-          if (zt) {   // structurally zero: every term of the sum is an exact zero
-            kout[off] = make_double2(0.0, 0.0);
-            continue;
-          }
-          double2 v = zadd(acc[j].value(i), kout[off]);
-          if (a >= 0) v = zaxpy(src * t.lcoef[c], __ldcg((t.lkind[c] ? st->L : st->P) + (size_t)a * GE::MAT + loc), v);
-          if (t.fixed[c] == 1) v = zaxpy(src, st->fixed0[loc], v);
-          if (t.fixed[c] == 2) v = zaxpy(src, st->fixed6[loc], v);
-          kout[off] = v;
+          loc[i] = (size_t)(row0 + (r & 15)) * DP + col;
+          kv[i] = __ldcg(kout + (size_t)c * GE::MAT + loc[i]);
+          iv[i] = a >= 0 ? __ldcg(ins + loc[i]) : make_double2(0.0, 0.0);
+          fv[i] = fx ? __ldg(fxp + loc[i]) : make_double2(0.0, 0.0);
+        }
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          double2 v = zadd(acc[j].value(i), kv[i]);
+          if (a >= 0) v = zaxpy(src * t.lcoef[c], iv[i], v);
+          if (fx) v = zaxpy(src, fv[i], v);
+          kout[(size_t)c * GE::MAT + loc[i]] = v;
         }
       }
     }
