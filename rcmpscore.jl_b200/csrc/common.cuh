@@ -184,6 +184,11 @@ RCMPS_DEVICE_INLINE void bulk_g2s(void* dst, const void* src, uint32_t bytes, ui
 RCMPS_DEVICE_INLINE void fence_proxy_async_global() {
   asm volatile("fence.proxy.async.global;" ::: "memory");
 }
+// Orders this thread's (and, after a barrier, the block's) generic accesses of shared memory
+// before later bulk copies into the same bytes.
+RCMPS_DEVICE_INLINE void fence_proxy_async_shared() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
 
 // ------------------------------------------------------------------ clusters
 RCMPS_DEVICE_INLINE uint32_t cluster_rank() {

@@ -99,6 +99,7 @@ struct RowGemmRing {
     if (!(s.n == 1 && krows == DP)) kh = -1;
     if (threadIdx.x == 0) {
       fence_proxy_async_global();
+      fence_proxy_async_shared();   // the ring may have been read or written as plain shared memory
       for (int q = 0; q < NST && q < nch; ++q) issue(s, q);
     }
     for (int q = 0; q < nch; ++q) {
@@ -124,6 +125,34 @@ struct RowGemmRing {
       if (threadIdx.x == 0 && q + NST < nch) issue(s, q + NST);
     }
     gq += nch;
+  }
+
+  // acc[TPW] += A * B with B (DP x DP) resident in shared memory (leading dimension ldb), the
+  // same k-steps in the same order as run(). Call with all threads; ends with a __syncthreads.
+  template <int MB>
+  __device__ void run_smem(ZFrag* acc, const double2* A, int lda, const double2* B, int ldb,
+                           const ZSkip& z = ZSkip()) {
+    constexpr int TN = Tiling<DP, MB, NW>::TN, TPW = Tiling<DP, MB, NW>::TPW;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int tile0 = warp * TPW;
+    const int mt = tile0 / TN;
+    int kh = -1;
+    const bool zt = band_zero<MB>(z, kh);
+    if (!zt) {
+      for (int q = 0; q < DP / KC; ++q) {
+        if (kh >= 0 && ((q * KC >= z.half) ? 1 : 0) != kh) continue;
+#pragma unroll
+        for (int ks = 0; ks < KC / 8; ++ks) {
+          AFrag a;
+          load_a(A, lda, mt * 16, q * KC + ks * 8, lane, a);
+          BFrag b[TPW];
+#pragma unroll
+          for (int j = 0; j < TPW; ++j) load_b(B + (size_t)q * KC * ldb, ldb, ks * 8, ((tile0 + j) % TN) * 8, lane, b[j]);
+          zmma_tiles<TPW>(acc, a, b);
+        }
+      }
+    }
+    __syncthreads();
   }
 
   // Coordinates of fragment entry i of tile j for this thread: row in [0, MB), col in [0, DP).
@@ -154,6 +183,10 @@ struct RowGemm : RowGemmRing<DP, NW, KC, NST> {
   __device__ void run(ZFrag* acc, const double2* A, int lda, const typename Base::Segs& s,
                       const typename Base::ZSkip& z = typename Base::ZSkip()) {
     Base::template run<MB>(acc, A, lda, s, z);
+  }
+  __device__ void run_smem(ZFrag* acc, const double2* A, int lda, const double2* B, int ldb,
+                           const typename Base::ZSkip& z = typename Base::ZSkip()) {
+    Base::template run_smem<MB>(acc, A, lda, B, ldb, z);
   }
   __device__ static bool band_zero(const typename Base::ZSkip& z) {
     int kh;

@@ -7,7 +7,7 @@
 //   m  = sum_i sum_k f_k (w R^dag b_k + c_k b_{k+1}) - (sum_i sum_k w f_k b_k) R^dag
 //   nn = sum_i sum_k (w b_k R + c_k b_{k+1}) f_k - R (sum_i sum_k w b_k f_k)
 // The k = 0 terms are linear in the adjoint samples (f_0 = rho is constant) and are formed
-// once from B0 = sum w b_0 and B1 = sum j b_1 in the finalize kernel, as are the deferred
+// once from B0 = sum w b_0 and B1 = sum j b_1 (pullback_bsum) in the finalize kernel, as are the deferred
 // products with R^dag and R. The samples are Hermitian and the weights real, so in exact
 // arithmetic nn = m^dag: the reference's covector (m + nn^dag)/2 equals m, and only m is formed
 // (the two differ by rounding, about 1e-15 relative). Per node and k >= 1 this leaves three D^3
@@ -32,7 +32,11 @@ struct PGeo {
   using GM = RowGemm<DP, MB, NW, KC, NST>;
   static constexpr int NT = 32 * NW;
   static constexpr size_t BUF = (size_t)MB * LDA;      // double2 per A buffer
-  static constexpr size_t SMEM = (2 * BUF + (size_t)NST * KC * (DP + kBPad)) * 16 + 128;
+  static constexpr size_t RING = (size_t)NST * KC * (DP + kBPad);   // double2
+  static constexpr size_t SMEM = (2 * BUF + RING) * 16 + 128;
+  // W_k = w R^dag b_k + c b_{k+1} fits the ring area (DP rows of DP + kBPad) when the state has a
+  // single row block: the second product then reads it from shared memory.
+  static constexpr bool WSMEM = NRB == 1 && (size_t)DP * (DP + kBPad) <= RING;
 };
 
 template <int DP>
@@ -44,8 +48,9 @@ pullback_kernel(PullbackArgs a) {
   double2* bufX = reinterpret_cast<double2*>(smem_raw);
   double2* bufY = bufX + PG::BUF;
   double2* ring = bufY + PG::BUF;
-  uint64_t* full = reinterpret_cast<uint64_t*>(ring + (size_t)PG::NST * PG::KC * (DP + kBPad));
-  int* flag = reinterpret_cast<int*>(full + PG::NST);
+  uint64_t* full = reinterpret_cast<uint64_t*>(ring + PG::RING);
+  uint64_t* ybar = full + PG::NST;   // rows of a sample block landed in bufY
+  int* flag = reinterpret_cast<int*>(ybar + 1);
 
   constexpr int MAT = DP * DP, VEC = 7 * MAT;
   const int n = a.nodes;
@@ -59,9 +64,27 @@ pullback_kernel(PullbackArgs a) {
   gm.full = full;
   gm.wait_flag = flag;
   gm.gq = 0;
-  if (tid == 0) *flag = 0;
+  if (tid == 0) {
+    *flag = 0;
+    mbar_init(ybar, 1);
+  }
   gm.init();
   __syncthreads();
+  uint32_t yphase = 0;
+  // rows [row0, row0 + rows) of a D x D sample matrix into bufY (leading dimension LDA) by 1-D
+  // bulk copies, all in flight at once; returns once they landed. Call with all threads, after
+  // the block's last use of bufY.
+  auto load_rows_bulk = [&](const double2* src, int row0, int rows) {
+    if (tid == 0) {
+      fence_proxy_async_shared();
+      mbar_expect_tx(ybar, (uint32_t)(rows * DP * 16));
+      for (int r = 0; r < rows; ++r) bulk_g2s(bufY + r * PG::LDA, src + (size_t)(row0 + r) * DP, DP * 16, ybar);
+    }
+  };
+  auto await_rows = [&]() {
+    mbar_wait(ybar, yphase, flag);
+    yphase ^= 1u;
+  };
 
   // a CTA takes items in turn (the grid may be smaller than the item count, so that the pullback
   // can leave SMs to concurrent work)
@@ -109,7 +132,39 @@ pullback_kernel(PullbackArgs a) {
           typename GM::Segs sb;
           sb.n = 1;
           sb.rows[0] = DP;
-          if (pass == 0) {
+          if (pass == 0 && PG::WSMEM) {
+            // W_k = w R^dag b_k + c b_{k+1} into the ring area, once the product's chunks are
+            // consumed; b_{k+1} lands in bufY meanwhile, f_k after the epilogue
+            double2* W = ring;
+            constexpr int LDW = DP + kBPad;
+            if (k < 3) load_rows_bulk(adj(i, k + 1), 0, DP);
+  #pragma unroll
+            for (int j = 0; j < GM::TPW; ++j) tmp[j].zero();
+            sb.ptr[0] = adj(i, k);
+            const int pk = k & 1;
+            const auto z0 = zsk(0, 1, 1 ^ pk);   // R^dag b_k
+            gm.run(tmp, bufX, PG::LDA, sb, z0);
+            if (k < 3) await_rows();
+            // a structurally zero block of W_k is never read by the live tiles of the next
+            // product, so it is not written
+            if (!GM::band_zero(z0)) {
+  #pragma unroll
+              for (int j = 0; j < GM::TPW; ++j)
+  #pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                  int row, col;
+                  GM::coord(j, e, row, col);
+                  double2 v = zscale(w, tmp[j].value(e));
+                  if (k < 3) v = zaxpy(c, bufY[row * PG::LDA + col], v);
+                  else if (row == col) v.x += c;
+                  W[row * LDW + col] = v;
+                }
+            }
+            __syncthreads();
+            load_rows_bulk(fwd(i, k), 0, DP);
+            await_rows();
+            gm.run_smem(acc, bufY, PG::LDA, W, LDW, zsk(0, k & 1, 1));   // f_k W_k
+          } else if (pass == 0) {
             // W_k = w R^dag b_k + c b_{k+1} (all rows) -> scratch
             for (int rbw = 0; rbw < PG::NRB; ++rbw) {
               if (PG::NRB > 1) {
@@ -141,12 +196,18 @@ pullback_kernel(PullbackArgs a) {
             }
             fence_proxy_async_global();   // W_k is read next by bulk copies
             __syncthreads();
-            load_rows(bufY, fwd(i, k), rb * PG::MB, 1.0);
-            __syncthreads();
+            load_rows_bulk(fwd(i, k), rb * PG::MB, PG::MB);
+            await_rows();
             sb.ptr[0] = wscr + (k - 1) * MAT;
             gm.run(acc, bufY, PG::LDA, sb, zsk(rb * PG::MB, k & 1, 1));   // f_k W_k
           } else {   // pass 1
-            load_rows(bufY, fwd(i, k), rb * PG::MB, w);   // P += w f_k b_k
+            // P += w f_k b_k: the rows of f_k land in bufY and are scaled there
+            load_rows_bulk(fwd(i, k), rb * PG::MB, PG::MB);
+            await_rows();
+            for (int e = tid; e < PG::MB * DP; e += PG::NT) {
+              double2* y = bufY + (e / DP) * PG::LDA + e % DP;
+              *y = zscale(w, *y);
+            }
             __syncthreads();
             sb.ptr[0] = adj(i, k);
             gm.run(acc, bufY, PG::LDA, sb, zsk(rb * PG::MB, k & 1, 0));
@@ -191,6 +252,28 @@ cudaError_t quartic_env_launch(const PullbackArgs& a, cudaStream_t s) {
   return cudaGetLastError();
 }
 
+// B0 = sum_i w_i b_0 and B1 = sum_i j_i b_1 (adjoint samples at node n - 1 - i) into the
+// finalize buffers, one element per thread in node order, many CTAs per state (the sums read every
+// node's b_0 and b_1 from HBM: 2 n D^2 complex values per state).
+constexpr int kBsumThreads = 128;
+__global__ void __launch_bounds__(kBsumThreads) pullback_bsum(PullbackArgs a) {
+  const int state = blockIdx.y;
+  const int dp = a.dp, MAT = dp * dp, VEC = 7 * MAT, n = a.nodes;
+  const int e = blockIdx.x * kBsumThreads + threadIdx.x;
+  if (e >= MAT) return;
+  const double2* samples = a.samples + (size_t)state * a.samples_stride;
+  double2 b0 = make_double2(0, 0), b1 = make_double2(0, 0);
+#pragma unroll 8
+  for (int i = 0; i < n; ++i) {
+    const double2* bs = samples + (size_t)(n - 1 - i) * VEC;
+    b0 = zaxpy(a.wj[2 * i], __ldcs(bs + 3 * MAT + e), b0);
+    b1 = zaxpy(a.wj[2 * i + 1], __ldcs(bs + 4 * MAT + e), b1);
+  }
+  double2* t = a.fin + (size_t)state * 8 * MAT;
+  t[4 * MAT + e] = b0;
+  t[5 * MAT + e] = b1;
+}
+
 // Naive dense helpers for the finalize step (a few D^3 products per state).
 __device__ void dmat_mul(double2* C, const double2* A, const double2* B, int dp, bool ah, bool bh, double alpha,
                          bool add) {
@@ -208,11 +291,11 @@ __device__ void dmat_mul(double2* C, const double2* A, const double2* B, int dp,
   __syncthreads();
 }
 
-// One CTA per state: reduce partials, add the k = 0 terms and the deferred products, and write
-// value, covector = g m (= g (m + nn^dag)/2) and environment = g Herm(b_0 at the endpoint).
+// One CTA per state (after pullback_bsum): reduce partials, add the k = 0 terms and the deferred
+// products, and write value, covector = g m (= g (m + nn^dag)/2) and environment = g Herm(b_0 at the endpoint).
 __global__ void pullback_finalize(PullbackArgs a, int nblk) {
   const int state = blockIdx.x;
-  const int dp = a.dp, MAT = dp * dp, VEC = 7 * MAT, n = a.nodes;
+  const int dp = a.dp, MAT = dp * dp, VEC = 7 * MAT;
   const double2* samples = a.samples + (size_t)state * a.samples_stride;
   const double2* ops = a.ops + (size_t)state * a.ops_stride;
   const double2 *R = ops + 2 * MAT, *rho = ops + 7 * MAT;
@@ -226,14 +309,6 @@ __global__ void pullback_finalize(PullbackArgs a, int nblk) {
     }
     m[e] = s[0];
     P[e] = s[1];
-    double2 b0 = make_double2(0, 0), b1 = make_double2(0, 0);
-    for (int i = 0; i < n; ++i) {
-      const double2* bs = samples + (size_t)(n - 1 - i) * VEC;
-      b0 = zaxpy(a.wj[2 * i], bs[3 * MAT + e], b0);
-      b1 = zaxpy(a.wj[2 * i + 1], bs[4 * MAT + e], b1);
-    }
-    B0[e] = b0;
-    B1[e] = b1;
   }
   __syncthreads();
   // m += rho R^dag B0 + rho B1 - (P + rho B0) R^dag
@@ -305,6 +380,9 @@ cudaError_t pullback_launch(const PullbackArgs& a, int nblk, cudaStream_t s) {
     default: return cudaErrorInvalidValue;
   }
   if (e != cudaSuccess) return e;
+  note_launch();
+  pullback_bsum<<<dim3((a.dp * a.dp + kBsumThreads - 1) / kBsumThreads, a.nstates), kBsumThreads, 0, s>>>(a);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
   note_launch();
   pullback_finalize<<<a.nstates, 256, 0, s>>>(a, nblk);
   return cudaGetLastError();
