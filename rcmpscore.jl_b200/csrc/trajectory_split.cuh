@@ -250,25 +250,45 @@ struct RhsSplit {
       const int part = narrow ? (lane >> 4) : h;       // 0 real, 1 imaginary
       const SysTab& t = T();
       const double sj = (U.g2 ? st->split_g2_scale[U.dir * 64 + j] : ss.g1scale[U.c * 64 + j]) * 0x1p-14;
+      if (!U.g2) {
 #pragma unroll 4
-      for (int i = 0; i < 16; ++i) {
-        const int n = narrow ? i : 16 * (lane >> 4) + i;   // the N index
-        const double sn = U.g2 ? ss.g2scale[U.g2i * 32 + n] : st->split_g1_scale[(rank * 2 + U.dir) * 32 + n];
-        const double val = sum[i] * sj * sn;
-        if (!U.g2) {
+        for (int i = 0; i < 16; ++i) {
+          const int n = narrow ? i : 16 * (lane >> 4) + i;   // the N index
+          const double sn = st->split_g1_scale[(rank * 2 + U.dir) * 32 + n];
+          const double val = sum[i] * sj * sn;
           const int r = n & 15;
           const size_t off = (size_t)U.c * GE::MAT + (size_t)(row0 + r) * DP + j;
           if (n < 16) reinterpret_cast<double*>(kout + off)[part] = jac * val;
           else reinterpret_cast<double*>(st->P + off)[part] = val;
-        } else {
-          const int cc = U.c + n / 16, r = n % 16;
-          const size_t loc = (size_t)(row0 + r) * DP + j, off = (size_t)cc * GE::MAT + loc;
-          double v = val + reinterpret_cast<const double*>(kout + off)[part];
-          const int a = t.lsrc[cc];
-          if (a >= 0) v += src * t.lcoef[cc] * reinterpret_cast<const double*>(st->P + (size_t)a * GE::MAT + loc)[part];
-          if (t.fixed[cc] == 1) v += src * reinterpret_cast<const double*>(st->fixed0 + loc)[part];
-          if (t.fixed[cc] == 2) v += src * reinterpret_cast<const double*>(st->fixed6 + loc)[part];
-          reinterpret_cast<double*>(kout + off)[part] = v;
+        }
+      } else {
+        // four entries at a time: their operands (k, the insertion P_a, the fixed term) are all
+        // loaded before the first of their stores, so the L2 round trips overlap
+        for (int i0 = 0; i0 < 16; i0 += 4) {
+          double kv[4], pv[4], fv[4];
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            const int n = narrow ? i0 + u : 16 * (lane >> 4) + i0 + u;
+            const int cc = U.c + n / 16, r = n % 16;
+            const size_t loc = (size_t)(row0 + r) * DP + j, off = (size_t)cc * GE::MAT + loc;
+            const int a = t.lsrc[cc], fx = t.fixed[cc];
+            kv[u] = reinterpret_cast<const double*>(kout + off)[part];
+            pv[u] = a >= 0 ? reinterpret_cast<const double*>(st->P + (size_t)a * GE::MAT + loc)[part] : 0.0;
+            fv[u] = fx ? reinterpret_cast<const double*>((fx == 2 ? st->fixed6 : st->fixed0) + loc)[part] : 0.0;
+          }
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            const int i = i0 + u;
+            const int n = narrow ? i : 16 * (lane >> 4) + i;   // the N index
+            const double sn = ss.g2scale[U.g2i * 32 + n];
+            const double val = sum[i] * sj * sn;
+            const int cc = U.c + n / 16, r = n % 16;
+            const size_t off = (size_t)cc * GE::MAT + (size_t)(row0 + r) * DP + j;
+            double v = val + kv[u];
+            if (t.lsrc[cc] >= 0) v += src * t.lcoef[cc] * pv[u];
+            if (t.fixed[cc]) v += src * fv[u];
+            reinterpret_cast<double*>(kout + off)[part] = v;
+          }
         }
       }
     }
