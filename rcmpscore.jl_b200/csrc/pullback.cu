@@ -71,16 +71,17 @@ pullback_kernel(PullbackArgs a) {
   gm.init();
   __syncthreads();
   uint32_t yphase = 0;
-  // rows [row0, row0 + rows) of a D x D sample matrix into bufY (leading dimension LDA) by 1-D
-  // bulk copies, all in flight at once; returns once they landed. Call with all threads, after
-  // the block's last use of bufY.
-  auto load_rows_bulk = [&](const double2* src, int row0, int rows) {
+  // rows [row0, row0 + rows) of a D x D matrix into dst (bufX or bufY, leading dimension LDA) by
+  // 1-D bulk copies, all in flight at once, completing on ybar (await_rows). Call with all
+  // threads, after the block's last use of dst.
+  auto load_rows_to = [&](double2* dst, const double2* src, int row0, int rows) {
     if (tid == 0) {
       fence_proxy_async_shared();
       mbar_expect_tx(ybar, (uint32_t)(rows * DP * 16));
-      for (int r = 0; r < rows; ++r) bulk_g2s(bufY + r * PG::LDA, src + (size_t)(row0 + r) * DP, DP * 16, ybar);
+      for (int r = 0; r < rows; ++r) bulk_g2s(dst + r * PG::LDA, src + (size_t)(row0 + r) * DP, DP * 16, ybar);
     }
   };
+  auto load_rows_bulk = [&](const double2* src, int row0, int rows) { load_rows_to(bufY, src, row0, rows); };
   auto await_rows = [&]() {
     mbar_wait(ybar, yphase, flag);
     yphase ^= 1u;
@@ -167,10 +168,18 @@ pullback_kernel(PullbackArgs a) {
           } else if (pass == 0) {
             // W_k = w R^dag b_k + c b_{k+1} (all rows) -> scratch
             for (int rbw = 0; rbw < PG::NRB; ++rbw) {
-              if (PG::NRB > 1) {
-                load_rows(bufX, Rh, rbw * PG::MB, 1.0);
-                __syncthreads();
+              // the row block of R^dag this product takes into bufX and, for the epilogue, the
+              // same rows of b_{k+1} into bufY (free until f_k is loaded), on one barrier phase
+              if (tid == 0) {
+                fence_proxy_async_shared();
+                mbar_expect_tx(ybar, (uint32_t)((k < 3 ? 2 : 1) * PG::MB * DP * 16));
+                for (int r = 0; r < PG::MB; ++r) {
+                  bulk_g2s(bufX + r * PG::LDA, Rh + (size_t)(rbw * PG::MB + r) * DP, DP * 16, ybar);
+                  if (k < 3)
+                    bulk_g2s(bufY + r * PG::LDA, adj(i, k + 1) + (size_t)(rbw * PG::MB + r) * DP, DP * 16, ybar);
+                }
               }
+              await_rows();
   #pragma unroll
               for (int j = 0; j < GM::TPW; ++j) tmp[j].zero();
               sb.ptr[0] = adj(i, k);
@@ -186,13 +195,14 @@ pullback_kernel(PullbackArgs a) {
                   for (int e = 0; e < 4; ++e) {
                     int row, col;
                     GM::coord(j, e, row, col);
-                    row += rbw * PG::MB;
                     double2 v = zscale(w, tmp[j].value(e));
-                    if (k < 3) v = zaxpy(c, adj(i, k + 1)[row * DP + col], v);
-                    else if (row == col) v.x += c;
+                    if (k < 3) v = zaxpy(c, bufY[row * PG::LDA + col], v);
+                    row += rbw * PG::MB;
+                    if (k == 3 && row == col) v.x += c;
                     wscr[(k - 1) * MAT + row * DP + col] = v;
                   }
               }
+              __syncthreads();   // bufX and bufY are refilled by the next row block
             }
             fence_proxy_async_global();   // W_k is read next by bulk copies
             __syncthreads();
