@@ -818,12 +818,16 @@ trajectory_kernel(const TrajState* __restrict__ states, const double* __restrict
         C.max_h = fmax(C.max_h, h);
       }
       C.h = h;
-      for (int s = 1; s < 16; ++s) {
-        const double ts = s == 12 ? __dadd_rn(t, h) : __dadd_rn(t, __dmul_rn(c_dop_c[s], h));
-        if (fabs(ts) > RCMPS_SOURCE_AMAX * (1.0 + 1e-14)) C.status = kSourceDomain;
-        C.jac[s] = 2.0 * fabs(ts);
-        C.src[s] = source_value(ts);
-      }
+    }
+    __syncthreads();
+    // the stage times' Jacobian and source values, one stage per lane of warp 0
+    if (tid >= 1 && tid < 16) {
+      const int s = tid;
+      const double t = C.t, h = C.h;
+      const double ts = s == 12 ? __dadd_rn(t, h) : __dadd_rn(t, __dmul_rn(c_dop_c[s], h));
+      if (fabs(ts) > RCMPS_SOURCE_AMAX * (1.0 + 1e-14)) C.status = kSourceDomain;
+      C.jac[s] = 2.0 * fabs(ts);
+      C.src[s] = source_value(ts);
     }
     __syncthreads();
     if (C.status) break;   // uniform across the cluster: every CTA computes the same
