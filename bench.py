@@ -324,17 +324,25 @@ def run_b200(args, rank, world, local_rank):
                 "fp64_equivalent_tflops": fp64eq / (traj_ms_split / 1000.0) / 1e12}
 
     split_roofline = split_roofline_of(traj, rhs_calls) if split else None
-    # DRAM traffic of one launch: bytes per right-hand side of one state from an ncu capture of a
-    # smaller case at the same D, times this launch's right-hand sides (traffic grows with them)
+    # DRAM traffic of one launch: bytes per right-hand side of one state times this launch's
+    # right-hand sides. The rate comes from an ncu capture of this very launch where one was taken
+    # (the default 32-state workload and layout: its stage vectors exceed L2 and are re-read from
+    # DRAM), otherwise from a two-state capture at the same D, a lower bound for larger batches.
     traffic = None
     tf = ROOT / "profiles" / "trajectory_traffic.json"
     if tf.exists():
         try:
             rec = json.loads(tf.read_text())
-            per = rec.get("dram_bytes_per_state_rhs", {})
-            if all(str(d) in per for d in dims):
-                traffic = sum(per[str(dims[i])] * rhs_calls[i] for i in range(n))
-        except (OSError, ValueError):
+            full = rec.get("measured_launches", {}).get(args.workload)
+            default_layout = (not split and args.trajectory_groups == 0 and args.quartic_route == "auto"
+                              and args.half_window == 30.0 and args.n_quad == 512 and not quartic_only)
+            if full and default_layout:
+                traffic = full["dram_bytes_per_state_rhs"] * sum(rhs_calls[i] for i in range(n))
+            else:
+                per = rec.get("dram_bytes_per_state_rhs", {})
+                if all(str(d) in per for d in dims):
+                    traffic = sum(per[str(dims[i])] * rhs_calls[i] for i in range(n))
+        except (OSError, ValueError, KeyError):
             traffic = None
 
     # end to end through the host-buffer C entry: copies of inputs and results inside the timed region
