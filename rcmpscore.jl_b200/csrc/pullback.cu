@@ -82,8 +82,9 @@ pullback_kernel(PullbackArgs a) {
     }
   };
   auto load_rows_bulk = [&](const double2* src, int row0, int rows) { load_rows_to(bufY, src, row0, rows); };
+  int ygave = -1;   // the phase of a bounded wait on ybar that gave up (its copies may still land)
   auto await_rows = [&]() {
-    mbar_wait(ybar, yphase, flag);
+    if (!mbar_wait(ybar, yphase, flag)) ygave = (int)yphase;
     yphase ^= 1u;
   };
 
@@ -238,6 +239,8 @@ pullback_kernel(PullbackArgs a) {
     }
     if (tid == 0 && *flag) atomicExch(a.error_flag + state, 1);
   }
+  // after a wait gave up, wait (bounded) for that phase's copies before the CTA leaves
+  if (tid == 0 && ygave >= 0) mbar_wait(ybar, (uint32_t)ygave, nullptr);
   gm.drain();
 }
 
